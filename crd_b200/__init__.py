@@ -1,0 +1,16 @@
+"""crd_b200: a B200-native (sm_100a) replacement for crd-hesap-fft's plan + execute path.
+
+The compute runs in ``libcrdfft.so`` (hand-written CUDA kernels behind the C ABI in ``include/crdfft.h``); this
+package is the Python mirror of the reference's plan classes over that ABI (``crd_b200.fft``).
+"""
+
+from .fft import (BluesteinPlan, FftPlan, Forward, Inverse, NdFftPlan, Plan, RealFftPlan, fft, ifft_normalized,
+                  self_check)
+from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP16_SCALED, PREC_FP32,
+                   PREC_SPLIT_BF16, R2C, CrdFftError)
+
+__all__ = [
+    "BluesteinPlan", "FftPlan", "NdFftPlan", "Plan", "RealFftPlan", "fft", "ifft_normalized", "self_check",
+    "Forward", "Inverse", "C2C", "R2C", "C2R", "FORWARD", "INVERSE", "NORM_NONE", "NORM_INVERSE", "PREC_FP32",
+    "PREC_SPLIT_BF16", "PREC_FP16_SCALED", "CrdFftError",
+]

@@ -1,0 +1,145 @@
+"""ctypes binding of libcrdfft.so (the C ABI declared in include/crdfft.h).
+
+The library is built in-tree (``make -C crd_b200``, or ``__graft_entry__.build()``). There is no fallback: if the
+shared object is missing or fails to load, every entry point raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcrdfft.so")
+
+OK = 0
+INVALID_DESC = 1
+UNSUPPORTED_SIZE = 2
+OOM = 3
+LAUNCH = 4
+DEVICE_TIMEOUT = 5
+NUMERIC_SELFCHECK = 6
+INVALID_ARG = 7
+NO_DEVICE = 8
+
+FORWARD = 0
+INVERSE = 1
+
+C2C = 0
+R2C = 1
+C2R = 2
+
+PREC_FP32 = 0
+PREC_SPLIT_BF16 = 1
+PREC_FP16_SCALED = 2
+
+NORM_NONE = 0
+NORM_INVERSE = 1
+
+# Every function include/crdfft.h declares; the CPU tests check the library exports each of them.
+EXPORTS = (
+    "crdfft_plan_create",
+    "crdfft_plan_destroy",
+    "crdfft_execute",
+    "crdfft_plan_info_get",
+    "crdfft_workspace_size",
+    "crdfft_set_workspace",
+    "crdfft_status_string",
+    "crdfft_fft_plan_create",
+    "crdfft_fft_execute",
+    "crdfft_fft_execute_batched",
+    "crdfft_real_plan_create",
+    "crdfft_rfft",
+    "crdfft_irfft",
+    "crdfft_bluestein_plan_create",
+    "crdfft_bluestein_execute",
+    "crdfft_nd_plan_create",
+    "crdfft_nd_execute",
+    "crdfft_fft",
+    "crdfft_ifft_normalized",
+    "crdfft_self_check",
+    "crdfft_debug_fail_alloc_after",
+)
+
+
+class CrdFftError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        self.status = status
+        msg = lib().crdfft_status_string(status).decode() if _lib is not None else str(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [
+        ("rank", ctypes.c_int32),
+        ("kind", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("norm", ctypes.c_int32),
+        ("dims", ctypes.c_int64 * 3),
+        ("batch", ctypes.c_int64),
+        ("istride", ctypes.c_int64),
+        ("idist", ctypes.c_int64),
+        ("ostride", ctypes.c_int64),
+        ("odist", ctypes.c_int64),
+    ]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("algorithm", ctypes.c_char * 64),
+        ("passes", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("workspace_bytes", ctypes.c_int64),
+        ("table_bytes", ctypes.c_int64),
+        ("factors", ctypes.c_int64 * 8),
+    ]
+
+
+_lib = None
+
+
+def lib():
+    """Load libcrdfft.so once. Raises if it is absent: the CUDA path has no substitute."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C crd_b200` (nvcc, sm_100a)")
+    L = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    pp = ctypes.POINTER(ctypes.c_void_p)
+    i32, i64 = ctypes.c_int32, ctypes.c_int64
+    sig = {
+        "crdfft_plan_create": ([ctypes.POINTER(Desc), pp], i32),
+        "crdfft_plan_destroy": ([vp], i32),
+        "crdfft_execute": ([vp, vp, vp, i32, vp], i32),
+        "crdfft_plan_info_get": ([vp, ctypes.POINTER(PlanInfo)], i32),
+        "crdfft_workspace_size": ([vp], ctypes.c_size_t),
+        "crdfft_set_workspace": ([vp, vp, ctypes.c_size_t], i32),
+        "crdfft_status_string": ([i32], ctypes.c_char_p),
+        "crdfft_fft_plan_create": ([i64, pp], i32),
+        "crdfft_fft_execute": ([vp, vp, i32, vp], i32),
+        "crdfft_fft_execute_batched": ([vp, vp, i64, i32, vp], i32),
+        "crdfft_real_plan_create": ([i64, pp], i32),
+        "crdfft_rfft": ([vp, vp, vp, vp], i32),
+        "crdfft_irfft": ([vp, vp, vp, vp], i32),
+        "crdfft_bluestein_plan_create": ([i64, pp], i32),
+        "crdfft_bluestein_execute": ([vp, vp, i32, vp], i32),
+        "crdfft_nd_plan_create": ([i32, ctypes.POINTER(i64), pp], i32),
+        "crdfft_nd_execute": ([vp, vp, i32, vp], i32),
+        "crdfft_fft": ([vp, i64, i32, vp], i32),
+        "crdfft_ifft_normalized": ([vp, i64, vp], i32),
+        "crdfft_self_check": ([], i32),
+        "crdfft_debug_fail_alloc_after": ([i32], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return _lib
+
+
+def check(status: int, what: str = "") -> None:
+    if status != OK:
+        raise CrdFftError(status, what)

@@ -1,0 +1,234 @@
+// Register-resident DFT codelets for radix 2, 3, 4, 5, 7, 8 and 16, and the complex helpers the pass kernels use.
+//
+// These replace the reference's machine-generated straight-line SIMD codelets (engine/numerics/hesap-fft/kernels/
+// fft_*_codelets_*.cpp, emitted by scripts/gen_fft_batched.py and scripts/gen_fft_codelets.py) and add the odd radices
+// 3, 5 and 7, which the reference does not have (its non-power-of-two sizes go through Bluestein,
+// include/crd/hesap/fft/bluestein.hpp:29-139). Every codelet computes the forward DFT y_k = sum_j x_j W_R^{jk},
+// W_R = exp(-2πi/R), in place on R complex values in registers; the inverse is obtained by conjugating the pass's
+// input and output (IDFT(x) = conj(DFT(conj x))). The constants are cos/sin of 2πj/R written out to 20 digits.
+
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace crdfft
+{
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+// -i * a
+__device__ __forceinline__ float2 cmul_mi(float2 a) { return make_float2(a.y, -a.x); }
+// +i * a
+__device__ __forceinline__ float2 cmul_pi(float2 a) { return make_float2(-a.y, a.x); }
+
+// Multiply by the compile-time root W_16^J (forward sign), specialised so the trivial roots cost no multiplies.
+template <int J> __device__ __forceinline__ float2 w16mul(float2 a)
+{
+    constexpr float C = 0.92387953251128675613f; // cos(π/8)
+    constexpr float S = 0.38268343236508977173f; // sin(π/8)
+    constexpr float H = 0.70710678118654752440f; // cos(π/4)
+    constexpr int j = J & 15;
+    if constexpr (j == 0)
+        return a;
+    else if constexpr (j == 4)
+        return cmul_mi(a);
+    else if constexpr (j == 8)
+        return make_float2(-a.x, -a.y);
+    else if constexpr (j == 12)
+        return cmul_pi(a);
+    else if constexpr (j == 2) // H(1 - i)
+        return make_float2(H * (a.x + a.y), H * (a.y - a.x));
+    else if constexpr (j == 6) // H(-1 - i)
+        return make_float2(H * (a.y - a.x), -H * (a.x + a.y));
+    else if constexpr (j == 10) // H(-1 + i)
+        return make_float2(-H * (a.x + a.y), H * (a.x - a.y));
+    else if constexpr (j == 14) // H(1 + i)
+        return make_float2(H * (a.x - a.y), H * (a.x + a.y));
+    else
+    {
+        // W_16^j = cos(2πj/16) - i sin(2πj/16); the remaining j are odd.
+        constexpr float c = (j == 1 || j == 15) ? C : (j == 3 || j == 13) ? S : (j == 5 || j == 11) ? -S : -C;
+        constexpr float s = (j == 1 || j == 7) ? S : (j == 3 || j == 5) ? C : (j == 9 || j == 15) ? -S : -C;
+        return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+    }
+}
+
+template <int R> struct Dft;
+
+template <> struct Dft<2>
+{
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        const float2 a = v[0], b = v[1];
+        v[0] = cadd(a, b);
+        v[1] = csub(a, b);
+    }
+};
+
+template <> struct Dft<4>
+{
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const float2 s13 = cadd(v[1], v[3]), d13 = cmul_mi(csub(v[1], v[3]));
+        v[0] = cadd(s02, s13);
+        v[2] = csub(s02, s13);
+        v[1] = cadd(d02, d13);
+        v[3] = csub(d02, d13);
+    }
+};
+
+template <> struct Dft<8>
+{
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        float2 e[4] = {v[0], v[2], v[4], v[6]};
+        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        Dft<4>::run(e);
+        Dft<4>::run(o);
+        o[1] = w16mul<2>(o[1]);
+        o[2] = w16mul<4>(o[2]);
+        o[3] = w16mul<6>(o[3]);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+        {
+            v[k] = cadd(e[k], o[k]);
+            v[k + 4] = csub(e[k], o[k]);
+        }
+    }
+};
+
+template <> struct Dft<16>
+{
+    // 16 = 4 x 4: DFT4 over n1 for each n2 (x[4 n1 + n2]), twiddle W_16^{n2 k1}, DFT4 over n2 -> y[k1 + 4 k2].
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        float2 a[4][4];
+#pragma unroll
+        for (int n2 = 0; n2 < 4; ++n2)
+        {
+#pragma unroll
+            for (int n1 = 0; n1 < 4; ++n1)
+                a[n2][n1] = v[4 * n1 + n2];
+            Dft<4>::run(a[n2]);
+        }
+        a[1][1] = w16mul<1>(a[1][1]);
+        a[1][2] = w16mul<2>(a[1][2]);
+        a[1][3] = w16mul<3>(a[1][3]);
+        a[2][1] = w16mul<2>(a[2][1]);
+        a[2][2] = w16mul<4>(a[2][2]);
+        a[2][3] = w16mul<6>(a[2][3]);
+        a[3][1] = w16mul<3>(a[3][1]);
+        a[3][2] = w16mul<6>(a[3][2]);
+        a[3][3] = w16mul<9>(a[3][3]);
+#pragma unroll
+        for (int k1 = 0; k1 < 4; ++k1)
+        {
+            float2 b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            Dft<4>::run(b);
+#pragma unroll
+            for (int k2 = 0; k2 < 4; ++k2)
+                v[k1 + 4 * k2] = b[k2];
+        }
+    }
+};
+
+// Odd prime radix p in {3, 5, 7}: with a_k = x_k + x_{p-k}, b_k = x_k - x_{p-k} (k = 1 .. h, h = (p-1)/2),
+//   y_m     = x_0 + sum_k cos(2πkm/p) a_k - i sum_k sin(2πkm/p) b_k
+//   y_{p-m} = x_0 + sum_k cos(2πkm/p) a_k + i sum_k sin(2πkm/p) b_k.
+template <int P> struct OddRoots;
+template <> struct OddRoots<3>
+{
+    __device__ __forceinline__ static float c(int j) { return -0.5f; }
+    __device__ __forceinline__ static float s(int j) { return j == 1 ? 0.86602540378443864676f : -0.86602540378443864676f; }
+};
+template <> struct OddRoots<5>
+{
+    __device__ __forceinline__ static float c(int j)
+    {
+        return (j == 1 || j == 4) ? 0.30901699437494742410f : -0.80901699437494742410f;
+    }
+    __device__ __forceinline__ static float s(int j)
+    {
+        return j == 1 ? 0.95105651629515357212f
+             : j == 2 ? 0.58778525229247312917f
+             : j == 3 ? -0.58778525229247312917f
+                      : -0.95105651629515357212f;
+    }
+};
+template <> struct OddRoots<7>
+{
+    __device__ __forceinline__ static float c(int j)
+    {
+        return (j == 1 || j == 6) ? 0.62348980185873353053f
+             : (j == 2 || j == 5) ? -0.22252093395631440429f
+                                  : -0.90096886790241912624f;
+    }
+    __device__ __forceinline__ static float s(int j)
+    {
+        return j == 1 ? 0.78183148246802980871f
+             : j == 2 ? 0.97492791218182360702f
+             : j == 3 ? 0.43388373911755812048f
+             : j == 4 ? -0.43388373911755812048f
+             : j == 5 ? -0.97492791218182360702f
+                      : -0.78183148246802980871f;
+    }
+};
+
+template <int P> struct OddDft
+{
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        constexpr int h = (P - 1) / 2;
+        float2 a[h + 1], b[h + 1];
+        float2 y0 = v[0];
+#pragma unroll
+        for (int k = 1; k <= h; ++k)
+        {
+            a[k] = cadd(v[k], v[P - k]);
+            b[k] = csub(v[k], v[P - k]);
+            y0 = cadd(y0, a[k]);
+        }
+        float2 out[P];
+        out[0] = y0;
+#pragma unroll
+        for (int m = 1; m <= h; ++m)
+        {
+            float2 re = v[0];
+            float2 im = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 1; k <= h; ++k)
+            {
+                const float c = OddRoots<P>::c((k * m) % P);
+                const float s = OddRoots<P>::s((k * m) % P);
+                re.x = fmaf(c, a[k].x, re.x);
+                re.y = fmaf(c, a[k].y, re.y);
+                im.x = fmaf(s, b[k].x, im.x);
+                im.y = fmaf(s, b[k].y, im.y);
+            }
+            out[m] = make_float2(re.x + im.y, re.y - im.x);
+            out[P - m] = make_float2(re.x - im.y, re.y + im.x);
+        }
+#pragma unroll
+        for (int k = 0; k < P; ++k)
+            v[k] = out[k];
+    }
+};
+
+template <> struct Dft<3> : OddDft<3>
+{
+};
+template <> struct Dft<5> : OddDft<5>
+{
+};
+template <> struct Dft<7> : OddDft<7>
+{
+};
+
+} // namespace crdfft

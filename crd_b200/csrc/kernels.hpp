@@ -1,0 +1,56 @@
+// Host-side entry points of the CUDA translation units, called by the planner (plan.cpp).
+
+#pragma once
+
+#include "pass_desc.hpp"
+
+#include <cuda_runtime.h>
+
+namespace crdfft
+{
+
+// One launch of the line-FFT kernel (line_fft.cu).
+cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void* in, void* out, cudaStream_t stream);
+int pass_lines_per_cta_limit();
+int pass_line_pitch(int n);
+int pass_threads_limit();
+bool pass_has_kernel(const PassDesc& d, const PassShape& sh);
+
+// Real <-> half-length complex recombination (real_ops.cu), the math of the reference's RealFftPlan
+// (include/crd/hesap/fft/real_fft.hpp:41-92), over `batch` transforms of real length n = 2h.
+//   r2c_post: z (h complex per transform, zdist apart) -> out (h+1 complex per transform, odist apart)
+//   c2r_pre:  in (h+1 complex, idist apart) -> z (h complex, zdist apart), ready for the inverse half FFT
+struct RealRecombine
+{
+    long long h;
+    long long batch;
+    long long zdist;
+    long long xdist; // the (h+1)-element spectrum side
+    const void* wn;  // float2 W_n^k, k = 0 .. h
+    float scale;     // applied to the output
+};
+cudaError_t launch_r2c_post(const RealRecombine& p, const void* z, void* out, cudaStream_t stream);
+cudaError_t launch_c2r_pre(const RealRecombine& p, const void* in, void* z, cudaStream_t stream);
+
+// Bluestein helpers (real_ops.cu): chirp pre-multiply with zero padding, pointwise spectrum product, chirp
+// post-multiply. The math of include/crd/hesap/fft/bluestein.hpp:87-136.
+struct ChirpDesc
+{
+    long long n;      // transform length
+    long long m;      // padded power-of-two length (>= 2n - 1)
+    long long batch;
+    long long xdist;  // distance between transforms on the n side
+    long long wdist;  // distance between transforms on the m side (scratch)
+    const void* chirp; // float2 exp(+iπ k²/n), k < n
+    const void* bfft;  // float2 FFT_m(b_circ), length m
+    int conj;          // inverse direction: conjugate x on the way in and the result on the way out
+    float scale;       // final scale (1/m, times 1/n for the normalised inverse)
+};
+cudaError_t launch_chirp_pre(const ChirpDesc& p, const void* x, void* w, cudaStream_t stream);
+cudaError_t launch_spectrum_mul(const ChirpDesc& p, void* w, cudaStream_t stream);
+cudaError_t launch_chirp_post(const ChirpDesc& p, const void* w, void* x, cudaStream_t stream);
+
+// Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
+cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);
+
+} // namespace crdfft

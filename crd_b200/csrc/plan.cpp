@@ -1,0 +1,1167 @@
+// The planner and the C ABI (include/crdfft.h). A plan is a list of steps per direction, each a kernel launch with
+// its buffers named symbolically (the caller's input, the caller's output, the plan's workspace). The planner is the
+// deterministic plan-from-size rule of the reference (include/crd/hesap/fft/fft.hpp:3-8, 112-210): no runtime
+// measurement here; the same descriptor always builds the same steps, and execution uses no atomics, so a plan is
+// bit-identical run to run.
+//
+//   n <= 16384 (a line fits one CTA's shared memory)  one pass, one HBM read and one write per element
+//   larger 7-smooth n                                 four-step n = n1 * n2: pass 1 column FFTs of length n1 with
+//                                                     the W_n^{n2 k1} twiddle fused into the store, pass 2 row FFTs
+//                                                     of length n2 with the transposed store; the batch runs in
+//                                                     waves whose intermediate fits in L2 (the reference's Bailey
+//                                                     four-step, kernels/fft_kernels.cpp:2363-2658)
+//   n with a prime factor above 7                     Bluestein chirp-z over a power-of-two plan (bluestein.hpp)
+//   R2C / C2R                                         half-length complex plan + recombine pass (real_fft.hpp)
+//   rank 2 / 3                                        one pass per axis, inverse by the conjugation trick
+//                                                     (nd_fft.hpp:105-147)
+
+#include "../../include/crdfft.h"
+#include "kernels.hpp"
+#include "pass_desc.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+namespace crdfft
+{
+namespace
+{
+
+constexpr int kMaxSmemBytes = 200 * 1024;
+
+std::atomic<int> g_fail_alloc_after{0};
+
+cudaError_t dev_alloc(void** p, size_t bytes)
+{
+    int k = g_fail_alloc_after.load();
+    if (k > 0)
+    {
+        if (k == 1)
+        {
+            g_fail_alloc_after.store(0);
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+        g_fail_alloc_after.store(k - 1);
+    }
+    return cudaMalloc(p, bytes == 0 ? 256 : bytes);
+}
+
+enum class Buf : int
+{
+    In,
+    Out,
+    Ws
+};
+
+struct BufRef
+{
+    Buf b = Buf::In;
+    long long off = 0; // in complex (8-byte) elements
+};
+
+enum class StepKind : int
+{
+    Line,
+    R2CPost,
+    C2RPre,
+    ChirpPre,
+    SpecMul,
+    ChirpPost,
+    Scale
+};
+
+struct Step
+{
+    StepKind kind = StepKind::Line;
+    PassDesc pass{};
+    PassShape shape{};
+    RealRecombine real{};
+    ChirpDesc chirp{};
+    BufRef src, dst;
+    long long count = 0;
+    float scale = 1.0f;
+};
+
+// 7-smooth test and the radix schedule: powers of two as 16s with an 8, 4 or 2 for the remainder, then 7s, 5s, 3s.
+bool radices_for(long long n, std::vector<int>& out)
+{
+    out.clear();
+    if (n < 1)
+        return false;
+    long long m = n;
+    int twos = 0;
+    while (m % 2 == 0)
+    {
+        m /= 2;
+        ++twos;
+    }
+    std::vector<int> odd;
+    for (int p : {7, 5, 3})
+        while (m % p == 0)
+        {
+            m /= p;
+            odd.push_back(p);
+        }
+    if (m != 1)
+        return false;
+    const int a = twos / 4, b = twos % 4;
+    if (b == 1 && a >= 1)
+    {
+        for (int i = 0; i < a - 1; ++i)
+            out.push_back(16);
+        out.push_back(8);
+        out.push_back(4);
+    }
+    else
+    {
+        for (int i = 0; i < a; ++i)
+            out.push_back(16);
+        if (b == 1)
+            out.push_back(2);
+        else if (b == 2)
+            out.push_back(4);
+        else if (b == 3)
+            out.push_back(8);
+    }
+    for (int p : odd)
+        out.push_back(p);
+    return true;
+}
+
+bool is_smooth(long long n)
+{
+    std::vector<int> r;
+    return radices_for(n, r);
+}
+
+// Line lengths one pass transforms: every 7-smooth n up to 8192, and 16384.
+bool single_pass_ok(long long n) { return n >= 1 && (n <= 8192 || n == 16384) && is_smooth(n); }
+
+// The four-step split n = n1 * n2 (pass 1 transforms columns of length n1, pass 2 rows of length n2): the divisor
+// n2 <= sqrt(n) closest to it, both halves within one CTA.
+bool four_step_split(long long n, long long* n1, long long* n2)
+{
+    const long long s = static_cast<long long>(std::sqrt(static_cast<double>(n)));
+    for (long long d = s + 1; d >= 1; --d)
+    {
+        if (d * d > n || n % d != 0)
+            continue;
+        const long long other = n / d;
+        if (single_pass_ok(d) && single_pass_ok(other))
+        {
+            *n2 = d;
+            *n1 = other;
+            return true;
+        }
+    }
+    return false;
+}
+
+struct Plan
+{
+    crdfft_desc desc{};
+    int device = 0;
+    std::vector<Step> steps[2];
+    std::vector<void*> tables;
+    std::map<long long, void*> tw_by_n;
+    long long table_bytes = 0;
+    size_t ws_bytes = 0;
+    void* ws = nullptr;
+    bool ws_owned = false;
+    std::string algorithm;
+    std::vector<long long> factors;
+    // FftPlan::execute_batched sub-plans, one per batch value used (element-major layout).
+    std::map<long long, Plan*> batched;
+    std::mutex batched_mu;
+    int api_kind = 0; // 0 general, 1 FftPlan, 2 RealFftPlan, 3 BluesteinPlan, 4 NdFftPlan
+
+    ~Plan()
+    {
+        for (auto& kv : batched)
+            delete kv.second;
+        for (void* p : tables)
+            cudaFree(p);
+        if (ws_owned && ws != nullptr)
+            cudaFree(ws);
+    }
+};
+
+crdfft_status upload_table(Plan& p, const std::vector<float>& host, void** dev)
+{
+    const size_t bytes = host.size() * sizeof(float);
+    void* d = nullptr;
+    if (dev_alloc(&d, bytes) != cudaSuccess)
+        return CRDFFT_OOM;
+    p.tables.push_back(d);
+    p.table_bytes += static_cast<long long>(bytes);
+    if (cudaMemcpy(d, host.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+        return CRDFFT_LAUNCH;
+    *dev = d;
+    return CRDFFT_OK;
+}
+
+// W_n^k = exp(-2πik/n), computed in extended precision and rounded to FP64; the callers narrow it to FP32 (the
+// reference's convention, fft.hpp:253-260). The angle is reduced to at most π/4 with exact integer arithmetic
+// (k mod n, octant of 8k/n), and the quarter turns are applied by exact swaps and negations, so the table is exact at
+// the quarter points and symmetric.
+void root(long long k, long long n, double* re, double* im)
+{
+    k %= n;
+    if (k < 0)
+        k += n;
+    const long double quarter_pi = 0.78539816339744830961566084581987572L;
+    const unsigned __int128 num = static_cast<unsigned __int128>(k) * 8u;
+    const long long oct = static_cast<long long>(num / static_cast<unsigned __int128>(n));
+    const long long rem = static_cast<long long>(num - static_cast<unsigned __int128>(oct) * n);
+    long double c, s;
+    long long quarters;
+    if ((oct & 1) == 0)
+    {
+        const long double th = quarter_pi * static_cast<long double>(rem) / static_cast<long double>(n);
+        c = std::cos(th);
+        s = std::sin(th);
+        quarters = oct / 2;
+    }
+    else
+    {
+        const long double th = quarter_pi * static_cast<long double>(n - rem) / static_cast<long double>(n);
+        c = std::cos(th);
+        s = -std::sin(th);
+        quarters = (oct + 1) / 2;
+    }
+    long double cr = c, sr = s;
+    switch (quarters & 3)
+    {
+        case 0: cr = c; sr = s; break;
+        case 1: cr = -s; sr = c; break;
+        case 2: cr = -c; sr = -s; break;
+        default: cr = s; sr = -c; break;
+    }
+    *re = static_cast<double>(cr);
+    *im = static_cast<double>(-sr);
+}
+
+crdfft_status twiddle_table(Plan& p, long long n, const void** out)
+{
+    auto it = p.tw_by_n.find(n);
+    if (it != p.tw_by_n.end())
+    {
+        *out = it->second;
+        return CRDFFT_OK;
+    }
+    std::vector<float> h(static_cast<size_t>(2 * n));
+    for (long long k = 0; k < n; ++k)
+    {
+        double re, im;
+        root(k, n, &re, &im);
+        h[2 * k] = static_cast<float>(re);
+        h[2 * k + 1] = static_cast<float>(im);
+    }
+    void* d = nullptr;
+    const crdfft_status st = upload_table(p, h, &d);
+    if (st != CRDFFT_OK)
+        return st;
+    p.tw_by_n[n] = d;
+    *out = d;
+    return CRDFFT_OK;
+}
+
+PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, int P)
+{
+    PassShape sh{};
+    sh.map = map;
+    sh.direct_load = dl;
+    sh.direct_store = ds;
+    sh.points_per_thread = P;
+    const int T = static_cast<int>((n + P - 1) / P);
+    sh.threads_per_line = T;
+    const int pitch_bytes = pass_line_pitch(static_cast<int>(n)) * 8;
+    int lpc = map == PassMap::Row ? std::max(1, 256 / T) : std::max(1, 512 / T);
+    lpc = std::min(lpc, pass_lines_per_cta_limit());
+    while (lpc > 1 && lpc * T > pass_threads_limit())
+        --lpc;
+    const bool needs_smem = !(dl && ds && nstages == 1);
+    while (needs_smem && lpc > 1 && lpc * pitch_bytes > kMaxSmemBytes)
+        --lpc;
+    sh.lines_per_cta = lpc;
+    sh.smem_bytes = needs_smem ? lpc * pitch_bytes : 0;
+    return sh;
+}
+
+// The launch shape of a pass: 16 points a thread, or 32 where a compile-time schedule exists for it (lines longer
+// than 8192, and long columns, which then keep 4+ adjacent lines a CTA for 32-byte coalesced segments).
+bool shape_for(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
+{
+    const bool want32 = d.n > 8192 || (map == PassMap::Col && d.n >= 2048);
+    if (want32)
+    {
+        const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, 32);
+        if (sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit() && pass_has_kernel(d, sh))
+        {
+            *out = sh;
+            return true;
+        }
+    }
+    const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, 16);
+    if (sh.threads_per_line * sh.lines_per_cta > pass_threads_limit() || !pass_has_kernel(d, sh))
+        return false;
+    *out = sh;
+    return true;
+}
+
+crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lpg, LineMap in, LineMap out,
+                             BufRef src, BufRef dst, bool conj_in, bool conj_out, float scale, Step* step)
+{
+    std::vector<int> rad;
+    if (!single_pass_ok(n) || !radices_for(n, rad) || static_cast<int>(rad.size()) > kMaxStages)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    Step s;
+    s.kind = StepKind::Line;
+    PassDesc& d = s.pass;
+    d = PassDesc{};
+    d.n = static_cast<int>(n);
+    d.nstages = static_cast<int>(rad.size());
+    for (size_t i = 0; i < rad.size(); ++i)
+        d.radix[i] = rad[i];
+    d.lines = lines;
+    d.lines_per_group = lpg;
+    d.in = in;
+    d.out = out;
+    const crdfft_status st = twiddle_table(p, n, &d.tw);
+    if (st != CRDFFT_OK)
+        return st;
+    d.ftw_M = 0;
+    d.conj_in = conj_in ? 1 : 0;
+    d.conj_out = conj_out ? 1 : 0;
+    d.scale = scale;
+    // Thread map: along the elements when the loading side is unit-stride, across lines when adjacent lines are
+    // adjacent in memory (columns); the store side decides for the rest.
+    PassMap map;
+    if (in.estride == 1)
+        map = PassMap::Row;
+    else if (in.ldist == 1 && lpg > 1)
+        map = PassMap::Col;
+    else if (out.ldist == 1 && lpg > 1 && out.estride != 1)
+        map = PassMap::Col;
+    else
+        map = PassMap::Row;
+    bool dl, ds;
+    if (map == PassMap::Row)
+    {
+        dl = in.estride == 1;
+        ds = out.estride == 1;
+    }
+    else
+    {
+        dl = in.ldist == 1 && lpg > 1;
+        ds = out.ldist == 1 && lpg > 1;
+    }
+    if (d.nstages == 0) // n == 1: no butterflies; the pass is a copy with the epilogue, staged through smem
+        dl = ds = false;
+    if (!shape_for(d, map, dl, ds, &s.shape))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    s.src = src;
+    s.dst = dst;
+    *step = s;
+    return CRDFFT_OK;
+}
+
+// Four-step twiddle tables for W_M^m = hi[m / base] * lo[m % base].
+crdfft_status four_step_tables(Plan& p, long long M, int* base, const void** hi, const void** lo)
+{
+    long long b = 1;
+    while (b * b < M)
+        b <<= 1;
+    const long long nhi = (M + b - 1) / b;
+    std::vector<float> th(static_cast<size_t>(2 * nhi)), tl(static_cast<size_t>(2 * b));
+    for (long long i = 0; i < nhi; ++i)
+    {
+        double re, im;
+        root(i * b, M, &re, &im);
+        th[2 * i] = static_cast<float>(re);
+        th[2 * i + 1] = static_cast<float>(im);
+    }
+    for (long long i = 0; i < b; ++i)
+    {
+        double re, im;
+        root(i, M, &re, &im);
+        tl[2 * i] = static_cast<float>(re);
+        tl[2 * i + 1] = static_cast<float>(im);
+    }
+    void* dh = nullptr;
+    void* dl = nullptr;
+    crdfft_status st = upload_table(p, th, &dh);
+    if (st != CRDFFT_OK)
+        return st;
+    st = upload_table(p, tl, &dl);
+    if (st != CRDFFT_OK)
+        return st;
+    *base = static_cast<int>(b);
+    *hi = dh;
+    *lo = dl;
+    return CRDFFT_OK;
+}
+
+long long wave_bytes()
+{
+    const char* e = std::getenv("CRDFFT_WAVE_BYTES");
+    if (e != nullptr)
+    {
+        const long long v = std::atoll(e);
+        if (v > 0)
+            return v;
+    }
+    return 48LL << 20;
+}
+
+// A batch of 1-D complex transforms of length n: element j of transform t at base + t*dist + j*stride on each side.
+// Appends the steps of one direction; `ws_off` is where in the workspace this transform's scratch may start; the
+// scratch it needs is returned in *ws_need (complex elements).
+crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istride, long long idist,
+                          long long ostride, long long odist, BufRef src, BufRef dst, bool conj_in, bool conj_out,
+                          float scale, long long ws_off, std::vector<Step>& steps, long long* ws_need)
+{
+    *ws_need = 0;
+    if (single_pass_ok(n))
+    {
+        LineMap in{idist, 0, istride};
+        LineMap out{odist, 0, ostride};
+        long long lpg = 1;
+        if (idist == 1 && odist == 1 && batch > 1)
+        {
+            // element-major batch: lines are adjacent in memory
+            in = LineMap{0, 1, istride};
+            out = LineMap{0, 1, ostride};
+            lpg = batch;
+        }
+        Step s;
+        const crdfft_status st =
+            make_line_step(p, n, batch, lpg, in, out, src, dst, conj_in, conj_out, scale, &s);
+        if (st != CRDFFT_OK)
+            return st;
+        steps.push_back(s);
+        return CRDFFT_OK;
+    }
+    long long n1 = 0, n2 = 0;
+    if (!four_step_split(n, &n1, &n2))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    int base = 0;
+    const void* hi = nullptr;
+    const void* lo = nullptr;
+    crdfft_status st = four_step_tables(p, n, &base, &hi, &lo);
+    if (st != CRDFFT_OK)
+        return st;
+    long long wave = std::max(1LL, wave_bytes() / (n * 8));
+    wave = std::min(wave, batch);
+    *ws_need = wave * n;
+    for (long long t0 = 0; t0 < batch; t0 += wave)
+    {
+        const long long w = std::min(wave, batch - t0);
+        // pass 1: columns n2' in [0, n2), elements n1' along stride n2 -> scratch Y[t][k1][n2']
+        Step s1;
+        st = make_line_step(p, n1, w * n2, n2, LineMap{idist, istride, n2 * istride}, LineMap{n, 1, n2},
+                            BufRef{src.b, src.off + t0 * idist}, BufRef{Buf::Ws, ws_off}, conj_in, false, 1.0f, &s1);
+        if (st != CRDFFT_OK)
+            return st;
+        s1.pass.ftw_M = n;
+        s1.pass.ftw_base = base;
+        s1.pass.ftw_hi = hi;
+        s1.pass.ftw_lo = lo;
+        steps.push_back(s1);
+        // pass 2: rows k1 of length n2 -> X[t][k1 + n1 k2]
+        Step s2;
+        st = make_line_step(p, n2, w * n1, n1, LineMap{n, n2, 1}, LineMap{odist, ostride, n1 * ostride},
+                            BufRef{Buf::Ws, ws_off}, BufRef{dst.b, dst.off + t0 * odist}, false, conj_out, scale, &s2);
+        if (st != CRDFFT_OK)
+            return st;
+        steps.push_back(s2);
+    }
+    return CRDFFT_OK;
+}
+
+crdfft_status build_c2c_rank1(Plan& p)
+{
+    const crdfft_desc& d = p.desc;
+    const long long n = d.dims[0];
+    const long long istride = d.istride ? d.istride : 1;
+    const long long ostride = d.ostride ? d.ostride : 1;
+    const long long idist = d.idist ? d.idist : n;
+    const long long odist = d.odist ? d.odist : n;
+    const float inv_scale = d.norm == CRDFFT_NORM_INVERSE ? static_cast<float>(1.0 / static_cast<double>(n)) : 1.0f;
+    if (is_smooth(n))
+    {
+        long long ws_f = 0, ws_i = 0;
+        crdfft_status st = plan_c2c_1d(p, n, d.batch, istride, idist, ostride, odist, BufRef{Buf::In, 0},
+                                       BufRef{Buf::Out, 0}, false, false, 1.0f, 0, p.steps[0], &ws_f);
+        if (st != CRDFFT_OK)
+            return st;
+        st = plan_c2c_1d(p, n, d.batch, istride, idist, ostride, odist, BufRef{Buf::In, 0}, BufRef{Buf::Out, 0},
+                         true, true, inv_scale, 0, p.steps[1], &ws_i);
+        if (st != CRDFFT_OK)
+            return st;
+        p.ws_bytes = static_cast<size_t>(std::max(ws_f, ws_i)) * 8;
+        if (single_pass_ok(n))
+        {
+            p.algorithm = "single-pass";
+            p.factors = {n};
+        }
+        else
+        {
+            long long n1, n2;
+            four_step_split(n, &n1, &n2);
+            p.algorithm = "four-step";
+            p.factors = {n1, n2};
+        }
+        return CRDFFT_OK;
+    }
+    // Bluestein: m = smallest power of two >= 2n - 1 (bluestein.hpp:36-41).
+    long long m = 1;
+    while (m < 2 * n - 1)
+        m <<= 1;
+    // chirp_k = exp(+iπ k²/n), k² reduced mod 2n (bluestein.hpp:47-53)
+    std::vector<float> chirp(static_cast<size_t>(2 * n));
+    std::vector<std::complex<double>> bcirc(static_cast<size_t>(m), {0.0, 0.0});
+    for (long long k = 0; k < n; ++k)
+    {
+        const long long kk = static_cast<long long>((static_cast<unsigned __int128>(k) * k) % (2 * n));
+        // exp(+iπ kk/n) = conj(W_{2n}^{kk})
+        double re, im;
+        root(kk, 2 * n, &re, &im);
+        chirp[2 * k] = static_cast<float>(re);
+        chirp[2 * k + 1] = static_cast<float>(-im);
+        const std::complex<double> c(re, -im);
+        bcirc[static_cast<size_t>(k)] = c;
+        if (k > 0)
+            bcirc[static_cast<size_t>(m - k)] = c;
+    }
+    // FFT_m(b_circ) in FP64 on the host (the reference runs its f32 plan on the narrowed chirp; an FP64 spectrum
+    // narrowed once is at least as accurate).
+    std::vector<std::complex<double>> bf(static_cast<size_t>(m));
+    {
+        // iterative radix-2 DIT in FP64
+        std::vector<std::complex<double>> a = bcirc;
+        int lg = 0;
+        while ((1LL << lg) < m)
+            ++lg;
+        for (long long i = 0; i < m; ++i)
+        {
+            long long r = 0;
+            for (int b = 0; b < lg; ++b)
+                if (i & (1LL << b))
+                    r |= 1LL << (lg - 1 - b);
+            if (i < r)
+                std::swap(a[static_cast<size_t>(i)], a[static_cast<size_t>(r)]);
+        }
+        for (long long len = 2; len <= m; len <<= 1)
+        {
+            for (long long k = 0; k < len / 2; ++k)
+            {
+                double wr, wi;
+                root(k * (m / len), m, &wr, &wi);
+                const std::complex<double> w(wr, wi);
+                for (long long s = 0; s < m; s += len)
+                {
+                    const std::complex<double> u = a[static_cast<size_t>(s + k)];
+                    const std::complex<double> v = a[static_cast<size_t>(s + k + len / 2)] * w;
+                    a[static_cast<size_t>(s + k)] = u + v;
+                    a[static_cast<size_t>(s + k + len / 2)] = u - v;
+                }
+            }
+        }
+        bf = a;
+    }
+    std::vector<float> bff(static_cast<size_t>(2 * m));
+    for (long long k = 0; k < m; ++k)
+    {
+        bff[static_cast<size_t>(2 * k)] = static_cast<float>(bf[static_cast<size_t>(k)].real());
+        bff[static_cast<size_t>(2 * k + 1)] = static_cast<float>(bf[static_cast<size_t>(k)].imag());
+    }
+    void* dchirp = nullptr;
+    void* dbf = nullptr;
+    crdfft_status st = upload_table(p, chirp, &dchirp);
+    if (st != CRDFFT_OK)
+        return st;
+    st = upload_table(p, bff, &dbf);
+    if (st != CRDFFT_OK)
+        return st;
+    const long long B = d.batch;
+    const long long conv = B * m; // the padded sequences live at the start of the workspace
+    long long inner_f = 0, inner_i = 0;
+    for (int dir = 0; dir < 2; ++dir)
+    {
+        std::vector<Step>& steps = p.steps[dir];
+        ChirpDesc c{};
+        c.n = n;
+        c.m = m;
+        c.batch = B;
+        c.wdist = m;
+        c.chirp = dchirp;
+        c.bfft = dbf;
+        c.conj = dir;
+        Step pre;
+        pre.kind = StepKind::ChirpPre;
+        pre.chirp = c;
+        pre.chirp.xdist = idist;
+        pre.src = BufRef{Buf::In, 0};
+        pre.dst = BufRef{Buf::Ws, 0};
+        if (istride != 1 || ostride != 1)
+            return CRDFFT_UNSUPPORTED_SIZE;
+        steps.push_back(pre);
+        long long need = 0;
+        st = plan_c2c_1d(p, m, B, 1, m, 1, m, BufRef{Buf::Ws, 0}, BufRef{Buf::Ws, 0}, false, false, 1.0f, conv,
+                         steps, &need);
+        if (st != CRDFFT_OK)
+            return st;
+        inner_f = std::max(inner_f, need);
+        Step mul;
+        mul.kind = StepKind::SpecMul;
+        mul.chirp = c;
+        mul.dst = BufRef{Buf::Ws, 0};
+        steps.push_back(mul);
+        st = plan_c2c_1d(p, m, B, 1, m, 1, m, BufRef{Buf::Ws, 0}, BufRef{Buf::Ws, 0}, true, true, 1.0f, conv,
+                         steps, &need);
+        if (st != CRDFFT_OK)
+            return st;
+        inner_i = std::max(inner_i, need);
+        Step post;
+        post.kind = StepKind::ChirpPost;
+        post.chirp = c;
+        post.chirp.xdist = odist;
+        double sc = 1.0 / static_cast<double>(m);
+        if (dir == 1 && d.norm == CRDFFT_NORM_INVERSE)
+            sc /= static_cast<double>(n);
+        post.chirp.scale = static_cast<float>(sc);
+        post.src = BufRef{Buf::Ws, 0};
+        post.dst = BufRef{Buf::Out, 0};
+        steps.push_back(post);
+    }
+    p.ws_bytes = static_cast<size_t>(conv + std::max(inner_f, inner_i)) * 8;
+    p.algorithm = "bluestein";
+    p.factors = {n, m};
+    return CRDFFT_OK;
+}
+
+crdfft_status build_real(Plan& p)
+{
+    const crdfft_desc& d = p.desc;
+    const long long n = d.dims[0];
+    if (n < 2 || (n & 1) != 0)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const long long h = n / 2;
+    if (!is_smooth(h))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    if ((d.istride != 0 && d.istride != 1) || (d.ostride != 0 && d.ostride != 1))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    // W_n^k, k = 0 .. h (real_fft.hpp:25-35)
+    std::vector<float> wn(static_cast<size_t>(2 * (h + 1)));
+    for (long long k = 0; k <= h; ++k)
+    {
+        double re, im;
+        root(k, n, &re, &im);
+        wn[static_cast<size_t>(2 * k)] = static_cast<float>(re);
+        wn[static_cast<size_t>(2 * k + 1)] = static_cast<float>(im);
+    }
+    void* dwn = nullptr;
+    crdfft_status st = upload_table(p, wn, &dwn);
+    if (st != CRDFFT_OK)
+        return st;
+    long long need = 0;
+    if (d.kind == CRDFFT_R2C)
+    {
+        const long long idist = d.idist ? d.idist : n;       // floats
+        const long long odist = d.odist ? d.odist : h + 1;   // complex
+        if (idist % 2 != 0)
+            return CRDFFT_UNSUPPORTED_SIZE;
+        st = plan_c2c_1d(p, h, d.batch, 1, idist / 2, 1, odist, BufRef{Buf::In, 0}, BufRef{Buf::Out, 0}, false,
+                         false, 1.0f, 0, p.steps[0], &need);
+        if (st != CRDFFT_OK)
+            return st;
+        Step post;
+        post.kind = StepKind::R2CPost;
+        post.real = RealRecombine{h, d.batch, odist, odist, dwn, 1.0f};
+        post.src = BufRef{Buf::Out, 0};
+        post.dst = BufRef{Buf::Out, 0};
+        p.steps[0].push_back(post);
+    }
+    else
+    {
+        const long long idist = d.idist ? d.idist : h + 1;   // complex
+        const long long odist = d.odist ? d.odist : n;       // floats
+        if (odist % 2 != 0)
+            return CRDFFT_UNSUPPORTED_SIZE;
+        Step pre;
+        pre.kind = StepKind::C2RPre;
+        pre.real = RealRecombine{h, d.batch, odist / 2, idist, dwn, 1.0f};
+        pre.src = BufRef{Buf::In, 0};
+        pre.dst = BufRef{Buf::Out, 0};
+        p.steps[1].push_back(pre);
+        // IFFT_h unnormalised gives h z; the reference scales by 1/h (normalised irfft); unnormalised C2R is
+        // n times that.
+        const float sc = d.norm == CRDFFT_NORM_INVERSE ? static_cast<float>(1.0 / static_cast<double>(h)) : 2.0f;
+        st = plan_c2c_1d(p, h, d.batch, 1, odist / 2, 1, odist / 2, BufRef{Buf::Out, 0}, BufRef{Buf::Out, 0}, true,
+                         true, sc, 0, p.steps[1], &need);
+        if (st != CRDFFT_OK)
+            return st;
+    }
+    p.ws_bytes = static_cast<size_t>(need) * 8;
+    p.algorithm = single_pass_ok(h) ? "real+single-pass" : "real+four-step";
+    p.factors = {h};
+    return CRDFFT_OK;
+}
+
+crdfft_status build_nd(Plan& p)
+{
+    const crdfft_desc& d = p.desc;
+    const int rank = d.rank;
+    long long total = 1;
+    for (int i = 0; i < rank; ++i)
+        total *= d.dims[i];
+    const long long idist = d.idist ? d.idist : total;
+    const long long odist = d.odist ? d.odist : total;
+    if (idist != total || odist != total || d.istride > 1 || d.ostride > 1)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const float inv_scale =
+        d.norm == CRDFFT_NORM_INVERSE ? static_cast<float>(1.0 / static_cast<double>(total)) : 1.0f;
+    for (int dir = 0; dir < 2; ++dir)
+    {
+        // Axes from the last (unit stride) to the first; the first pass reads the input, later ones work in place
+        // on the output. The inverse conjugates on the way in and out (nd_fft.hpp:116-146).
+        bool first = true;
+        int last_axis = -1;
+        for (int ax = rank - 1; ax >= 0; --ax)
+            if (d.dims[ax] > 1)
+                last_axis = ax;
+        for (int ax = rank - 1; ax >= 0; --ax)
+        {
+            const long long n = d.dims[ax];
+            if (n == 1)
+                continue;
+            if (!single_pass_ok(n))
+                return CRDFFT_UNSUPPORTED_SIZE;
+            long long st_ax = 1;
+            for (int j = ax + 1; j < rank; ++j)
+                st_ax *= d.dims[j];
+            const long long lines = d.batch * (total / n);
+            LineMap m = st_ax == 1 ? LineMap{n, 0, 1} : LineMap{n * st_ax, 1, st_ax};
+            const long long lpg = st_ax == 1 ? 1 : st_ax;
+            const bool is_last = ax == last_axis;
+            Step s;
+            const crdfft_status st =
+                make_line_step(p, n, lines, lpg, m, m, first ? BufRef{Buf::In, 0} : BufRef{Buf::Out, 0},
+                               BufRef{Buf::Out, 0}, dir == 1 && first, dir == 1 && is_last,
+                               (dir == 1 && is_last) ? inv_scale : 1.0f, &s);
+            if (st != CRDFFT_OK)
+                return st;
+            p.steps[dir].push_back(s);
+            first = false;
+        }
+        if (first)
+        {
+            // every axis has length 1: a copy with the inverse's scale
+            Step s;
+            const crdfft_status st = make_line_step(p, 1, d.batch * total, 1, LineMap{1, 0, 1}, LineMap{1, 0, 1},
+                                                    BufRef{Buf::In, 0}, BufRef{Buf::Out, 0}, false, false,
+                                                    dir == 1 ? inv_scale : 1.0f, &s);
+            if (st != CRDFFT_OK)
+                return st;
+            p.steps[dir].push_back(s);
+        }
+    }
+    p.algorithm = "nd-axes";
+    for (int i = 0; i < rank; ++i)
+        p.factors.push_back(d.dims[i]);
+    return CRDFFT_OK;
+}
+
+crdfft_status validate(const crdfft_desc& d)
+{
+    if (d.rank < 1 || d.rank > 3 || d.batch < 1)
+        return CRDFFT_INVALID_DESC;
+    if (d.kind < CRDFFT_C2C || d.kind > CRDFFT_C2R || d.norm < 0 || d.norm > 1)
+        return CRDFFT_INVALID_DESC;
+    if (d.precision < 0 || d.precision > 2)
+        return CRDFFT_INVALID_DESC;
+    for (int i = 0; i < d.rank; ++i)
+        if (d.dims[i] < 1)
+            return CRDFFT_INVALID_DESC;
+    if (d.istride < 0 || d.ostride < 0 || d.idist < 0 || d.odist < 0)
+        return CRDFFT_INVALID_DESC;
+    if (d.rank > 1 && (d.istride > 1 || d.ostride > 1))
+        return CRDFFT_INVALID_DESC;
+    if (d.kind != CRDFFT_C2C && d.rank != 1)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    if (d.precision != CRDFFT_PREC_FP32)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    return CRDFFT_OK;
+}
+
+crdfft_status create(const crdfft_desc* desc, Plan** out)
+{
+    if (desc == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    *out = nullptr;
+    crdfft_status st = validate(*desc);
+    if (st != CRDFFT_OK)
+        return st;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return CRDFFT_NO_DEVICE;
+    std::unique_ptr<Plan> p(new Plan());
+    p->desc = *desc;
+    p->device = dev;
+    if (desc->kind != CRDFFT_C2C)
+        st = build_real(*p);
+    else if (desc->rank == 1)
+        st = build_c2c_rank1(*p);
+    else
+        st = build_nd(*p);
+    if (st != CRDFFT_OK)
+        return st;
+    if (p->ws_bytes > 0)
+    {
+        if (dev_alloc(&p->ws, p->ws_bytes) != cudaSuccess)
+        {
+            p->ws = nullptr;
+            return CRDFFT_OOM;
+        }
+        p->ws_owned = true;
+    }
+    *out = p.release();
+    return CRDFFT_OK;
+}
+
+void* resolve(const BufRef& r, const void* in, void* out, void* ws)
+{
+    char* base = r.b == Buf::In ? static_cast<char*>(const_cast<void*>(in))
+               : r.b == Buf::Out ? static_cast<char*>(out)
+                                 : static_cast<char*>(ws);
+    return base + r.off * 8;
+}
+
+crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stream)
+{
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != p.device)
+        return CRDFFT_NO_DEVICE;
+    if (p.ws_bytes > 0 && p.ws == nullptr)
+        return CRDFFT_INVALID_ARG;
+    for (const Step& s : p.steps[dir])
+    {
+        void* src = resolve(s.src, in, out, p.ws);
+        void* dst = resolve(s.dst, in, out, p.ws);
+        cudaError_t e = cudaSuccess;
+        switch (s.kind)
+        {
+            case StepKind::Line: e = launch_line_pass(s.pass, s.shape, src, dst, stream); break;
+            case StepKind::R2CPost: e = launch_r2c_post(s.real, src, dst, stream); break;
+            case StepKind::C2RPre: e = launch_c2r_pre(s.real, src, dst, stream); break;
+            case StepKind::ChirpPre: e = launch_chirp_pre(s.chirp, src, dst, stream); break;
+            case StepKind::SpecMul: e = launch_spectrum_mul(s.chirp, dst, stream); break;
+            case StepKind::ChirpPost: e = launch_chirp_post(s.chirp, src, dst, stream); break;
+            case StepKind::Scale: e = launch_scale(dst, s.count, s.scale, stream); break;
+        }
+        if (e != cudaSuccess)
+            return CRDFFT_LAUNCH;
+    }
+    return CRDFFT_OK;
+}
+
+crdfft_status simple_plan(int api_kind, const crdfft_desc& d, crdfft_plan** plan)
+{
+    if (plan == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan* p = nullptr;
+    const crdfft_status st = create(&d, &p);
+    if (st != CRDFFT_OK)
+    {
+        *plan = nullptr;
+        return st;
+    }
+    p->api_kind = api_kind;
+    *plan = reinterpret_cast<crdfft_plan*>(p);
+    return CRDFFT_OK;
+}
+
+crdfft_desc desc_1d(long long n, int kind, int norm)
+{
+    crdfft_desc d{};
+    d.rank = 1;
+    d.kind = kind;
+    d.precision = CRDFFT_PREC_FP32;
+    d.norm = norm;
+    d.dims[0] = n;
+    d.batch = 1;
+    return d;
+}
+
+Plan* as_plan(crdfft_plan* p) { return reinterpret_cast<Plan*>(p); }
+
+} // namespace
+} // namespace crdfft
+
+using namespace crdfft;
+
+extern "C" {
+
+crdfft_status crdfft_plan_create(const crdfft_desc* desc, crdfft_plan** plan)
+{
+    if (plan == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan* p = nullptr;
+    const crdfft_status st = create(desc, &p);
+    *plan = reinterpret_cast<crdfft_plan*>(p);
+    return st;
+}
+
+crdfft_status crdfft_plan_destroy(crdfft_plan* plan)
+{
+    delete as_plan(plan);
+    return CRDFFT_OK;
+}
+
+crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32_t direction, void* stream)
+{
+    if (plan == nullptr || in == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    if (direction != CRDFFT_FORWARD && direction != CRDFFT_INVERSE)
+        return CRDFFT_INVALID_ARG;
+    if ((p.desc.kind == CRDFFT_R2C && direction != CRDFFT_FORWARD) ||
+        (p.desc.kind == CRDFFT_C2R && direction != CRDFFT_INVERSE))
+        return CRDFFT_INVALID_ARG;
+    return run(p, in, out, direction, static_cast<cudaStream_t>(stream));
+}
+
+crdfft_status crdfft_plan_info_get(const crdfft_plan* plan, crdfft_plan_info* info)
+{
+    if (plan == nullptr || info == nullptr)
+        return CRDFFT_INVALID_ARG;
+    const Plan& p = *reinterpret_cast<const Plan*>(plan);
+    std::memset(info, 0, sizeof(*info));
+    std::strncpy(info->algorithm, p.algorithm.c_str(), sizeof(info->algorithm) - 1);
+    info->passes = static_cast<int32_t>(p.steps[p.desc.kind == CRDFFT_C2R ? 1 : 0].size());
+    info->device = p.device;
+    info->workspace_bytes = static_cast<int64_t>(p.ws_bytes);
+    info->table_bytes = p.table_bytes;
+    for (size_t i = 0; i < p.factors.size() && i < 7; ++i)
+        info->factors[i] = p.factors[i];
+    return CRDFFT_OK;
+}
+
+size_t crdfft_workspace_size(const crdfft_plan* plan)
+{
+    return plan == nullptr ? 0 : reinterpret_cast<const Plan*>(plan)->ws_bytes;
+}
+
+crdfft_status crdfft_set_workspace(crdfft_plan* plan, void* workspace, size_t bytes)
+{
+    if (plan == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    if (workspace == nullptr)
+    {
+        if (p.ws_owned || p.ws_bytes == 0)
+            return CRDFFT_OK;
+        void* w = nullptr;
+        if (dev_alloc(&w, p.ws_bytes) != cudaSuccess)
+            return CRDFFT_OOM;
+        p.ws = w;
+        p.ws_owned = true;
+        return CRDFFT_OK;
+    }
+    if (bytes < p.ws_bytes || (reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
+        return CRDFFT_INVALID_ARG;
+    if (p.ws_owned && p.ws != nullptr)
+        cudaFree(p.ws);
+    p.ws = workspace;
+    p.ws_owned = false;
+    return CRDFFT_OK;
+}
+
+const char* crdfft_status_string(crdfft_status status)
+{
+    switch (status)
+    {
+        case CRDFFT_OK: return "ok";
+        case CRDFFT_INVALID_DESC: return "invalid descriptor";
+        case CRDFFT_UNSUPPORTED_SIZE: return "unsupported size or layout";
+        case CRDFFT_OOM: return "device out of memory";
+        case CRDFFT_LAUNCH: return "kernel launch failed";
+        case CRDFFT_DEVICE_TIMEOUT: return "device-side wait timed out";
+        case CRDFFT_NUMERIC_SELFCHECK: return "device self-check failed";
+        case CRDFFT_INVALID_ARG: return "invalid argument";
+        case CRDFFT_NO_DEVICE: return "no CUDA device / wrong device";
+    }
+    return "unknown status";
+}
+
+crdfft_status crdfft_fft_plan_create(int64_t n, crdfft_plan** plan)
+{
+    return simple_plan(1, desc_1d(n, CRDFFT_C2C, CRDFFT_NORM_NONE), plan);
+}
+
+crdfft_status crdfft_fft_execute(crdfft_plan* plan, void* data, int32_t direction, void* stream)
+{
+    return crdfft_execute(plan, data, data, direction, stream);
+}
+
+crdfft_status crdfft_fft_execute_batched(crdfft_plan* plan, void* data, int64_t batch, int32_t direction,
+                                         void* stream)
+{
+    if (plan == nullptr || data == nullptr || batch < 1)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    if (p.desc.rank != 1 || p.desc.kind != CRDFFT_C2C)
+        return CRDFFT_INVALID_ARG;
+    Plan* sub = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(p.batched_mu);
+        auto it = p.batched.find(batch);
+        if (it != p.batched.end())
+            sub = it->second;
+        else
+        {
+            crdfft_desc d = p.desc;
+            d.batch = batch;
+            d.istride = batch;
+            d.ostride = batch;
+            d.idist = 1;
+            d.odist = 1;
+            const crdfft_status st = create(&d, &sub);
+            if (st != CRDFFT_OK)
+                return st;
+            p.batched[batch] = sub;
+        }
+    }
+    return crdfft_execute(reinterpret_cast<crdfft_plan*>(sub), data, data, direction, stream);
+}
+
+crdfft_status crdfft_real_plan_create(int64_t n, crdfft_plan** plan)
+{
+    // One plan answers both verbs: the forward steps are R2C, the inverse steps C2R.
+    if (plan == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan* f = nullptr;
+    crdfft_desc d = desc_1d(n, CRDFFT_R2C, CRDFFT_NORM_INVERSE);
+    crdfft_status st = create(&d, &f);
+    if (st != CRDFFT_OK)
+    {
+        *plan = nullptr;
+        return st;
+    }
+    Plan* inv = nullptr;
+    d.kind = CRDFFT_C2R;
+    st = create(&d, &inv);
+    if (st != CRDFFT_OK)
+    {
+        delete f;
+        *plan = nullptr;
+        return st;
+    }
+    // Fold the C2R steps, tables and workspace into the R2C plan.
+    f->steps[1] = inv->steps[1];
+    for (void* t : inv->tables)
+        f->tables.push_back(t);
+    inv->tables.clear();
+    f->table_bytes += inv->table_bytes;
+    if (inv->ws_bytes > f->ws_bytes)
+    {
+        if (f->ws_owned && f->ws)
+            cudaFree(f->ws);
+        f->ws = inv->ws;
+        f->ws_owned = inv->ws_owned;
+        f->ws_bytes = inv->ws_bytes;
+        inv->ws = nullptr;
+        inv->ws_owned = false;
+    }
+    delete inv;
+    f->api_kind = 2;
+    f->desc.kind = CRDFFT_C2C; // both directions allowed through the verbs below
+    *plan = reinterpret_cast<crdfft_plan*>(f);
+    return CRDFFT_OK;
+}
+
+crdfft_status crdfft_rfft(crdfft_plan* plan, const float* real_in, void* out, void* stream)
+{
+    if (plan == nullptr || as_plan(plan)->api_kind != 2 || real_in == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    return run(*as_plan(plan), real_in, out, 0, static_cast<cudaStream_t>(stream));
+}
+
+crdfft_status crdfft_irfft(crdfft_plan* plan, const void* in, float* real_out, void* stream)
+{
+    if (plan == nullptr || as_plan(plan)->api_kind != 2 || in == nullptr || real_out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    return run(*as_plan(plan), in, real_out, 1, static_cast<cudaStream_t>(stream));
+}
+
+crdfft_status crdfft_bluestein_plan_create(int64_t n, crdfft_plan** plan)
+{
+    return simple_plan(3, desc_1d(n, CRDFFT_C2C, CRDFFT_NORM_INVERSE), plan);
+}
+
+crdfft_status crdfft_bluestein_execute(crdfft_plan* plan, void* data, int32_t direction, void* stream)
+{
+    return crdfft_execute(plan, data, data, direction, stream);
+}
+
+crdfft_status crdfft_nd_plan_create(int32_t ndim, const int64_t* dims, crdfft_plan** plan)
+{
+    if (dims == nullptr || ndim < 1 || ndim > 3)
+        return CRDFFT_INVALID_DESC;
+    crdfft_desc d{};
+    d.rank = ndim;
+    d.kind = CRDFFT_C2C;
+    d.precision = CRDFFT_PREC_FP32;
+    d.norm = CRDFFT_NORM_INVERSE;
+    for (int i = 0; i < ndim; ++i)
+        d.dims[i] = dims[i];
+    d.batch = 1;
+    return simple_plan(4, d, plan);
+}
+
+crdfft_status crdfft_nd_execute(crdfft_plan* plan, void* data, int32_t direction, void* stream)
+{
+    return crdfft_execute(plan, data, data, direction, stream);
+}
+
+crdfft_status crdfft_fft(void* data, int64_t n, int32_t direction, void* stream)
+{
+    crdfft_plan* p = nullptr;
+    crdfft_status st = crdfft_fft_plan_create(n, &p);
+    if (st != CRDFFT_OK)
+        return st;
+    st = crdfft_fft_execute(p, data, direction, stream);
+    cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    crdfft_plan_destroy(p);
+    return st;
+}
+
+crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream)
+{
+    crdfft_plan* p = nullptr;
+    crdfft_desc d = desc_1d(n, CRDFFT_C2C, CRDFFT_NORM_INVERSE);
+    crdfft_status st = simple_plan(1, d, &p);
+    if (st != CRDFFT_OK)
+        return st;
+    st = crdfft_execute(p, data, data, CRDFFT_INVERSE, stream);
+    cudaStreamSynchronize(static_cast<cudaStream_t>(stream));
+    crdfft_plan_destroy(p);
+    return st;
+}
+
+void crdfft_debug_fail_alloc_after(int32_t k) { g_fail_alloc_after.store(k < 0 ? 0 : k); }
+
+} // extern "C"

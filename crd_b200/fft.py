@@ -1,0 +1,259 @@
+"""Python mirror of crd-hesap-fft's plan classes over the C ABI (include/crdfft.h), on CUDA tensors.
+
+Each class keeps the reference's name, constructor meaning, verbs and normalisation
+(engine/numerics/hesap-fft/include/crd/hesap/fft/):
+
+* ``FftPlan(n)`` - fft.hpp:220-470: ``execute(data, direction)`` in place, unnormalised both ways;
+  ``execute_batched(data, batch, direction)`` element-major (element i of transform t at data[i*batch + t]).
+* ``RealFftPlan(n)`` - real_fft.hpp:18-101: ``rfft(real_in, out)`` (n reals -> n/2+1 complex, unnormalised) and
+  ``irfft(in, real_out)`` (normalised by 1/n).
+* ``BluesteinPlan(n)`` - bluestein.hpp:29-149: any n; ``execute`` forward unnormalised, inverse normalised by 1/n.
+* ``NdFftPlan(dims)`` - nd_fft.hpp:28-194: row-major 1-3 dims; inverse normalised by 1/prod(dims).
+* ``fft(data, direction)`` / ``ifft_normalized(data)`` - fft.hpp:1006-1029.
+
+``Plan(desc)`` exposes the general descriptor (batch, strides, R2C/C2R, precision) the benchmarks use.
+
+Tensors must be CUDA tensors on the plan's device: complex64 (or float32 on the real side of R2C/C2R), contiguous
+in the layout the plan describes. Work is enqueued on torch's current CUDA stream, so it orders with the caller's
+torch work. The reference's preconditions (sizes, power-of-two-ness where it asserts them) become ``ValueError``;
+library status codes become ``CrdFftError``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Iterable, Optional, Sequence
+
+import torch
+
+from . import _lib
+from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP32, R2C, CrdFftError, Desc,
+                   PlanInfo, check, lib)
+
+Forward = FORWARD
+Inverse = INVERSE
+
+
+def _dir(direction) -> int:
+    if isinstance(direction, str):
+        direction = {"forward": FORWARD, "inverse": INVERSE}[direction.lower()]
+    d = int(direction)
+    if d not in (FORWARD, INVERSE):
+        raise ValueError(f"direction must be 0 (forward) or 1 (inverse), not {direction!r}")
+    return d
+
+
+def _stream(stream) -> ctypes.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    if isinstance(stream, torch.cuda.Stream):
+        return ctypes.c_void_p(stream.cuda_stream)
+    return ctypes.c_void_p(int(stream))
+
+
+def _ptr(t: torch.Tensor, dtype: torch.dtype, what: str) -> ctypes.c_void_p:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{what} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise ValueError(f"{what} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{what} must be contiguous")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class _Handle:
+    def __init__(self):
+        self._h = ctypes.c_void_p()
+
+    def _release(self):
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().crdfft_plan_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self._release()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        inf = PlanInfo()
+        check(lib().crdfft_plan_info_get(self._h, ctypes.byref(inf)), "plan_info")
+        return {
+            "algorithm": inf.algorithm.decode(),
+            "passes": inf.passes,
+            "device": inf.device,
+            "workspace_bytes": inf.workspace_bytes,
+            "table_bytes": inf.table_bytes,
+            "factors": [int(f) for f in inf.factors if f],
+        }
+
+    def workspace_size(self) -> int:
+        return int(lib().crdfft_workspace_size(self._h))
+
+    def set_workspace(self, ws: Optional[torch.Tensor]) -> None:
+        if ws is None:
+            check(lib().crdfft_set_workspace(self._h, None, 0), "set_workspace")
+            self._ws = None
+            return
+        nbytes = ws.numel() * ws.element_size()
+        check(lib().crdfft_set_workspace(self._h, ctypes.c_void_p(ws.data_ptr()), nbytes), "set_workspace")
+        self._ws = ws  # keep it alive
+
+
+class Plan(_Handle):
+    """The general descriptor plan (crdfft_plan_create)."""
+
+    def __init__(self, dims: Sequence[int], batch: int = 1, kind: int = C2C, precision: int = PREC_FP32,
+                 norm: int = NORM_NONE, istride: int = 0, idist: int = 0, ostride: int = 0, odist: int = 0):
+        super().__init__()
+        dims = [int(d) for d in dims]
+        if not 1 <= len(dims) <= 3:
+            raise ValueError("rank must be 1, 2 or 3")
+        d = Desc()
+        d.rank = len(dims)
+        d.kind = kind
+        d.precision = precision
+        d.norm = norm
+        for i, v in enumerate(dims):
+            d.dims[i] = v
+        d.batch = batch
+        d.istride, d.idist, d.ostride, d.odist = istride, idist, ostride, odist
+        self.dims = tuple(dims)
+        self.batch = batch
+        self.kind = kind
+        check(lib().crdfft_plan_create(ctypes.byref(d), ctypes.byref(self._h)), "plan_create")
+
+    def execute(self, inp: torch.Tensor, out: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+        in_dtype = torch.float32 if self.kind == R2C else torch.complex64
+        out_dtype = torch.float32 if self.kind == C2R else torch.complex64
+        pi = _ptr(inp, in_dtype, "input")
+        po = _ptr(out, out_dtype, "output")
+        check(lib().crdfft_execute(self._h, pi, po, _dir(direction), _stream(stream)), "execute")
+        return out
+
+
+class FftPlan(_Handle):
+    """FftPlan<float>(alloc, n) - one size-n complex transform (fft.hpp:224)."""
+
+    def __init__(self, n: int):
+        super().__init__()
+        if n < 1:
+            raise ValueError("n must be >= 1")
+        self.n = int(n)
+        check(lib().crdfft_fft_plan_create(self.n, ctypes.byref(self._h)), "FftPlan")
+
+    def size(self) -> int:
+        return self.n
+
+    def execute(self, data: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+        """In place, unnormalised (fft.hpp:409-413)."""
+        if data.numel() != self.n:
+            raise ValueError(f"data holds {data.numel()} values, the plan {self.n}")
+        check(lib().crdfft_fft_execute(self._h, _ptr(data, torch.complex64, "data"), _dir(direction),
+                                       _stream(stream)), "execute")
+        return data
+
+    def execute_batched(self, data: torch.Tensor, batch: int, direction=FORWARD, stream=None) -> torch.Tensor:
+        """Element-major batch in place (fft.hpp:462-470): element i of transform t at data[i*batch + t]."""
+        if data.numel() != self.n * batch:
+            raise ValueError(f"data holds {data.numel()} values, expected n*batch = {self.n * batch}")
+        check(lib().crdfft_fft_execute_batched(self._h, _ptr(data, torch.complex64, "data"), int(batch),
+                                               _dir(direction), _stream(stream)), "execute_batched")
+        return data
+
+
+class RealFftPlan(_Handle):
+    """RealFftPlan<float>(alloc, n): real[n] <-> complex[n/2+1] (real_fft.hpp:18-101)."""
+
+    def __init__(self, n: int):
+        super().__init__()
+        if n < 2 or n % 2:
+            raise ValueError("n must be even and >= 2")
+        self.n = int(n)
+        check(lib().crdfft_real_plan_create(self.n, ctypes.byref(self._h)), "RealFftPlan")
+
+    def size(self) -> int:
+        return self.n
+
+    def rfft(self, real_in: torch.Tensor, out: torch.Tensor, stream=None) -> torch.Tensor:
+        if real_in.numel() != self.n or out.numel() != self.n // 2 + 1:
+            raise ValueError("rfft wants real_in[n] and out[n/2+1]")
+        check(lib().crdfft_rfft(self._h, _ptr(real_in, torch.float32, "real_in"), _ptr(out, torch.complex64, "out"),
+                                _stream(stream)), "rfft")
+        return out
+
+    def irfft(self, inp: torch.Tensor, real_out: torch.Tensor, stream=None) -> torch.Tensor:
+        if inp.numel() != self.n // 2 + 1 or real_out.numel() != self.n:
+            raise ValueError("irfft wants in[n/2+1] and real_out[n]")
+        check(lib().crdfft_irfft(self._h, _ptr(inp, torch.complex64, "in"), _ptr(real_out, torch.float32, "real_out"),
+                                 _stream(stream)), "irfft")
+        return real_out
+
+
+class BluesteinPlan(_Handle):
+    """BluesteinPlan<float>(alloc, n): any n >= 1; inverse normalised by 1/n (bluestein.hpp:29-149)."""
+
+    def __init__(self, n: int):
+        super().__init__()
+        if n < 1:
+            raise ValueError("n must be >= 1")
+        self.n = int(n)
+        check(lib().crdfft_bluestein_plan_create(self.n, ctypes.byref(self._h)), "BluesteinPlan")
+
+    def size(self) -> int:
+        return self.n
+
+    def execute(self, data: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+        if data.numel() != self.n:
+            raise ValueError(f"data holds {data.numel()} values, the plan {self.n}")
+        check(lib().crdfft_bluestein_execute(self._h, _ptr(data, torch.complex64, "data"), _dir(direction),
+                                             _stream(stream)), "execute")
+        return data
+
+
+class NdFftPlan(_Handle):
+    """NdFftPlan<float>(alloc, dims): row-major N-D transform; inverse normalised by 1/prod(dims)
+    (nd_fft.hpp:28-194)."""
+
+    def __init__(self, dims: Iterable[int]):
+        super().__init__()
+        dims = [int(d) for d in dims]
+        if not 1 <= len(dims) <= 3 or any(d < 1 for d in dims):
+            raise ValueError("1 to 3 dims, each >= 1")
+        self.dims = tuple(dims)
+        arr = (ctypes.c_int64 * len(dims))(*dims)
+        check(lib().crdfft_nd_plan_create(len(dims), arr, ctypes.byref(self._h)), "NdFftPlan")
+
+    def execute(self, data: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+        total = 1
+        for d in self.dims:
+            total *= d
+        if data.numel() != total:
+            raise ValueError(f"data holds {data.numel()} values, the plan {total}")
+        check(lib().crdfft_nd_execute(self._h, _ptr(data, torch.complex64, "data"), _dir(direction),
+                                      _stream(stream)), "execute")
+        return data
+
+
+def fft(data: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+    """One-shot in-place transform, unnormalised (fft.hpp:1006-1012)."""
+    check(lib().crdfft_fft(_ptr(data, torch.complex64, "data"), data.numel(), _dir(direction), _stream(stream)), "fft")
+    return data
+
+
+def ifft_normalized(data: torch.Tensor, stream=None) -> torch.Tensor:
+    """One-shot in-place inverse scaled by 1/n (fft.hpp:1015-1029)."""
+    check(lib().crdfft_ifft_normalized(_ptr(data, torch.complex64, "data"), data.numel(), _stream(stream)),
+          "ifft_normalized")
+    return data
+
+
+def self_check() -> None:
+    """The device known-answer check (the role of src/fft_self_check.cpp); raises CrdFftError on a mismatch."""
+    check(lib().crdfft_self_check(), "self_check")
+
+
+def fail_alloc_after(k: int) -> None:
+    """Test hook: the k-th device allocation from now fails (0 = off)."""
+    lib().crdfft_debug_fail_alloc_after(int(k))

@@ -1,0 +1,179 @@
+/*
+ * crdfft.h - C ABI of the B200 FFT execution path (plan creation + execute), a drop-in for crd-hesap-fft's
+ * plan/execute surface (reference: engine/numerics/hesap-fft/include/crd/hesap/fft/).
+ *
+ * Data are device pointers to interleaved single-precision complex values ({float re; float im;}, the layout of
+ * crd::hesap::Complex<f32>, engine/numerics/hesap/include/crd/hesap/complex.hpp:30-35) or to plain floats for the
+ * real side of R2C/C2R. Every call is stream-ordered on the CUDA stream passed as `stream` (NULL = legacy default
+ * stream). No function aborts: each returns a crdfft_status. Plans are immutable after creation; one plan may be
+ * executed from several threads only on distinct workspaces (crdfft_set_workspace), as the reference's "one plan
+ * per thread" rule (fft.hpp:17-18) asks of its scratch.
+ *
+ * Sign and normalisation follow the reference:
+ *   forward  X_k = sum_j x_j exp(-2 pi i j k / n)           (fft.hpp:257-259)
+ *   inverse  x_j = sum_k X_k exp(+2 pi i j k / n) * s       s = 1 (CRDFFT_NORM_NONE, FftPlan, fft.hpp:16)
+ *                                                           s = 1/n (CRDFFT_NORM_INVERSE: BluesteinPlan,
+ *                                                           bluestein.hpp:84-86; RealFftPlan::irfft,
+ *                                                           real_fft.hpp:87-91; NdFftPlan, nd_fft.hpp:138-146)
+ */
+#ifndef CRDFFT_H
+#define CRDFFT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference's preconditions are CRD_ASSERTs and its out-of-memory is fatal (fft.hpp:237,411,468,
+ * 480-483); here each becomes a returned code. */
+typedef enum crdfft_status
+{
+    CRDFFT_OK = 0,
+    CRDFFT_INVALID_DESC = 1,      /* malformed descriptor (rank, dims, strides, kind) */
+    CRDFFT_UNSUPPORTED_SIZE = 2,  /* a size or layout this build does not plan */
+    CRDFFT_OOM = 3,               /* a device allocation for tables or workspace failed */
+    CRDFFT_LAUNCH = 4,            /* a kernel launch or CUDA runtime call failed */
+    CRDFFT_DEVICE_TIMEOUT = 5,    /* a bounded device-side wait gave up (persistent kernels) */
+    CRDFFT_NUMERIC_SELFCHECK = 6, /* the device known-answer check disagreed with the host FP64 DFT */
+    CRDFFT_INVALID_ARG = 7,       /* null plan/pointer, wrong direction, size mismatch */
+    CRDFFT_NO_DEVICE = 8          /* no CUDA device, or the plan's device is not current */
+} crdfft_status;
+
+/* FftDirection (include/crd/hesap/fft/fft_kernels.hpp:20-24). */
+typedef enum crdfft_direction
+{
+    CRDFFT_FORWARD = 0,
+    CRDFFT_INVERSE = 1
+} crdfft_direction;
+
+typedef enum crdfft_kind
+{
+    CRDFFT_C2C = 0, /* complex -> complex */
+    CRDFFT_R2C = 1, /* real[n] -> complex[n/2+1] (RealFftPlan::rfft, real_fft.hpp:41-64); forward only */
+    CRDFFT_C2R = 2  /* complex[n/2+1] -> real[n] (RealFftPlan::irfft, real_fft.hpp:67-92); inverse only */
+} crdfft_kind;
+
+typedef enum crdfft_precision
+{
+    CRDFFT_PREC_FP32 = 0,       /* FP32 butterflies, FP32 data */
+    CRDFFT_PREC_SPLIT_BF16 = 1, /* radix-16 stages as tensor-core GEMM on bf16 hi+lo splits, FP32 accumulate */
+    CRDFFT_PREC_FP16_SCALED = 2 /* radix-16 stages on fp16 with a per-transform scale, FP32 accumulate */
+} crdfft_precision;
+
+typedef enum crdfft_norm
+{
+    CRDFFT_NORM_NONE = 0,   /* unnormalised both ways (FftPlan) */
+    CRDFFT_NORM_INVERSE = 1 /* inverse scaled by 1/prod(dims) (Bluestein, Real, Nd plans) */
+} crdfft_norm;
+
+/* A plan descriptor. dims are row-major (dims[rank-1] varies fastest). For R2C/C2R, dims[rank-1] is the real
+ * length n and the complex side holds n/2+1 values along that axis. Strides and distances count elements of the
+ * side they describe (complex elements, or floats on the real side); 0 selects the packed layout:
+ *   istride = 1, idist = prod(input dims).
+ * The reference's element-major execute_batched (fft.hpp:462-470) is istride = ostride = batch, idist = odist = 1. */
+typedef struct crdfft_desc
+{
+    int32_t rank;      /* 1, 2 or 3 */
+    int32_t kind;      /* crdfft_kind */
+    int32_t precision; /* crdfft_precision */
+    int32_t norm;      /* crdfft_norm */
+    int64_t dims[3];
+    int64_t batch;     /* >= 1 */
+    int64_t istride;   /* rank 1 only; 0 = 1 */
+    int64_t idist;     /* 0 = packed */
+    int64_t ostride;   /* rank 1 only; 0 = 1 */
+    int64_t odist;     /* 0 = packed */
+} crdfft_desc;
+
+typedef struct crdfft_plan crdfft_plan;
+
+typedef struct crdfft_plan_info
+{
+    char algorithm[64];      /* "single-pass", "four-step", "bluestein", "real+single-pass", "nd-axes", ... */
+    int32_t passes;          /* kernel launches one forward execute issues */
+    int32_t device;          /* the CUDA device the plan lives on */
+    int64_t workspace_bytes; /* scratch one execute needs */
+    int64_t table_bytes;     /* device twiddle / chirp tables the plan owns */
+    int64_t factors[8];      /* the line lengths of the passes (e.g. n1, n2 of the four-step), 0-terminated */
+} crdfft_plan_info;
+
+/* ---- General plan (cuFFT-style descriptor) ------------------------------------------------------------------ */
+
+/* Build a plan on the current CUDA device. Computes twiddle tables in FP64 on the host and narrows them to FP32
+ * (the reference's convention, fft.hpp:251-260), uploads them and allocates the workspace. Replaces the FftPlan /
+ * RealFftPlan / BluesteinPlan / NdFftPlan constructors (fft.hpp:224-304, real_fft.hpp:21-36, bluestein.hpp:31-75,
+ * nd_fft.hpp:31-79). */
+crdfft_status crdfft_plan_create(const crdfft_desc* desc, crdfft_plan** plan);
+
+/* Release a plan, its tables and its owned workspace. NULL is accepted. */
+crdfft_status crdfft_plan_destroy(crdfft_plan* plan);
+
+/* Run the plan: `in` -> `out` (in == out allowed for C2C, the reference's in-place execute, fft.hpp:409-413).
+ * `direction` is crdfft_direction; R2C plans accept only CRDFFT_FORWARD and C2R plans only CRDFFT_INVERSE. */
+crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32_t direction, void* stream);
+
+crdfft_status crdfft_plan_info_get(const crdfft_plan* plan, crdfft_plan_info* info);
+
+/* Bytes of scratch one execute of this plan uses (0 when it needs none). */
+size_t crdfft_workspace_size(const crdfft_plan* plan);
+
+/* Point the plan at caller-owned device scratch of at least crdfft_workspace_size bytes (256-byte aligned); the
+ * plan frees the workspace it allocated. NULL restores a plan-owned workspace. */
+crdfft_status crdfft_set_workspace(crdfft_plan* plan, void* workspace, size_t bytes);
+
+const char* crdfft_status_string(crdfft_status status);
+
+/* ---- The reference's plan classes, verb for verb ------------------------------------------------------------- */
+
+/* FftPlan<float>(alloc, n) (fft.hpp:224): one size-n complex transform, unnormalised both ways. */
+crdfft_status crdfft_fft_plan_create(int64_t n, crdfft_plan** plan);
+/* FftPlan::execute(data, dir) (fft.hpp:409-413): in place. */
+crdfft_status crdfft_fft_execute(crdfft_plan* plan, void* data, int32_t direction, void* stream);
+/* FftPlan::execute_batched(data, batch, dir) (fft.hpp:462-470): `batch` transforms, element i of transform t at
+ * data[i*batch + t], in place. */
+crdfft_status crdfft_fft_execute_batched(crdfft_plan* plan, void* data, int64_t batch, int32_t direction,
+                                         void* stream);
+
+/* RealFftPlan<float>(alloc, n) (real_fft.hpp:21-36); n even, >= 2. */
+crdfft_status crdfft_real_plan_create(int64_t n, crdfft_plan** plan);
+/* RealFftPlan::rfft(real_in[n], out[n/2+1]) (real_fft.hpp:41-64), unnormalised. */
+crdfft_status crdfft_rfft(crdfft_plan* plan, const float* real_in, void* out, void* stream);
+/* RealFftPlan::irfft(in[n/2+1], real_out[n]) (real_fft.hpp:67-92), normalised by 1/n. */
+crdfft_status crdfft_irfft(crdfft_plan* plan, const void* in, float* real_out, void* stream);
+
+/* BluesteinPlan<float>(alloc, n) (bluestein.hpp:31): any n >= 1; forward unnormalised, inverse normalised by 1/n.
+ * 7-smooth n run natively in mixed radix; other n run the chirp-z algorithm over a power-of-two plan. */
+crdfft_status crdfft_bluestein_plan_create(int64_t n, crdfft_plan** plan);
+/* BluesteinPlan::execute(data, dir) (bluestein.hpp:87-136): in place. */
+crdfft_status crdfft_bluestein_execute(crdfft_plan* plan, void* data, int32_t direction, void* stream);
+
+/* NdFftPlan<float>(alloc, dims) (nd_fft.hpp:31): row-major ndim in 1..3; inverse normalised by 1/prod(dims). */
+crdfft_status crdfft_nd_plan_create(int32_t ndim, const int64_t* dims, crdfft_plan** plan);
+/* NdFftPlan::execute(data, dir) (nd_fft.hpp:105-147): in place. */
+crdfft_status crdfft_nd_execute(crdfft_plan* plan, void* data, int32_t direction, void* stream);
+
+/* One-shot fft(alloc, data, dir) (fft.hpp:1006-1012) and ifft_normalized (fft.hpp:1015-1029): build a transient
+ * plan, run it in place, release it (synchronises the stream before releasing). */
+crdfft_status crdfft_fft(void* data, int64_t n, int32_t direction, void* stream);
+crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream);
+
+/* ---- Self-check and fault injection ------------------------------------------------------------------------- */
+
+/* The device known-answer check (the role of the reference's fft_self_check, src/fft_self_check.cpp:153-211):
+ * runs a set of small transforms (radices 2..16, 3, 5, 7, a four-step and a real transform) on the current device
+ * and compares them with a host FP64 DFT: max|gpu - dft| <= 1e-5 (1 + max|dft|). CRDFFT_OK or
+ * CRDFFT_NUMERIC_SELFCHECK. */
+crdfft_status crdfft_self_check(void);
+
+/* Test hook: make the k-th device allocation from now fail (k >= 1), as if the device were out of memory; 0 turns
+ * it off. The reference tests its out-of-memory paths with a refusing allocator in a child process
+ * (tests/numerics/hesap-fft/CMakeLists.txt:26-36); here plan creation returns CRDFFT_OOM instead. */
+void crdfft_debug_fail_alloc_after(int32_t k);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRDFFT_H */

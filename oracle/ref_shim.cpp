@@ -1,0 +1,282 @@
+// Test infrastructure: a C ABI over the reference's own crd-hesap-fft plans, compiled together with the reference's
+// sources by oracle/Makefile into oracle/_ref/libcrdref.so. Tests and the CPU-baseline leg of bench.py load it with
+// ctypes; the product never links it. Every function forwards to the reference class named in its comment and adds
+// only the batching loop the reference's batch semantics describe: a batch of independent transforms is split into
+// contiguous ranges, one range and one plan per thread (engine/numerics/hesap-fft/include/crd/hesap/fft/detail/
+// batch_arms.hpp:59-77).
+
+#include <crd/hesap/complex.hpp>
+#include <crd/hesap/fft/bluestein.hpp>
+#include <crd/hesap/fft/fft.hpp>
+#include <crd/hesap/fft/fft_dispatch.hpp>
+#include <crd/hesap/fft/nd_fft.hpp>
+#include <crd/hesap/fft/real_fft.hpp>
+#include <crd/memory/allocators/malloc_allocator.hpp>
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <thread>
+#include <vector>
+
+namespace fft = crd::hesap::fft;
+namespace cont = crd::containers;
+using crd::hesap::Complex;
+
+namespace
+{
+
+crd::memory::MallocAllocator& alloc()
+{
+    static crd::memory::MallocAllocator a("crdref-shim");
+    return a;
+}
+
+fft::FftDirection dir_of(int dir)
+{
+    return dir == 0 ? fft::FftDirection::Forward : fft::FftDirection::Inverse;
+}
+
+bool is_pow2(std::size_t n)
+{
+    return n != 0 && (n & (n - 1)) == 0;
+}
+
+// Runs fn(first, last) over [0, count) in `threads` contiguous ranges, one std::thread each (range j is
+// [j*count/threads, (j+1)*count/threads)), the partition of batch_arms.hpp:59-77.
+template <typename F> void fan_out(int threads, std::size_t count, const F& fn)
+{
+    if (threads <= 1 || count <= 1)
+    {
+        fn(std::size_t{0}, count);
+        return;
+    }
+    const std::size_t t = static_cast<std::size_t>(threads) < count ? static_cast<std::size_t>(threads) : count;
+    std::vector<std::thread> pool;
+    pool.reserve(t);
+    for (std::size_t j = 0; j < t; ++j)
+    {
+        pool.emplace_back([&fn, j, t, count]() { fn(j * count / t, (j + 1) * count / t); });
+    }
+    for (auto& th : pool)
+    {
+        th.join();
+    }
+}
+
+// A batch of contiguous size-n complex transforms of type T, in place. Power-of-two sizes run FftPlan<T>::execute
+// (fft.hpp:409-413, unnormalised both ways); other sizes run BluesteinPlan<T>::execute (bluestein.hpp:87-136, whose
+// inverse is normalised by 1/n).
+template <typename T> int c2c(std::size_t n, std::size_t batch, T* data, int dir, int threads)
+{
+    if (n == 0)
+    {
+        return -1;
+    }
+    auto* x = reinterpret_cast<Complex<T>*>(data);
+    fan_out(threads, batch,
+            [&](std::size_t first, std::size_t last)
+            {
+                if (is_pow2(n))
+                {
+                    const fft::FftPlan<T> plan(&alloc(), n);
+                    for (std::size_t t = first; t < last; ++t)
+                    {
+                        plan.execute(cont::Span<Complex<T>>(x + t * n, n), dir_of(dir));
+                    }
+                }
+                else
+                {
+                    const fft::BluesteinPlan<T> plan(&alloc(), n);
+                    for (std::size_t t = first; t < last; ++t)
+                    {
+                        plan.execute(cont::Span<Complex<T>>(x + t * n, n), dir_of(dir));
+                    }
+                }
+            });
+    return 0;
+}
+
+} // namespace
+
+extern "C"
+{
+
+// The CPU level the reference's runtime dispatch selected (crd::CpuLevel value: 0 portable .. 4 avx512). The first
+// call runs the reference's known-answer self-check (src/fft_self_check.cpp) on the selected table.
+int crdref_level(void)
+{
+    return static_cast<int>(fft::fft_kernels().level);
+}
+
+// Reference's known-answer self-check over a level's table: 0 when both golden digests match, 1 otherwise
+// (src/fft_self_check.cpp:153-211, kAnswers64/kAnswers32 at :96-97).
+int crdref_self_check_level(int level)
+{
+    for (const auto& entry : fft::fft_kernel_levels())
+    {
+        if (static_cast<int>(entry.level) == level)
+        {
+            return fft::fft_self_check(*entry.table) == nullptr ? 0 : 1;
+        }
+    }
+    return -1;
+}
+
+// The algorithm name FftPlan<float>(n) runs forward (fft.hpp:224-227 planner; fft_kernels.hpp fft_algorithm_name).
+const char* crdref_plan_algorithm_f32(std::size_t n)
+{
+    if (!is_pow2(n))
+    {
+        return "bluestein";
+    }
+    const fft::FftPlan<float> plan(&alloc(), n);
+    return fft::fft_algorithm_name(plan.state().forward);
+}
+
+int crdref_c2c_f32(std::size_t n, std::size_t batch, float* data, int dir, int threads)
+{
+    return c2c<float>(n, batch, data, dir, threads);
+}
+
+int crdref_c2c_f64(std::size_t n, std::size_t batch, double* data, int dir, int threads)
+{
+    return c2c<double>(n, batch, data, dir, threads);
+}
+
+// FftPlan<T>::execute_reference: the reference's own radix-2 in-place oracle (fft.hpp:417-460). Power of two only.
+int crdref_execute_reference_f32(std::size_t n, float* data, int dir)
+{
+    if (!is_pow2(n))
+    {
+        return -1;
+    }
+    const fft::FftPlan<float> plan(&alloc(), n);
+    plan.execute_reference(cont::Span<Complex<float>>(reinterpret_cast<Complex<float>*>(data), n), dir_of(dir));
+    return 0;
+}
+
+int crdref_execute_reference_f64(std::size_t n, double* data, int dir)
+{
+    if (!is_pow2(n))
+    {
+        return -1;
+    }
+    const fft::FftPlan<double> plan(&alloc(), n);
+    plan.execute_reference(cont::Span<Complex<double>>(reinterpret_cast<Complex<double>*>(data), n), dir_of(dir));
+    return 0;
+}
+
+// FftPlan<float>::execute_batched: element-major batch, element i of transform t at data[i*batch + t]
+// (fft.hpp:462-470).
+int crdref_execute_batched_f32(std::size_t n, std::size_t batch, float* data, int dir)
+{
+    if (!is_pow2(n))
+    {
+        return -1;
+    }
+    const fft::FftPlan<float> plan(&alloc(), n);
+    plan.execute_batched(cont::Span<Complex<float>>(reinterpret_cast<Complex<float>*>(data), n * batch), batch,
+                         dir_of(dir));
+    return 0;
+}
+
+// The Stockham plan of the self-check (FftPlan(alloc, n, FftAlgorithm::Stockham)), so its known-answer cases can be
+// dumped as golden vectors. n is a power of two from 2 to 128.
+int crdref_stockham_f32(std::size_t n, std::size_t batch, float* data, int dir)
+{
+    if (!is_pow2(n))
+    {
+        return -1;
+    }
+    const fft::FftPlan<float> plan(&alloc(), n, fft::FftAlgorithm::Stockham);
+    auto* x = reinterpret_cast<Complex<float>*>(data);
+    if (batch == 0)
+    {
+        plan.execute(cont::Span<Complex<float>>(x, n), dir_of(dir));
+    }
+    else
+    {
+        plan.execute_batched(cont::Span<Complex<float>>(x, n * batch), batch, dir_of(dir));
+    }
+    return 0;
+}
+
+// RealFftPlan<float>::rfft over a batch: real[n] -> complex[n/2+1] per transform (real_fft.hpp:41-64).
+int crdref_rfft_f32(std::size_t n, std::size_t batch, const float* in, float* out, int threads)
+{
+    if (n < 4 || !is_pow2(n))
+    {
+        return -1;
+    }
+    const std::size_t h = n / 2 + 1;
+    fan_out(threads, batch,
+            [&](std::size_t first, std::size_t last)
+            {
+                const fft::RealFftPlan<float> plan(&alloc(), n);
+                for (std::size_t t = first; t < last; ++t)
+                {
+                    plan.rfft(cont::ConstSpan<float>(in + t * n, n),
+                              cont::Span<Complex<float>>(reinterpret_cast<Complex<float>*>(out) + t * h, h));
+                }
+            });
+    return 0;
+}
+
+// RealFftPlan<float>::irfft over a batch: complex[n/2+1] -> real[n], normalised by 1/n (real_fft.hpp:67-92).
+int crdref_irfft_f32(std::size_t n, std::size_t batch, const float* in, float* out, int threads)
+{
+    if (n < 4 || !is_pow2(n))
+    {
+        return -1;
+    }
+    const std::size_t h = n / 2 + 1;
+    fan_out(threads, batch,
+            [&](std::size_t first, std::size_t last)
+            {
+                const fft::RealFftPlan<float> plan(&alloc(), n);
+                for (std::size_t t = first; t < last; ++t)
+                {
+                    plan.irfft(
+                        cont::ConstSpan<Complex<float>>(reinterpret_cast<const Complex<float>*>(in) + t * h, h),
+                        cont::Span<float>(out + t * n, n));
+                }
+            });
+    return 0;
+}
+
+// NdFftPlan<T>::execute, in place on a row-major array of ndim dims (nd_fft.hpp:105-147; inverse normalised by
+// 1/prod(dims)). Runs on the calling thread (one set of axis plans).
+int crdref_nd_f32(std::size_t ndim, const std::size_t* dims, float* data, int dir)
+{
+    if (ndim == 0)
+    {
+        return -1;
+    }
+    std::size_t total = 1;
+    for (std::size_t i = 0; i < ndim; ++i)
+    {
+        total *= dims[i];
+    }
+    const fft::NdFftPlan<float> plan(&alloc(), cont::ConstSpan<std::size_t>(dims, ndim));
+    plan.execute(cont::Span<Complex<float>>(reinterpret_cast<Complex<float>*>(data), total), dir_of(dir));
+    return 0;
+}
+
+int crdref_nd_f64(std::size_t ndim, const std::size_t* dims, double* data, int dir)
+{
+    if (ndim == 0)
+    {
+        return -1;
+    }
+    std::size_t total = 1;
+    for (std::size_t i = 0; i < ndim; ++i)
+    {
+        total *= dims[i];
+    }
+    const fft::NdFftPlan<double> plan(&alloc(), cont::ConstSpan<std::size_t>(dims, ndim));
+    plan.execute(cont::Span<Complex<double>>(reinterpret_cast<Complex<double>*>(data), total), dir_of(dir));
+    return 0;
+}
+
+} // extern "C"

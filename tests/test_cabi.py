@@ -1,0 +1,76 @@
+"""CPU tests of the boundary: libcrdfft.so loads (no GPU needed) and exports every entry point include/crdfft.h
+declares; the Python mirror's tables agree with the header; descriptor validation and error strings need no device.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from crd_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include")))
+           if f.endswith(".h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(crdfft_[a-z0-9_]+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return sorted(names)
+
+
+def test_header_declares_the_reference_verbs():
+    names = declared_functions()
+    for verb in ("crdfft_fft_plan_create", "crdfft_fft_execute", "crdfft_fft_execute_batched",
+                 "crdfft_real_plan_create", "crdfft_rfft", "crdfft_irfft", "crdfft_bluestein_plan_create",
+                 "crdfft_bluestein_execute", "crdfft_nd_plan_create", "crdfft_nd_execute", "crdfft_fft",
+                 "crdfft_ifft_normalized", "crdfft_plan_create", "crdfft_execute", "crdfft_plan_destroy"):
+        assert verb in names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    assert sorted(_lib.EXPORTS) == declared_functions()
+    _lib.lib()  # loads and sets every signature
+
+
+def test_status_strings():
+    L = _lib.lib()
+    for code in range(9):
+        assert L.crdfft_status_string(code)
+    assert L.crdfft_status_string(3) == b"device out of memory"
+
+
+def test_descriptor_sizes_match_header():
+    # crdfft_desc: 4 int32 + 3 int64 dims + 5 int64 = 80 bytes; crdfft_plan_info: 64 + 2*4 + 2*8 + 8*8 = 152
+    assert ctypes.sizeof(_lib.Desc) == 80
+    assert ctypes.sizeof(_lib.PlanInfo) == 152
+
+
+def test_invalid_descriptor_rejected_without_device():
+    L = _lib.lib()
+    d = _lib.Desc()
+    d.rank = 0
+    d.batch = 1
+    h = ctypes.c_void_p()
+    assert L.crdfft_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.INVALID_DESC
+    d.rank = 1
+    d.dims[0] = 16
+    d.batch = 0
+    assert L.crdfft_plan_create(ctypes.byref(d), ctypes.byref(h)) == _lib.INVALID_DESC
+    assert L.crdfft_plan_create(None, ctypes.byref(h)) == _lib.INVALID_ARG
+    assert L.crdfft_execute(None, None, None, 0, None) == _lib.INVALID_ARG
+    assert L.crdfft_plan_destroy(None) == _lib.OK

@@ -1,0 +1,258 @@
+"""GPU parity: the CUDA path (through the C ABI in include/crdfft.h) against the FP64 oracle and the reference's own
+FP32 outputs, on the reference tests' seeded inputs.
+
+Tolerances, written per test:
+* rel-L2 against the FP64 oracle <= 1e-6 (the FP32 accuracy bar of this project), and
+* max|gpu - oracle| / (1 + max|oracle|) within the reference's own f32 class: 2e-4 below 2^19, 1e-3 from 2^19
+  (tests/numerics/hesap-fft/test_fft_kernels.cpp:138-163), and against the reference's FP32 output too.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import crd_b200 as cf
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+REL_L2 = 1e-6
+
+
+def _check(got, want, n, what=""):
+    rl2 = oracle.rel_l2(got, want)
+    mr = oracle.max_rel(got, want)
+    assert rl2 <= REL_L2, f"{what} n={n}: rel-L2 {rl2:.3e} > {REL_L2}"
+    assert mr <= oracle.f32_class(n), f"{what} n={n}: max-rel {mr:.3e}"
+    return rl2
+
+
+def _c2c(n, batch, inverse, seed=None, norm=cf.NORM_NONE):
+    seed = (0x9E3779B97F4A7C15 ^ n) if seed is None else seed
+    x = oracle.lcg_complex64(seed, n * batch).reshape(batch, n)
+    t = torch.from_numpy(x).cuda()
+    o = torch.empty_like(t)
+    plan = cf.Plan([n], batch=batch, norm=norm)
+    plan.execute(t, o, cf.INVERSE if inverse else cf.FORWARD)
+    torch.cuda.synchronize()
+    return x, o.cpu().numpy(), plan
+
+
+SINGLE = [1, 2, 3, 4, 5, 7, 8, 9, 16, 32, 64, 105, 128, 240, 256, 512, 1000, 1024, 2048, 3000, 4096, 6144, 8192,
+          16384]
+
+
+@pytest.mark.parametrize("n", SINGLE)
+@pytest.mark.parametrize("inverse", [False, True])
+def test_c2c_single_pass(n, inverse):
+    batch = 5 if n <= 4096 else 2
+    x, got, plan = _c2c(n, batch, inverse)
+    assert plan.info()["algorithm"] == "single-pass"
+    _check(got, oracle.fft64(x, inverse), n)
+
+
+@pytest.mark.parametrize("n", [32768, 65536, 107520, 3 * 5 * 7 * 2 ** 9, 2 ** 20])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_c2c_four_step(n, inverse):
+    batch = 3 if n < 2 ** 20 else 2
+    x, got, plan = _c2c(n, batch, inverse)
+    assert plan.info()["algorithm"] == "four-step"
+    _check(got, oracle.fft64(x, inverse), n)
+
+
+def test_four_step_waves(monkeypatch):
+    """A batch larger than one L2 wave runs as several waves; each transform must come out the same."""
+    monkeypatch.setenv("CRDFFT_WAVE_BYTES", str(65536 * 8 * 2))  # two transforms a wave
+    x, got, plan = _c2c(65536, 5, False, seed=77)
+    _check(got, oracle.fft64(x), 65536)
+
+
+@pytest.mark.parametrize("n", [11, 17, 143, 1009, 1031])
+def test_bluestein_sizes(n):
+    """Sizes with a prime factor above 7 run the chirp-z path; inverse normalised as BluesteinPlan's."""
+    for inverse in (False, True):
+        x, got, plan = _c2c(n, 3, inverse, norm=cf.NORM_INVERSE)
+        assert plan.info()["algorithm"] == "bluestein"
+        want = oracle.fft64(x, inverse) / (n if inverse else 1)
+        _check(got, want, n)
+
+
+@pytest.mark.parametrize("n", [17, 100, 360, 1009, 4000])
+def test_bluestein_plan_class(n):
+    """BluesteinPlan<float>(n).execute in place vs the FP64 restatement of the reference's Bluestein."""
+    x = oracle.lcg_complex64(0x9E3779B97F4A7C15 ^ n, n)
+    for inverse in (False, True):
+        t = torch.from_numpy(x.copy()).cuda()
+        cf.BluesteinPlan(n).execute(t, cf.INVERSE if inverse else cf.FORWARD)
+        _check(t.cpu().numpy(), oracle.bluestein64(x, inverse), n)
+
+
+@pytest.mark.parametrize("n,batch", [(64, 7), (64, 8), (1024, 3), (105, 4), (65536, 2)])
+def test_execute_batched_element_major(n, batch):
+    """FftPlan::execute_batched: element i of transform t at data[i*batch + t] (fft.hpp:462-470)."""
+    x = oracle.lcg_complex64(n * 31 + batch, n * batch)
+    t = torch.from_numpy(x.copy()).cuda()
+    cf.FftPlan(n).execute_batched(t, batch, cf.FORWARD)
+    got = t.cpu().numpy().reshape(n, batch).T
+    _check(got, oracle.fft64(x.reshape(n, batch).T), n)
+
+
+@pytest.mark.parametrize("n", [2, 4, 64, 1024, 8192, 2 ** 15, 2 ** 20])
+def test_real_plan(n):
+    """RealFftPlan: rfft unnormalised, irfft normalised (real_fft.hpp:41-92)."""
+    x = oracle.lcg_float32(31337 + n, n)
+    plan = cf.RealFftPlan(n)
+    tin = torch.from_numpy(x).cuda()
+    spec = torch.empty(n // 2 + 1, dtype=torch.complex64, device="cuda")
+    plan.rfft(tin, spec)
+    back = torch.empty(n, dtype=torch.float32, device="cuda")
+    plan.irfft(spec, back)
+    torch.cuda.synchronize()
+    want = oracle.rfft64(x.astype(np.float64))
+    _check(spec.cpu().numpy(), want, n, "rfft")
+    got_back = back.cpu().numpy()
+    assert np.max(np.abs(got_back - x)) <= 1e-5 * (1 + np.max(np.abs(x)))
+
+
+@pytest.mark.parametrize("n,batch", [(1024, 4), (2 ** 20, 2)])
+def test_r2c_c2r_batched(n, batch):
+    x = oracle.lcg_float32(n + batch, n * batch).reshape(batch, n)
+    r2c = cf.Plan([n], batch=batch, kind=cf.R2C)
+    c2r = cf.Plan([n], batch=batch, kind=cf.C2R)
+    tin = torch.from_numpy(x).cuda()
+    spec = torch.empty(batch, n // 2 + 1, dtype=torch.complex64, device="cuda")
+    r2c.execute(tin, spec, cf.FORWARD)
+    back = torch.empty(batch, n, dtype=torch.float32, device="cuda")
+    c2r.execute(spec, back, cf.INVERSE)  # unnormalised C2R: n * x
+    torch.cuda.synchronize()
+    _check(spec.cpu().numpy(), oracle.rfft64(x.astype(np.float64)), n, "r2c")
+    assert np.max(np.abs(back.cpu().numpy() / n - x)) <= 1e-5 * (1 + np.max(np.abs(x)))
+
+
+@pytest.mark.parametrize("dims", [(8, 16), (4, 6, 5), (16, 12), (64, 128), (32, 64, 16), (105, 48), (256, 256)])
+def test_nd_plan(dims):
+    total = int(np.prod(dims))
+    x = oracle.lcg_complex64(0x9E3779B97F4A7C15 ^ total, total).reshape(dims)
+    for inverse in (False, True):
+        t = torch.from_numpy(x.copy()).cuda()
+        cf.NdFftPlan(dims).execute(t, cf.INVERSE if inverse else cf.FORWARD)
+        _check(t.cpu().numpy(), oracle.nd64(x, inverse), max(dims))
+
+
+def test_against_reference_f32_outputs(golden):
+    """The GPU agrees with the reference's own FP32 outputs at the reference's f32 class."""
+    for n in (16, 105, 240, 1024, 4096):
+        x = golden[f"c2c_{n}_in"]
+        pow2 = (n & (n - 1)) == 0
+        for inverse, key in ((False, "fwd"), (True, "inv")):
+            t = torch.from_numpy(x.copy()).cuda()
+            if pow2:
+                cf.FftPlan(n).execute(t, cf.INVERSE if inverse else cf.FORWARD)
+            else:
+                cf.BluesteinPlan(n).execute(t, cf.INVERSE if inverse else cf.FORWARD)
+            ref = golden[f"c2c_{n}_{key}"].astype(np.complex128)
+            assert oracle.max_rel(t.cpu().numpy(), ref) < oracle.f32_class(n)
+    for n in (64, 1024):
+        plan = cf.RealFftPlan(n)
+        spec = torch.empty(n // 2 + 1, dtype=torch.complex64, device="cuda")
+        plan.rfft(torch.from_numpy(golden[f"rfft_{n}_in"]).cuda(), spec)
+        assert oracle.max_rel(spec.cpu().numpy(), golden[f"rfft_{n}_out"].astype(np.complex128)) < 2e-4
+        out = torch.empty(n, dtype=torch.float32, device="cuda")
+        plan.irfft(torch.from_numpy(golden[f"irfft_{n}_in"]).cuda(), out)
+        want = golden[f"irfft_{n}_out"]
+        assert np.max(np.abs(out.cpu().numpy() - want)) < 2e-4 * (1 + np.max(np.abs(want)))
+    for dims in ((8, 16), (4, 6, 5), (16, 12)):
+        tag = "x".join(str(d) for d in dims)
+        for inverse, key in ((False, "fwd"), (True, "inv")):
+            t = torch.from_numpy(golden[f"nd_{tag}_in"].copy()).cuda()
+            cf.NdFftPlan(dims).execute(t, cf.INVERSE if inverse else cf.FORWARD)
+            assert oracle.max_rel(t.cpu().numpy(), golden[f"nd_{tag}_{key}"].astype(np.complex128)) < 2e-4
+
+
+def test_selfcheck_known_answers(golden):
+    """The reference's own known-answer cases (src/fft_self_check.cpp:67-77) on the GPU, vs its outputs."""
+    for idx in range(26):
+        n, batch, inv, tiny = (int(v) for v in golden[f"selfcheck_{idx}_meta"])
+        if tiny:
+            continue  # subnormal results: the GPU flushes nothing here, but FP32 FMA contraction differs in ulps
+        x = golden[f"selfcheck_{idx}_in"]
+        t = torch.from_numpy(x.copy()).cuda()
+        plan = cf.FftPlan(n)
+        if batch == 0:
+            plan.execute(t, inv)
+        else:
+            plan.execute_batched(t, batch, inv)
+        ref = golden[f"selfcheck_{idx}_out"].astype(np.complex128)
+        scale = np.max(np.abs(ref))
+        assert np.max(np.abs(t.cpu().numpy() - ref)) <= 2e-7 * scale + 1e-30
+
+
+def test_device_self_check():
+    cf.self_check()
+
+
+def test_run_twice_bit_identical_and_in_place():
+    """Fixed schedules, no atomics: two runs give the same bits; in-place equals out-of-place."""
+    for n, batch in ((1024, 64), (65536, 3), (107520, 2)):
+        x = oracle.lcg_complex64(n, n * batch).reshape(batch, n)
+        t = torch.from_numpy(x).cuda()
+        plan = cf.Plan([n], batch=batch)
+        a = torch.empty_like(t)
+        b = torch.empty_like(t)
+        plan.execute(t, a)
+        plan.execute(t, b)
+        c = t.clone()
+        plan.execute(c, c)
+        torch.cuda.synchronize()
+        assert torch.equal(a.view(torch.float32), b.view(torch.float32))
+        assert torch.equal(a.view(torch.float32), c.view(torch.float32))
+
+
+def test_guard_words_kept():
+    """NaN canaries just before and after the output survive (test_fft_kernels.cpp:65-135 guard words)."""
+    for n, batch in ((1024, 7), (65536, 2), (1000, 3)):
+        x = oracle.lcg_complex64(n ^ 5, n * batch)
+        buf = torch.full((n * batch + 64,), complex(float("nan"), float("nan")), dtype=torch.complex64,
+                         device="cuda")
+        out = buf[32:32 + n * batch]
+        plan = cf.Plan([n], batch=batch)
+        plan.execute(torch.from_numpy(x).cuda(), out)
+        torch.cuda.synchronize()
+        host = buf.cpu().numpy()
+        assert np.all(np.isnan(host[:32])) and np.all(np.isnan(host[32 + n * batch:]))
+        assert np.all(np.isfinite(host[32:32 + n * batch]))
+
+
+def test_special_values_propagate():
+    """Inf/NaN inputs propagate into the outputs that depend on them instead of vanishing (the reference's
+    special-value cases, test_fft_kernels.cpp:345-420)."""
+    n = 1024
+    x = np.zeros(n, dtype=np.complex64)
+    x[3] = np.inf
+    t = torch.from_numpy(x).cuda()
+    o = torch.empty_like(t)
+    cf.Plan([n]).execute(t, o)
+    got = o.cpu().numpy()
+    assert not np.all(np.isfinite(got))
+
+
+def test_errors_are_status_codes():
+    with pytest.raises(cf.CrdFftError) as e:
+        cf.Plan([0])
+    assert e.value.status == 1
+    with pytest.raises(cf.CrdFftError) as e:
+        cf.Plan([16], batch=0)
+    assert e.value.status == 1
+    from crd_b200 import fft as F
+
+    F.fail_alloc_after(1)
+    try:
+        with pytest.raises(cf.CrdFftError) as e:
+            cf.Plan([1024])
+        assert e.value.status == 3
+    finally:
+        F.fail_alloc_after(0)
+    p = cf.Plan([1024])  # allocation works again
+    assert p.info()["algorithm"] == "single-pass"
