@@ -59,6 +59,8 @@ EXPORTS = (
     "crdfft_ifft_normalized",
     "crdfft_self_check",
     "crdfft_debug_fail_alloc_after",
+    "crdfft_device_status",
+    "crdfft_debug_stall_waits",
 )
 
 
@@ -131,6 +133,8 @@ def lib():
         "crdfft_ifft_normalized": ([vp, i64, vp], i32),
         "crdfft_self_check": ([], i32),
         "crdfft_debug_fail_alloc_after": ([i32], None),
+        "crdfft_device_status": ([vp, vp], i32),
+        "crdfft_debug_stall_waits": ([i32], None),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -14,6 +14,8 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
 int pass_threads_limit();
+int pass_pipe_threads();
+int pass_pipe_smem(int n, PassMap map, int lpc);
 bool pass_has_kernel(const PassDesc& d, const PassShape& sh);
 
 // Real <-> half-length complex recombination (real_ops.cu), the math of the reference's RealFftPlan

@@ -1,45 +1,120 @@
-// Launcher of the line-FFT pass kernel (line_fft.cuh): picks the compile-time schedule when one exists for the pass,
-// else the run-time schedule, and launches one CTA per `lines_per_cta` lines.
+// Launchers of the line-FFT pass kernels (line_fft.cuh): the pipelined persistent kernel where the planner chose it,
+// else the compile-time schedule when one exists for the pass, else the run-time schedule.
 
 #include "kernels.hpp"
 #include "line_fft.cuh"
+
+#include <mutex>
+#include <unordered_map>
 
 namespace crdfft
 {
 
 int pass_lines_per_cta_limit() { return lfft::kMaxLinesPerCta; }
 int pass_threads_limit() { return lfft::kMaxThreads; }
+int pass_pipe_threads() { return lfft::kPipeThreads; }
 int pass_line_pitch(int n) { return lfft::line_pitch(n); }
+
+int pass_pipe_smem(int n, PassMap map, int lpc)
+{
+    const int elems = map == PassMap::Row ? lpc * lfft::pipe_row_pitch(n) : n * lfft::pipe_col_pitch(lpc);
+    return 128 + 2 * elems * 8;
+}
 
 bool pass_has_kernel(const PassDesc& d, const PassShape& sh)
 {
+    if (sh.pipelined)
+        return lfft::select_pipe(d, sh) != nullptr;
     return lfft::select_static(d, sh) != nullptr || lfft::select_dynamic(d, sh) != nullptr;
 }
 
+namespace
+{
+
+// CTAs of a pipelined kernel resident per SM (queried once per kernel and shape).
+int resident_ctas(const void* fn, int threads, int smem)
+{
+    static std::mutex mu;
+    static std::unordered_map<const void*, std::unordered_map<long long, int>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    const long long key = (static_cast<long long>(threads) << 32) | static_cast<unsigned>(smem);
+    auto& m = cache[fn];
+    auto it = m.find(key);
+    if (it != m.end())
+        return it->second;
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, threads, smem) != cudaSuccess || blocks < 1)
+        blocks = 1;
+    m[key] = blocks;
+    return blocks;
+}
+
+int sm_count()
+{
+    static int count = 0;
+    if (count == 0)
+    {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+        if (count < 1)
+            count = 1;
+    }
+    return count;
+}
+
+} // namespace
+
 cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void* in, void* out, cudaStream_t stream)
 {
-    lfft::KernelFn fn = lfft::select_static(d, sh);
-    if (fn == nullptr)
-        fn = lfft::select_dynamic(d, sh);
-    if (fn == nullptr)
-        return cudaErrorInvalidConfiguration;
     const int T = (d.n + sh.points_per_thread - 1) / sh.points_per_thread;
     const int threads = T * sh.lines_per_cta;
-    if (threads > lfft::kMaxThreads || sh.lines_per_cta > lfft::kMaxLinesPerCta || sh.lines_per_cta < 1)
+    if (sh.lines_per_cta > lfft::kMaxLinesPerCta || sh.lines_per_cta < 1)
         return cudaErrorInvalidConfiguration;
-    const long long grid = (d.lines + sh.lines_per_cta - 1) / sh.lines_per_cta;
-    if (grid <= 0)
+    const long long groups = (d.lines + sh.lines_per_cta - 1) / sh.lines_per_cta;
+    if (groups <= 0)
         return cudaSuccess;
-    if (grid > 0x7fffffffLL)
-        return cudaErrorInvalidConfiguration;
-    if (sh.smem_bytes > 48 * 1024)
+    if (sh.pipelined && (reinterpret_cast<uintptr_t>(in) & 15u) == 0)
     {
-        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem_bytes);
+        lfft::PipeFn fn = lfft::select_pipe(d, sh);
+        if (fn == nullptr || threads > lfft::kPipeThreads)
+            return cudaErrorInvalidConfiguration;
+        if (sh.smem_bytes > 48 * 1024)
+        {
+            const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, sh.smem_bytes);
+            if (e != cudaSuccess)
+                return e;
+        }
+        const long long cap = static_cast<long long>(sm_count()) *
+                              resident_ctas(reinterpret_cast<const void*>(fn), threads, sh.smem_bytes);
+        const long long grid = groups < cap ? groups : cap;
+        fn<<<static_cast<unsigned>(grid), threads, sh.smem_bytes, stream>>>(
+            d, static_cast<const float2*>(in), static_cast<float2*>(out), sh.lines_per_cta, groups);
+        return cudaGetLastError();
+    }
+    PassShape cs = sh;
+    if (sh.pipelined)
+    {
+        // an input pointer off a 16-byte boundary: the classic kernel with the same thread map
+        cs.pipelined = false;
+        cs.direct_load = sh.map == PassMap::Row ? d.in.estride == 1 : d.in.ldist == 1;
+        cs.smem_bytes = sh.lines_per_cta * lfft::line_pitch(d.n) * 8;
+    }
+    lfft::KernelFn fn = lfft::select_static(d, cs);
+    if (fn == nullptr)
+        fn = lfft::select_dynamic(d, cs);
+    if (fn == nullptr || threads > lfft::kMaxThreads)
+        return cudaErrorInvalidConfiguration;
+    if (groups > 0x7fffffffLL)
+        return cudaErrorInvalidConfiguration;
+    if (cs.smem_bytes > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, cs.smem_bytes);
         if (e != cudaSuccess)
             return e;
     }
-    fn<<<static_cast<unsigned>(grid), threads, sh.smem_bytes, stream>>>(d, static_cast<const float2*>(in),
-                                                                         static_cast<float2*>(out));
+    fn<<<static_cast<unsigned>(groups), threads, cs.smem_bytes, stream>>>(d, static_cast<const float2*>(in),
+                                                                           static_cast<float2*>(out));
     return cudaGetLastError();
 }
 

@@ -1,8 +1,8 @@
 #pragma once
 
-// The line-FFT pass kernel: a CTA transforms `lines_per_cta` lines of length n held in shared memory with the
+// The line-FFT pass kernels: a CTA transforms `lines_per_cta` lines of length n held in shared memory with the
 // self-sorting (Stockham) decimation-in-time schedule, one register-resident radix-R butterfly per thread per
-// iteration. It stands in for the reference's Stockham / standalone-hier / in-place-3 / deep-split engines
+// iteration. They stand in for the reference's Stockham / standalone-hier / in-place-3 / deep-split engines
 // (engine/numerics/hesap-fft/kernels/fft_kernels.cpp:266-353, 520-585, 1603-1676, 359-515): where the reference runs
 // log_R(n) passes over a cache-resident buffer, a pass here reads each element from HBM once and writes it once, and
 // the intermediate stages exchange through shared memory.
@@ -13,16 +13,24 @@
 //     v   = DFT_R(v)
 //     y[(j - k) R + k + r L] = v_r
 // so the first stage reads x[j + r n/R] and the last writes y[j + r n/R]: both coalesced when threads run along j.
-// Those two stages go straight to and from global memory (direct_load / direct_store) when the thread map makes the
-// access coalesced; otherwise the CTA stages the lines through shared memory cooperatively.
+//
+// Two kernels share the stage code:
+//  * line_fft_kernel ("classic"): one CTA per group of lines; the first stage reads global memory itself when the
+//    thread map makes that coalesced (direct_load), else the CTA stages the lines through shared memory; likewise the
+//    last stage and the store.
+//  * pipe_fft_kernel ("pipelined"): persistent CTAs; warp 0 brings the next group of lines into the second of two
+//    shared-memory buffers with bulk asynchronous copies (cp.async.bulk, completion on an mbarrier) while the CTA
+//    transforms the current group, so HBM reads stay in flight through the compute. Every barrier wait is bounded.
 
 #include "codelets.cuh"
 #include "kernels.hpp"
-#include <initializer_list>
-#include <type_traits>
 #include "pass_desc.hpp"
 
 #include <cuda_runtime.h>
+
+#include <cstdint>
+#include <initializer_list>
+#include <type_traits>
 
 namespace crdfft
 {
@@ -31,11 +39,30 @@ namespace lfft
 
 constexpr int kMaxLinesPerCta = 256;
 constexpr int kMaxThreads = 512;
+constexpr int kPipeThreads = 256;
 
-// Shared-memory slot of element e within a line: one pad slot every 16 complex (128 bytes) keeps the strided stage
-// accesses (stride R or L between threads) spread over the banks.
-__device__ __forceinline__ int spad(int e) { return e + (e >> 4); }
+// Classic layout: one pad slot every 16 complex (128 bytes) keeps the strided stage accesses spread over the banks.
 __host__ __device__ constexpr int line_pitch(int n) { return (n + (n >> 4)) | 1; }
+// Pipelined row layout: two pad slots (16 bytes) every 16 complex, so each 128-byte chunk of a line lands on a
+// 16-byte boundary for the bulk copy; the line pitch is 2 mod 4 slots to spread cross-line accesses.
+__host__ __device__ constexpr int pipe_row_pitch(int n)
+{
+    return ((n + 2 * ((n + 15) >> 4)) & 3) == 0 ? n + 2 * ((n + 15) >> 4) + 2 : n + 2 * ((n + 15) >> 4);
+}
+// Pipelined column layout: element e of line ll at e * pitch + ll, pitch = lines + 2 (16-byte aligned rows).
+__host__ __device__ constexpr int pipe_col_pitch(int lpc) { return lpc + 2; }
+
+template <int PAD> struct LayRow
+{
+    float2* p;
+    __device__ __forceinline__ float2& at(int e) const { return p[e + (e >> 4) * PAD]; }
+};
+struct LayCol
+{
+    float2* p;
+    int pitch;
+    __device__ __forceinline__ float2& at(int e) const { return p[e * pitch]; }
+};
 
 template <int... Rs> struct Sched
 {
@@ -49,45 +76,40 @@ struct Ctx
 {
     const float2* in;  // this thread's line in global memory (element 0)
     float2* out;
-    float2* sl;        // this thread's line in shared memory
     long long q;       // line index within its group (four-step twiddle row)
     int jt;            // thread index within the line
     int T;             // threads per line
     bool ok;           // the line exists (the last CTA may be partial)
+    float in_im;       // +1, or -1 to conjugate the input
+    float out_re;      // output scale
+    float out_im;      // output scale, negated to conjugate
 };
 
-__device__ __forceinline__ float2 load_in(const PassDesc& d, const float2* p)
+__device__ __forceinline__ float2 load_in(const Ctx& c, const float2* p)
 {
     float2 x = __ldcs(p);
-    if (d.conj_in)
-        x.y = -x.y;
+    x.y *= c.in_im;
     return x;
 }
 
-// W_M^{(q e) mod M} = hi[m / base] * lo[m % base], the four-step twiddle.
+// W_M^{q e} = hi[m >> shift] * lo[m & mask], m = q e < M (the four-step twiddle).
 __device__ __forceinline__ float2 four_step_twiddle(const PassDesc& d, long long q, int e)
 {
-    const long long m = (q * static_cast<long long>(e)) % d.ftw_M;
-    const int hi = static_cast<int>(m / d.ftw_base);
-    const int lo = static_cast<int>(m - static_cast<long long>(hi) * d.ftw_base);
+    const unsigned m = static_cast<unsigned>(q) * static_cast<unsigned>(e);
     const float2* th = static_cast<const float2*>(d.ftw_hi);
     const float2* tl = static_cast<const float2*>(d.ftw_lo);
-    return cmul(__ldg(th + hi), __ldg(tl + lo));
+    return cmul(__ldg(th + (m >> d.ftw_shift)), __ldg(tl + (m & ((1u << d.ftw_shift) - 1u))));
 }
 
-__device__ __forceinline__ float2 epilogue(const PassDesc& d, long long q, int e, float2 v)
+__device__ __forceinline__ float2 epilogue(const PassDesc& d, const Ctx& c, long long q, int e, float2 v)
 {
     if (d.ftw_M != 0)
         v = cmul(v, four_step_twiddle(d, q, e));
-    if (d.conj_out)
-        v.y = -v.y;
-    if (d.scale != 1.0f)
-        v = cscale(v, d.scale);
-    return v;
+    return make_float2(v.x * c.out_re, v.y * c.out_im);
 }
 
-template <int R, int P, bool FROM_GLOBAL, bool TO_GLOBAL>
-__device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, int n, int L)
+template <int R, int P, bool FROM_GLOBAL, bool TO_GLOBAL, class Lay>
+__device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L)
 {
     constexpr int B = (P + R - 1) / R;
     const int nb = n / R;
@@ -103,9 +125,9 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, int n, in
             {
                 const int e = j + r * nb;
                 if constexpr (FROM_GLOBAL)
-                    v[b][r] = load_in(d, c.in + static_cast<long long>(e) * d.in.estride);
+                    v[b][r] = load_in(c, c.in + static_cast<long long>(e) * d.in.estride);
                 else
-                    v[b][r] = c.sl[spad(e)];
+                    v[b][r] = lay.at(e);
             }
         }
     }
@@ -133,9 +155,9 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, int n, in
             {
                 const int e = base + r * L;
                 if constexpr (TO_GLOBAL)
-                    __stcs(c.out + static_cast<long long>(e) * d.out.estride, epilogue(d, c.q, e, v[b][r]));
+                    __stcs(c.out + static_cast<long long>(e) * d.out.estride, epilogue(d, c, c.q, e, v[b][r]));
                 else
-                    c.sl[spad(e)] = v[b][r];
+                    lay.at(e) = v[b][r];
             }
         }
     }
@@ -143,17 +165,18 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, int n, in
         __syncthreads();
 }
 
-template <int P, bool DL, bool DS, int L, int R, int... Rest>
-__device__ __forceinline__ void run_static(const PassDesc& d, const Ctx& c, int n)
+template <int P, bool DL, bool DS, int L, int R, int... Rest, class Lay>
+__device__ __forceinline__ void run_static(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
 {
     constexpr bool last = sizeof...(Rest) == 0;
-    stage<R, P, (L == 1) && DL, last && DS>(d, c, n, L);
+    stage<R, P, (L == 1) && DL, last && DS>(d, c, lay, n, L);
     if constexpr (!last)
-        run_static<P, DL, DS, L * R, Rest...>(d, c, n);
+        run_static<P, DL, DS, L * R, Rest...>(d, c, lay, n);
 }
 
-template <int R, int P, bool DL, bool DS>
-__device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, int n, int L, bool first, bool last)
+template <int R, int P, bool DL, bool DS, class Lay>
+__device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L, bool first,
+                                          bool last)
 {
     if constexpr (DL)
     {
@@ -163,11 +186,11 @@ __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, int n
             {
                 if (last)
                 {
-                    stage<R, P, true, true>(d, c, n, L);
+                    stage<R, P, true, true>(d, c, lay, n, L);
                     return;
                 }
             }
-            stage<R, P, true, false>(d, c, n, L);
+            stage<R, P, true, false>(d, c, lay, n, L);
             return;
         }
     }
@@ -175,15 +198,15 @@ __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, int n
     {
         if (last)
         {
-            stage<R, P, false, true>(d, c, n, L);
+            stage<R, P, false, true>(d, c, lay, n, L);
             return;
         }
     }
-    stage<R, P, false, false>(d, c, n, L);
+    stage<R, P, false, false>(d, c, lay, n, L);
 }
 
-template <int P, bool DL, bool DS>
-__device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, int n)
+template <int P, bool DL, bool DS, class Lay>
+__device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
 {
     int L = 1;
     for (int s = 0; s < d.nstages; ++s)
@@ -193,13 +216,13 @@ __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, int
         const bool last = s == d.nstages - 1;
         switch (R)
         {
-            case 2: stage_dyn<2, P, DL, DS>(d, c, n, L, first, last); break;
-            case 3: stage_dyn<3, P, DL, DS>(d, c, n, L, first, last); break;
-            case 4: stage_dyn<4, P, DL, DS>(d, c, n, L, first, last); break;
-            case 5: stage_dyn<5, P, DL, DS>(d, c, n, L, first, last); break;
-            case 7: stage_dyn<7, P, DL, DS>(d, c, n, L, first, last); break;
-            case 8: stage_dyn<8, P, DL, DS>(d, c, n, L, first, last); break;
-            default: stage_dyn<16, P, DL, DS>(d, c, n, L, first, last); break;
+            case 2: stage_dyn<2, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            case 3: stage_dyn<3, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            case 4: stage_dyn<4, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            case 5: stage_dyn<5, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            case 7: stage_dyn<7, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            case 8: stage_dyn<8, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            default: stage_dyn<16, P, DL, DS>(d, c, lay, n, L, first, last); break;
         }
         L *= R;
     }
@@ -207,21 +230,23 @@ __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, int
 
 template <class S> struct SchedRun
 {
-    template <int P, bool DL, bool DS> __device__ __forceinline__ static void go(const PassDesc& d, const Ctx& c, int n)
+    template <int P, bool DL, bool DS, class Lay>
+    __device__ __forceinline__ static void go(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
     {
-        run_dyn_or_static<P, DL, DS>(d, c, n, static_cast<S*>(nullptr));
+        run_s<P, DL, DS>(d, c, lay, n, static_cast<S*>(nullptr));
     }
-    template <int P, bool DL, bool DS, int... Rs>
-    __device__ __forceinline__ static void run_dyn_or_static(const PassDesc& d, const Ctx& c, int n, Sched<Rs...>*)
+    template <int P, bool DL, bool DS, class Lay, int... Rs>
+    __device__ __forceinline__ static void run_s(const PassDesc& d, const Ctx& c, const Lay& lay, int n, Sched<Rs...>*)
     {
-        run_static<P, DL, DS, 1, Rs...>(d, c, n);
+        run_static<P, DL, DS, 1, Rs...>(d, c, lay, n);
     }
 };
 template <> struct SchedRun<DynSched>
 {
-    template <int P, bool DL, bool DS> __device__ __forceinline__ static void go(const PassDesc& d, const Ctx& c, int n)
+    template <int P, bool DL, bool DS, class Lay>
+    __device__ __forceinline__ static void go(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
     {
-        run_dynamic<P, DL, DS>(d, c, n);
+        run_dynamic<P, DL, DS>(d, c, lay, n);
     }
 };
 
@@ -241,13 +266,23 @@ __device__ __forceinline__ long long line_offset(const LineMap& m, long long lin
     return g * m.gdist + q * m.ldist;
 }
 
+__device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
+{
+    c.in_im = d.conj_in ? -1.0f : 1.0f;
+    c.out_re = d.scale;
+    c.out_im = d.conj_out ? -d.scale : d.scale;
+}
+
+// ---- classic kernel ---------------------------------------------------------------------------------------------
+
 template <class S, int P, PassMap MAP, bool DL, bool DS>
 __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
-                                                        float2* __restrict__ gout)
+                                                               float2* __restrict__ gout)
 {
     extern __shared__ float2 sm[];
     __shared__ long long s_in_off[kMaxLinesPerCta];
     __shared__ long long s_out_off[kMaxLinesPerCta];
+    __shared__ int s_q[kMaxLinesPerCta];
 
     const int n = sched_n<S>(d);
     const int T = (n + P - 1) / P;
@@ -275,6 +310,7 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
             const long long line = line0 + i;
             s_in_off[i] = line_offset(d.in, line, d.lines_per_group);
             s_out_off[i] = line_offset(d.out, line, d.lines_per_group);
+            s_q[i] = static_cast<int>(line % d.lines_per_group);
         }
         __syncthreads();
     }
@@ -285,9 +321,10 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
     c.q = line % d.lines_per_group;
     c.in = gin + line_offset(d.in, line, d.lines_per_group);
     c.out = gout + line_offset(d.out, line, d.lines_per_group);
-    c.sl = sm + ll * pitch;
     c.jt = jt;
     c.T = T;
+    init_scales(d, c);
+    const LayRow<1> lay{sm + ll * pitch};
 
     if constexpr (!DL)
     {
@@ -308,12 +345,12 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
                 a = i - e * lpc;
             }
             if (line0 + a < d.lines)
-                sm[a * pitch + spad(e)] = load_in(d, gin + s_in_off[a] + static_cast<long long>(e) * d.in.estride);
+                LayRow<1>{sm + a * pitch}.at(e) = load_in(c, gin + s_in_off[a] + static_cast<long long>(e) * d.in.estride);
         }
         __syncthreads();
     }
 
-    SchedRun<S>::template go<P, DL, DS>(d, c, n);
+    SchedRun<S>::template go<P, DL, DS>(d, c, lay, n);
 
     if constexpr (!DS)
     {
@@ -332,18 +369,228 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
                 e = i / lpc;
                 a = i - e * lpc;
             }
-            const long long ln = line0 + a;
-            if (ln < d.lines)
-            {
-                const long long q = ln % d.lines_per_group;
+            if (line0 + a < d.lines)
                 __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride,
-                       epilogue(d, q, e, sm[a * pitch + spad(e)]));
-            }
+                       epilogue(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
         }
     }
 }
 
+// ---- pipelined kernel -------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+// Bulk asynchronous copy global -> this CTA's shared memory; `bytes` a multiple of 16, both addresses 16-byte aligned.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait on a phase of an mbarrier; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int limit)
+{
+    for (int i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    return false;
+}
+
+// Warp 0 issues the copies of group `grp` into `buf`; lane 0 first arms the barrier with the byte count.
+template <int N, PassMap MAP>
+__device__ __forceinline__ void pipe_issue(const PassDesc& d, const float2* gin, long long grp, int lpc, float2* buf,
+                                           uint64_t* bar, int lane, bool stall)
+{
+    const long long line0 = grp * lpc;
+    if constexpr (MAP == PassMap::Row)
+    {
+        constexpr int chunks = (N + 15) / 16;
+        const long long left = d.lines - line0;
+        const int nl = left < lpc ? static_cast<int>(left) : lpc;
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<uint32_t>(nl) * N * 8u + (stall ? 16u : 0u));
+        __syncwarp();
+        const int pitch = pipe_row_pitch(N);
+        for (int i = lane; i < nl * chunks; i += 32)
+        {
+            const int ll = i / chunks;
+            const int ch = i - ll * chunks;
+            const int cnt = (N - ch * 16) < 16 ? (N - ch * 16) : 16;
+            const float2* src = gin + line_offset(d.in, line0 + ll, d.lines_per_group) + ch * 16;
+            bulk_load(buf + ll * pitch + ch * 18, src, static_cast<uint32_t>(cnt) * 8u, bar);
+        }
+    }
+    else
+    {
+        // lpc adjacent lines of one group: row e is lpc consecutive complex values
+        if (lane == 0)
+            mbar_expect_tx(bar, static_cast<uint32_t>(N) * lpc * 8u + (stall ? 16u : 0u));
+        __syncwarp();
+        const int pitch = pipe_col_pitch(lpc);
+        const float2* base = gin + line_offset(d.in, line0, d.lines_per_group);
+        for (int e = lane; e < N; e += 32)
+            bulk_load(buf + e * pitch, base + static_cast<long long>(e) * d.in.estride,
+                      static_cast<uint32_t>(lpc) * 8u, bar);
+    }
+}
+
+template <class S, int P, PassMap MAP, bool DS>
+__global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
+                                                                   float2* __restrict__ gout, int lpc,
+                                                                   long long ngroups)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ long long s_out_off[kMaxLinesPerCta];
+    __shared__ int s_q[kMaxLinesPerCta];
+    constexpr int N = S::n;
+    constexpr int T = (N + P - 1) / P;
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw);
+    float2* buf0 = reinterpret_cast<float2*>(smem_raw + 128);
+    const int buf_elems = MAP == PassMap::Row ? lpc * pipe_row_pitch(N) : N * pipe_col_pitch(lpc);
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5;
+    const int lane = tid & 31;
+
+    int ll, jt;
+    if constexpr (MAP == PassMap::Row)
+    {
+        ll = tid / T;
+        jt = tid - ll * T;
+    }
+    else
+    {
+        jt = tid / lpc;
+        ll = tid - jt * lpc;
+    }
+
+    if (tid == 0)
+    {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    long long grp = blockIdx.x;
+    if (warp == 0 && grp < ngroups)
+        pipe_issue<N, MAP>(d, gin, grp, lpc, buf0, &bars[0], lane, d.debug_stall != 0);
+
+    Ctx c;
+    c.jt = jt;
+    c.T = T;
+    init_scales(d, c);
+
+    for (int it = 0; grp < ngroups; grp += gridDim.x, ++it)
+    {
+        const int b = it & 1;
+        const long long next = grp + gridDim.x;
+        const bool issued_next = next < ngroups;
+        if (warp == 0 && issued_next)
+            pipe_issue<N, MAP>(d, gin, next, lpc, buf0 + (b ^ 1) * buf_elems, &bars[b ^ 1], lane, false);
+        if (!mbar_wait_bounded(&bars[b], static_cast<uint32_t>((it >> 1) & 1), d.spin_limit))
+        {
+            // Give up on this group: record the error, let the copies already issued into the other buffer land
+            // (bounded again), and leave without touching shared memory further.
+            if (tid == 0 && d.err != nullptr)
+                atomicOr(d.err, 1);
+            if (issued_next)
+                mbar_wait_bounded(&bars[b ^ 1], static_cast<uint32_t>(((it + 1) >> 1) & 1), d.spin_limit);
+            return;
+        }
+        float2* buf = buf0 + b * buf_elems;
+        if constexpr (!DS)
+        {
+            // per-line output offsets for the store below (visible after the stages' barriers)
+            for (int i = tid; i < lpc; i += blockDim.x)
+            {
+                const long long ln = grp * lpc + i;
+                s_out_off[i] = line_offset(d.out, ln, d.lines_per_group);
+                s_q[i] = static_cast<int>(ln % d.lines_per_group);
+            }
+        }
+        const long long line = grp * lpc + ll;
+        c.ok = line < d.lines;
+        c.q = line % d.lines_per_group;
+        c.in = gin;
+        c.out = gout + line_offset(d.out, line, d.lines_per_group);
+        if constexpr (MAP == PassMap::Row)
+        {
+            const LayRow<2> lay{buf + ll * pipe_row_pitch(N)};
+            SchedRun<S>::template go<P, false, DS>(d, c, lay, N);
+        }
+        else
+        {
+            const LayCol lay{buf + ll, pipe_col_pitch(lpc)};
+            SchedRun<S>::template go<P, false, DS>(d, c, lay, N);
+        }
+        if constexpr (!DS)
+        {
+            // Store through shared memory: threads run along whichever axis is unit-stride in the output.
+            const long long line0 = grp * lpc;
+            const bool along_e = d.out.estride == 1;
+            for (int i = tid; i < lpc * N; i += blockDim.x)
+            {
+                int a, e;
+                if (along_e)
+                {
+                    a = i / N;
+                    e = i - a * N;
+                }
+                else
+                {
+                    e = i / lpc;
+                    a = i - e * lpc;
+                }
+                if (line0 + a < d.lines)
+                {
+                    float2 v;
+                    if constexpr (MAP == PassMap::Row)
+                        v = LayRow<2>{buf + a * pipe_row_pitch(N)}.at(e);
+                    else
+                        v = buf[e * pipe_col_pitch(lpc) + a];
+                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride, epilogue(d, c, s_q[a], e, v));
+                }
+            }
+        }
+        fence_proxy_async(); // this CTA's generic accesses to buf are ordered before the next bulk copy into it
+        __syncthreads();
+    }
+}
+
 using KernelFn = void (*)(const PassDesc, const float2*, float2*);
+using PipeFn = void (*)(const PassDesc, const float2*, float2*, int, long long);
 
 template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds)
 {
@@ -360,9 +607,17 @@ template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds)
     return line_fft_kernel<S, P, PassMap::Col, false, false>;
 }
 
-// Instances live in line_fft_static.cu (compile-time schedules) and line_fft_dyn.cu (schedule read from the
-// descriptor); each returns nullptr when it has no kernel for the pass.
+template <class S, int P> PipeFn pick_pipe(PassMap map, bool ds)
+{
+    if (map == PassMap::Row)
+        return ds ? pipe_fft_kernel<S, P, PassMap::Row, true> : pipe_fft_kernel<S, P, PassMap::Row, false>;
+    return ds ? pipe_fft_kernel<S, P, PassMap::Col, true> : pipe_fft_kernel<S, P, PassMap::Col, false>;
+}
+
+// Instances live in line_fft_static.cu (compile-time schedules, classic and pipelined) and line_fft_dyn.cu
+// (schedule read from the descriptor); each returns nullptr when it has no kernel for the pass.
 KernelFn select_static(const PassDesc& d, const PassShape& sh);
+PipeFn select_pipe(const PassDesc& d, const PassShape& sh);
 KernelFn select_dynamic(const PassDesc& d, const PassShape& sh);
 
 } // namespace lfft

@@ -34,15 +34,23 @@ struct PassDesc
     LineMap in;
     LineMap out;
     const void* tw;              // float2 W_n^k, k in [0, n): (cos 2πk/n, -sin 2πk/n) narrowed from f64
-    // Four-step twiddle, fused into the store: output element k of line q is multiplied by W_M^{(q*k) mod M},
-    // W_M^m = hi[m / base] * lo[m % base]. Off when ftw_M == 0.
+    // Four-step twiddle, fused into the store: output element k of line q is multiplied by W_M^{q*k}
+    // (q < n2, k < n1, so q*k < M: no reduction), W_M^m = hi[m >> ftw_shift] * lo[m & (2^ftw_shift - 1)].
+    // Off when ftw_M == 0.
     const void* ftw_hi;
     const void* ftw_lo;
     long long ftw_M;
     int ftw_base;
+    int ftw_shift;
     int conj_in;                 // conjugate every input element (inverse via conj(DFT(conj x)))
     int conj_out;                // conjugate every output element
     float scale;                 // multiply every output element (1 = off)
+    // Pipelined kernel only: a device word the kernel ORs 1 into when a bounded shared-memory barrier wait gives up
+    // (the host reads it with crdfft_device_status), the wait's iteration limit, and a test hook that makes the
+    // first wait of every CTA expect bytes no copy delivers, so that the wait runs out without any fault.
+    int* err;
+    int spin_limit;
+    int debug_stall;
 };
 
 // The kernel variants the planner can pick for a pass.
@@ -55,6 +63,7 @@ enum class PassMap : int
 // How a launch is shaped. Chosen by the host planner from n and the two line maps.
 struct PassShape
 {
+    bool pipelined;         // persistent CTAs, input lines brought into shared memory by bulk async copies
     PassMap map;
     int threads_per_line;   // T
     int lines_per_cta;      // LPC

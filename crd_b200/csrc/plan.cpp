@@ -41,6 +41,8 @@ namespace
 constexpr int kMaxSmemBytes = 200 * 1024;
 
 std::atomic<int> g_fail_alloc_after{0};
+std::atomic<int> g_debug_stall{0};
+constexpr int kSpinLimit = 1 << 22; // bounded waits: about a second of try_wait polling
 
 cudaError_t dev_alloc(void** p, size_t bytes)
 {
@@ -182,6 +184,7 @@ struct Plan
     bool ws_owned = false;
     std::string algorithm;
     std::vector<long long> factors;
+    int* err = nullptr; // device word the pipelined kernels flag a given-up wait in
     // FftPlan::execute_batched sub-plans, one per batch value used (element-major layout).
     std::map<long long, Plan*> batched;
     std::mutex batched_mu;
@@ -300,10 +303,56 @@ PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, in
     return sh;
 }
 
+// The pipelined (persistent, bulk-copy) shape when the pass qualifies: a compile-time schedule with a pipelined
+// instance, 16 points a thread, and 16-byte aligned, 16-byte multiple copies: rows of even length with even line
+// offsets (row map), or tiles of an even number of adjacent columns inside one group with even strides (column map).
+bool pipe_shape(const PassDesc& d, PassMap map, PassShape* out)
+{
+    const int P = 16;
+    const int T = (d.n + P - 1) / P;
+    if (T > pass_pipe_threads())
+        return false;
+    PassShape sh{};
+    sh.pipelined = true;
+    sh.map = map;
+    sh.points_per_thread = P;
+    sh.threads_per_line = T;
+    sh.direct_load = false;
+    int lpc = pass_pipe_threads() / T;
+    if (map == PassMap::Row)
+    {
+        if (d.in.estride != 1 || (d.n & 1) != 0 || (d.in.gdist & 1) != 0)
+            return false;
+        if (d.lines_per_group > 1 && (d.in.ldist & 1) != 0)
+            return false;
+        lpc = std::max(1, std::min<int>(lpc, static_cast<int>(std::min<long long>(d.lines, 256))));
+        sh.direct_store = d.out.estride == 1;
+    }
+    else
+    {
+        if (d.in.ldist != 1 || d.lines_per_group < 2 || (d.in.estride & 1) != 0 || (d.in.gdist & 1) != 0)
+            return false;
+        lpc &= ~1;
+        while (lpc >= 2 && (d.lines_per_group % lpc != 0 || d.lines % lpc != 0))
+            lpc -= 2;
+        if (lpc < 4)
+            return false;
+        sh.direct_store = d.out.ldist == 1;
+    }
+    sh.lines_per_cta = lpc;
+    sh.smem_bytes = pass_pipe_smem(d.n, map, lpc);
+    if (sh.smem_bytes > 110 * 1024 || !pass_has_kernel(d, sh))
+        return false;
+    *out = sh;
+    return true;
+}
+
 // The launch shape of a pass: 16 points a thread, or 32 where a compile-time schedule exists for it (lines longer
 // than 8192, and long columns, which then keep 4+ adjacent lines a CTA for 32-byte coalesced segments).
 bool shape_for(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
 {
+    if (std::getenv("CRDFFT_NO_PIPELINE") == nullptr && pipe_shape(d, map, out))
+        return true;
     const bool want32 = d.n > 8192 || (map == PassMap::Col && d.n >= 2048);
     if (want32)
     {
@@ -343,6 +392,9 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     if (st != CRDFFT_OK)
         return st;
     d.ftw_M = 0;
+    d.err = p.err;
+    d.debug_stall = g_debug_stall.load();
+    d.spin_limit = d.debug_stall ? (1 << 14) : kSpinLimit;
     d.conj_in = conj_in ? 1 : 0;
     d.conj_out = conj_out ? 1 : 0;
     d.scale = scale;
@@ -379,7 +431,7 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
 }
 
 // Four-step twiddle tables for W_M^m = hi[m / base] * lo[m % base].
-crdfft_status four_step_tables(Plan& p, long long M, int* base, const void** hi, const void** lo)
+crdfft_status four_step_tables(Plan& p, long long M, int* base, int* shift, const void** hi, const void** lo)
 {
     long long b = 1;
     while (b * b < M)
@@ -409,6 +461,9 @@ crdfft_status four_step_tables(Plan& p, long long M, int* base, const void** hi,
     if (st != CRDFFT_OK)
         return st;
     *base = static_cast<int>(b);
+    *shift = 0;
+    while ((1LL << *shift) < b)
+        ++*shift;
     *hi = dh;
     *lo = dl;
     return CRDFFT_OK;
@@ -457,10 +512,12 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     long long n1 = 0, n2 = 0;
     if (!four_step_split(n, &n1, &n2))
         return CRDFFT_UNSUPPORTED_SIZE;
-    int base = 0;
+    int base = 0, shift = 0;
     const void* hi = nullptr;
     const void* lo = nullptr;
-    crdfft_status st = four_step_tables(p, n, &base, &hi, &lo);
+    if (n >= (1LL << 31))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    crdfft_status st = four_step_tables(p, n, &base, &shift, &hi, &lo);
     if (st != CRDFFT_OK)
         return st;
     long long wave = std::max(1LL, wave_bytes() / (n * 8));
@@ -477,6 +534,7 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
             return st;
         s1.pass.ftw_M = n;
         s1.pass.ftw_base = base;
+        s1.pass.ftw_shift = shift;
         s1.pass.ftw_hi = hi;
         s1.pass.ftw_lo = lo;
         steps.push_back(s1);
@@ -821,6 +879,15 @@ crdfft_status create(const crdfft_desc* desc, Plan** out)
     std::unique_ptr<Plan> p(new Plan());
     p->desc = *desc;
     p->device = dev;
+    {
+        void* e = nullptr;
+        if (dev_alloc(&e, 256) != cudaSuccess)
+            return CRDFFT_OOM;
+        p->tables.push_back(e);
+        if (cudaMemset(e, 0, 256) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        p->err = static_cast<int*>(e);
+    }
     if (desc->kind != CRDFFT_C2C)
         st = build_real(*p);
     else if (desc->rank == 1)
@@ -1163,5 +1230,32 @@ crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream)
 }
 
 void crdfft_debug_fail_alloc_after(int32_t k) { g_fail_alloc_after.store(k < 0 ? 0 : k); }
+
+void crdfft_debug_stall_waits(int32_t on) { g_debug_stall.store(on ? 1 : 0); }
+
+crdfft_status crdfft_device_status(crdfft_plan* plan, void* stream)
+{
+    if (plan == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    int flag = 0;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(&flag, p.err, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return CRDFFT_LAUNCH;
+    if (flag != 0)
+    {
+        if (cudaMemsetAsync(p.err, 0, sizeof(int), s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        return CRDFFT_DEVICE_TIMEOUT;
+    }
+    for (auto& kv : p.batched)
+    {
+        const crdfft_status st = crdfft_device_status(reinterpret_cast<crdfft_plan*>(kv.second), stream);
+        if (st != CRDFFT_OK)
+            return st;
+    }
+    return CRDFFT_OK;
+}
 
 } // extern "C"

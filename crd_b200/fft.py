@@ -254,6 +254,17 @@ def self_check() -> None:
     check(lib().crdfft_self_check(), "self_check")
 
 
+def device_status(plan: _Handle, stream=None) -> None:
+    """Raise CrdFftError(DEVICE_TIMEOUT) if a kernel of `plan` gave up a bounded wait since the last call
+    (crdfft_device_status; synchronises the stream)."""
+    check(lib().crdfft_device_status(plan._h, _stream(stream)), "device_status")
+
+
+def stall_waits(on: bool) -> None:
+    """Test hook: plans created while on make their pipelined kernels' first barrier wait run out."""
+    lib().crdfft_debug_stall_waits(1 if on else 0)
+
+
 def fail_alloc_after(k: int) -> None:
     """Test hook: the k-th device allocation from now fails (0 = off)."""
     lib().crdfft_debug_fail_alloc_after(int(k))

@@ -172,6 +172,16 @@ crdfft_status crdfft_self_check(void);
  * (tests/numerics/hesap-fft/CMakeLists.txt:26-36); here plan creation returns CRDFFT_OOM instead. */
 void crdfft_debug_fail_alloc_after(int32_t k);
 
+/* Read and clear the plan's device status word, after the work queued on `stream`: CRDFFT_DEVICE_TIMEOUT when a
+ * kernel of this plan gave up a bounded wait since the last call (its outputs are then incomplete), else CRDFFT_OK.
+ * Synchronises the stream. */
+crdfft_status crdfft_device_status(crdfft_plan* plan, void* stream);
+
+/* Test hook: plans created while this is on make the first shared-memory barrier wait of each CTA of their
+ * pipelined kernels expect bytes that no copy delivers, so the bounded wait runs out and the kernel reports
+ * CRDFFT_DEVICE_TIMEOUT through crdfft_device_status instead of hanging. 0 turns it off. */
+void crdfft_debug_stall_waits(int32_t on);
+
 #ifdef __cplusplus
 }
 #endif

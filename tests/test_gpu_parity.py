@@ -245,14 +245,53 @@ def test_errors_are_status_codes():
     with pytest.raises(cf.CrdFftError) as e:
         cf.Plan([16], batch=0)
     assert e.value.status == 1
-    from crd_b200 import fft as F
+    from crd_b200.fft import fail_alloc_after
 
-    F.fail_alloc_after(1)
+    fail_alloc_after(1)
     try:
         with pytest.raises(cf.CrdFftError) as e:
             cf.Plan([1024])
         assert e.value.status == 3
     finally:
-        F.fail_alloc_after(0)
+        fail_alloc_after(0)
     p = cf.Plan([1024])  # allocation works again
     assert p.info()["algorithm"] == "single-pass"
+
+
+def test_bounded_wait_reports_timeout():
+    """A pipelined kernel whose barrier wait can never complete (the test hook arms it for more bytes than any copy
+    delivers) gives up after its iteration limit, reports CRDFFT_DEVICE_TIMEOUT, and leaves the context usable."""
+    from crd_b200.fft import device_status, stall_waits
+
+    n, batch = 1024, 64
+    x = torch.from_numpy(oracle.lcg_complex64(3, n * batch)).cuda()
+    y = torch.empty_like(x)
+    stall_waits(True)
+    try:
+        bad = cf.Plan([n], batch=batch)
+    finally:
+        stall_waits(False)
+    bad.execute(x, y)
+    with pytest.raises(cf.CrdFftError) as e:
+        device_status(bad)
+    assert e.value.status == 5
+    device_status(bad)  # the word was cleared
+    good = cf.Plan([n], batch=batch)
+    good.execute(x, y)
+    device_status(good)
+    want = oracle.fft64(x.cpu().numpy().reshape(batch, n))
+    assert oracle.rel_l2(y.cpu().numpy().reshape(batch, n), want) <= REL_L2
+
+
+def test_pipelined_and_classic_agree_bitwise(monkeypatch):
+    """The pipelined kernel and the classic kernel run the same butterflies in the same order: same bits."""
+    for n, batch in ((1024, 33), (4096, 9), (65536, 2)):
+        x = torch.from_numpy(oracle.lcg_complex64(n + 1, n * batch)).cuda()
+        a = torch.empty_like(x)
+        b = torch.empty_like(x)
+        cf.Plan([n], batch=batch).execute(x, a)
+        monkeypatch.setenv("CRDFFT_NO_PIPELINE", "1")
+        cf.Plan([n], batch=batch).execute(x, b)
+        monkeypatch.delenv("CRDFFT_NO_PIPELINE")
+        torch.cuda.synchronize()
+        assert torch.equal(a.view(torch.float32), b.view(torch.float32)), n
