@@ -243,6 +243,13 @@ def run_ours(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    import crd_b200.hesap as F
+
+    if args.wisdom and os.path.exists(args.wisdom):
+        with open(args.wisdom) as f:
+            F.wisdom_import(f.read())
+    F.set_planner(args.planner)
+
     # One 2 GiB input (uniform[-1,1) from the seed, every size views it as its own batch) and one 2 GiB output.
     max_pts = max(n * b for n, b in SIZES)
     gen = torch.Generator(device=dev)
@@ -254,6 +261,11 @@ def run_ours(args) -> None:
         p = cf.Plan([n], batch=b)
         plans.append(p)
     launches_per_step = sum(p.info()["passes"] for p in plans)
+    if args.planner_log and rank == 0:
+        with open(args.planner_log, "w") as f:
+            f.write(F.planner_log())
+        with open(args.planner_log + ".wisdom", "w") as f:
+            f.write(F.wisdom_export())
     stream = torch.cuda.current_stream()
 
     def step(events=None):
@@ -390,7 +402,7 @@ def run_ours(args) -> None:
             "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward",
-                       "precision": "fp32", "placement": "out-of-place",
+                       "precision": "fp32", "placement": "out-of-place", "planner": args.planner,
                        "l2": "inputs 2 GiB per size (> 126 MB L2), no flush needed",
                        "parallelism": f"replicas{world}"},
             "roofline": {"bound": "hbm", "kernel": "line_fft_kernel N=4096 single pass",
@@ -419,6 +431,12 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--planner", choices=["estimate", "measure"], default="measure",
+                    help="measure: time each pass's candidate launch shapes at plan creation (outside the timed "
+                         "region) and keep the fastest")
+    ap.add_argument("--wisdom", default=os.path.join(ROOT, "profiles", "wisdom_b200.txt"),
+                    help="planner wisdom to load first (if the file exists)")
+    ap.add_argument("--planner-log", default=None, help="write the planner's timing log here")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)

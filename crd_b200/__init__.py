@@ -1,10 +1,10 @@
 """crd_b200: a B200-native (sm_100a) replacement for crd-hesap-fft's plan + execute path.
 
 The compute runs in ``libcrdfft.so`` (hand-written CUDA kernels behind the C ABI in ``include/crdfft.h``); this
-package is the Python mirror of the reference's plan classes over that ABI (``crd_b200.fft``).
+package is the Python mirror of the reference's plan classes over that ABI (``crd_b200.hesap``).
 """
 
-from .fft import (BluesteinPlan, FftPlan, Forward, Inverse, NdFftPlan, Plan, RealFftPlan, fft, ifft_normalized,
+from .hesap import (BluesteinPlan, FftPlan, Forward, Inverse, NdFftPlan, Plan, RealFftPlan, fft, ifft_normalized,
                   self_check)
 from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP16_SCALED, PREC_FP32,
                    PREC_SPLIT_BF16, R2C, CrdFftError)

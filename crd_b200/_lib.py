@@ -61,6 +61,11 @@ EXPORTS = (
     "crdfft_debug_fail_alloc_after",
     "crdfft_device_status",
     "crdfft_debug_stall_waits",
+    "crdfft_set_planner_mode",
+    "crdfft_wisdom_export",
+    "crdfft_wisdom_import",
+    "crdfft_wisdom_forget",
+    "crdfft_planner_log",
 )
 
 
@@ -135,6 +140,11 @@ def lib():
         "crdfft_debug_fail_alloc_after": ([i32], None),
         "crdfft_device_status": ([vp, vp], i32),
         "crdfft_debug_stall_waits": ([i32], None),
+        "crdfft_set_planner_mode": ([i32], None),
+        "crdfft_wisdom_export": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
+        "crdfft_wisdom_import": ([ctypes.c_char_p], i32),
+        "crdfft_wisdom_forget": ([], None),
+        "crdfft_planner_log": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

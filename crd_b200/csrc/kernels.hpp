@@ -17,6 +17,8 @@ int pass_threads_limit();
 int pass_pipe_threads();
 int pass_pipe_smem(int n, PassMap map, int lpc);
 bool pass_has_kernel(const PassDesc& d, const PassShape& sh);
+// A compile-time schedule exists for the pass's radices at this many points a thread.
+bool pass_has_static(const PassDesc& d, int points_per_thread);
 
 // Real <-> half-length complex recombination (real_ops.cu), the math of the reference's RealFftPlan
 // (include/crd/hesap/fft/real_fft.hpp:41-92), over `batch` transforms of real length n = 2h.

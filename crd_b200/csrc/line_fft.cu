@@ -9,6 +9,46 @@
 
 namespace crdfft
 {
+namespace lfft
+{
+// The compile-time schedules (one translation unit each, sched_*.cu).
+KernelFn s_1024_classic(const PassDesc&, const PassShape&);
+KernelFn s_256_classic(const PassDesc&, const PassShape&);
+KernelFn s_512_classic(const PassDesc&, const PassShape&);
+KernelFn s_4096_classic(const PassDesc&, const PassShape&);
+KernelFn s_4096c_classic(const PassDesc&, const PassShape&);
+KernelFn s_16384_classic(const PassDesc&, const PassShape&);
+KernelFn s_105_classic(const PassDesc&, const PassShape&);
+PipeFn s_1024_pipe(const PassDesc&, const PassShape&);
+PipeFn s_256_pipe(const PassDesc&, const PassShape&);
+PipeFn s_512_pipe(const PassDesc&, const PassShape&);
+PipeFn s_4096_pipe(const PassDesc&, const PassShape&);
+PipeFn s_105_pipe(const PassDesc&, const PassShape&);
+
+KernelFn select_static(const PassDesc& d, const PassShape& sh)
+{
+    for (auto f : {s_1024_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic, s_16384_classic,
+                   s_105_classic})
+        if (KernelFn k = f(d, sh))
+            return k;
+    return nullptr;
+}
+
+PipeFn select_pipe(const PassDesc& d, const PassShape& sh)
+{
+    for (auto f : {s_1024_pipe, s_256_pipe, s_512_pipe, s_4096_pipe, s_105_pipe})
+        if (PipeFn k = f(d, sh))
+            return k;
+    return nullptr;
+}
+} // namespace lfft
+
+bool pass_has_static(const PassDesc& d, int points_per_thread)
+{
+    PassShape sh{};
+    sh.points_per_thread = points_per_thread;
+    return lfft::select_static(d, sh) != nullptr;
+}
 
 int pass_lines_per_cta_limit() { return lfft::kMaxLinesPerCta; }
 int pass_threads_limit() { return lfft::kMaxThreads; }

@@ -18,7 +18,7 @@
 //  * line_fft_kernel ("classic"): one CTA per group of lines; the first stage reads global memory itself when the
 //    thread map makes that coalesced (direct_load), else the CTA stages the lines through shared memory; likewise the
 //    last stage and the store.
-//  * pipe_fft_kernel ("pipelined"): persistent CTAs; warp 0 brings the next group of lines into the second of two
+//  * pipe_fft_kernel ("pipelined"): persistent CTAs; the CTA brings the next group of lines into the second of two
 //    shared-memory buffers with bulk asynchronous copies (cp.async.bulk, completion on an mbarrier) while the CTA
 //    transforms the current group, so HBM reads stay in flight through the compute. Every barrier wait is bounded.
 
@@ -64,6 +64,15 @@ struct LayCol
     __device__ __forceinline__ float2& at(int e) const { return p[e * pitch]; }
 };
 
+// Compile-time facts of a launch: the thread map (which fixes the unit-stride side of direct loads and stores) and
+// whether any epilogue work exists (input conjugation, output conjugation or scale, four-step twiddle); a plain
+// forward pass compiles all of it out.
+template <PassMap M, bool E> struct Kind
+{
+    static constexpr PassMap map = M;
+    static constexpr bool epi = E;
+};
+
 template <int... Rs> struct Sched
 {
     static constexpr int n = (Rs * ... * 1);
@@ -85,10 +94,11 @@ struct Ctx
     float out_im;      // output scale, negated to conjugate
 };
 
-__device__ __forceinline__ float2 load_in(const Ctx& c, const float2* p)
+template <bool EPI> __device__ __forceinline__ float2 load_in(const Ctx& c, const float2* p)
 {
     float2 x = __ldcs(p);
-    x.y *= c.in_im;
+    if constexpr (EPI)
+        x.y *= c.in_im;
     return x;
 }
 
@@ -101,14 +111,22 @@ __device__ __forceinline__ float2 four_step_twiddle(const PassDesc& d, long long
     return cmul(__ldg(th + (m >> d.ftw_shift)), __ldg(tl + (m & ((1u << d.ftw_shift) - 1u))));
 }
 
+template <bool EPI>
 __device__ __forceinline__ float2 epilogue(const PassDesc& d, const Ctx& c, long long q, int e, float2 v)
 {
-    if (d.ftw_M != 0)
-        v = cmul(v, four_step_twiddle(d, q, e));
-    return make_float2(v.x * c.out_re, v.y * c.out_im);
+    if constexpr (EPI)
+    {
+        if (d.ftw_M != 0)
+            v = cmul(v, four_step_twiddle(d, q, e));
+        return make_float2(v.x * c.out_re, v.y * c.out_im);
+    }
+    else
+        return v;
 }
 
-template <int R, int P, bool FROM_GLOBAL, bool TO_GLOBAL, class Lay>
+// APPLY_IN: this stage reads the pass input from shared memory and applies the input conjugation itself (the
+// pipelined kernel's first stage; the classic kernel conjugates while loading). K is a Kind<map, epi>.
+template <int R, int P, bool FROM_GLOBAL, bool TO_GLOBAL, bool APPLY_IN, class K, class Lay>
 __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L)
 {
     constexpr int B = (P + R - 1) / R;
@@ -120,14 +138,36 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay
         const int j = c.jt + b * c.T;
         if (c.ok && j < nb)
         {
-#pragma unroll
-            for (int r = 0; r < R; ++r)
+            if constexpr (FROM_GLOBAL)
             {
-                const int e = j + r * nb;
-                if constexpr (FROM_GLOBAL)
-                    v[b][r] = load_in(c, c.in + static_cast<long long>(e) * d.in.estride);
+                // Row map: the input is unit-stride (a direct load is chosen only then); column map: runtime stride.
+                const float2* src;
+                long long step;
+                if constexpr (K::map == PassMap::Row)
+                {
+                    src = c.in + j;
+                    step = nb;
+                }
                 else
-                    v[b][r] = lay.at(e);
+                {
+                    src = c.in + static_cast<long long>(j) * d.in.estride;
+                    step = static_cast<long long>(nb) * d.in.estride;
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    v[b][r] = load_in<K::epi>(c, src + r * step);
+            }
+            else
+            {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                {
+                    const float2 x = lay.at(j + r * nb);
+                    if constexpr (APPLY_IN && K::epi)
+                        v[b][r] = make_float2(x.x, x.y * c.in_im);
+                    else
+                        v[b][r] = x;
+                }
             }
         }
     }
@@ -143,21 +183,36 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay
             const int k = j % L;
             if (L > 1)
             {
-                const int m = n / (L * R);
+                const int m = k * (n / (L * R));
 #pragma unroll
                 for (int r = 1; r < R; ++r)
-                    v[b][r] = cmul(v[b][r], __ldg(tw + r * k * m));
+                    v[b][r] = cmul(v[b][r], __ldg(tw + r * m));
             }
             Dft<R>::run(v[b]);
             const int base = (j - k) * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
+            if constexpr (TO_GLOBAL)
             {
-                const int e = base + r * L;
-                if constexpr (TO_GLOBAL)
-                    __stcs(c.out + static_cast<long long>(e) * d.out.estride, epilogue(d, c, c.q, e, v[b][r]));
+                float2* dst;
+                long long step;
+                if constexpr (K::map == PassMap::Row)
+                {
+                    dst = c.out + base;
+                    step = L;
+                }
                 else
-                    lay.at(e) = v[b][r];
+                {
+                    dst = c.out + static_cast<long long>(base) * d.out.estride;
+                    step = static_cast<long long>(L) * d.out.estride;
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    __stcs(dst + r * step, epilogue<K::epi>(d, c, c.q, base + r * L, v[b][r]));
+            }
+            else
+            {
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                    lay.at(base + r * L) = v[b][r];
             }
         }
     }
@@ -165,16 +220,16 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay
         __syncthreads();
 }
 
-template <int P, bool DL, bool DS, int L, int R, int... Rest, class Lay>
+template <int P, bool DL, bool DS, bool PIPE, class K, int L, int R, int... Rest, class Lay>
 __device__ __forceinline__ void run_static(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
 {
     constexpr bool last = sizeof...(Rest) == 0;
-    stage<R, P, (L == 1) && DL, last && DS>(d, c, lay, n, L);
+    stage<R, P, (L == 1) && DL, last && DS, (L == 1) && PIPE, K>(d, c, lay, n, L);
     if constexpr (!last)
-        run_static<P, DL, DS, L * R, Rest...>(d, c, lay, n);
+        run_static<P, DL, DS, PIPE, K, L * R, Rest...>(d, c, lay, n);
 }
 
-template <int R, int P, bool DL, bool DS, class Lay>
+template <int R, int P, bool DL, bool DS, class K, class Lay>
 __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L, bool first,
                                           bool last)
 {
@@ -186,11 +241,11 @@ __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const
             {
                 if (last)
                 {
-                    stage<R, P, true, true>(d, c, lay, n, L);
+                    stage<R, P, true, true, false, K>(d, c, lay, n, L);
                     return;
                 }
             }
-            stage<R, P, true, false>(d, c, lay, n, L);
+            stage<R, P, true, false, false, K>(d, c, lay, n, L);
             return;
         }
     }
@@ -198,14 +253,14 @@ __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const
     {
         if (last)
         {
-            stage<R, P, false, true>(d, c, lay, n, L);
+            stage<R, P, false, true, false, K>(d, c, lay, n, L);
             return;
         }
     }
-    stage<R, P, false, false>(d, c, lay, n, L);
+    stage<R, P, false, false, false, K>(d, c, lay, n, L);
 }
 
-template <int P, bool DL, bool DS, class Lay>
+template <int P, bool DL, bool DS, class K, class Lay>
 __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
 {
     int L = 1;
@@ -216,13 +271,13 @@ __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, con
         const bool last = s == d.nstages - 1;
         switch (R)
         {
-            case 2: stage_dyn<2, P, DL, DS>(d, c, lay, n, L, first, last); break;
-            case 3: stage_dyn<3, P, DL, DS>(d, c, lay, n, L, first, last); break;
-            case 4: stage_dyn<4, P, DL, DS>(d, c, lay, n, L, first, last); break;
-            case 5: stage_dyn<5, P, DL, DS>(d, c, lay, n, L, first, last); break;
-            case 7: stage_dyn<7, P, DL, DS>(d, c, lay, n, L, first, last); break;
-            case 8: stage_dyn<8, P, DL, DS>(d, c, lay, n, L, first, last); break;
-            default: stage_dyn<16, P, DL, DS>(d, c, lay, n, L, first, last); break;
+            case 2: stage_dyn<2, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            case 3: stage_dyn<3, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            case 4: stage_dyn<4, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            case 5: stage_dyn<5, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            case 7: stage_dyn<7, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            case 8: stage_dyn<8, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            default: stage_dyn<16, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
         }
         L *= R;
     }
@@ -230,23 +285,24 @@ __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, con
 
 template <class S> struct SchedRun
 {
-    template <int P, bool DL, bool DS, class Lay>
+    template <int P, bool DL, bool DS, bool PIPE, class K, class Lay>
     __device__ __forceinline__ static void go(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
     {
-        run_s<P, DL, DS>(d, c, lay, n, static_cast<S*>(nullptr));
+        run_s<P, DL, DS, PIPE, K>(d, c, lay, n, static_cast<S*>(nullptr));
     }
-    template <int P, bool DL, bool DS, class Lay, int... Rs>
+    template <int P, bool DL, bool DS, bool PIPE, class K, class Lay, int... Rs>
     __device__ __forceinline__ static void run_s(const PassDesc& d, const Ctx& c, const Lay& lay, int n, Sched<Rs...>*)
     {
-        run_static<P, DL, DS, 1, Rs...>(d, c, lay, n);
+        run_static<P, DL, DS, PIPE, K, 1, Rs...>(d, c, lay, n);
     }
 };
 template <> struct SchedRun<DynSched>
 {
-    template <int P, bool DL, bool DS, class Lay>
+    template <int P, bool DL, bool DS, bool PIPE, class K, class Lay>
     __device__ __forceinline__ static void go(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
     {
-        run_dynamic<P, DL, DS>(d, c, lay, n);
+        static_assert(!PIPE, "the pipelined kernel runs compile-time schedules only");
+        run_dynamic<P, DL, DS, K>(d, c, lay, n);
     }
 };
 
@@ -275,7 +331,7 @@ __device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
 
 // ---- classic kernel ---------------------------------------------------------------------------------------------
 
-template <class S, int P, PassMap MAP, bool DL, bool DS>
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
 __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
                                                                float2* __restrict__ gout)
 {
@@ -345,12 +401,13 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
                 a = i - e * lpc;
             }
             if (line0 + a < d.lines)
-                LayRow<1>{sm + a * pitch}.at(e) = load_in(c, gin + s_in_off[a] + static_cast<long long>(e) * d.in.estride);
+                LayRow<1>{sm + a * pitch}.at(e) =
+                    load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * d.in.estride);
         }
         __syncthreads();
     }
 
-    SchedRun<S>::template go<P, DL, DS>(d, c, lay, n);
+    SchedRun<S>::template go<P, DL, DS, false, Kind<MAP, EPI>>(d, c, lay, n);
 
     if constexpr (!DS)
     {
@@ -371,7 +428,7 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
             }
             if (line0 + a < d.lines)
                 __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride,
-                       epilogue(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
+                       epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
         }
     }
 }
@@ -428,10 +485,27 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
-// Warp 0 issues the copies of group `grp` into `buf`; lane 0 first arms the barrier with the byte count.
+// Bytes of group `grp` (the last group may hold fewer lines).
+template <int N, PassMap MAP>
+__device__ __forceinline__ uint32_t pipe_group_bytes(const PassDesc& d, long long grp, int lpc)
+{
+    const long long left = d.lines - grp * lpc;
+    const int nl = left < lpc ? static_cast<int>(left) : lpc;
+    return static_cast<uint32_t>(nl) * N * 8u;
+}
+
+// 32-bit line offset (lines < 2^31, offsets < 2^31 elements per group stride product kept in 64 bits).
+__device__ __forceinline__ long long line_offset32(const LineMap& m, int line, int lpg)
+{
+    const int g = lpg == 1 ? line : line / lpg;
+    const int q = line - g * lpg;
+    return static_cast<long long>(g) * m.gdist + static_cast<long long>(q) * m.ldist;
+}
+
+// All threads of the CTA issue the copies of group `grp` into `buf` (the barrier is armed separately).
 template <int N, PassMap MAP>
 __device__ __forceinline__ void pipe_issue(const PassDesc& d, const float2* gin, long long grp, int lpc, float2* buf,
-                                           uint64_t* bar, int lane, bool stall)
+                                           uint64_t* bar, int tid, int nthreads)
 {
     const long long line0 = grp * lpc;
     if constexpr (MAP == PassMap::Row)
@@ -439,34 +513,29 @@ __device__ __forceinline__ void pipe_issue(const PassDesc& d, const float2* gin,
         constexpr int chunks = (N + 15) / 16;
         const long long left = d.lines - line0;
         const int nl = left < lpc ? static_cast<int>(left) : lpc;
-        if (lane == 0)
-            mbar_expect_tx(bar, static_cast<uint32_t>(nl) * N * 8u + (stall ? 16u : 0u));
-        __syncwarp();
-        const int pitch = pipe_row_pitch(N);
-        for (int i = lane; i < nl * chunks; i += 32)
+        constexpr int pitch = pipe_row_pitch(N);
+        const int lpg = static_cast<int>(d.lines_per_group);
+        for (int i = tid; i < nl * chunks; i += nthreads)
         {
             const int ll = i / chunks;
             const int ch = i - ll * chunks;
             const int cnt = (N - ch * 16) < 16 ? (N - ch * 16) : 16;
-            const float2* src = gin + line_offset(d.in, line0 + ll, d.lines_per_group) + ch * 16;
+            const float2* src = gin + line_offset32(d.in, static_cast<int>(line0) + ll, lpg) + ch * 16;
             bulk_load(buf + ll * pitch + ch * 18, src, static_cast<uint32_t>(cnt) * 8u, bar);
         }
     }
     else
     {
         // lpc adjacent lines of one group: row e is lpc consecutive complex values
-        if (lane == 0)
-            mbar_expect_tx(bar, static_cast<uint32_t>(N) * lpc * 8u + (stall ? 16u : 0u));
-        __syncwarp();
         const int pitch = pipe_col_pitch(lpc);
-        const float2* base = gin + line_offset(d.in, line0, d.lines_per_group);
-        for (int e = lane; e < N; e += 32)
+        const float2* base = gin + line_offset32(d.in, static_cast<int>(line0), static_cast<int>(d.lines_per_group));
+        for (int e = tid; e < N; e += nthreads)
             bulk_load(buf + e * pitch, base + static_cast<long long>(e) * d.in.estride,
                       static_cast<uint32_t>(lpc) * 8u, bar);
     }
 }
 
-template <class S, int P, PassMap MAP, bool DS>
+template <class S, int P, PassMap MAP, bool DS, bool EPI>
 __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
                                                                    float2* __restrict__ gout, int lpc,
                                                                    long long ngroups)
@@ -480,8 +549,6 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
     float2* buf0 = reinterpret_cast<float2*>(smem_raw + 128);
     const int buf_elems = MAP == PassMap::Row ? lpc * pipe_row_pitch(N) : N * pipe_col_pitch(lpc);
     const int tid = threadIdx.x;
-    const int warp = tid >> 5;
-    const int lane = tid & 31;
 
     int ll, jt;
     if constexpr (MAP == PassMap::Row)
@@ -499,13 +566,20 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
     {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
+        mbar_init(&bars[2], 1); // never armed: the test hook's wait on it can only run out
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
     long long grp = blockIdx.x;
-    if (warp == 0 && grp < ngroups)
-        pipe_issue<N, MAP>(d, gin, grp, lpc, buf0, &bars[0], lane, d.debug_stall != 0);
+    if (grp < ngroups)
+    {
+        // An arming arrive and the copies it counts may land in either order: the phase cannot complete before the
+        // arrive, and the transaction count may run below zero until it.
+        if (tid == 0)
+            mbar_expect_tx(&bars[0], pipe_group_bytes<N, MAP>(d, grp, lpc));
+        pipe_issue<N, MAP>(d, gin, grp, lpc, buf0, &bars[0], tid, blockDim.x);
+    }
 
     Ctx c;
     c.jt = jt;
@@ -517,14 +591,21 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
         const int b = it & 1;
         const long long next = grp + gridDim.x;
         const bool issued_next = next < ngroups;
-        if (warp == 0 && issued_next)
-            pipe_issue<N, MAP>(d, gin, next, lpc, buf0 + (b ^ 1) * buf_elems, &bars[b ^ 1], lane, false);
-        if (!mbar_wait_bounded(&bars[b], static_cast<uint32_t>((it >> 1) & 1), d.spin_limit))
+        if (issued_next)
         {
-            // Give up on this group: record the error, let the copies already issued into the other buffer land
-            // (bounded again), and leave without touching shared memory further.
+            if (tid == 0)
+                mbar_expect_tx(&bars[b ^ 1], pipe_group_bytes<N, MAP>(d, next, lpc));
+            pipe_issue<N, MAP>(d, gin, next, lpc, buf0 + (b ^ 1) * buf_elems, &bars[b ^ 1], tid, blockDim.x);
+        }
+        const bool stalled = d.debug_stall != 0 && it == 0;
+        if (!mbar_wait_bounded(stalled ? &bars[2] : &bars[b], static_cast<uint32_t>((it >> 1) & 1), d.spin_limit))
+        {
+            // Give up on this group: record the error, let every copy this CTA issued land (bounded again), and
+            // leave without touching shared memory further.
             if (tid == 0 && d.err != nullptr)
                 atomicOr(d.err, 1);
+            if (stalled)
+                mbar_wait_bounded(&bars[b], static_cast<uint32_t>((it >> 1) & 1), d.spin_limit);
             if (issued_next)
                 mbar_wait_bounded(&bars[b ^ 1], static_cast<uint32_t>(((it + 1) >> 1) & 1), d.spin_limit);
             return;
@@ -548,12 +629,12 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
         if constexpr (MAP == PassMap::Row)
         {
             const LayRow<2> lay{buf + ll * pipe_row_pitch(N)};
-            SchedRun<S>::template go<P, false, DS>(d, c, lay, N);
+            SchedRun<S>::template go<P, false, DS, true, Kind<MAP, EPI>>(d, c, lay, N);
         }
         else
         {
             const LayCol lay{buf + ll, pipe_col_pitch(lpc)};
-            SchedRun<S>::template go<P, false, DS>(d, c, lay, N);
+            SchedRun<S>::template go<P, false, DS, true, Kind<MAP, EPI>>(d, c, lay, N);
         }
         if constexpr (!DS)
         {
@@ -580,7 +661,8 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
                         v = LayRow<2>{buf + a * pipe_row_pitch(N)}.at(e);
                     else
                         v = buf[e * pipe_col_pitch(lpc) + a];
-                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride, epilogue(d, c, s_q[a], e, v));
+                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride,
+                           epilogue<EPI>(d, c, s_q[a], e, v));
                 }
             }
         }
@@ -592,27 +674,70 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
 using KernelFn = void (*)(const PassDesc, const float2*, float2*);
 using PipeFn = void (*)(const PassDesc, const float2*, float2*, int, long long);
 
-template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds)
+template <class S, int P, bool EPI> KernelFn pick_e(PassMap map, bool dl, bool ds)
 {
     if (map == PassMap::Row)
     {
-        if (dl && ds) return line_fft_kernel<S, P, PassMap::Row, true, true>;
-        if (dl) return line_fft_kernel<S, P, PassMap::Row, true, false>;
-        if (ds) return line_fft_kernel<S, P, PassMap::Row, false, true>;
-        return line_fft_kernel<S, P, PassMap::Row, false, false>;
+        if (dl && ds) return line_fft_kernel<S, P, PassMap::Row, true, true, EPI>;
+        if (dl) return line_fft_kernel<S, P, PassMap::Row, true, false, EPI>;
+        if (ds) return line_fft_kernel<S, P, PassMap::Row, false, true, EPI>;
+        return line_fft_kernel<S, P, PassMap::Row, false, false, EPI>;
     }
-    if (dl && ds) return line_fft_kernel<S, P, PassMap::Col, true, true>;
-    if (dl) return line_fft_kernel<S, P, PassMap::Col, true, false>;
-    if (ds) return line_fft_kernel<S, P, PassMap::Col, false, true>;
-    return line_fft_kernel<S, P, PassMap::Col, false, false>;
+    if (dl && ds) return line_fft_kernel<S, P, PassMap::Col, true, true, EPI>;
+    if (dl) return line_fft_kernel<S, P, PassMap::Col, true, false, EPI>;
+    if (ds) return line_fft_kernel<S, P, PassMap::Col, false, true, EPI>;
+    return line_fft_kernel<S, P, PassMap::Col, false, false, EPI>;
 }
 
-template <class S, int P> PipeFn pick_pipe(PassMap map, bool ds)
+template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds, bool epi)
+{
+    return epi ? pick_e<S, P, true>(map, dl, ds) : pick_e<S, P, false>(map, dl, ds);
+}
+
+template <class S, int P, bool EPI> PipeFn pick_pipe_e(PassMap map, bool ds)
 {
     if (map == PassMap::Row)
-        return ds ? pipe_fft_kernel<S, P, PassMap::Row, true> : pipe_fft_kernel<S, P, PassMap::Row, false>;
-    return ds ? pipe_fft_kernel<S, P, PassMap::Col, true> : pipe_fft_kernel<S, P, PassMap::Col, false>;
+        return ds ? pipe_fft_kernel<S, P, PassMap::Row, true, EPI> : pipe_fft_kernel<S, P, PassMap::Row, false, EPI>;
+    return ds ? pipe_fft_kernel<S, P, PassMap::Col, true, EPI> : pipe_fft_kernel<S, P, PassMap::Col, false, EPI>;
 }
+
+template <class S, int P> PipeFn pick_pipe(PassMap map, bool ds, bool epi)
+{
+    return epi ? pick_pipe_e<S, P, true>(map, ds) : pick_pipe_e<S, P, false>(map, ds);
+}
+
+// Whether a pass has any epilogue work (the EPI instances).
+inline bool pass_epi(const PassDesc& d)
+{
+    return d.conj_in != 0 || d.conj_out != 0 || d.scale != 1.0f || d.ftw_M != 0;
+}
+
+inline bool same_radices(const PassDesc& d, std::initializer_list<int> rs)
+{
+    if (static_cast<int>(rs.size()) != d.nstages)
+        return false;
+    int i = 0;
+    for (int r : rs)
+        if (d.radix[i++] != r)
+            return false;
+    return true;
+}
+
+// One translation unit per compile-time schedule defines its selectors with these (parallel compilation).
+#define CRDFFT_DEFINE_SCHEDULE(NAME, P_, ...)                                                                         \
+    KernelFn NAME##_classic(const PassDesc& d, const PassShape& sh)                                                   \
+    {                                                                                                                  \
+        if (sh.points_per_thread == P_ && same_radices(d, {__VA_ARGS__}))                                              \
+            return pick<Sched<__VA_ARGS__>, P_>(sh.map, sh.direct_load, sh.direct_store, pass_epi(d));                 \
+        return nullptr;                                                                                                \
+    }
+#define CRDFFT_DEFINE_PIPE(NAME, P_, ...)                                                                             \
+    PipeFn NAME##_pipe(const PassDesc& d, const PassShape& sh)                                                        \
+    {                                                                                                                  \
+        if (sh.points_per_thread == P_ && same_radices(d, {__VA_ARGS__}))                                              \
+            return pick_pipe<Sched<__VA_ARGS__>, P_>(sh.map, sh.direct_store, pass_epi(d));                           \
+        return nullptr;                                                                                                \
+    }
 
 // Instances live in line_fft_static.cu (compile-time schedules, classic and pipelined) and line_fft_dyn.cu
 // (schedule read from the descriptor); each returns nullptr when it has no kernel for the pass.

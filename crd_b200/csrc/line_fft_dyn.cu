@@ -12,7 +12,7 @@ KernelFn select_dynamic(const PassDesc& d, const PassShape& sh)
 {
     if (sh.points_per_thread != 16)
         return nullptr;
-    return pick<DynSched, 16>(sh.map, sh.direct_load, sh.direct_store);
+    return pick<DynSched, 16>(sh.map, sh.direct_load, sh.direct_store, pass_epi(d));
 }
 
 } // namespace lfft

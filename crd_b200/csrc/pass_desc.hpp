@@ -47,7 +47,7 @@ struct PassDesc
     float scale;                 // multiply every output element (1 = off)
     // Pipelined kernel only: a device word the kernel ORs 1 into when a bounded shared-memory barrier wait gives up
     // (the host reads it with crdfft_device_status), the wait's iteration limit, and a test hook that makes the
-    // first wait of every CTA expect bytes no copy delivers, so that the wait runs out without any fault.
+    // first wait of every CTA target a barrier nothing completes, so that the wait runs out without any fault.
     int* err;
     int spin_limit;
     int debug_stall;

@@ -18,6 +18,7 @@
 #include "../../include/crdfft.h"
 #include "kernels.hpp"
 #include "pass_desc.hpp"
+#include "tuner.hpp"
 
 #include <cuda_runtime.h>
 
@@ -151,24 +152,53 @@ bool is_smooth(long long n)
 // Line lengths one pass transforms: every 7-smooth n up to 8192, and 16384.
 bool single_pass_ok(long long n) { return n >= 1 && (n <= 8192 || n == 16384) && is_smooth(n); }
 
-// The four-step split n = n1 * n2 (pass 1 transforms columns of length n1, pass 2 rows of length n2): the divisor
-// n2 <= sqrt(n) closest to it, both halves within one CTA.
+bool has_static_schedule(long long n)
+{
+    std::vector<int> rad;
+    if (!radices_for(n, rad) || static_cast<int>(rad.size()) > kMaxStages)
+        return false;
+    PassDesc d{};
+    d.n = static_cast<int>(n);
+    d.nstages = static_cast<int>(rad.size());
+    for (size_t i = 0; i < rad.size(); ++i)
+        d.radix[i] = rad[i];
+    return pass_has_static(d, 16);
+}
+
+// The four-step split n = n1 * n2 (pass 1 transforms the n2 columns of length n1, pass 2 the n1 rows of length n2),
+// both halves within one CTA. Preference, in order: both halves have compile-time schedules (e.g. 107520 = 105 x
+// 1024); n2 a multiple of 16, so pass 1's column tiles stay whole; closest to square.
 bool four_step_split(long long n, long long* n1, long long* n2)
 {
-    const long long s = static_cast<long long>(std::sqrt(static_cast<double>(n)));
-    for (long long d = s + 1; d >= 1; --d)
+    long long best1 = 0, best2 = 0;
+    double best_score = 1e300;
+    for (long long d = 1; d * d <= n; ++d)
     {
-        if (d * d > n || n % d != 0)
+        if (n % d != 0)
             continue;
         const long long other = n / d;
-        if (single_pass_ok(d) && single_pass_ok(other))
+        if (!single_pass_ok(d) || !single_pass_ok(other))
+            continue;
+        const bool stat = has_static_schedule(d) && has_static_schedule(other);
+        for (int o = 0; o < 2; ++o)
         {
-            *n2 = d;
-            *n1 = other;
-            return true;
+            const long long a = o ? d : other; // n1
+            const long long b = o ? other : d; // n2
+            const double score = (stat ? 0.0 : 1e6) + (b % 16 != 0 ? 10.0 : 0.0) +
+                                 std::fabs(std::log(static_cast<double>(a) / static_cast<double>(b)));
+            if (score < best_score)
+            {
+                best_score = score;
+                best1 = a;
+                best2 = b;
+            }
         }
     }
-    return false;
+    if (best1 == 0)
+        return false;
+    *n1 = best1;
+    *n2 = best2;
+    return true;
 }
 
 struct Plan
@@ -281,7 +311,8 @@ crdfft_status twiddle_table(Plan& p, long long n, const void** out)
     return CRDFFT_OK;
 }
 
-PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, int P)
+// A classic launch shape with P points a thread and `lpc` lines a CTA (0: the default for the map).
+PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, int P, int lpc = 0)
 {
     PassShape sh{};
     sh.map = map;
@@ -291,7 +322,8 @@ PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, in
     const int T = static_cast<int>((n + P - 1) / P);
     sh.threads_per_line = T;
     const int pitch_bytes = pass_line_pitch(static_cast<int>(n)) * 8;
-    int lpc = map == PassMap::Row ? std::max(1, 256 / T) : std::max(1, 512 / T);
+    if (lpc <= 0)
+        lpc = map == PassMap::Row ? std::max(1, 256 / T) : std::max(1, 512 / T);
     lpc = std::min(lpc, pass_lines_per_cta_limit());
     while (lpc > 1 && lpc * T > pass_threads_limit())
         --lpc;
@@ -306,7 +338,7 @@ PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, in
 // The pipelined (persistent, bulk-copy) shape when the pass qualifies: a compile-time schedule with a pipelined
 // instance, 16 points a thread, and 16-byte aligned, 16-byte multiple copies: rows of even length with even line
 // offsets (row map), or tiles of an even number of adjacent columns inside one group with even strides (column map).
-bool pipe_shape(const PassDesc& d, PassMap map, PassShape* out)
+bool pipe_shape(const PassDesc& d, PassMap map, PassShape* out, int want_lpc = 0)
 {
     const int P = 16;
     const int T = (d.n + P - 1) / P;
@@ -318,7 +350,9 @@ bool pipe_shape(const PassDesc& d, PassMap map, PassShape* out)
     sh.points_per_thread = P;
     sh.threads_per_line = T;
     sh.direct_load = false;
-    int lpc = pass_pipe_threads() / T;
+    int lpc = want_lpc > 0 ? want_lpc : pass_pipe_threads() / T;
+    if (lpc * T > pass_pipe_threads())
+        return false;
     if (map == PassMap::Row)
     {
         if (d.in.estride != 1 || (d.n & 1) != 0 || (d.in.gdist & 1) != 0)
@@ -347,11 +381,12 @@ bool pipe_shape(const PassDesc& d, PassMap map, PassShape* out)
     return true;
 }
 
-// The launch shape of a pass: 16 points a thread, or 32 where a compile-time schedule exists for it (lines longer
-// than 8192, and long columns, which then keep 4+ adjacent lines a CTA for 32-byte coalesced segments).
-bool shape_for(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
+// The heuristic launch shape of a pass (the planner's estimate when no measurement decides): the classic kernel,
+// 16 points a thread, or 32 where a compile-time schedule exists for it (lines longer than 8192, and long columns,
+// which then keep 4+ adjacent lines a CTA for 32-byte coalesced segments).
+bool heuristic_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
 {
-    if (std::getenv("CRDFFT_NO_PIPELINE") == nullptr && pipe_shape(d, map, out))
+    if (std::getenv("CRDFFT_PIPELINE") != nullptr && pipe_shape(d, map, out))
         return true;
     const bool want32 = d.n > 8192 || (map == PassMap::Col && d.n >= 2048);
     if (want32)
@@ -370,8 +405,90 @@ bool shape_for(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
     return true;
 }
 
+// Every launch shape the planner can measure for a pass: classic at 16 and 32 points a thread with one, two or
+// four times the default lines a CTA, and the pipelined kernel at its default and half lines a CTA.
+std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl, bool ds)
+{
+    std::vector<PassShape> out;
+    auto add = [&](const PassShape& sh) {
+        if (sh.threads_per_line * sh.lines_per_cta > (sh.pipelined ? pass_pipe_threads() : pass_threads_limit()))
+            return;
+        if (!pass_has_kernel(d, sh))
+            return;
+        for (const PassShape& o : out)
+            if (o.pipelined == sh.pipelined && o.points_per_thread == sh.points_per_thread &&
+                o.lines_per_cta == sh.lines_per_cta)
+                return;
+        out.push_back(sh);
+    };
+    for (int P : {16, 32})
+    {
+        const int T = (d.n + P - 1) / P;
+        const int base = map == PassMap::Row ? std::max(1, 256 / T) : std::max(1, 512 / T);
+        for (int mul : {1, 2, 4})
+        {
+            const int lpc = std::max(1, base * mul / 2);
+            add(shape_with(d.n, d.nstages, map, dl, ds, P, lpc));
+        }
+    }
+    PassShape ps;
+    if (pipe_shape(d, map, &ps))
+        add(ps);
+    if (pipe_shape(d, map, &ps, std::max(1, (pass_pipe_threads() / ((d.n + 15) / 16)) / 2)))
+        add(ps);
+    return out;
+}
+
+// The planner's choice of launch shape for a pass: remembered wisdom for its geometry class if any; else, in
+// measure mode, the fastest of the timed candidates (remembered); else the heuristic.
+bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
+{
+    const std::string key = pass_key(d, map, dl, ds);
+    WisdomEntry w;
+    if (wisdom_lookup(key, &w))
+    {
+        PassShape sh;
+        if (w.pipelined ? pipe_shape(d, map, &sh, w.lines_per_cta)
+                        : (sh = shape_with(d.n, d.nstages, map, dl, ds, w.points_per_thread, w.lines_per_cta),
+                           sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit() && pass_has_kernel(d, sh)))
+        {
+            *out = sh;
+            return true;
+        }
+    }
+    if (planner_mode() == kPlannerMeasure)
+    {
+        const std::vector<PassShape> cands = candidate_shapes(d, map, dl, ds);
+        std::vector<float> ms;
+        const int best = measure_shapes(d, key, cands, &ms);
+        if (best >= 0)
+        {
+            WisdomEntry e;
+            e.pipelined = cands[best].pipelined;
+            e.points_per_thread = cands[best].points_per_thread;
+            e.lines_per_cta = cands[best].lines_per_cta;
+            e.ms = ms[best];
+            wisdom_store(key, e);
+            *out = cands[best];
+            return true;
+        }
+    }
+    return heuristic_shape(d, map, dl, ds, out);
+}
+
+// Four-step twiddle of a pass (pass 1 of the four-step), or none.
+struct FourStepTw
+{
+    long long M = 0;
+    int base = 0;
+    int shift = 0;
+    const void* hi = nullptr;
+    const void* lo = nullptr;
+};
+
 crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lpg, LineMap in, LineMap out,
-                             BufRef src, BufRef dst, bool conj_in, bool conj_out, float scale, Step* step)
+                             BufRef src, BufRef dst, bool conj_in, bool conj_out, float scale, Step* step,
+                             const FourStepTw& ftw = FourStepTw{})
 {
     std::vector<int> rad;
     if (!single_pass_ok(n) || !radices_for(n, rad) || static_cast<int>(rad.size()) > kMaxStages)
@@ -391,7 +508,11 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     const crdfft_status st = twiddle_table(p, n, &d.tw);
     if (st != CRDFFT_OK)
         return st;
-    d.ftw_M = 0;
+    d.ftw_M = ftw.M;
+    d.ftw_base = ftw.base;
+    d.ftw_shift = ftw.shift;
+    d.ftw_hi = ftw.hi;
+    d.ftw_lo = ftw.lo;
     d.err = p.err;
     d.debug_stall = g_debug_stall.load();
     d.spin_limit = d.debug_stall ? (1 << 14) : kSpinLimit;
@@ -422,7 +543,7 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     }
     if (d.nstages == 0) // n == 1: no butterflies; the pass is a copy with the epilogue, staged through smem
         dl = ds = false;
-    if (!shape_for(d, map, dl, ds, &s.shape))
+    if (!choose_shape(d, map, dl, ds, &s.shape))
         return CRDFFT_UNSUPPORTED_SIZE;
     s.src = src;
     s.dst = dst;
@@ -528,15 +649,17 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         const long long w = std::min(wave, batch - t0);
         // pass 1: columns n2' in [0, n2), elements n1' along stride n2 -> scratch Y[t][k1][n2']
         Step s1;
+        FourStepTw ftw;
+        ftw.M = n;
+        ftw.base = base;
+        ftw.shift = shift;
+        ftw.hi = hi;
+        ftw.lo = lo;
         st = make_line_step(p, n1, w * n2, n2, LineMap{idist, istride, n2 * istride}, LineMap{n, 1, n2},
-                            BufRef{src.b, src.off + t0 * idist}, BufRef{Buf::Ws, ws_off}, conj_in, false, 1.0f, &s1);
+                            BufRef{src.b, src.off + t0 * idist}, BufRef{Buf::Ws, ws_off}, conj_in, false, 1.0f, &s1,
+                            ftw);
         if (st != CRDFFT_OK)
             return st;
-        s1.pass.ftw_M = n;
-        s1.pass.ftw_base = base;
-        s1.pass.ftw_shift = shift;
-        s1.pass.ftw_hi = hi;
-        s1.pass.ftw_lo = lo;
         steps.push_back(s1);
         // pass 2: rows k1 of length n2 -> X[t][k1 + n1 k2]
         Step s2;
@@ -1232,6 +1355,39 @@ crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream)
 void crdfft_debug_fail_alloc_after(int32_t k) { g_fail_alloc_after.store(k < 0 ? 0 : k); }
 
 void crdfft_debug_stall_waits(int32_t on) { g_debug_stall.store(on ? 1 : 0); }
+
+void crdfft_set_planner_mode(int32_t mode) { set_planner_mode(mode); }
+
+static crdfft_status copy_out(const std::string& s, char* buf, size_t cap, size_t* needed)
+{
+    if (needed != nullptr)
+        *needed = s.size() + 1;
+    if (buf == nullptr || cap == 0)
+        return CRDFFT_OK;
+    if (cap < s.size() + 1)
+        return CRDFFT_INVALID_ARG;
+    std::memcpy(buf, s.c_str(), s.size() + 1);
+    return CRDFFT_OK;
+}
+
+crdfft_status crdfft_wisdom_export(char* buf, size_t cap, size_t* needed)
+{
+    return copy_out(wisdom_export(), buf, cap, needed);
+}
+
+crdfft_status crdfft_wisdom_import(const char* text)
+{
+    if (text == nullptr)
+        return CRDFFT_INVALID_ARG;
+    return wisdom_import(text) < 0 ? CRDFFT_INVALID_ARG : CRDFFT_OK;
+}
+
+void crdfft_wisdom_forget(void) { wisdom_forget(); }
+
+crdfft_status crdfft_planner_log(char* buf, size_t cap, size_t* needed)
+{
+    return copy_out(planner_log_export(), buf, cap, needed);
+}
 
 crdfft_status crdfft_device_status(crdfft_plan* plan, void* stream)
 {

@@ -1,0 +1,234 @@
+// The measuring planner (tuner.hpp).
+
+#include "tuner.hpp"
+
+#include "kernels.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+
+namespace crdfft
+{
+namespace
+{
+
+std::atomic<int> g_mode{-1};
+std::mutex g_mu;
+std::map<std::string, WisdomEntry> g_wisdom;
+std::string g_log;
+
+std::string device_name()
+{
+    int dev = 0;
+    cudaDeviceProp prop{};
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess)
+        return "unknown";
+    std::string n = prop.name;
+    for (char& c : n)
+        if (c == ' ' || c == '|')
+            c = '_';
+    return n;
+}
+
+int ilog2(long long v)
+{
+    int r = 0;
+    while (v > 1)
+    {
+        v >>= 1;
+        ++r;
+    }
+    return r;
+}
+
+// Largest element offset + 1 a line map reaches over the first `lines` lines.
+long long extent(const LineMap& m, long long lines, long long lpg, int n)
+{
+    const long long gmax = (lines - 1) / lpg;
+    const long long qmax = std::min(lines - 1, lpg - 1);
+    return gmax * m.gdist + qmax * m.ldist + static_cast<long long>(n - 1) * m.estride + 1;
+}
+
+} // namespace
+
+int planner_mode()
+{
+    int m = g_mode.load();
+    if (m < 0)
+    {
+        const char* e = std::getenv("CRDFFT_PLANNER");
+        m = (e != nullptr && std::strcmp(e, "measure") == 0) ? kPlannerMeasure : kPlannerEstimate;
+        g_mode.store(m);
+    }
+    return m;
+}
+
+void set_planner_mode(int mode) { g_mode.store(mode == kPlannerMeasure ? kPlannerMeasure : kPlannerEstimate); }
+
+std::string pass_key(const PassDesc& d, PassMap map, bool dl, bool ds)
+{
+    std::ostringstream k;
+    k << device_name() << "|n" << d.n << ":r";
+    for (int i = 0; i < d.nstages; ++i)
+        k << (i ? "." : "") << d.radix[i];
+    const bool epi = d.conj_in || d.conj_out || d.scale != 1.0f || d.ftw_M != 0;
+    k << ":m" << static_cast<int>(map) << ":dl" << dl << ":ds" << ds << ":e" << epi << ":ie" << (d.in.estride == 1)
+      << ":oe" << (d.out.estride == 1) << ":lg" << ilog2(d.lines) << ":pg" << ilog2(d.lines_per_group)
+      << ":pp" << ((d.lines_per_group % 16) == 0) << ((d.in.estride & 1) == 0) << ((d.in.gdist & 1) == 0);
+    return k.str();
+}
+
+bool wisdom_lookup(const std::string& key, WisdomEntry* e)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_wisdom.find(key);
+    if (it == g_wisdom.end())
+        return false;
+    *e = it->second;
+    return true;
+}
+
+void wisdom_store(const std::string& key, const WisdomEntry& e)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_wisdom[key] = e;
+}
+
+std::string wisdom_export()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::ostringstream o;
+    o << "crdfft-wisdom 1\n";
+    for (const auto& kv : g_wisdom)
+        o << kv.first << ' ' << (kv.second.pipelined ? 1 : 0) << ' ' << kv.second.points_per_thread << ' '
+          << kv.second.lines_per_cta << ' ' << kv.second.ms << '\n';
+    return o.str();
+}
+
+int wisdom_import(const std::string& text)
+{
+    std::istringstream in(text);
+    std::string line;
+    if (!std::getline(in, line) || line.rfind("crdfft-wisdom 1", 0) != 0)
+        return -1;
+    std::map<std::string, WisdomEntry> got;
+    while (std::getline(in, line))
+    {
+        if (line.empty())
+            continue;
+        std::istringstream ls(line);
+        std::string key;
+        int pipe = 0;
+        WisdomEntry e;
+        if (!(ls >> key >> pipe >> e.points_per_thread >> e.lines_per_cta >> e.ms))
+            return -1;
+        if ((e.points_per_thread != 16 && e.points_per_thread != 32) || e.lines_per_cta < 1 ||
+            e.lines_per_cta > 256)
+            return -1;
+        e.pipelined = pipe != 0;
+        got[key] = e;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (const auto& kv : got)
+        g_wisdom[kv.first] = kv.second;
+    return static_cast<int>(got.size());
+}
+
+void wisdom_forget()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_wisdom.clear();
+    g_log.clear();
+}
+
+std::string planner_log_export()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_log;
+}
+
+int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector<PassShape>& cands,
+                   std::vector<float>* ms)
+{
+    ms->assign(cands.size(), -1.0f);
+    if (cands.empty())
+        return -1;
+    PassDesc d = d0;
+    // Whole groups, up to 64 MiB of line data (at least one group; column tiles stay whole).
+    const long long per_line = static_cast<long long>(d.n) * 8;
+    long long lines = std::max<long long>(1, (64LL << 20) / per_line);
+    if (d.lines_per_group > 1)
+        lines = std::max(d.lines_per_group, lines / d.lines_per_group * d.lines_per_group);
+    lines = std::min(lines, d.lines);
+    d.lines = lines;
+    const long long in_ext = extent(d.in, lines, d.lines_per_group, d.n);
+    const long long out_ext = extent(d.out, lines, d.lines_per_group, d.n);
+    void* in = nullptr;
+    void* out = nullptr;
+    if (cudaMalloc(&in, static_cast<size_t>(in_ext) * 8) != cudaSuccess)
+        return -1;
+    if (cudaMalloc(&out, static_cast<size_t>(out_ext) * 8) != cudaSuccess)
+    {
+        cudaFree(in);
+        return -1;
+    }
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemsetAsync(in, 0, static_cast<size_t>(in_ext) * 8, st);
+    int best = -1;
+    for (size_t i = 0; i < cands.size(); ++i)
+    {
+        if (launch_line_pass(d, cands[i], in, out, st) != cudaSuccess)
+            continue;
+        float bestt = 1e30f;
+        bool ok = true;
+        for (int r = 0; r < 3 && ok; ++r)
+        {
+            cudaEventRecord(e0, st);
+            ok = launch_line_pass(d, cands[i], in, out, st) == cudaSuccess;
+            cudaEventRecord(e1, st);
+            float t = 0.0f;
+            ok = ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess;
+            if (ok)
+                bestt = std::min(bestt, t);
+        }
+        if (!ok)
+            continue;
+        // Normalise to the full pass (time per line times its lines), for the wisdom and the log.
+        const float full = bestt * static_cast<float>(static_cast<double>(d0.lines) / static_cast<double>(lines));
+        (*ms)[i] = full;
+        if (best < 0 || full < (*ms)[best])
+            best = static_cast<int>(i);
+    }
+    cudaStreamSynchronize(st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    cudaFree(in);
+    cudaFree(out);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        for (size_t i = 0; i < cands.size(); ++i)
+        {
+            char buf[256];
+            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d lines=%lld ms=%.6f%s\n", key.c_str(),
+                          cands[i].pipelined ? 1 : 0, cands[i].points_per_thread, cands[i].lines_per_cta, d0.lines,
+                          static_cast<double>((*ms)[i]), static_cast<int>(i) == best ? " best" : "");
+            g_log += buf;
+        }
+    }
+    return best;
+}
+
+} // namespace crdfft

@@ -1,0 +1,51 @@
+// The measuring planner: times the candidate launch shapes of a pass on the device and keeps the fastest as
+// "wisdom" (keyed by device name and the pass's geometry class), which later plans reuse without measuring and which
+// can be exported and imported as text. Every measurement is also appended to a log (the training data of the
+// learned cost model). The reference plans from the size alone (its board of per-level winners was measured
+// offline, include/crd/hesap/fft/detail/level_plans_gen.hpp:33-148); here the board is measured on the device.
+
+#pragma once
+
+#include "pass_desc.hpp"
+
+#include <string>
+#include <vector>
+
+namespace crdfft
+{
+
+enum PlannerMode : int
+{
+    kPlannerEstimate = 0, // wisdom if present, else the heuristic
+    kPlannerMeasure = 1,  // wisdom if present, else time every candidate and remember the fastest
+};
+
+int planner_mode();
+void set_planner_mode(int mode);
+
+struct WisdomEntry
+{
+    bool pipelined = false;
+    int points_per_thread = 16;
+    int lines_per_cta = 1;
+    float ms = 0.0f;
+};
+
+// The geometry class of a pass: line length and radices, thread map, direct load/store, epilogue, line counts
+// bucketed by powers of two, and the parities the pipelined kernel's eligibility depends on.
+std::string pass_key(const PassDesc& d, PassMap map, bool dl, bool ds);
+
+bool wisdom_lookup(const std::string& key, WisdomEntry* e);
+void wisdom_store(const std::string& key, const WisdomEntry& e);
+std::string wisdom_export();
+int wisdom_import(const std::string& text); // entries read, or -1 on a malformed line
+void wisdom_forget();
+
+// Times each candidate (1 warm-up, min of 3 launches, CUDA events) on scratch buffers sized for up to 64 MiB of
+// the pass's lines; returns the index of the fastest, or -1 if none could run. ms receives each candidate's time
+// (or a negative value when it failed). Appends every timing to the planner log.
+int measure_shapes(const PassDesc& d, const std::string& key, const std::vector<PassShape>& cands,
+                   std::vector<float>* ms);
+std::string planner_log_export();
+
+} // namespace crdfft

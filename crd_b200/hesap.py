@@ -254,6 +254,41 @@ def self_check() -> None:
     check(lib().crdfft_self_check(), "self_check")
 
 
+PLANNER_ESTIMATE = 0
+PLANNER_MEASURE = 1
+
+
+def set_planner(mode) -> None:
+    """CRDFFT_PLANNER_ESTIMATE (0, default) or CRDFFT_PLANNER_MEASURE (1); "estimate"/"measure" also accepted."""
+    if isinstance(mode, str):
+        mode = {"estimate": PLANNER_ESTIMATE, "measure": PLANNER_MEASURE}[mode]
+    lib().crdfft_set_planner_mode(int(mode))
+
+
+def _text(fn) -> str:
+    need = ctypes.c_size_t(0)
+    check(fn(None, 0, ctypes.byref(need)), "size")
+    buf = ctypes.create_string_buffer(need.value)
+    check(fn(buf, need.value, ctypes.byref(need)), "export")
+    return buf.value.decode()
+
+
+def wisdom_export() -> str:
+    return _text(lib().crdfft_wisdom_export)
+
+
+def wisdom_import(text: str) -> None:
+    check(lib().crdfft_wisdom_import(text.encode()), "wisdom_import")
+
+
+def wisdom_forget() -> None:
+    lib().crdfft_wisdom_forget()
+
+
+def planner_log() -> str:
+    return _text(lib().crdfft_planner_log)
+
+
 def device_status(plan: _Handle, stream=None) -> None:
     """Raise CrdFftError(DEVICE_TIMEOUT) if a kernel of `plan` gave up a bounded wait since the last call
     (crdfft_device_status; synchronises the stream)."""

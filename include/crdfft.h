@@ -159,6 +159,30 @@ crdfft_status crdfft_nd_execute(crdfft_plan* plan, void* data, int32_t direction
 crdfft_status crdfft_fft(void* data, int64_t n, int32_t direction, void* stream);
 crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream);
 
+/* ---- Planner ----------------------------------------------------------------------------------------------- */
+
+/* How plan creation picks each pass's launch shape (kernel variant, points a thread, lines a CTA):
+ *   CRDFFT_PLANNER_ESTIMATE  remembered wisdom for the pass's geometry class, else a fixed heuristic (default)
+ *   CRDFFT_PLANNER_MEASURE   remembered wisdom, else time every candidate on the device (scratch buffers of up to
+ *                            64 MiB per pass) and remember the fastest
+ * The reference plans from the size alone from a board measured offline (detail/level_plans_gen.hpp:33-148); here
+ * the board is measured on the device and kept as wisdom. The environment variable CRDFFT_PLANNER=measure sets the
+ * initial mode. Once a pass class has wisdom, every later plan of that class makes the same choice. */
+#define CRDFFT_PLANNER_ESTIMATE 0
+#define CRDFFT_PLANNER_MEASURE 1
+void crdfft_set_planner_mode(int32_t mode);
+
+/* Wisdom as text ("crdfft-wisdom 1" then one line per pass class: key, pipelined, points a thread, lines a CTA,
+ * measured ms), keyed by device name. Export writes a NUL-terminated string into buf when cap suffices and reports
+ * the size needed; import merges entries and rejects a malformed text (CRDFFT_INVALID_ARG) without changes. */
+crdfft_status crdfft_wisdom_export(char* buf, size_t cap, size_t* needed);
+crdfft_status crdfft_wisdom_import(const char* text);
+void crdfft_wisdom_forget(void);
+
+/* Every timing the measuring planner took in this process, one line per candidate ("<key> pipelined=.. P=.. lpc=..
+ * lines=.. ms=..", the winner marked "best"): the training data of the learned cost model. */
+crdfft_status crdfft_planner_log(char* buf, size_t cap, size_t* needed);
+
 /* ---- Self-check and fault injection ------------------------------------------------------------------------- */
 
 /* The device known-answer check (the role of the reference's fft_self_check, src/fft_self_check.cpp:153-211):
@@ -177,9 +201,9 @@ void crdfft_debug_fail_alloc_after(int32_t k);
  * Synchronises the stream. */
 crdfft_status crdfft_device_status(crdfft_plan* plan, void* stream);
 
-/* Test hook: plans created while this is on make the first shared-memory barrier wait of each CTA of their
- * pipelined kernels expect bytes that no copy delivers, so the bounded wait runs out and the kernel reports
- * CRDFFT_DEVICE_TIMEOUT through crdfft_device_status instead of hanging. 0 turns it off. */
+/* Test hook: plans created while this is on make each CTA of their pipelined kernels first wait on a shared-memory
+ * barrier that nothing completes, so the bounded wait runs out; the CTA then lets its own copies land and returns,
+ * and crdfft_device_status reports CRDFFT_DEVICE_TIMEOUT. 0 turns it off. */
 void crdfft_debug_stall_waits(int32_t on);
 
 #ifdef __cplusplus

@@ -245,7 +245,7 @@ def test_errors_are_status_codes():
     with pytest.raises(cf.CrdFftError) as e:
         cf.Plan([16], batch=0)
     assert e.value.status == 1
-    from crd_b200.fft import fail_alloc_after
+    from crd_b200.hesap import fail_alloc_after
 
     fail_alloc_after(1)
     try:
@@ -258,19 +258,21 @@ def test_errors_are_status_codes():
     assert p.info()["algorithm"] == "single-pass"
 
 
-def test_bounded_wait_reports_timeout():
-    """A pipelined kernel whose barrier wait can never complete (the test hook arms it for more bytes than any copy
-    delivers) gives up after its iteration limit, reports CRDFFT_DEVICE_TIMEOUT, and leaves the context usable."""
-    from crd_b200.fft import device_status, stall_waits
+def test_bounded_wait_reports_timeout(monkeypatch):
+    """A pipelined kernel whose barrier wait can never complete (the test hook points it at a barrier that nothing
+    completes) gives up after its iteration limit, reports CRDFFT_DEVICE_TIMEOUT, and leaves the context usable."""
+    from crd_b200.hesap import device_status, stall_waits
 
     n, batch = 1024, 64
     x = torch.from_numpy(oracle.lcg_complex64(3, n * batch)).cuda()
     y = torch.empty_like(x)
+    monkeypatch.setenv("CRDFFT_PIPELINE", "1")
     stall_waits(True)
     try:
         bad = cf.Plan([n], batch=batch)
     finally:
         stall_waits(False)
+        monkeypatch.delenv("CRDFFT_PIPELINE")
     bad.execute(x, y)
     with pytest.raises(cf.CrdFftError) as e:
         device_status(bad)
@@ -290,8 +292,39 @@ def test_pipelined_and_classic_agree_bitwise(monkeypatch):
         a = torch.empty_like(x)
         b = torch.empty_like(x)
         cf.Plan([n], batch=batch).execute(x, a)
-        monkeypatch.setenv("CRDFFT_NO_PIPELINE", "1")
+        monkeypatch.setenv("CRDFFT_PIPELINE", "1")
         cf.Plan([n], batch=batch).execute(x, b)
-        monkeypatch.delenv("CRDFFT_NO_PIPELINE")
+        monkeypatch.delenv("CRDFFT_PIPELINE")
         torch.cuda.synchronize()
         assert torch.equal(a.view(torch.float32), b.view(torch.float32)), n
+
+
+def test_measuring_planner_and_wisdom():
+    """The measuring planner times each pass's candidates, remembers the fastest as wisdom, and a plan built from
+    exported-then-imported wisdom makes the same choice and the same bits."""
+    from crd_b200 import hesap as H
+
+    n, batch = 4096, 256
+    x = torch.from_numpy(oracle.lcg_complex64(9, n * batch)).cuda()
+    a = torch.empty_like(x)
+    b = torch.empty_like(x)
+    H.wisdom_forget()
+    H.set_planner("measure")
+    try:
+        cf.Plan([n], batch=batch).execute(x, a)
+    finally:
+        H.set_planner("estimate")
+    log = H.planner_log()
+    assert "best" in log and "n4096" in log
+    text = H.wisdom_export()
+    assert text.startswith("crdfft-wisdom 1") and "n4096" in text
+    H.wisdom_forget()
+    H.wisdom_import(text)
+    cf.Plan([n], batch=batch).execute(x, b)
+    torch.cuda.synchronize()
+    assert torch.equal(a.view(torch.float32), b.view(torch.float32))
+    with pytest.raises(cf.CrdFftError):
+        H.wisdom_import("not wisdom")
+    H.wisdom_forget()
+    want = oracle.fft64(x.cpu().numpy().reshape(batch, n))
+    assert oracle.rel_l2(a.cpu().numpy().reshape(batch, n), want) <= REL_L2
