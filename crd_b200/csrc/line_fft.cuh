@@ -102,13 +102,15 @@ template <bool EPI> __device__ __forceinline__ float2 load_in(const Ctx& c, cons
     return x;
 }
 
-// W_M^{q e} = hi[m >> shift] * lo[m & mask], m = q e < M (the four-step twiddle).
+// The four-step twiddle W_M^{q e} (line q < n2, element e < n1 = d.n) as W_M^{16 (q>>4) e} * W_M^{(q&15) e}: the
+// first factor from hi[(q>>4) n1 + e], the same for the 16 lines of an aligned tile (a broadcast load), the second
+// from lo[16 e + (q&15)], consecutive across those lines (a coalesced load).
 __device__ __forceinline__ float2 four_step_twiddle(const PassDesc& d, long long q, int e)
 {
-    const unsigned m = static_cast<unsigned>(q) * static_cast<unsigned>(e);
+    const int qi = static_cast<int>(q);
     const float2* th = static_cast<const float2*>(d.ftw_hi);
     const float2* tl = static_cast<const float2*>(d.ftw_lo);
-    return cmul(__ldg(th + (m >> d.ftw_shift)), __ldg(tl + (m & ((1u << d.ftw_shift) - 1u))));
+    return cmul(__ldg(th + (qi >> 4) * d.n + e), __ldg(tl + e * 16 + (qi & 15)));
 }
 
 template <bool EPI>
@@ -126,8 +128,12 @@ __device__ __forceinline__ float2 epilogue(const PassDesc& d, const Ctx& c, long
 
 // APPLY_IN: this stage reads the pass input from shared memory and applies the input conjugation itself (the
 // pipelined kernel's first stage; the classic kernel conjugates while loading). K is a Kind<map, epi>.
+// Twiddles: the pass's stage-ordered table holds, for each stage after the first, W_{LR}^{r k} at
+// tw_off + (r - 1) L + k (r = 1 .. R-1, k < L), so the threads of a warp (consecutive k, or equal k across lines)
+// read consecutive or equal addresses: coalesced loads of exact, FP64-derived values (the reference's per-pass
+// combine-twiddle table, include/crd/hesap/fft/fft.hpp:355-403).
 template <int R, int P, bool FROM_GLOBAL, bool TO_GLOBAL, bool APPLY_IN, class K, class Lay>
-__device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L)
+__device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L, int tw_off)
 {
     constexpr int B = (P + R - 1) / R;
     const int nb = n / R;
@@ -173,7 +179,7 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay
     }
     if constexpr (!FROM_GLOBAL && !TO_GLOBAL)
         __syncthreads(); // every thread has read the stage's input before any thread overwrites it in place
-    const float2* tw = static_cast<const float2*>(d.tw);
+    const float2* tw = static_cast<const float2*>(d.tw) + tw_off;
 #pragma unroll
     for (int b = 0; b < B; ++b)
     {
@@ -183,10 +189,9 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay
             const int k = j % L;
             if (L > 1)
             {
-                const int m = k * (n / (L * R));
 #pragma unroll
                 for (int r = 1; r < R; ++r)
-                    v[b][r] = cmul(v[b][r], __ldg(tw + r * m));
+                    v[b][r] = cmul(v[b][r], __ldg(tw + (r - 1) * L + k));
             }
             Dft<R>::run(v[b]);
             const int base = (j - k) * R + k;
@@ -220,18 +225,18 @@ __device__ __forceinline__ void stage(const PassDesc& d, const Ctx& c, const Lay
         __syncthreads();
 }
 
-template <int P, bool DL, bool DS, bool PIPE, class K, int L, int R, int... Rest, class Lay>
+template <int P, bool DL, bool DS, bool PIPE, class K, int L, int OFF, int R, int... Rest, class Lay>
 __device__ __forceinline__ void run_static(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
 {
     constexpr bool last = sizeof...(Rest) == 0;
-    stage<R, P, (L == 1) && DL, last && DS, (L == 1) && PIPE, K>(d, c, lay, n, L);
+    stage<R, P, (L == 1) && DL, last && DS, (L == 1) && PIPE, K>(d, c, lay, n, L, OFF);
     if constexpr (!last)
-        run_static<P, DL, DS, PIPE, K, L * R, Rest...>(d, c, lay, n);
+        run_static<P, DL, DS, PIPE, K, L * R, OFF + (L > 1 ? (R - 1) * L : 0), Rest...>(d, c, lay, n);
 }
 
 template <int R, int P, bool DL, bool DS, class K, class Lay>
-__device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L, bool first,
-                                          bool last)
+__device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const Lay& lay, int n, int L, int off,
+                                          bool first, bool last)
 {
     if constexpr (DL)
     {
@@ -241,11 +246,11 @@ __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const
             {
                 if (last)
                 {
-                    stage<R, P, true, true, false, K>(d, c, lay, n, L);
+                    stage<R, P, true, true, false, K>(d, c, lay, n, L, off);
                     return;
                 }
             }
-            stage<R, P, true, false, false, K>(d, c, lay, n, L);
+            stage<R, P, true, false, false, K>(d, c, lay, n, L, off);
             return;
         }
     }
@@ -253,17 +258,18 @@ __device__ __forceinline__ void stage_dyn(const PassDesc& d, const Ctx& c, const
     {
         if (last)
         {
-            stage<R, P, false, true, false, K>(d, c, lay, n, L);
+            stage<R, P, false, true, false, K>(d, c, lay, n, L, off);
             return;
         }
     }
-    stage<R, P, false, false, false, K>(d, c, lay, n, L);
+    stage<R, P, false, false, false, K>(d, c, lay, n, L, off);
 }
 
 template <int P, bool DL, bool DS, class K, class Lay>
 __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, const Lay& lay, int n)
 {
     int L = 1;
+    int off = 0;
     for (int s = 0; s < d.nstages; ++s)
     {
         const int R = d.radix[s];
@@ -271,14 +277,16 @@ __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, con
         const bool last = s == d.nstages - 1;
         switch (R)
         {
-            case 2: stage_dyn<2, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
-            case 3: stage_dyn<3, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
-            case 4: stage_dyn<4, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
-            case 5: stage_dyn<5, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
-            case 7: stage_dyn<7, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
-            case 8: stage_dyn<8, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
-            default: stage_dyn<16, P, DL, DS, K>(d, c, lay, n, L, first, last); break;
+            case 2: stage_dyn<2, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            case 3: stage_dyn<3, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            case 4: stage_dyn<4, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            case 5: stage_dyn<5, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            case 7: stage_dyn<7, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            case 8: stage_dyn<8, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            default: stage_dyn<16, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
         }
+        if (L > 1)
+            off += (R - 1) * L;
         L *= R;
     }
 }
@@ -293,7 +301,7 @@ template <class S> struct SchedRun
     template <int P, bool DL, bool DS, bool PIPE, class K, class Lay, int... Rs>
     __device__ __forceinline__ static void run_s(const PassDesc& d, const Ctx& c, const Lay& lay, int n, Sched<Rs...>*)
     {
-        run_static<P, DL, DS, PIPE, K, 1, Rs...>(d, c, lay, n);
+        run_static<P, DL, DS, PIPE, K, 1, 0, Rs...>(d, c, lay, n);
     }
 };
 template <> struct SchedRun<DynSched>

@@ -33,10 +33,11 @@ struct PassDesc
     long long lines_per_group;   // lines per address group (a transform, for multi-line-per-transform passes)
     LineMap in;
     LineMap out;
-    const void* tw;              // float2 W_n^k, k in [0, n): (cos 2πk/n, -sin 2πk/n) narrowed from f64
+    const void* tw;              // float2 stage-ordered twiddles: for each stage after the first (radix R, after
+                                 // radices multiplying to L), W_{LR}^{r k} at (r-1) L + k, stages back to back
     // Four-step twiddle, fused into the store: output element k of line q is multiplied by W_M^{q*k}
-    // (q < n2, k < n1, so q*k < M: no reduction), W_M^m = hi[m >> ftw_shift] * lo[m & (2^ftw_shift - 1)].
-    // Off when ftw_M == 0.
+    // (q < n2, k < n1 = n) = hi[(q>>4) n + k] * lo[16 k + (q&15)] with hi = W_M^{16 a k}, lo = W_M^{b k}.
+    // Off when ftw_M == 0. (ftw_base / ftw_shift are unused by the kernels.)
     const void* ftw_hi;
     const void* ftw_lo;
     long long ftw_M;

@@ -286,6 +286,9 @@ void root(long long k, long long n, double* re, double* im)
     *im = static_cast<double>(-sr);
 }
 
+// The stage-ordered twiddle table of a line length n with the planner's radix schedule: for each stage after the
+// first (radix R, after radices multiplying to L), W_{LR}^{r k} = W_n^{r k n/(L R)} at (r-1) L + k. Each entry is
+// computed in FP64 and narrowed once (fft.hpp:251-260).
 crdfft_status twiddle_table(Plan& p, long long n, const void** out)
 {
     auto it = p.tw_by_n.find(n);
@@ -294,14 +297,26 @@ crdfft_status twiddle_table(Plan& p, long long n, const void** out)
         *out = it->second;
         return CRDFFT_OK;
     }
-    std::vector<float> h(static_cast<size_t>(2 * n));
-    for (long long k = 0; k < n; ++k)
+    std::vector<int> rad;
+    if (!radices_for(n, rad))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    std::vector<float> h;
+    long long L = 1;
+    for (int R : rad)
     {
-        double re, im;
-        root(k, n, &re, &im);
-        h[2 * k] = static_cast<float>(re);
-        h[2 * k + 1] = static_cast<float>(im);
+        if (L > 1)
+            for (int r = 1; r < R; ++r)
+                for (long long k = 0; k < L; ++k)
+                {
+                    double re, im;
+                    root(static_cast<long long>(r) * k * (n / (L * R)), n, &re, &im);
+                    h.push_back(static_cast<float>(re));
+                    h.push_back(static_cast<float>(im));
+                }
+        L *= R;
     }
+    if (h.empty())
+        h.assign(2, 0.0f);
     void* d = nullptr;
     const crdfft_status st = upload_table(p, h, &d);
     if (st != CRDFFT_OK)
@@ -551,28 +566,28 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     return CRDFFT_OK;
 }
 
-// Four-step twiddle tables for W_M^m = hi[m / base] * lo[m % base].
-crdfft_status four_step_tables(Plan& p, long long M, int* base, int* shift, const void** hi, const void** lo)
+// Four-step twiddle tables for pass 1 (columns of length n1, n2 of them): hi[a n1 + e] = W_M^{16 a e} for
+// a < ceil(n2/16), lo[16 e + b] = W_M^{b e} for b < 16, e < n1 (exact FP64 roots, narrowed).
+crdfft_status four_step_tables(Plan& p, long long M, long long n1, long long n2, const void** hi, const void** lo)
 {
-    long long b = 1;
-    while (b * b < M)
-        b <<= 1;
-    const long long nhi = (M + b - 1) / b;
-    std::vector<float> th(static_cast<size_t>(2 * nhi)), tl(static_cast<size_t>(2 * b));
-    for (long long i = 0; i < nhi; ++i)
-    {
-        double re, im;
-        root(i * b, M, &re, &im);
-        th[2 * i] = static_cast<float>(re);
-        th[2 * i + 1] = static_cast<float>(im);
-    }
-    for (long long i = 0; i < b; ++i)
-    {
-        double re, im;
-        root(i, M, &re, &im);
-        tl[2 * i] = static_cast<float>(re);
-        tl[2 * i + 1] = static_cast<float>(im);
-    }
+    const long long na = (n2 + 15) / 16;
+    std::vector<float> th(static_cast<size_t>(2 * na * n1)), tl(static_cast<size_t>(2 * 16 * n1));
+    for (long long a = 0; a < na; ++a)
+        for (long long e = 0; e < n1; ++e)
+        {
+            double re, im;
+            root(16 * a * e, M, &re, &im);
+            th[static_cast<size_t>(2 * (a * n1 + e))] = static_cast<float>(re);
+            th[static_cast<size_t>(2 * (a * n1 + e) + 1)] = static_cast<float>(im);
+        }
+    for (long long e = 0; e < n1; ++e)
+        for (long long b = 0; b < 16; ++b)
+        {
+            double re, im;
+            root(b * e, M, &re, &im);
+            tl[static_cast<size_t>(2 * (16 * e + b))] = static_cast<float>(re);
+            tl[static_cast<size_t>(2 * (16 * e + b) + 1)] = static_cast<float>(im);
+        }
     void* dh = nullptr;
     void* dl = nullptr;
     crdfft_status st = upload_table(p, th, &dh);
@@ -581,10 +596,6 @@ crdfft_status four_step_tables(Plan& p, long long M, int* base, int* shift, cons
     st = upload_table(p, tl, &dl);
     if (st != CRDFFT_OK)
         return st;
-    *base = static_cast<int>(b);
-    *shift = 0;
-    while ((1LL << *shift) < b)
-        ++*shift;
     *hi = dh;
     *lo = dl;
     return CRDFFT_OK;
@@ -633,12 +644,11 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     long long n1 = 0, n2 = 0;
     if (!four_step_split(n, &n1, &n2))
         return CRDFFT_UNSUPPORTED_SIZE;
-    int base = 0, shift = 0;
     const void* hi = nullptr;
     const void* lo = nullptr;
     if (n >= (1LL << 31))
         return CRDFFT_UNSUPPORTED_SIZE;
-    crdfft_status st = four_step_tables(p, n, &base, &shift, &hi, &lo);
+    crdfft_status st = four_step_tables(p, n, n1, n2, &hi, &lo);
     if (st != CRDFFT_OK)
         return st;
     long long wave = std::max(1LL, wave_bytes() / (n * 8));
@@ -651,8 +661,6 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         Step s1;
         FourStepTw ftw;
         ftw.M = n;
-        ftw.base = base;
-        ftw.shift = shift;
         ftw.hi = hi;
         ftw.lo = lo;
         st = make_line_step(p, n1, w * n2, n2, LineMap{idist, istride, n2 * istride}, LineMap{n, 1, n2},
