@@ -1,0 +1,186 @@
+// Cluster-fused four-step: one thread-block cluster of C CTAs transforms one line of length N = N1 * N2 that is too
+// long for one CTA's shared memory but fits the cluster's, with one HBM read and one HBM write per element.
+//
+//   phase A  CTA c transforms columns n2 in [c N2/C, (c+1) N2/C): length-N1 DFTs over n1 of x[n1 N2 + n2],
+//            read straight from HBM (coalesced across the CTA's adjacent columns), result kept in shared memory
+//   exchange cluster barrier; CTA c gathers rows k1 in [c N1/C, (c+1) N1/C) of all columns from the other CTAs'
+//            shared memory (distributed shared memory reads), multiplying by the four-step twiddle W_N^{n2 k1};
+//            a second cluster barrier, then it stores them into its own (reused) shared memory
+//   phase B  CTA c transforms its rows: length-N2 DFTs over n2, written straight to X[k1 + N1 k2] (coalesced across
+//            its adjacent rows)
+//
+// It replaces the reference's four-step / deep-split passes at these sizes (engine/numerics/hesap-fft/kernels/
+// fft_kernels.cpp:359-515, 2363-2658), whose intermediate round-trips through memory. The stage code is the
+// line-FFT kernel's (line_fft.cuh). The cluster barriers are hardware barriers; nothing here spins on a flag.
+
+#include "kernels.hpp"
+#include "line_fft.cuh"
+
+#include <cooperative_groups.h>
+
+namespace cg = cooperative_groups;
+
+namespace crdfft
+{
+namespace lfft
+{
+namespace
+{
+
+template <class S1, class S2, int C, int P, bool EPI>
+__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__((S1::n * S2::n) / (P * C), 2)
+    cluster_fft_kernel(const PassDesc dA, const PassDesc dB, const float2* __restrict__ gin, float2* __restrict__ gout)
+{
+    constexpr int N1 = S1::n;
+    constexpr int N2 = S2::n;
+    constexpr int N = N1 * N2;
+    constexpr int LA = N2 / C; // columns a CTA transforms in phase A
+    constexpr int LB = N1 / C; // rows a CTA transforms in phase B
+    constexpr int TA = (N1 + P - 1) / P;
+    constexpr int TB = (N2 + P - 1) / P;
+    constexpr int THREADS = N / (P * C);
+    static_assert(TA * LA == THREADS && TB * LB == THREADS, "both phases use every thread");
+    constexpr int PA = LA + 1; // odd pitches: conflict-free column access
+    constexpr int PB = LB + 1;
+    extern __shared__ float2 buf[];
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const int rank = static_cast<int>(cluster.block_rank());
+    const long long t = blockIdx.x / C; // transform
+    const int tid = threadIdx.x;
+
+    // ---- phase A: columns
+    {
+        Ctx c;
+        init_scales(dA, c);
+        const int jt = tid / LA;
+        const int ll = tid - jt * LA;
+        c.jt = jt;
+        c.T = TA;
+        c.ok = true;
+        c.q = rank * LA + ll;
+        c.in = gin + t * N + rank * LA + ll;
+        c.out = nullptr;
+        const LayCol lay{buf + ll, PA};
+        SchedRun<S1>::template go<P, true, false, false, Kind<PassMap::Col, EPI>>(dA, c, lay, N1);
+    }
+    cluster.sync(); // every CTA's columns are in its shared memory
+
+    // ---- exchange: rows k1 of this CTA, all n2, times W_N^{n2 k1}
+    constexpr int PER = (LB * N2) / THREADS;
+    float2 v[PER];
+    const float2* th = static_cast<const float2*>(dA.ftw_hi);
+    const float2* tl = static_cast<const float2*>(dA.ftw_lo);
+#pragma unroll
+    for (int i = 0; i < PER; ++i)
+    {
+        const int f = i * THREADS + tid;
+        const int n2 = f % N2;
+        const int kl = f / N2;
+        const int k1 = rank * LB + kl;
+        const int src = n2 / LA;
+        const float2* remote = cluster.map_shared_rank(buf, src);
+        const float2 x = remote[k1 * PA + (n2 - src * LA)];
+        v[i] = cmul(x, cmul(__ldg(th + (n2 >> 4) * N1 + k1), __ldg(tl + k1 * 16 + (n2 & 15))));
+    }
+    cluster.sync(); // every CTA has read what it needs; shared memory may be reused
+#pragma unroll
+    for (int i = 0; i < PER; ++i)
+    {
+        const int f = i * THREADS + tid;
+        const int n2 = f % N2;
+        const int kl = f / N2;
+        buf[n2 * PB + kl] = v[i];
+    }
+    __syncthreads();
+
+    // ---- phase B: rows, stored transposed to X[k1 + N1 k2]
+    {
+        Ctx c;
+        init_scales(dB, c);
+        const int jt = tid / LB;
+        const int ll = tid - jt * LB;
+        c.jt = jt;
+        c.T = TB;
+        c.ok = true;
+        c.q = 0;
+        c.in = nullptr;
+        c.out = gout + t * N + rank * LB + ll;
+        const LayCol lay{buf + ll, PB};
+        SchedRun<S2>::template go<P, false, true, false, Kind<PassMap::Col, EPI>>(dB, c, lay, N2);
+    }
+}
+
+using ClusterFn = void (*)(const PassDesc, const PassDesc, const float2*, float2*);
+
+template <class S1, class S2, int C, int P> struct ClusterInst
+{
+    static constexpr int threads = (S1::n * S2::n) / (P * C);
+    static constexpr int smem_elems =
+        (S1::n * (S2::n / C + 1)) > (S2::n * (S1::n / C + 1)) ? (S1::n * (S2::n / C + 1)) : (S2::n * (S1::n / C + 1));
+    static ClusterFn get(bool epi)
+    {
+        return epi ? cluster_fft_kernel<S1, S2, C, P, true> : cluster_fft_kernel<S1, S2, C, P, false>;
+    }
+};
+
+struct ClusterEntry
+{
+    int n1, n2, cluster, threads, smem_bytes;
+    ClusterFn fn_epi, fn_plain;
+};
+
+template <class I> ClusterEntry entry(int n1, int n2, int c)
+{
+    return ClusterEntry{n1, n2, c, I::threads, I::smem_elems * 8, I::get(true), I::get(false)};
+}
+
+const ClusterEntry* find(long long n1, long long n2)
+{
+    static const ClusterEntry table[] = {
+        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 8, 16>>(256, 256, 8), // 65536
+    };
+    for (const ClusterEntry& e : table)
+        if (e.n1 == n1 && e.n2 == n2)
+            return &e;
+    return nullptr;
+}
+
+} // namespace
+} // namespace lfft
+
+bool cluster_split(long long n, long long* n1, long long* n2)
+{
+    for (long long a : {256LL})
+        if (n % a == 0 && lfft::find(a, n / a) != nullptr)
+        {
+            *n1 = a;
+            *n2 = n / a;
+            return true;
+        }
+    return false;
+}
+
+cudaError_t launch_cluster_fft(const PassDesc& a, const PassDesc& b, long long batch, const void* in, void* out,
+                               cudaStream_t stream)
+{
+    const lfft::ClusterEntry* e = lfft::find(a.n, b.n);
+    if (e == nullptr || batch < 1)
+        return cudaErrorInvalidConfiguration;
+    const bool epi = lfft::pass_epi(a) || lfft::pass_epi(b);
+    lfft::ClusterFn fn = epi ? e->fn_epi : e->fn_plain;
+    if (e->smem_bytes > 48 * 1024)
+    {
+        const cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, e->smem_bytes);
+        if (err != cudaSuccess)
+            return err;
+    }
+    const long long grid = batch * e->cluster;
+    if (grid > 0x7fffffffLL)
+        return cudaErrorInvalidConfiguration;
+    fn<<<static_cast<unsigned>(grid), e->threads, e->smem_bytes, stream>>>(a, b, static_cast<const float2*>(in),
+                                                                             static_cast<float2*>(out));
+    return cudaGetLastError();
+}
+
+} // namespace crdfft

@@ -54,6 +54,14 @@ cudaError_t launch_chirp_pre(const ChirpDesc& p, const void* x, void* w, cudaStr
 cudaError_t launch_spectrum_mul(const ChirpDesc& p, void* w, cudaStream_t stream);
 cudaError_t launch_chirp_post(const ChirpDesc& p, const void* w, void* x, cudaStream_t stream);
 
+// Cluster-fused four-step (cluster_fft.cu): one thread-block cluster per transform of n = a.n * b.n, columns of
+// length a.n (descriptor a: in.estride = b.n, stage twiddles, four-step twiddle tables), rows of length b.n
+// (descriptor b: out.estride = a.n), contiguous transforms n apart. cluster_split names the split when a compiled
+// instance exists for n.
+bool cluster_split(long long n, long long* n1, long long* n2);
+cudaError_t launch_cluster_fft(const PassDesc& a, const PassDesc& b, long long batch, const void* in, void* out,
+                               cudaStream_t stream);
+
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);
 

@@ -330,6 +330,39 @@ __device__ __forceinline__ long long line_offset(const LineMap& m, long long lin
     return g * m.gdist + q * m.ldist;
 }
 
+// Visits every (line a < lpc, element e < n) of the CTA's tile once across its threads, consecutive threads along
+// e (along_e) or along the lines; blockDim is a multiple of lpc. No division inside the loop.
+template <class F> __device__ __forceinline__ void for_tile(int n, int lpc, bool along_e, F&& f)
+{
+    const int tid = threadIdx.x;
+    const int nt = blockDim.x;
+    if (along_e)
+    {
+        int a = tid / n;
+        int e = tid - a * n;
+        const int da = nt / n;
+        const int de = nt - da * n;
+        while (a < lpc)
+        {
+            f(a, e);
+            e += de;
+            a += da;
+            if (e >= n)
+            {
+                e -= n;
+                ++a;
+            }
+        }
+    }
+    else
+    {
+        const int a = tid % lpc;
+        const int step = nt / lpc;
+        for (int e = tid / lpc; e < n; e += step)
+            f(a, e);
+    }
+}
+
 __device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
 {
     c.in_im = d.conj_in ? -1.0f : 1.0f;
@@ -393,25 +426,12 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
     if constexpr (!DL)
     {
         // Cooperative coalesced load of the CTA's lines: threads run along whichever axis is unit-stride in memory.
-        const int total = lpc * n;
-        const bool along_e = d.in.estride == 1;
-        for (int i = tid; i < total; i += blockDim.x)
-        {
-            int a, e;
-            if (along_e)
-            {
-                a = i / n;
-                e = i - a * n;
-            }
-            else
-            {
-                e = i / lpc;
-                a = i - e * lpc;
-            }
-            if (line0 + a < d.lines)
-                LayRow<1>{sm + a * pitch}.at(e) =
-                    load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * d.in.estride);
-        }
+        const long long lines_here = d.lines - line0;
+        const long long es = d.in.estride;
+        for_tile(n, lpc, es == 1, [&](int a, int e) {
+            if (a < lines_here)
+                LayRow<1>{sm + a * pitch}.at(e) = load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * es);
+        });
         __syncthreads();
     }
 
@@ -419,25 +439,13 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
 
     if constexpr (!DS)
     {
-        const int total = lpc * n;
-        const bool along_e = d.out.estride == 1;
-        for (int i = tid; i < total; i += blockDim.x)
-        {
-            int a, e;
-            if (along_e)
-            {
-                a = i / n;
-                e = i - a * n;
-            }
-            else
-            {
-                e = i / lpc;
-                a = i - e * lpc;
-            }
-            if (line0 + a < d.lines)
-                __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride,
+        const long long lines_here = d.lines - line0;
+        const long long es = d.out.estride;
+        for_tile(n, lpc, es == 1, [&](int a, int e) {
+            if (a < lines_here)
+                __stcs(gout + s_out_off[a] + static_cast<long long>(e) * es,
                        epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
-        }
+        });
     }
 }
 
@@ -647,32 +655,19 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
         if constexpr (!DS)
         {
             // Store through shared memory: threads run along whichever axis is unit-stride in the output.
-            const long long line0 = grp * lpc;
-            const bool along_e = d.out.estride == 1;
-            for (int i = tid; i < lpc * N; i += blockDim.x)
-            {
-                int a, e;
-                if (along_e)
-                {
-                    a = i / N;
-                    e = i - a * N;
-                }
-                else
-                {
-                    e = i / lpc;
-                    a = i - e * lpc;
-                }
-                if (line0 + a < d.lines)
+            const long long lines_here = d.lines - grp * lpc;
+            const long long es = d.out.estride;
+            for_tile(N, lpc, es == 1, [&](int a, int e) {
+                if (a < lines_here)
                 {
                     float2 v;
                     if constexpr (MAP == PassMap::Row)
                         v = LayRow<2>{buf + a * pipe_row_pitch(N)}.at(e);
                     else
                         v = buf[e * pipe_col_pitch(lpc) + a];
-                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * d.out.estride,
-                           epilogue<EPI>(d, c, s_q[a], e, v));
+                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * es, epilogue<EPI>(d, c, s_q[a], e, v));
                 }
-            }
+            });
         }
         fence_proxy_async(); // this CTA's generic accesses to buf are ordered before the next bulk copy into it
         __syncthreads();

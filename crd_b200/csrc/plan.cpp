@@ -77,6 +77,7 @@ struct BufRef
 enum class StepKind : int
 {
     Line,
+    Cluster,
     R2CPost,
     C2RPre,
     ChirpPre,
@@ -89,6 +90,7 @@ struct Step
 {
     StepKind kind = StepKind::Line;
     PassDesc pass{};
+    PassDesc pass2{}; // Cluster: the row phase
     PassShape shape{};
     RealRecombine real{};
     ChirpDesc chirp{};
@@ -501,17 +503,14 @@ struct FourStepTw
     const void* lo = nullptr;
 };
 
-crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lpg, LineMap in, LineMap out,
-                             BufRef src, BufRef dst, bool conj_in, bool conj_out, float scale, Step* step,
-                             const FourStepTw& ftw = FourStepTw{})
+// The descriptor of a line pass (no launch shape yet).
+crdfft_status make_pass_desc(Plan& p, long long n, long long lines, long long lpg, LineMap in, LineMap out,
+                             bool conj_in, bool conj_out, float scale, const FourStepTw& ftw, PassDesc* out_desc)
 {
     std::vector<int> rad;
     if (!single_pass_ok(n) || !radices_for(n, rad) || static_cast<int>(rad.size()) > kMaxStages)
         return CRDFFT_UNSUPPORTED_SIZE;
-    Step s;
-    s.kind = StepKind::Line;
-    PassDesc& d = s.pass;
-    d = PassDesc{};
+    PassDesc d{};
     d.n = static_cast<int>(n);
     d.nstages = static_cast<int>(rad.size());
     for (size_t i = 0; i < rad.size(); ++i)
@@ -534,6 +533,20 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     d.conj_in = conj_in ? 1 : 0;
     d.conj_out = conj_out ? 1 : 0;
     d.scale = scale;
+    *out_desc = d;
+    return CRDFFT_OK;
+}
+
+crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lpg, LineMap in, LineMap out,
+                             BufRef src, BufRef dst, bool conj_in, bool conj_out, float scale, Step* step,
+                             const FourStepTw& ftw = FourStepTw{})
+{
+    Step s;
+    s.kind = StepKind::Line;
+    PassDesc& d = s.pass;
+    const crdfft_status st = make_pass_desc(p, n, lines, lpg, in, out, conj_in, conj_out, scale, ftw, &d);
+    if (st != CRDFFT_OK)
+        return st;
     // Thread map: along the elements when the loading side is unit-stride, across lines when adjacent lines are
     // adjacent in memory (columns); the store side decides for the rest.
     PassMap map;
@@ -610,7 +623,7 @@ long long wave_bytes()
         if (v > 0)
             return v;
     }
-    return 48LL << 20;
+    return 512LL << 20;
 }
 
 // A batch of 1-D complex transforms of length n: element j of transform t at base + t*dist + j*stride on each side.
@@ -642,6 +655,35 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         return CRDFFT_OK;
     }
     long long n1 = 0, n2 = 0;
+    if (istride == 1 && ostride == 1 && idist == n && odist == n && std::getenv("CRDFFT_NO_CLUSTER") == nullptr &&
+        cluster_split(n, &n1, &n2))
+    {
+        // One cluster per transform: columns of n1, DSMEM transpose with the four-step twiddle, rows of n2.
+        Step s;
+        s.kind = StepKind::Cluster;
+        const void* hi = nullptr;
+        const void* lo = nullptr;
+        crdfft_status st = four_step_tables(p, n, n1, n2, &hi, &lo);
+        if (st != CRDFFT_OK)
+            return st;
+        FourStepTw ftw;
+        ftw.M = n;
+        ftw.hi = hi;
+        ftw.lo = lo;
+        st = make_pass_desc(p, n1, batch * n2, n2, LineMap{n, 1, n2}, LineMap{n, 1, n2}, conj_in, false, 1.0f, ftw,
+                            &s.pass);
+        if (st != CRDFFT_OK)
+            return st;
+        st = make_pass_desc(p, n2, batch * n1, n1, LineMap{n, n2, 1}, LineMap{n, 1, n1}, false, conj_out, scale,
+                            FourStepTw{}, &s.pass2);
+        if (st != CRDFFT_OK)
+            return st;
+        s.count = batch;
+        s.src = src;
+        s.dst = dst;
+        steps.push_back(s);
+        return CRDFFT_OK;
+    }
     if (!four_step_split(n, &n1, &n2))
         return CRDFFT_UNSUPPORTED_SIZE;
     const void* hi = nullptr;
@@ -705,6 +747,11 @@ crdfft_status build_c2c_rank1(Plan& p)
         {
             p.algorithm = "single-pass";
             p.factors = {n};
+        }
+        else if (!p.steps[0].empty() && p.steps[0][0].kind == StepKind::Cluster)
+        {
+            p.algorithm = "cluster-four-step";
+            p.factors = {p.steps[0][0].pass.n, p.steps[0][0].pass2.n};
         }
         else
         {
@@ -1063,6 +1110,7 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
         switch (s.kind)
         {
             case StepKind::Line: e = launch_line_pass(s.pass, s.shape, src, dst, stream); break;
+            case StepKind::Cluster: e = launch_cluster_fft(s.pass, s.pass2, s.count, src, dst, stream); break;
             case StepKind::R2CPost: e = launch_r2c_post(s.real, src, dst, stream); break;
             case StepKind::C2RPre: e = launch_c2r_pre(s.real, src, dst, stream); break;
             case StepKind::ChirpPre: e = launch_chirp_pre(s.chirp, src, dst, stream); break;

@@ -58,15 +58,36 @@ def test_c2c_single_pass(n, inverse):
 def test_c2c_four_step(n, inverse):
     batch = 3 if n < 2 ** 20 else 2
     x, got, plan = _c2c(n, batch, inverse)
-    assert plan.info()["algorithm"] == "four-step"
+    assert plan.info()["algorithm"] in ("four-step", "cluster-four-step")
     _check(got, oracle.fft64(x, inverse), n)
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_cluster_four_step_matches_two_pass(inverse, monkeypatch):
+    """The cluster-fused four-step (DSMEM transpose) and the two-pass four-step agree with the oracle and with each
+    other, in place too."""
+    n, batch = 65536, 5
+    x, got, plan = _c2c(n, batch, inverse)
+    assert plan.info()["algorithm"] == "cluster-four-step"
+    want = oracle.fft64(x, inverse)
+    _check(got, want, n)
+    monkeypatch.setenv("CRDFFT_NO_CLUSTER", "1")
+    x2, got2, plan2 = _c2c(n, batch, inverse)
+    assert plan2.info()["algorithm"] == "four-step"
+    _check(got2, want, n)
+    monkeypatch.delenv("CRDFFT_NO_CLUSTER")
+    t = torch.from_numpy(x.copy()).cuda()
+    cf.Plan([n], batch=batch).execute(t, t, cf.INVERSE if inverse else cf.FORWARD)
+    _check(t.cpu().numpy(), want, n, "in place")
 
 
 def test_four_step_waves(monkeypatch):
     """A batch larger than one L2 wave runs as several waves; each transform must come out the same."""
-    monkeypatch.setenv("CRDFFT_WAVE_BYTES", str(65536 * 8 * 2))  # two transforms a wave
-    x, got, plan = _c2c(65536, 5, False, seed=77)
-    _check(got, oracle.fft64(x), 65536)
+    n = 1 << 17
+    monkeypatch.setenv("CRDFFT_WAVE_BYTES", str(n * 8 * 2))  # two transforms a wave
+    x, got, plan = _c2c(n, 5, False, seed=77)
+    assert plan.info()["algorithm"] == "four-step"
+    _check(got, oracle.fft64(x), n)
 
 
 @pytest.mark.parametrize("n", [11, 17, 143, 1009, 1031])
