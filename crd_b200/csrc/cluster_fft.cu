@@ -4,7 +4,8 @@
 //   phase A  CTA c transforms columns n2 in [c N2/C, (c+1) N2/C): length-N1 DFTs over n1 of x[n1 N2 + n2],
 //            read straight from HBM (coalesced across the CTA's adjacent columns), result kept in shared memory
 //   exchange cluster barrier; CTA c gathers rows k1 in [c N1/C, (c+1) N1/C) of all columns from the other CTAs'
-//            shared memory (distributed shared memory reads), multiplying by the four-step twiddle W_N^{n2 k1};
+//            shared memory (distributed shared memory reads), multiplying by the four-step twiddle W_N^{n2 k1}
+//            (a full N-entry table tw[k1 N2 + n2], L2-resident and shared by every transform);
 //            a second cluster barrier, then it stores them into its own (reused) shared memory
 //   phase B  CTA c transforms its rows: length-N2 DFTs over n2, written straight to X[k1 + N1 k2] (coalesced across
 //            its adjacent rows)
@@ -66,32 +67,28 @@ __global__ void __cluster_dims__(C, 1, 1) __launch_bounds__((S1::n * S2::n) / (P
     }
     cluster.sync(); // every CTA's columns are in its shared memory
 
-    // ---- exchange: rows k1 of this CTA, all n2, times W_N^{n2 k1}
+    // ---- exchange: rows k1 of this CTA, all n2, times W_N^{n2 k1}. A thread keeps one column n2 (THREADS is a
+    // multiple of N2), so it reads one remote CTA's shared memory, and the twiddles W_N^{n2 k1} come from the
+    // table tw[k1 N2 + n2], consecutive across the threads of a warp.
+    static_assert(THREADS % N2 == 0, "a thread keeps one column through the exchange");
     constexpr int PER = (LB * N2) / THREADS;
+    constexpr int KSTEP = THREADS / N2;
     float2 v[PER];
-    const float2* th = static_cast<const float2*>(dA.ftw_hi);
-    const float2* tl = static_cast<const float2*>(dA.ftw_lo);
+    const int n2 = tid % N2;
+    const int kl0 = tid / N2;
+    const int src = n2 / LA;
+    const float2* remote = cluster.map_shared_rank(buf, src) + (n2 - src * LA);
+    const float2* tw = static_cast<const float2*>(dA.ftw_hi) + n2;
 #pragma unroll
     for (int i = 0; i < PER; ++i)
     {
-        const int f = i * THREADS + tid;
-        const int n2 = f % N2;
-        const int kl = f / N2;
-        const int k1 = rank * LB + kl;
-        const int src = n2 / LA;
-        const float2* remote = cluster.map_shared_rank(buf, src);
-        const float2 x = remote[k1 * PA + (n2 - src * LA)];
-        v[i] = cmul(x, cmul(__ldg(th + (n2 >> 4) * N1 + k1), __ldg(tl + k1 * 16 + (n2 & 15))));
+        const int k1 = rank * LB + kl0 + i * KSTEP;
+        v[i] = cmul(remote[k1 * PA], __ldg(tw + k1 * N2));
     }
     cluster.sync(); // every CTA has read what it needs; shared memory may be reused
 #pragma unroll
     for (int i = 0; i < PER; ++i)
-    {
-        const int f = i * THREADS + tid;
-        const int n2 = f % N2;
-        const int kl = f / N2;
-        buf[n2 * PB + kl] = v[i];
-    }
+        buf[n2 * PB + kl0 + i * KSTEP] = v[i];
     __syncthreads();
 
     // ---- phase B: rows, stored transposed to X[k1 + N1 k2]
@@ -167,7 +164,8 @@ cudaError_t launch_cluster_fft(const PassDesc& a, const PassDesc& b, long long b
     const lfft::ClusterEntry* e = lfft::find(a.n, b.n);
     if (e == nullptr || batch < 1)
         return cudaErrorInvalidConfiguration;
-    const bool epi = lfft::pass_epi(a) || lfft::pass_epi(b);
+    // The four-step twiddle is applied in the exchange, so only conjugation and scale select the EPI instance.
+    const bool epi = a.conj_in != 0 || b.conj_out != 0 || b.scale != 1.0f;
     lfft::ClusterFn fn = epi ? e->fn_epi : e->fn_plain;
     if (e->smem_bytes > 48 * 1024)
     {
