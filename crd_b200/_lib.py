@@ -66,6 +66,7 @@ EXPORTS = (
     "crdfft_wisdom_import",
     "crdfft_wisdom_forget",
     "crdfft_planner_log",
+    "crdfft_execute_static_scratch",
 )
 
 
@@ -145,6 +146,7 @@ def lib():
         "crdfft_wisdom_import": ([ctypes.c_char_p], i32),
         "crdfft_wisdom_forget": ([], None),
         "crdfft_planner_log": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
+        "crdfft_execute_static_scratch": ([vp, vp, i64, i64, i32, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

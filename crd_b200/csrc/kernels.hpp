@@ -62,6 +62,16 @@ bool cluster_split(long long n, long long* n1, long long* n2);
 cudaError_t launch_cluster_fft(const PassDesc& a, const PassDesc& b, long long batch, const void* in, void* out,
                                cudaStream_t stream);
 
+// A bump arena of device memory: while bound to the calling thread, plan creation takes every device allocation
+// (tables, status word, workspace) from it instead of cudaMalloc, and plans built so never free.
+struct Arena
+{
+    char* base;
+    size_t size;
+    size_t used;
+};
+void arena_bind(Arena* a);
+
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);
 

@@ -42,11 +42,24 @@ namespace
 constexpr int kMaxSmemBytes = 200 * 1024;
 
 std::atomic<int> g_fail_alloc_after{0};
+thread_local Arena* t_arena = nullptr; // plan memory comes from this arena instead of cudaMalloc when set
 std::atomic<int> g_debug_stall{0};
 constexpr int kSpinLimit = 1 << 22; // bounded waits: about a second of try_wait polling
 
 cudaError_t dev_alloc(void** p, size_t bytes)
 {
+    if (t_arena != nullptr)
+    {
+        const size_t need = (bytes == 0 ? 256 : bytes + 255) / 256 * 256;
+        if (t_arena->used + need > t_arena->size)
+        {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+        *p = t_arena->base + t_arena->used;
+        t_arena->used += need;
+        return cudaSuccess;
+    }
     int k = g_fail_alloc_after.load();
     if (k > 0)
     {
@@ -221,11 +234,14 @@ struct Plan
     std::map<long long, Plan*> batched;
     std::mutex batched_mu;
     int api_kind = 0; // 0 general, 1 FftPlan, 2 RealFftPlan, 3 BluesteinPlan, 4 NdFftPlan
+    bool arena_backed = t_arena != nullptr; // device memory belongs to an arena: nothing to free
 
     ~Plan()
     {
         for (auto& kv : batched)
             delete kv.second;
+        if (arena_backed)
+            return;
         for (void* p : tables)
             cudaFree(p);
         if (ws_owned && ws != nullptr)
@@ -473,7 +489,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
             return true;
         }
     }
-    if (planner_mode() == kPlannerMeasure)
+    if (planner_mode() == kPlannerMeasure && t_arena == nullptr) // measuring allocates scratch: never from an arena
     {
         const std::vector<PassShape> cands = candidate_shapes(d, map, dl, ds);
         std::vector<float> ms;
@@ -616,6 +632,8 @@ crdfft_status four_step_tables(Plan& p, long long M, long long n1, long long n2,
 
 long long wave_bytes()
 {
+    if (t_arena != nullptr) // half of an arena holds the intermediate; tables and the status word use the rest
+        return static_cast<long long>(t_arena->size / 2);
     const char* e = std::getenv("CRDFFT_WAVE_BYTES");
     if (e != nullptr)
     {
@@ -1164,6 +1182,11 @@ crdfft_desc desc_1d(long long n, int kind, int norm)
 Plan* as_plan(crdfft_plan* p) { return reinterpret_cast<Plan*>(p); }
 
 } // namespace
+} // namespace crdfft
+
+namespace crdfft
+{
+void arena_bind(Arena* a) { t_arena = a; }
 } // namespace crdfft
 
 using namespace crdfft;

@@ -183,6 +183,19 @@ void crdfft_wisdom_forget(void);
  * lines=.. ms=..", the winner marked "best"): the training data of the learned cost model. */
 crdfft_status crdfft_planner_log(char* buf, size_t cap, size_t* needed);
 
+/* ---- Without device allocation ----------------------------------------------------------------------------- */
+
+/* No counterpart in the reference (its plans always allocate their tables from the caller's allocator).
+ * For callers that cannot allocate device memory (work enqueued while a stream is being captured, real-time
+ * callbacks that must never enter an allocator, processes whose device memory belongs to a pool they do not own):
+ * `batch` contiguous size-n complex transforms (FftPlan semantics: unnormalised both ways; in == out allowed), with
+ * every table and intermediate taken from a 64 MiB device array that the library holds on each GPU it is loaded on.
+ * Allocates no device memory. n up to 2^22 (larger: CRDFFT_UNSUPPORTED_SIZE). All calls on a device share the
+ * array: the last call's plan stays in it, and calls whose GPU work overlaps race, so order them on one stream.
+ * The first call on a device looks up the array's address; make it before any stream capture. */
+crdfft_status crdfft_execute_static_scratch(const void* in, void* out, int64_t n, int64_t batch, int32_t direction,
+                                            void* stream);
+
 /* ---- Self-check and fault injection ------------------------------------------------------------------------- */
 
 /* The device known-answer check (the role of the reference's fft_self_check, src/fft_self_check.cpp:153-211):
