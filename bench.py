@@ -123,6 +123,165 @@ class ClockSampler:
         }
 
 
+# ---- workloads -------------------------------------------------------------------------------------------------
+#
+# A workload is a list of ops; one step runs every op once. Each op has a device input and output, a run(in, out)
+# that enqueues it on the current stream, its FLOP count (5 N log2 N per complex transform, 2.5 N log2 N per real
+# one), its algorithmic HBM bytes, the number of kernel launches it issues, and a check that returns the rel-L2 of
+# its output against numpy's float64 FFT on a sample.
+
+WORKLOADS = ("mixed", "r2c", "uneven", "nd")
+
+
+class Op:
+    def __init__(self, name, inp, out, run, flops_, bytes_, launches, check, info=None):
+        self.name, self.inp, self.out, self.run = name, inp, out, run
+        self.flops, self.bytes, self.launches, self.check = flops_, bytes_, launches, check
+        self.info = info or {}
+
+
+def _rel(a, b):
+    import numpy as np
+
+    a = np.asarray(a, dtype=np.complex128)
+    b = np.asarray(b, dtype=np.complex128)
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+def build_mixed(dev, rank, cf):
+    """BASELINE configs[1], C2C part: forward C2C at N in {4096, 65536, 2^20, 107520}, batch filling 2 GiB."""
+    import numpy as np
+    import torch
+
+    max_pts = max(n * b for n, b in SIZES)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + rank)
+    xin = (torch.rand(2 * max_pts, generator=gen, device=dev, dtype=torch.float32) * 2 - 1).view(torch.complex64)
+    xout = torch.empty(max_pts, dtype=torch.complex64, device=dev)
+    ops = []
+    for n, b in SIZES:
+        plan = cf.Plan([n], batch=b)
+
+        def check(n=n, b=b):
+            worst = 0.0
+            for t in (0, b - 1):
+                x = xin[t * n:(t + 1) * n].cpu().numpy()
+                y = xout[t * n:(t + 1) * n].cpu().numpy()
+                worst = max(worst, _rel(y, np.fft.fft(x.astype(np.complex128))))
+            return worst
+
+        ops.append(Op(str(n), xin[: n * b], xout[: n * b],
+                      lambda i, o, plan=plan: plan.execute(i, o, cf.FORWARD), flops(n, b), algorithmic_bytes(n, b),
+                      plan.info()["passes"], check, {"batch": b, "algorithm": plan.info()["algorithm"]}))
+    return ops, {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward",
+                 "l2": "inputs 2 GiB per size (> 126 MB L2), no flush needed"}
+
+
+def build_r2c(dev, rank, cf):
+    """BASELINE configs[1], real part: R2C and C2R at N = 2^20, batch 512 (2 GiB of real input)."""
+    import numpy as np
+    import torch
+
+    n, b = 1 << 20, 512
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 7 + rank)
+    real = torch.rand(n * b, generator=gen, device=dev, dtype=torch.float32) * 2 - 1
+    spec = torch.empty(b * (n // 2 + 1), dtype=torch.complex64, device=dev)
+    back = torch.empty(n * b, dtype=torch.float32, device=dev)
+    r2c = cf.Plan([n], batch=b, kind=cf.R2C)
+    c2r = cf.Plan([n], batch=b, kind=cf.C2R)
+    fl = 2.5 * n * math.log2(n) * b
+    by = (4 * n + 8 * (n // 2 + 1)) * b
+
+    def check_r2c():
+        x = real[:n].cpu().numpy().astype(np.float64)
+        return _rel(spec[: n // 2 + 1].cpu().numpy(), np.fft.rfft(x))
+
+    def check_c2r():
+        s0 = spec[: n // 2 + 1].cpu().numpy().astype(np.complex128)
+        return _rel(back[:n].cpu().numpy(), np.fft.irfft(s0, n) * n)
+
+    ops = [Op("r2c", real, spec, lambda i, o: r2c.execute(i, o, cf.FORWARD), fl, by, r2c.info()["passes"],
+              check_r2c, {"batch": b, "algorithm": r2c.info()["algorithm"]}),
+           Op("c2r", spec, back, lambda i, o: c2r.execute(i, o, cf.INVERSE), fl, by, c2r.info()["passes"],
+              check_c2r, {"batch": b, "algorithm": c2r.info()["algorithm"]})]
+    return ops, {"workload": "r2c_c2r_fp32_N1048576_batch512", "sizes": [[n, b]],
+                 "l2": "2 GiB real input, no flush needed", "flops": "2.5 N log2 N per real transform"}
+
+
+def build_uneven(dev, rank, cf):
+    """20,000 transforms, sizes log-uniform over the 7-smooth integers in [16, 65536], each at
+    its own offset of a packed buffer, Gaussian inputs, one persistent graph-captured launch."""
+    import numpy as np
+    import torch
+
+    from crd_b200.workloads import uneven_sizes
+
+    sizes = uneven_sizes(20000, seed=0x5EED0003)
+    plan = cf.UnevenPlan(sizes)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 3 + rank)
+    xin = torch.randn(2 * plan.total, generator=gen, device=dev, dtype=torch.float32).view(torch.complex64)
+    xout = torch.empty(plan.total, dtype=torch.complex64, device=dev)
+    fl = sum(5.0 * s * math.log2(s) for s in sizes)
+    by = sum(16 * s for s in sizes)
+
+    def check():
+        worst = 0.0
+        x = xin.cpu().numpy()
+        y = xout.cpu().numpy()
+        for t in range(0, len(sizes), 997):
+            n, o = sizes[t], plan.offsets[t]
+            worst = max(worst, _rel(y[o:o + n], np.fft.fft(x[o:o + n].astype(np.complex128))))
+        return worst
+
+    return [Op("uneven", xin, xout, lambda i, o: plan.execute(i, o, cf.FORWARD), fl, by, 1, check,
+               {"transforms": len(sizes), "items": plan.info()["factors"][1], "algorithm": "uneven-batch"})], \
+        {"workload": "uneven_20000_7smooth_16_65536", "transforms": 20000, "size_classes": len(set(sizes)),
+         "l2": f"{by / 2**30:.2f} GiB moved per step (> 126 MB L2)"}
+
+
+def build_nd(dev, rank, cf):
+    """BASELINE configs[3], FP32 form: 2-D C2C 4096 x 4096 and 3-D C2C 512^3, uniform[-1,1) plus 1% of entries
+    scaled by 1e4. Four input buffers of each shape rotate across steps so the 128 MiB 2-D input is not L2-resident."""
+    import numpy as np
+    import torch
+
+    ops = []
+    for dims, nbuf in (((4096, 4096), 4), ((512, 512, 512), 1)):
+        total = int(np.prod(dims))
+        gen = torch.Generator(device=dev)
+        gen.manual_seed(SEED + 4 + rank + total)
+        bufs = []
+        for _ in range(nbuf):
+            x = (torch.rand(2 * total, generator=gen, device=dev, dtype=torch.float32) * 2 - 1).view(torch.complex64)
+            idx = torch.randperm(total, generator=gen, device=dev)[: total // 100]
+            x[idx] *= 1e4
+            bufs.append(x)
+        out = torch.empty(total, dtype=torch.complex64, device=dev)
+        plan = cf.Plan(list(dims), batch=1)
+        state = {"k": 0}
+
+        def run(i, o, plan=plan, bufs=bufs, state=state):
+            plan.execute(bufs[state["k"] % len(bufs)], o, cf.FORWARD)
+            state["k"] += 1
+
+        def check(plan=plan, bufs=bufs, out=out, dims=dims):
+            plan.execute(bufs[0], out, cf.FORWARD)
+            torch.cuda.synchronize()
+            x = bufs[0].cpu().numpy().reshape(dims).astype(np.complex128)
+            return _rel(out.cpu().numpy().reshape(dims), np.fft.fftn(x))
+
+        name = "x".join(str(d) for d in dims)
+        ops.append(Op(name, bufs[0], out, run, 5.0 * total * math.log2(total), 16 * total, plan.info()["passes"],
+                      check, {"algorithm": plan.info()["algorithm"]}))
+    return ops, {"workload": "nd_c2c_fp32_4096x4096_512x512x512", "inputs": "uniform[-1,1) + 1% x 1e4",
+                 "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"}
+
+
+BUILDERS = {"mixed": build_mixed, "r2c": build_r2c, "uneven": build_uneven, "nd": build_nd}
+
+
 # ---- the reference's CPU implementation (reference arm and cpu_baseline) -------------------------------------------
 
 
@@ -133,10 +292,10 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-def reference_cpu(steps: int, warmup: int, budget_bytes: int) -> dict:
-    """Time the reference's crd-hesap-fft (FftPlan<float> for powers of two, BluesteinPlan<float> for 107520; one
-    plan per thread over contiguous ranges, batch_arms.hpp:59-77) on this host, in place, over a sample of each
-    size's batch of at most budget_bytes. Returns GFLOP/s over all sizes."""
+def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> dict:
+    """Time the reference's crd-hesap-fft (oracle/_ref/libcrdref.so: FftPlan<float> for powers of two,
+    BluesteinPlan<float> otherwise, RealFftPlan<float>, NdFftPlan<float>; one plan per thread over contiguous
+    ranges, detail/batch_arms.hpp:59-77) on this host, in place, over a bounded sample of the workload."""
     import numpy as np
 
     import oracle  # the CPU checkers: only this leg of the benchmark uses them
@@ -148,35 +307,104 @@ def reference_cpu(steps: int, warmup: int, budget_bytes: int) -> dict:
     total_flops = 0.0
     total_time = 0.0
     sample = []
-    per_size = {}
-    for n, batch in SIZES:
-        count = max(1, min(batch, budget_bytes // (8 * n)))
-        count = max(count, min(batch, threads))
-        buf = oracle.lcg_complex64(SEED ^ n, n * count)
-        ptr = buf.view(np.float32).ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        rescale = np.float32(1.0 / math.sqrt(n))
+    per = {}
+
+    def timed(fn, fl, label, rescale=None):
+        nonlocal total_flops, total_time
         times = []
         for it in range(warmup + steps):
             t0 = time.perf_counter()
-            rc = R.crdref_c2c_f32(n, count, ptr, 0, threads)
+            fn()
             dt = time.perf_counter() - t0
-            if rc != 0:
-                raise RuntimeError(f"crdref_c2c_f32 failed for n={n}")
-            buf *= rescale  # untimed: keeps repeated in-place transforms in range
+            if rescale is not None:
+                rescale()  # untimed: keeps repeated in-place transforms in range
             if it >= warmup:
                 times.append(dt)
         t = sum(times)
-        total_flops += flops(n, count) * len(times)
+        total_flops += fl * len(times)
         total_time += t
-        per_size[str(n)] = round(flops(n, count) * len(times) / t / 1e9, 2)
-        sample.append(f"N={n} x{count} transforms x{len(times)} passes")
+        per[label] = round(fl * len(times) / t / 1e9, 2)
+
+    fp = ctypes.POINTER(ctypes.c_float)
+    if workload == "mixed":
+        for n, batch in SIZES:
+            count = max(1, min(batch, budget_bytes // (8 * n)))
+            count = max(count, min(batch, threads))
+            buf = oracle.lcg_complex64(SEED ^ n, n * count)
+            ptr = buf.view(np.float32).ctypes.data_as(fp)
+            sc = np.float32(1.0 / math.sqrt(n))
+
+            def run(n=n, count=count, ptr=ptr):
+                if R.crdref_c2c_f32(n, count, ptr, 0, threads) != 0:
+                    raise RuntimeError(f"crdref_c2c_f32 failed for n={n}")
+
+            def rs(buf=buf, sc=sc):
+                buf *= sc
+
+            timed(run, flops(n, count), str(n), rs)
+            sample.append(f"N={n} x{count} transforms")
+    elif workload == "r2c":
+        n = 1 << 20
+        count = max(threads, min(512, budget_bytes // (4 * n)))
+        x = oracle.lcg_float32(SEED, n * count)
+        spec = np.empty(count * (n // 2 + 1), dtype=np.complex64)
+        back = np.empty(n * count, dtype=np.float32)
+        fl = 2.5 * n * math.log2(n) * count
+        timed(lambda: R.crdref_rfft_f32(n, count, x.ctypes.data_as(fp), spec.view(np.float32).ctypes.data_as(fp),
+                                        threads), fl, "r2c")
+        timed(lambda: R.crdref_irfft_f32(n, count, spec.view(np.float32).ctypes.data_as(fp), back.ctypes.data_as(fp),
+                                         threads), fl, "c2r")
+        sample.append(f"RealFftPlan<float>(2^20) rfft+irfft x{count}")
+    elif workload == "uneven":
+        from crd_b200.workloads import uneven_sizes
+
+        all_sizes = uneven_sizes(20000, seed=0x5EED0003)
+        sizes, used = [], 0
+        for s in all_sizes:  # a bounded prefix of the batch
+            if used + 8 * s > budget_bytes:
+                break
+            sizes.append(s)
+            used += 8 * s
+        offs, total = [], 0
+        for s in sizes:
+            offs.append(total)
+            total += s
+        buf = oracle.gauss_complex64(0x5EED0003, total)
+        i64 = ctypes.c_int64 * len(sizes)
+        cs, co = i64(*sizes), i64(*offs)
+
+        def run():
+            R.crdref_uneven_f32(len(sizes), cs, co, buf.view(np.float32).ctypes.data_as(fp), 0, threads)
+
+        def rs():
+            buf[:] *= np.float32(1.0 / 256.0)
+
+        fl = sum(5.0 * s * math.log2(s) for s in sizes)
+        timed(run, fl, "uneven", rs)
+        sample.append(f"first {len(sizes)} of 20000 transforms ({len(set(sizes))} sizes), per-thread plan cache "
+                      "built in the warm-up pass")
+    elif workload == "nd":
+        for dims in ((4096, 4096), (512, 512, 512)):
+            total = int(np.prod(dims))
+            x = oracle.lcg_complex64(SEED + total, total)
+            d = (ctypes.c_size_t * len(dims))(*dims)
+            sc = np.float32(1.0 / math.sqrt(total))
+
+            def run(x=x, d=d, dims=dims):
+                R.crdref_nd_f32(len(dims), d, x.view(np.float32).ctypes.data_as(fp), 0)
+
+            def rs(x=x, sc=sc):
+                x *= sc
+
+            timed(run, 5.0 * total * math.log2(total), "x".join(map(str, dims)), rs)
+            sample.append(f"NdFftPlan<float>({'x'.join(map(str, dims))}) on 1 thread")
+        threads = 1
     return {
         "value": total_flops / total_time / 1e9,
         "cores": threads,
         "level": int(R.crdref_level()),
-        "algorithms": {str(n): R.crdref_plan_algorithm_f32(n).decode() for n, _ in SIZES},
-        "sample": "; ".join(sample) + f"; {threads} threads, one plan each, in place",
-        "per_size_gflops": per_size,
+        "sample": "; ".join(sample) + f"; {threads} threads, in place",
+        "per_op_gflops": per,
         "seconds": total_time,
     }
 
@@ -185,9 +413,12 @@ def run_reference_arm(args) -> None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    res = reference_cpu(args.steps, args.warmup, budget_bytes=1 << 30)
+    res = reference_cpu(args.workload, args.steps, args.warmup, budget_bytes=1 << 30)
     value = res["value"]
     ms_per_step = res["seconds"] / args.steps * 1e3
+    config = {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward"} \
+        if args.workload == "mixed" else {"workload": args.workload}
+    config["parallelism"] = "host threads"
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -202,11 +433,9 @@ def run_reference_arm(args) -> None:
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward",
-                   "l2": "per-size batches of 2 GiB (sampled to <= 1 GiB here)", "parallelism": "host threads"},
+        "config": config,
         "cpu_baseline": {"value": round(value, 2), "unit": "GFLOP/s", "cores": res["cores"], "kind": "reference",
-                         "sample": res["sample"], "level": res["level"], "algorithms": res["algorithms"],
-                         "per_size_gflops": res["per_size_gflops"]},
+                         "sample": res["sample"], "level": res["level"], "per_op_gflops": res["per_op_gflops"]},
         "e2e": {"value": round(value, 2), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -216,11 +445,11 @@ def run_reference_arm(args) -> None:
 
 
 def run_ours(args) -> None:
-    import numpy as np
     import torch
     import torch.distributed as dist
 
     import crd_b200 as cf
+    import crd_b200.hesap as F
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -243,24 +472,13 @@ def run_ours(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    import crd_b200.hesap as F
-
     if args.wisdom and os.path.exists(args.wisdom):
         with open(args.wisdom) as f:
             F.wisdom_import(f.read())
     F.set_planner(args.planner)
 
-    # One 2 GiB input (uniform[-1,1) from the seed, every size views it as its own batch) and one 2 GiB output.
-    max_pts = max(n * b for n, b in SIZES)
-    gen = torch.Generator(device=dev)
-    gen.manual_seed(SEED + rank)
-    xin = (torch.rand(2 * max_pts, generator=gen, device=dev, dtype=torch.float32) * 2 - 1).view(torch.complex64)
-    xout = torch.empty(max_pts, dtype=torch.complex64, device=dev)
-    plans = []
-    for n, b in SIZES:
-        p = cf.Plan([n], batch=b)
-        plans.append(p)
-    launches_per_step = sum(p.info()["passes"] for p in plans)
+    ops, config = BUILDERS[args.workload](dev, rank, cf)
+    launches_per_step = sum(op.launches for op in ops)
     if args.planner_log and rank == 0:
         with open(args.planner_log, "w") as f:
             f.write(F.planner_log())
@@ -269,10 +487,10 @@ def run_ours(args) -> None:
     stream = torch.cuda.current_stream()
 
     def step(events=None):
-        for i, ((n, b), p) in enumerate(zip(SIZES, plans)):
+        for i, op in enumerate(ops):
             if events is not None:
                 events[i][0].record(stream)
-            p.execute(xin[: n * b], xout[: n * b], cf.FORWARD)
+            op.run(op.inp, op.out)
             if events is not None:
                 events[i][1].record(stream)
 
@@ -290,7 +508,7 @@ def run_ours(args) -> None:
     sampler.start()
     time.sleep(0.3)
 
-    ev = [[[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] for _ in SIZES]
+    ev = [[[torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)] for _ in ops]
           for _ in range(args.steps)]
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
@@ -305,60 +523,48 @@ def run_ours(args) -> None:
     clocks = sampler.stop()
 
     total_ms = max_over_ranks(t_start.elapsed_time(t_end))
-    per_size_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps)) / args.steps
-                   for i in range(len(SIZES))]
-    step_flops = sum(flops(n, b) for n, b in SIZES)
+    per_ms = [sum(ev[k][i][0].elapsed_time(ev[k][i][1]) for k in range(args.steps)) / args.steps
+              for i in range(len(ops))]
+    step_flops = sum(op.flops for op in ops)
+    step_bytes = sum(op.bytes for op in ops)
     value = step_flops * args.steps * world / (total_ms / 1e3) / 1e9
     ms_per_step = total_ms / args.steps
 
-    # Accuracy of the measured outputs: transform 0 and the last of each size against numpy's float64 FFT.
-    rel = {}
-    for (n, b), p in zip(SIZES, plans):
-        p.execute(xin[: n * b], xout[: n * b], cf.FORWARD)
-        torch.cuda.synchronize()
-        worst = 0.0
-        for t in (0, b - 1):
-            x = xin[t * n:(t + 1) * n].cpu().numpy().astype(np.complex128)
-            y = xout[t * n:(t + 1) * n].cpu().numpy().astype(np.complex128)
-            want = np.fft.fft(x)
-            worst = max(worst, float(np.linalg.norm(y - want) / np.linalg.norm(want)))
-        rel[str(n)] = worst
+    rel = {op.name: op.check() for op in ops}
+    F.device_status(cf.Plan([16]))  # the library's status word path works (a fresh plan: OK)
 
     peaks = measured_peaks()
-    # Dominant kernel: the N=4096 single-pass line FFT (one launch moves its whole 2 GiB batch in and out).
-    i4096 = 0
-    dom_bytes = algorithmic_bytes(*SIZES[i4096])
-    dom_ms = per_size_ms[i4096] / max(1, plans[i4096].info()["passes"])
+    # Dominant kernel: the op with one launch per execute and the largest share of the step (for the default
+    # workload, the N = 4096 single-pass line FFT, whose one launch moves its whole 2 GiB batch in and out).
+    single = [i for i, op in enumerate(ops) if op.launches == 1] or list(range(len(ops)))
+    dom = max(single, key=lambda i: per_ms[i])
+    dom_bytes = ops[dom].bytes
+    dom_ms = per_ms[dom] / max(1, ops[dom].launches)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
-    traffic = profiled_traffic().get("line_fft_4096_bytes_per_launch")
-    per_size = {}
-    for (n, b), p, ms in zip(SIZES, plans, per_size_ms):
-        gbs = algorithmic_bytes(n, b) / (ms / 1e3) / 1e9
-        per_size[str(n)] = {
-            "batch": b,
-            "algorithm": p.info()["algorithm"],
-            "launches": p.info()["passes"],
-            "ms": round(ms, 4),
-            "gflops": round(flops(n, b) / (ms / 1e3) / 1e9, 1),
-            "hbm_gbs": round(gbs, 1),
-            "hbm_frac": round(gbs / peaks["hbm_gbs"], 4),
-            "rel_l2_vs_fp64": rel[str(n)],
-        }
+    traffic_doc = profiled_traffic()
+    traffic = traffic_doc.get(f"{args.workload}:{ops[dom].name}")
+    per = {}
+    for op, ms in zip(ops, per_ms):
+        gbs = op.bytes / (ms / 1e3) / 1e9
+        per[op.name] = dict(op.info, launches=op.launches, ms=round(ms, 4),
+                            gflops=round(op.flops / (ms / 1e3) / 1e9, 1), hbm_gbs=round(gbs, 1),
+                            hbm_frac=round(gbs / peaks["hbm_gbs"], 4), rel_l2_vs_fp64=rel[op.name])
 
-    # End to end through the public API with host buffers: every step copies each size's 2 GiB input from pinned
-    # host memory, transforms it, and copies the 2 GiB spectrum back.
+    # End to end through the public API with host buffers: every step copies each op's input from pinned host
+    # memory, runs it, and copies its whole output back.
     e2e = None
     if not args.no_e2e:
-        hin = torch.empty(max_pts, dtype=torch.complex64, pin_memory=True)
-        hin.copy_(xin)
-        hout = torch.empty(max_pts, dtype=torch.complex64, pin_memory=True)
+        hins = [torch.empty(op.inp.shape, dtype=op.inp.dtype, pin_memory=True) for op in ops]
+        houts = [torch.empty(op.out.shape, dtype=op.out.dtype, pin_memory=True) for op in ops]
+        for h, op in zip(hins, ops):
+            h.copy_(op.inp)
         e_steps = max(1, min(args.steps, 3))
 
         def e2e_step():
-            for (n, b), p in zip(SIZES, plans):
-                xin[: n * b].copy_(hin[: n * b], non_blocking=True)
-                p.execute(xin[: n * b], xout[: n * b], cf.FORWARD)
-                hout[: n * b].copy_(xout[: n * b], non_blocking=True)
+            for h, ho, op in zip(hins, houts, ops):
+                op.inp.copy_(h, non_blocking=True)
+                op.run(op.inp, op.out)
+                ho.copy_(op.out, non_blocking=True)
 
         e2e_step()
         torch.cuda.synchronize()
@@ -372,22 +578,25 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         barrier()
         e_ms = max_over_ranks(e0.elapsed_time(e1))
-        bytes_moved = sum(8 * n * b for n, b in SIZES)
+        h2d = sum(op.inp.numel() * op.inp.element_size() for op in ops)
+        d2h = sum(op.out.numel() * op.out.element_size() for op in ops)
         e2e = {"value": round(step_flops * e_steps * world / (e_ms / 1e3) / 1e9, 2), "unit": "GFLOP/s",
-               "h2d_bytes_per_step": bytes_moved, "d2h_bytes_per_step": bytes_moved, "steps": e_steps,
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e_steps,
                "ms_per_step": round(e_ms / e_steps, 3)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            res = reference_cpu(steps=2, warmup=1, budget_bytes=256 << 20)
+            res = reference_cpu(args.workload, steps=2, warmup=1, budget_bytes=256 << 20)
             cpu = {"value": round(res["value"], 2), "unit": "GFLOP/s", "cores": res["cores"], "kind": "reference",
-                   "sample": res["sample"], "level": res["level"], "per_size_gflops": res["per_size_gflops"]}
+                   "sample": res["sample"], "level": res["level"], "per_op_gflops": res["per_op_gflops"]}
         except Exception as exc:  # the GPU number stands; say why the baseline is missing
             cpu = {"value": None, "unit": "GFLOP/s", "cores": host_threads(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}
 
     if rank == 0:
+        config.update({"precision": "fp32", "placement": "out-of-place", "planner": args.planner,
+                       "parallelism": f"replicas{world}"})
         line = {
             "metric": METRIC,
             "value": round(value, 2),
@@ -401,17 +610,13 @@ def run_ours(args) -> None:
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward",
-                       "precision": "fp32", "placement": "out-of-place", "planner": args.planner,
-                       "l2": "inputs 2 GiB per size (> 126 MB L2), no flush needed",
-                       "parallelism": f"replicas{world}"},
-            "roofline": {"bound": "hbm", "kernel": "line_fft_kernel N=4096 single pass",
+            "config": config,
+            "roofline": {"bound": "hbm", "kernel": f"{ops[dom].name} ({ops[dom].info.get('algorithm', '')})",
                          "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peaks["source"],
                          "traffic": traffic, "algorithmic_bytes_per_launch": dom_bytes},
-            "hbm_frac_step": round(sum(algorithmic_bytes(n, b) for n, b in SIZES) / (ms_per_step / 1e3) / 1e9
-                                   / peaks["hbm_gbs"], 4),
-            "per_size": per_size,
+            "hbm_frac_step": round(step_bytes / (ms_per_step / 1e3) / 1e9 / peaks["hbm_gbs"], 4),
+            "per_op": per,
             "rel_l2_vs_fp64_max": max(rel.values()),
             "gpu_launches": launches_per_step * args.steps,
             "clocks": clocks,
@@ -429,6 +634,9 @@ def main() -> None:
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=WORKLOADS, default="mixed",
+                    help="mixed (default): configs[1] C2C sizes; r2c: R2C/C2R 2^20; uneven: configs[2]; "
+                         "nd: configs[3] FP32 2-D/3-D")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--planner", choices=["estimate", "measure"], default="measure",

@@ -67,6 +67,8 @@ EXPORTS = (
     "crdfft_wisdom_forget",
     "crdfft_planner_log",
     "crdfft_execute_static_scratch",
+    "crdfft_plan_create_uneven",
+    "crdfft_uneven_offsets",
 )
 
 
@@ -147,6 +149,8 @@ def lib():
         "crdfft_wisdom_forget": ([], None),
         "crdfft_planner_log": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
         "crdfft_execute_static_scratch": ([vp, vp, i64, i64, i32, vp], i32),
+        "crdfft_plan_create_uneven": ([ctypes.POINTER(i64), i64, ctypes.POINTER(i64), pp], i32),
+        "crdfft_uneven_offsets": ([ctypes.POINTER(i64), i64, ctypes.POINTER(i64)], i64),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -19,6 +19,7 @@
 #include "kernels.hpp"
 #include "pass_desc.hpp"
 #include "tuner.hpp"
+#include "uneven.hpp"
 
 #include <cuda_runtime.h>
 
@@ -32,6 +33,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 namespace crdfft
@@ -235,9 +237,17 @@ struct Plan
     std::mutex batched_mu;
     int api_kind = 0; // 0 general, 1 FftPlan, 2 RealFftPlan, 3 BluesteinPlan, 4 NdFftPlan
     bool arena_backed = t_arena != nullptr; // device memory belongs to an arena: nothing to free
+    // Uneven batch: the work list descriptor, its shared memory, and one instantiated graph per (in, out, direction)
+    bool uneven = false;
+    UnevenDesc udesc{};
+    int usmem = 0;
+    std::map<std::tuple<const void*, void*, int>, cudaGraphExec_t> graphs;
+    std::mutex graphs_mu;
 
     ~Plan()
     {
+        for (auto& kv : graphs)
+            cudaGraphExecDestroy(kv.second);
         for (auto& kv : batched)
             delete kv.second;
         if (arena_backed)
@@ -1048,6 +1058,214 @@ crdfft_status build_nd(Plan& p)
     return CRDFFT_OK;
 }
 
+template <typename T> crdfft_status upload_vec(Plan& p, const std::vector<T>& v, const T** out)
+{
+    void* d = nullptr;
+    const size_t bytes = std::max<size_t>(sizeof(T), v.size() * sizeof(T));
+    if (dev_alloc(&d, bytes) != cudaSuccess)
+        return CRDFFT_OOM;
+    p.tables.push_back(d);
+    p.table_bytes += static_cast<long long>(bytes);
+    if (!v.empty() && cudaMemcpy(d, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) != cudaSuccess)
+        return CRDFFT_LAUNCH;
+    *out = static_cast<const T*>(d);
+    return CRDFFT_OK;
+}
+
+// The uneven batch's work list (uneven.cu): transforms up to 8192 points grouped by length into CTA-sized items;
+// longer ones (7-smooth, up to 8192^2) as four-step column and row tiles through a workspace region of their own.
+// List order: every COL item (longest transforms first), then SMALL items (longest first), then ROW items.
+crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const int64_t* offsets)
+{
+    const int threads = uneven_threads();
+    std::map<long long, int> sched_of;
+    std::vector<UnevenSched> scheds;
+    auto sched_index = [&](long long n, int* idx) -> crdfft_status {
+        auto it = sched_of.find(n);
+        if (it != sched_of.end())
+        {
+            *idx = it->second;
+            return CRDFFT_OK;
+        }
+        std::vector<int> rad;
+        if (!radices_for(n, rad) || n > 8192 || static_cast<int>(rad.size()) > kMaxStages)
+            return CRDFFT_UNSUPPORTED_SIZE;
+        UnevenSched sc{};
+        sc.n = static_cast<int>(n);
+        sc.nstages = static_cast<int>(rad.size());
+        for (size_t i = 0; i < rad.size(); ++i)
+            sc.radix[i] = rad[i];
+        const crdfft_status st = twiddle_table(p, n, &sc.tw);
+        if (st != CRDFFT_OK)
+            return st;
+        *idx = static_cast<int>(scheds.size());
+        sched_of[n] = *idx;
+        scheds.push_back(sc);
+        return CRDFFT_OK;
+    };
+    std::map<long long, std::vector<long long>, std::greater<long long>> small; // n -> transforms
+    std::vector<long long> large;                                            // transforms, longest first
+    for (int64_t t = 0; t < count; ++t)
+    {
+        const long long n = sizes[t];
+        if (n < 2 || !is_smooth(n))
+            return CRDFFT_UNSUPPORTED_SIZE;
+        if (offsets[t] < 0)
+            return CRDFFT_INVALID_ARG;
+        if (n <= 8192)
+            small[n].push_back(t);
+        else
+            large.push_back(t);
+    }
+    std::stable_sort(large.begin(), large.end(), [&](long long a, long long b) { return sizes[a] > sizes[b]; });
+    std::vector<UnevenItem> col, mid, row;
+    std::vector<long long> line_off;
+    std::vector<const void*> fh, fl;
+    std::map<long long, int> ftw_of;
+    long long scratch = 0;
+    int maxsmem = 0;
+    for (size_t li = 0; li < large.size(); ++li)
+    {
+        const long long t = large[li];
+        const long long n = sizes[t];
+        long long n1 = 0, n2 = 0;
+        if (!four_step_split(n, &n1, &n2) || n1 > 8192 || n2 > 8192)
+            return CRDFFT_UNSUPPORTED_SIZE;
+        int s1 = 0, s2 = 0;
+        crdfft_status st = sched_index(n1, &s1);
+        if (st == CRDFFT_OK)
+            st = sched_index(n2, &s2);
+        if (st != CRDFFT_OK)
+            return st;
+        int fidx;
+        auto fit = ftw_of.find(n);
+        if (fit == ftw_of.end())
+        {
+            const void* hi = nullptr;
+            const void* lo = nullptr;
+            st = four_step_tables(p, n, n1, n2, &hi, &lo);
+            if (st != CRDFFT_OK)
+                return st;
+            fidx = static_cast<int>(fh.size());
+            fh.push_back(hi);
+            fl.push_back(lo);
+            ftw_of[n] = fidx;
+        }
+        else
+            fidx = fit->second;
+        const long long base = offsets[t];
+        const long long reg = scratch;
+        scratch += (n + 1) / 2 * 2;
+        const int lc = std::max(1, std::min(threads / static_cast<int>((n1 + 15) / 16),
+                                            kMaxSmemBytes / (pass_line_pitch(static_cast<int>(n1)) * 8)));
+        int ncol = 0;
+        for (long long q0 = 0; q0 < n2; q0 += lc, ++ncol)
+        {
+            UnevenItem it{};
+            it.kind = kUnevenCol;
+            it.sched = s1;
+            it.lines = static_cast<int>(std::min<long long>(lc, n2 - q0));
+            it.line_table = -1;
+            it.in_base = base + q0;
+            it.in_ldist = 1;
+            it.in_estride = n2;
+            it.out_base = reg + q0;
+            it.out_ldist = 1;
+            it.out_estride = n2;
+            it.transform = static_cast<int>(li);
+            it.q0 = static_cast<int>(q0);
+            it.ftw = fidx;
+            col.push_back(it);
+            maxsmem = std::max(maxsmem, it.lines * pass_line_pitch(static_cast<int>(n1)) * 8);
+        }
+        const int lr = std::max(1, std::min(threads / static_cast<int>((n2 + 15) / 16),
+                                            kMaxSmemBytes / (pass_line_pitch(static_cast<int>(n2)) * 8)));
+        for (long long k0 = 0; k0 < n1; k0 += lr)
+        {
+            UnevenItem it{};
+            it.kind = kUnevenRow;
+            it.sched = s2;
+            it.lines = static_cast<int>(std::min<long long>(lr, n1 - k0));
+            it.line_table = -1;
+            it.in_base = reg + k0 * n2;
+            it.in_ldist = n2;
+            it.in_estride = 1;
+            it.out_base = base + k0;
+            it.out_ldist = 1;
+            it.out_estride = n1;
+            it.transform = static_cast<int>(li);
+            it.need = ncol + (g_debug_stall.load() ? 1 : 0); // the test hook asks for a COL item that never comes
+            it.ftw = -1;
+            row.push_back(it);
+            maxsmem = std::max(maxsmem, it.lines * pass_line_pitch(static_cast<int>(n2)) * 8);
+        }
+    }
+    for (auto& kv : small)
+    {
+        const long long n = kv.first;
+        int sidx = 0;
+        const crdfft_status st = sched_index(n, &sidx);
+        if (st != CRDFFT_OK)
+            return st;
+        const int lpi = std::max(1, std::min(threads / static_cast<int>((n + 15) / 16),
+                                             kMaxSmemBytes / (pass_line_pitch(static_cast<int>(n)) * 8)));
+        const std::vector<long long>& ts = kv.second;
+        for (size_t i = 0; i < ts.size(); i += lpi)
+        {
+            UnevenItem it{};
+            it.kind = kUnevenSmall;
+            it.sched = sidx;
+            it.lines = static_cast<int>(std::min<size_t>(lpi, ts.size() - i));
+            it.line_table = static_cast<int>(line_off.size());
+            for (int a = 0; a < it.lines; ++a)
+                line_off.push_back(offsets[ts[i + a]]);
+            it.in_estride = 1;
+            it.out_estride = 1;
+            it.transform = -1;
+            it.ftw = -1;
+            mid.push_back(it);
+            maxsmem = std::max(maxsmem, it.lines * pass_line_pitch(static_cast<int>(n)) * 8);
+        }
+    }
+    std::vector<UnevenItem> items;
+    items.insert(items.end(), col.begin(), col.end());
+    items.insert(items.end(), mid.begin(), mid.end());
+    items.insert(items.end(), row.begin(), row.end());
+    UnevenDesc& u = p.udesc;
+    crdfft_status st = upload_vec(p, items, &u.items);
+    if (st == CRDFFT_OK)
+        st = upload_vec(p, scheds, &u.scheds);
+    if (st == CRDFFT_OK)
+        st = upload_vec(p, line_off, &u.line_off);
+    if (st == CRDFFT_OK)
+        st = upload_vec(p, fh, &u.tables.ftw_hi);
+    if (st == CRDFFT_OK)
+        st = upload_vec(p, fl, &u.tables.ftw_lo);
+    std::vector<int> counters(1 + large.size(), 0);
+    const int* cdev = nullptr;
+    if (st == CRDFFT_OK)
+        st = upload_vec(p, counters, &cdev);
+    if (st != CRDFFT_OK)
+        return st;
+    u.counter = const_cast<int*>(cdev);
+    u.done = u.counter + 1;
+    u.err = p.err;
+    u.nitems = static_cast<int>(items.size());
+    u.ntransforms = static_cast<int>(large.size());
+    u.spin_limit = g_debug_stall.load() ? (1 << 10) : (1 << 24);
+    u.conj = 0;
+    u.scale = 1.0f;
+    p.usmem = std::max(maxsmem, 1024);
+    p.ws_bytes = static_cast<size_t>(scratch) * 8;
+    p.uneven = true;
+    p.algorithm = "uneven-batch";
+    p.factors = {count, static_cast<long long>(items.size()), static_cast<long long>(large.size())};
+    // one launch per execute (counter reset + the persistent kernel)
+    p.steps[0].assign(1, Step{});
+    p.steps[1].assign(1, Step{});
+    return CRDFFT_OK;
+}
+
 crdfft_status validate(const crdfft_desc& d)
 {
     if (d.rank < 1 || d.rank > 3 || d.batch < 1)
@@ -1122,6 +1340,47 @@ void* resolve(const BufRef& r, const void* in, void* out, void* ws)
     return base + r.off * 8;
 }
 
+// The uneven batch's execute: the counter reset and the persistent kernel, captured once per (in, out, direction)
+// into a CUDA graph and launched as one graph on the caller's stream.
+crdfft_status run_uneven(Plan& p, const void* in, void* out, int dir, cudaStream_t stream)
+{
+    UnevenDesc u = p.udesc;
+    u.conj = dir;
+    const std::tuple<const void*, void*, int> key{in, out, dir};
+    cudaGraphExec_t exec = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(p.graphs_mu);
+        auto it = p.graphs.find(key);
+        if (it != p.graphs.end())
+            exec = it->second;
+    }
+    if (exec == nullptr)
+    {
+        cudaStream_t cap = nullptr;
+        if (cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess)
+        {
+            const cudaError_t le = launch_uneven(u, p.usmem, in, out, p.ws, cap);
+            e = cudaStreamEndCapture(cap, &g);
+            if (le != cudaSuccess)
+                e = le;
+        }
+        if (e == cudaSuccess)
+            e = cudaGraphInstantiate(&exec, g, 0);
+        if (g != nullptr)
+            cudaGraphDestroy(g);
+        cudaStreamDestroy(cap);
+        if (e != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        std::lock_guard<std::mutex> lk(p.graphs_mu);
+        p.graphs[key] = exec;
+    }
+    return cudaGraphLaunch(exec, stream) == cudaSuccess ? CRDFFT_OK : CRDFFT_LAUNCH;
+}
+
 crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stream)
 {
     int dev = -1;
@@ -1129,6 +1388,8 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
         return CRDFFT_NO_DEVICE;
     if (p.ws_bytes > 0 && p.ws == nullptr)
         return CRDFFT_INVALID_ARG;
+    if (p.uneven)
+        return run_uneven(p, in, out, dir, stream);
     for (const Step& s : p.steps[dir])
     {
         void* src = resolve(s.src, in, out, p.ws);
@@ -1445,6 +1706,67 @@ void crdfft_debug_fail_alloc_after(int32_t k) { g_fail_alloc_after.store(k < 0 ?
 void crdfft_debug_stall_waits(int32_t on) { g_debug_stall.store(on ? 1 : 0); }
 
 void crdfft_set_planner_mode(int32_t mode) { set_planner_mode(mode); }
+
+int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offsets)
+{
+    if (sizes == nullptr || count < 0)
+        return -1;
+    int64_t off = 0;
+    for (int64_t t = 0; t < count; ++t)
+    {
+        if (offsets != nullptr)
+            offsets[t] = off;
+        off += (sizes[t] + 1) / 2 * 2; // each transform starts on a 16-byte boundary
+    }
+    return off;
+}
+
+crdfft_status crdfft_plan_create_uneven(const int64_t* sizes, int64_t count, const int64_t* offsets,
+                                        crdfft_plan** plan)
+{
+    if (plan == nullptr || sizes == nullptr || count < 1)
+        return CRDFFT_INVALID_ARG;
+    *plan = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return CRDFFT_NO_DEVICE;
+    std::vector<int64_t> packed;
+    if (offsets == nullptr)
+    {
+        packed.resize(static_cast<size_t>(count));
+        crdfft_uneven_offsets(sizes, count, packed.data());
+        offsets = packed.data();
+    }
+    std::unique_ptr<Plan> p(new Plan());
+    p->desc = crdfft_desc{};
+    p->desc.rank = 1;
+    p->desc.kind = CRDFFT_C2C;
+    p->desc.batch = count;
+    p->device = dev;
+    {
+        void* e = nullptr;
+        if (dev_alloc(&e, 256) != cudaSuccess)
+            return CRDFFT_OOM;
+        p->tables.push_back(e);
+        if (cudaMemset(e, 0, 256) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        p->err = static_cast<int*>(e);
+    }
+    crdfft_status st = build_uneven(*p, sizes, count, offsets);
+    if (st != CRDFFT_OK)
+        return st;
+    if (p->ws_bytes > 0)
+    {
+        if (dev_alloc(&p->ws, p->ws_bytes) != cudaSuccess)
+        {
+            p->ws = nullptr;
+            return CRDFFT_OOM;
+        }
+        p->ws_owned = true;
+    }
+    *plan = reinterpret_cast<crdfft_plan*>(p.release());
+    return CRDFFT_OK;
+}
 
 static crdfft_status copy_out(const std::string& s, char* buf, size_t cap, size_t* needed)
 {

@@ -236,6 +236,43 @@ class NdFftPlan(_Handle):
         return data
 
 
+def uneven_offsets(sizes) -> tuple:
+    """Packed offsets (each transform on a 16-byte boundary) and the total complex elements for an uneven batch."""
+    n = len(sizes)
+    arr = (ctypes.c_int64 * n)(*[int(v) for v in sizes])
+    off = (ctypes.c_int64 * n)()
+    total = lib().crdfft_uneven_offsets(arr, n, off)
+    if total < 0:
+        raise ValueError("bad sizes")
+    return [int(v) for v in off], int(total)
+
+
+class UnevenPlan(_Handle):
+    """Independent complex transforms of different 7-smooth lengths in one persistent, graph-captured launch
+    (crdfft_plan_create_uneven). Transform t occupies elements offsets[t] .. offsets[t]+sizes[t]-1 of the input
+    and of the output buffer; both directions unnormalised."""
+
+    def __init__(self, sizes, offsets=None):
+        super().__init__()
+        self.sizes = [int(v) for v in sizes]
+        n = len(self.sizes)
+        arr = (ctypes.c_int64 * n)(*self.sizes)
+        if offsets is None:
+            self.offsets, self.total = uneven_offsets(self.sizes)
+        else:
+            self.offsets = [int(v) for v in offsets]
+            self.total = max(o + s for o, s in zip(self.offsets, self.sizes))
+        off = (ctypes.c_int64 * n)(*self.offsets)
+        check(lib().crdfft_plan_create_uneven(arr, n, off, ctypes.byref(self._h)), "UnevenPlan")
+
+    def execute(self, inp: torch.Tensor, out: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+        if inp.numel() < self.total or out.numel() < self.total:
+            raise ValueError(f"buffers must hold {self.total} complex values")
+        check(lib().crdfft_execute(self._h, _ptr(inp, torch.complex64, "input"), _ptr(out, torch.complex64, "output"),
+                                   _dir(direction), _stream(stream)), "execute")
+        return out
+
+
 def fft(data: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
     """One-shot in-place transform, unnormalised (fft.hpp:1006-1012)."""
     check(lib().crdfft_fft(_ptr(data, torch.complex64, "data"), data.numel(), _dir(direction), _stream(stream)), "fft")

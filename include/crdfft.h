@@ -159,6 +159,19 @@ crdfft_status crdfft_nd_execute(crdfft_plan* plan, void* data, int32_t direction
 crdfft_status crdfft_fft(void* data, int64_t n, int32_t direction, void* stream);
 crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream);
 
+/* ---- Uneven batches ---------------------------------------------------------------------------------------- */
+
+/* `count` independent forward/inverse complex transforms of different lengths (7-smooth, 2 .. 8192^2), transform t
+ * at element offset offsets[t] of the input and of the output (NULL: packed, see crdfft_uneven_offsets). The
+ * reference runs such a batch as a loop of per-size plans over crd-jobs ranges (detail/batch_arms.hpp:59-77); here
+ * one persistent launch walks a device work list, captured once per (in, out, direction) into a CUDA graph.
+ * Execute with crdfft_execute; both directions unnormalised. */
+crdfft_status crdfft_plan_create_uneven(const int64_t* sizes, int64_t count, const int64_t* offsets,
+                                        crdfft_plan** plan);
+/* Packed offsets for an uneven batch (each transform starting on a 16-byte boundary) into offsets[count] (may be
+ * NULL); returns the total number of complex elements the buffer needs, or -1. */
+int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offsets);
+
 /* ---- Planner ----------------------------------------------------------------------------------------------- */
 
 /* How plan creation picks each pass's launch shape (kernel variant, points a thread, lines a CTA):

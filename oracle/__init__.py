@@ -241,9 +241,11 @@ def ref():
         R.crdref_irfft_f32.argtypes = [_sz, _sz, _fp, _fp, ctypes.c_int]
         R.crdref_nd_f32.argtypes = [_sz, ctypes.POINTER(ctypes.c_size_t), _fp, ctypes.c_int]
         R.crdref_nd_f64.argtypes = [_sz, ctypes.POINTER(ctypes.c_size_t), _dp, ctypes.c_int]
+        R.crdref_uneven_f32.argtypes = [_sz, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _fp,
+                                        ctypes.c_int, ctypes.c_int]
         for f in ("crdref_c2c_f32", "crdref_c2c_f64", "crdref_execute_reference_f32", "crdref_execute_reference_f64",
                   "crdref_execute_batched_f32", "crdref_stockham_f32", "crdref_rfft_f32", "crdref_irfft_f32",
-                  "crdref_nd_f32", "crdref_nd_f64"):
+                  "crdref_nd_f32", "crdref_nd_f64", "crdref_uneven_f32"):
             getattr(R, f).restype = ctypes.c_int
         _ref = R
     return _ref

@@ -15,6 +15,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <map>
 #include <memory>
 #include <thread>
 #include <vector>
@@ -57,6 +58,26 @@ template <typename F> void fan_out(int threads, std::size_t count, const F& fn)
     for (std::size_t j = 0; j < t; ++j)
     {
         pool.emplace_back([&fn, j, t, count]() { fn(j * count / t, (j + 1) * count / t); });
+    }
+    for (auto& th : pool)
+    {
+        th.join();
+    }
+}
+
+// fan_out with the range index passed to fn(j, first, last).
+template <typename F> void fan_out_indexed(std::size_t t, std::size_t count, const F& fn)
+{
+    if (t <= 1)
+    {
+        fn(std::size_t{0}, std::size_t{0}, count);
+        return;
+    }
+    std::vector<std::thread> pool;
+    pool.reserve(t);
+    for (std::size_t j = 0; j < t; ++j)
+    {
+        pool.emplace_back([&fn, j, t, count]() { fn(j, j * count / t, (j + 1) * count / t); });
     }
     for (auto& th : pool)
     {
@@ -240,6 +261,50 @@ int crdref_irfft_f32(std::size_t n, std::size_t batch, const float* in, float* o
                     plan.irfft(
                         cont::ConstSpan<Complex<float>>(reinterpret_cast<const Complex<float>*>(in) + t * h, h),
                         cont::Span<float>(out + t * n, n));
+                }
+            });
+    return 0;
+}
+
+// An uneven batch: transform t of length sizes[t] at complex offset offsets[t], in place, forward or inverse;
+// contiguous ranges of transforms per thread (batch_arms.hpp:59-77), each thread keeping one plan per size across
+// calls (FftPlan<float> for powers of two, BluesteinPlan<float> otherwise) the way a caller with a plan cache would.
+int crdref_uneven_f32(std::size_t count, const std::int64_t* sizes, const std::int64_t* offsets, float* data, int dir,
+                      int threads)
+{
+    auto* x = reinterpret_cast<Complex<float>*>(data);
+    struct Cache
+    {
+        std::map<std::size_t, std::unique_ptr<fft::FftPlan<float>>> pow2;
+        std::map<std::size_t, std::unique_ptr<fft::BluesteinPlan<float>>> other;
+    };
+    // One cache per range index (ranges are stable for a given count and thread count), kept across calls.
+    static std::map<std::size_t, Cache> caches;
+    const std::size_t nt = threads < 1 ? 1 : (static_cast<std::size_t>(threads) < count ? threads : count);
+    for (std::size_t j = 0; j < nt; ++j)
+        (void)caches[j]; // created here, on one thread; each range then touches only its own
+    fan_out_indexed(nt, count,
+            [&](std::size_t j, std::size_t first, std::size_t last)
+            {
+                Cache& cache = caches.at(j);
+                for (std::size_t t = first; t < last; ++t)
+                {
+                    const std::size_t n = static_cast<std::size_t>(sizes[t]);
+                    cont::Span<Complex<float>> span(x + offsets[t], n);
+                    if (is_pow2(n))
+                    {
+                        auto& pl = cache.pow2[n];
+                        if (!pl)
+                            pl = std::make_unique<fft::FftPlan<float>>(&alloc(), n);
+                        pl->execute(span, dir_of(dir));
+                    }
+                    else
+                    {
+                        auto& pl = cache.other[n];
+                        if (!pl)
+                            pl = std::make_unique<fft::BluesteinPlan<float>>(&alloc(), n);
+                        pl->execute(span, dir_of(dir));
+                    }
                 }
             });
     return 0;

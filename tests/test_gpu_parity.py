@@ -349,3 +349,62 @@ def test_measuring_planner_and_wisdom():
     H.wisdom_forget()
     want = oracle.fft64(x.cpu().numpy().reshape(batch, n))
     assert oracle.rel_l2(a.cpu().numpy().reshape(batch, n), want) <= REL_L2
+
+
+def _uneven_case(count, seed):
+    from crd_b200.workloads import uneven_sizes
+
+    sizes = uneven_sizes(count, seed=seed)
+    plan = cf.UnevenPlan(sizes)
+    x = oracle.gauss_complex64(seed, plan.total)
+    return sizes, plan, x
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_uneven_batch(inverse):
+    """Config-3 style batch: 7-smooth sizes log-uniform in [16, 65536], Gaussian inputs, one persistent launch;
+    every transform against the FP64 oracle."""
+    sizes, plan, x = _uneven_case(240, 0x5EED0003 + int(inverse))
+    assert any(s > 8192 for s in sizes) and any(s <= 8192 for s in sizes)
+    tin = torch.from_numpy(x).cuda()
+    tout = torch.full_like(tin, complex(float("nan"), float("nan")))
+    plan.execute(tin, tout, cf.INVERSE if inverse else cf.FORWARD)
+    plan.execute(tin, tout, cf.INVERSE if inverse else cf.FORWARD)  # the cached graph, again
+    torch.cuda.synchronize()
+    from crd_b200.hesap import device_status
+
+    device_status(plan)
+    got = tout.cpu().numpy()
+    by_size = {}
+    for t, (n, off) in enumerate(zip(sizes, plan.offsets)):
+        by_size.setdefault(n, []).append(off)
+    for n, offs in by_size.items():
+        xs = np.stack([x[o:o + n] for o in offs])
+        gs = np.stack([got[o:o + n] for o in offs])
+        _check(gs, oracle.fft64(xs, inverse), n, f"uneven n={n}")
+
+
+def test_uneven_dependency_wait_times_out():
+    """A ROW item waiting for a COL item that never comes (the test hook adds one to its count) gives up after its
+    bounded wait, the plan reports CRDFFT_DEVICE_TIMEOUT, and the context stays usable."""
+    from crd_b200.hesap import device_status, stall_waits
+
+    sizes = [65536, 1024, 105]
+    stall_waits(True)
+    try:
+        bad = cf.UnevenPlan(sizes)
+    finally:
+        stall_waits(False)
+    x = torch.from_numpy(oracle.gauss_complex64(5, bad.total)).cuda()
+    y = torch.empty_like(x)
+    bad.execute(x, y)
+    with pytest.raises(cf.CrdFftError) as e:
+        device_status(bad)
+    assert e.value.status == 5
+    good = cf.UnevenPlan(sizes)
+    good.execute(x, y)
+    device_status(good)
+    xs = x.cpu().numpy()
+    ys = y.cpu().numpy()
+    for n, o in zip(sizes, good.offsets):
+        _check(ys[o:o + n], oracle.fft64(xs[o:o + n]), n)
