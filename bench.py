@@ -162,7 +162,9 @@ def build_mixed(dev, rank, cf):
     for n, b in SIZES:
         plan = cf.Plan([n], batch=b)
 
-        def check(n=n, b=b):
+        def check(n=n, b=b, plan=plan):
+            plan.execute(xin[: n * b], xout[: n * b], cf.FORWARD)  # the output buffer is shared: redo this op
+            torch.cuda.synchronize()
             worst = 0.0
             for t in (0, b - 1):
                 x = xin[t * n:(t + 1) * n].cpu().numpy()
@@ -194,10 +196,14 @@ def build_r2c(dev, rank, cf):
     by = (4 * n + 8 * (n // 2 + 1)) * b
 
     def check_r2c():
+        r2c.execute(real, spec, cf.FORWARD)
+        torch.cuda.synchronize()
         x = real[:n].cpu().numpy().astype(np.float64)
         return _rel(spec[: n // 2 + 1].cpu().numpy(), np.fft.rfft(x))
 
     def check_c2r():
+        c2r.execute(spec, back, cf.INVERSE)
+        torch.cuda.synchronize()
         s0 = spec[: n // 2 + 1].cpu().numpy().astype(np.complex128)
         return _rel(back[:n].cpu().numpy(), np.fft.irfft(s0, n) * n)
 
@@ -227,6 +233,8 @@ def build_uneven(dev, rank, cf):
     by = sum(16 * s for s in sizes)
 
     def check():
+        plan.execute(xin, xout, cf.FORWARD)
+        torch.cuda.synchronize()
         worst = 0.0
         x = xin.cpu().numpy()
         y = xout.cpu().numpy()

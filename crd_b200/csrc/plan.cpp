@@ -1058,6 +1058,30 @@ crdfft_status build_nd(Plan& p)
     return CRDFFT_OK;
 }
 
+// The split of a long uneven-batch transform: n = n1 * n2 with both halves at most `cap`, closest to square, n2
+// preferring a multiple of 16 (whole column tiles).
+bool uneven_split(long long n, long long cap, long long* n1, long long* n2)
+{
+    double best = 1e300;
+    for (long long d = 2; d * d <= n; ++d)
+    {
+        if (n % d != 0 || d > cap || n / d > cap || !is_smooth(d) || !is_smooth(n / d))
+            continue;
+        for (int o = 0; o < 2; ++o)
+        {
+            const long long a = o ? d : n / d, b = o ? n / d : d;
+            const double score = (b % 16 != 0 ? 10.0 : 0.0) + std::fabs(std::log(static_cast<double>(a) / b));
+            if (score < best)
+            {
+                best = score;
+                *n1 = a;
+                *n2 = b;
+            }
+        }
+    }
+    return best < 1e299;
+}
+
 template <typename T> crdfft_status upload_vec(Plan& p, const std::vector<T>& v, const T** out)
 {
     void* d = nullptr;
@@ -1072,12 +1096,14 @@ template <typename T> crdfft_status upload_vec(Plan& p, const std::vector<T>& v,
     return CRDFFT_OK;
 }
 
-// The uneven batch's work list (uneven.cu): transforms up to 8192 points grouped by length into CTA-sized items;
-// longer ones (7-smooth, up to 8192^2) as four-step column and row tiles through a workspace region of their own.
+// The uneven batch's work list (uneven.cu): transforms up to kUnevenSingle points grouped by length into CTA-sized
+// items; longer ones (7-smooth, up to kUnevenSingle^2) as four-step column and row tiles through a workspace region
+// of their own.
 // List order: every COL item (longest transforms first), then SMALL items (longest first), then ROW items.
 crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const int64_t* offsets)
 {
     const int threads = uneven_threads();
+    const long long kUnevenSingle = 16LL * threads; // the longest line one item transforms (16 points a thread)
     std::map<long long, int> sched_of;
     std::vector<UnevenSched> scheds;
     auto sched_index = [&](long long n, int* idx) -> crdfft_status {
@@ -1088,7 +1114,7 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
             return CRDFFT_OK;
         }
         std::vector<int> rad;
-        if (!radices_for(n, rad) || n > 8192 || static_cast<int>(rad.size()) > kMaxStages)
+        if (!radices_for(n, rad) || n > kUnevenSingle || static_cast<int>(rad.size()) > kMaxStages)
             return CRDFFT_UNSUPPORTED_SIZE;
         UnevenSched sc{};
         sc.n = static_cast<int>(n);
@@ -1112,7 +1138,7 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
             return CRDFFT_UNSUPPORTED_SIZE;
         if (offsets[t] < 0)
             return CRDFFT_INVALID_ARG;
-        if (n <= 8192)
+        if (n <= kUnevenSingle)
             small[n].push_back(t);
         else
             large.push_back(t);
@@ -1129,7 +1155,7 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
         const long long t = large[li];
         const long long n = sizes[t];
         long long n1 = 0, n2 = 0;
-        if (!four_step_split(n, &n1, &n2) || n1 > 8192 || n2 > 8192)
+        if (!uneven_split(n, kUnevenSingle, &n1, &n2))
             return CRDFFT_UNSUPPORTED_SIZE;
         int s1 = 0, s2 = 0;
         crdfft_status st = sched_index(n1, &s1);

@@ -3,8 +3,8 @@
 // crd-jobs ranges (include/crd/hesap/fft/detail/batch_arms.hpp:59-77, one plan per job); here one kernel walks a
 // device work list:
 //
-//   SMALL  up to `lines` transforms of one length n <= 8192, one CTA, all stages in shared memory
-//   COL    a tile of adjacent columns of one long transform (n = n1 n2 > 8192): length-n1 DFTs, four-step twiddle,
+//   SMALL  up to `lines` transforms of one length n <= 4096, one CTA, all stages in shared memory
+//   COL    a tile of adjacent columns of one long transform (n = n1 n2 > 4096): length-n1 DFTs, four-step twiddle,
 //          written to the transform's region of the workspace
 //   ROW    a tile of rows of that transform's workspace region: length-n2 DFTs, transposed store to the output
 //
@@ -26,50 +26,115 @@ namespace lfft
 namespace
 {
 
-constexpr int kUnevenThreads = 512;
+constexpr int kUnevenThreads = 256;
+
+// Shared-memory slot of element e of a line (the classic layout, line_fft.cuh LayRow<1>).
+__device__ __forceinline__ int spad(int e) { return e + (e >> 4); }
+
+// One stage of a run-time schedule, out of line so that each radix gets its own register allocation, with scalar
+// arguments only. j / L comes from a multiply-high by ceil(2^32 / L) (exact for j < 2^13 and L < 2^19).
+template <int R>
+__device__ __noinline__ void ustage(float2* sl, const float2* tw, int n, int L, unsigned magic, int jt, int T, bool ok)
+{
+    constexpr int B = (16 + R - 1) / R;
+    const int nb = n / R;
+    float2 v[B][R];
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+    {
+        const int j = jt + b * T;
+        if (ok && j < nb)
+        {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                v[b][r] = sl[spad(j + r * nb)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+    {
+        const int j = jt + b * T;
+        if (ok && j < nb)
+        {
+            const int q = L == 1 ? j : static_cast<int>(__umulhi(static_cast<unsigned>(j), magic));
+            const int k = j - q * L;
+            if (L > 1)
+            {
+#pragma unroll
+                for (int r = 1; r < R; ++r)
+                    v[b][r] = cmul(v[b][r], __ldg(tw + (r - 1) * L + k));
+            }
+            Dft<R>::run(v[b]);
+            const int base = q * L * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                sl[spad(base + r * L)] = v[b][r];
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void uneven_stages(const UnevenSched& s, float2* sl, int jt, int T, bool ok)
+{
+    int L = 1;
+    const float2* tw = static_cast<const float2*>(s.tw);
+    for (int st = 0; st < s.nstages; ++st)
+    {
+        const int R = s.radix[st];
+        const unsigned magic = L == 1 ? 0u : (0xFFFFFFFFu / static_cast<unsigned>(L)) + 1u;
+        switch (R)
+        {
+            case 2: ustage<2>(sl, tw, s.n, L, magic, jt, T, ok); break;
+            case 3: ustage<3>(sl, tw, s.n, L, magic, jt, T, ok); break;
+            case 4: ustage<4>(sl, tw, s.n, L, magic, jt, T, ok); break;
+            case 5: ustage<5>(sl, tw, s.n, L, magic, jt, T, ok); break;
+            case 7: ustage<7>(sl, tw, s.n, L, magic, jt, T, ok); break;
+            case 8: ustage<8>(sl, tw, s.n, L, magic, jt, T, ok); break;
+            default: ustage<16>(sl, tw, s.n, L, magic, jt, T, ok); break;
+        }
+        if (L > 1)
+            tw += (R - 1) * L;
+        L *= R;
+    }
+}
 
 // Loads an item's lines into shared memory (row layout, one pad slot per 16), coalesced along whichever side of the
-// global layout is unit-stride.
-__device__ __forceinline__ void uneven_load(const UnevenItem& it, const UnevenSched& s, const float2* src,
-                                            const long long* line_off, float2* sm, int pitch, float in_im, bool l2_only)
+// global layout is unit-stride; line a starts at base[a].
+__device__ __forceinline__ void uneven_load(int n, int lines, long long estride, const long long* base,
+                                            const float2* src, float2* sm, int pitch, float in_im, bool l2_only)
 {
-    const int n = s.n;
-    const bool along_e = it.in_estride == 1;
-    for_tile(n, it.lines, along_e, [&](int a, int e) {
-        const long long base = it.line_table >= 0 ? line_off[it.line_table + a] : it.in_base + a * it.in_ldist;
-        const float2* p = src + base + static_cast<long long>(e) * it.in_estride;
+    for_tile(n, lines, estride == 1, [&](int a, int e) {
+        const float2* p = src + base[a] + static_cast<long long>(e) * estride;
         float2 x = l2_only ? __ldcg(p) : __ldcs(p);
         x.y *= in_im;
         LayRow<1>{sm + a * pitch}.at(e) = x;
     });
 }
 
-__device__ __forceinline__ void uneven_store(const UnevenItem& it, const UnevenSched& s, const UnevenTables& tb,
-                                             float2* dst, const long long* line_off, const float2* sm, int pitch,
-                                             float out_re, float out_im)
+__device__ __forceinline__ void uneven_store(int n, int lines, long long estride, const long long* base, int q0,
+                                             const float2* fh, const float2* fl, float2* dst, const float2* sm,
+                                             int pitch, float out_re, float out_im)
 {
-    const int n = s.n;
-    const bool along_e = it.out_estride == 1;
-    const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(tb.ftw_hi[it.ftw]) : nullptr;
-    const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(tb.ftw_lo[it.ftw]) : nullptr;
-    for_tile(n, it.lines, along_e, [&](int a, int e) {
-        const long long base = it.line_table >= 0 ? line_off[it.line_table + a] : it.out_base + a * it.out_ldist;
+    for_tile(n, lines, estride == 1, [&](int a, int e) {
         float2 v = LayRow<1>{const_cast<float2*>(sm) + a * pitch}.at(e);
         if (fh != nullptr)
         {
-            const int q = it.q0 + a; // column index of the long transform
+            const int q = q0 + a; // column index of the long transform
             v = cmul(v, cmul(__ldg(fh + (q >> 4) * n + e), __ldg(fl + e * 16 + (q & 15))));
         }
-        __stcs(dst + base + static_cast<long long>(e) * it.out_estride, make_float2(v.x * out_re, v.y * out_im));
+        __stcs(dst + base[a] + static_cast<long long>(e) * estride, make_float2(v.x * out_re, v.y * out_im));
     });
 }
 
-__global__ void __launch_bounds__(kUnevenThreads, 1)
+__global__ void __launch_bounds__(kUnevenThreads, 3)
     uneven_kernel(const UnevenDesc u, const float2* __restrict__ gin, float2* __restrict__ gout, float2* scratch)
 {
     extern __shared__ float2 sm[];
     __shared__ int s_item;
     __shared__ int s_go;
+    __shared__ long long s_in[kMaxLinesPerCta];
+    __shared__ long long s_out[kMaxLinesPerCta];
     const int tid = threadIdx.x;
     const float in_im = u.conj ? -1.0f : 1.0f;
     const float out_im = u.conj ? -u.scale : u.scale;
@@ -82,7 +147,7 @@ __global__ void __launch_bounds__(kUnevenThreads, 1)
         if (idx >= u.nitems)
             break;
         const UnevenItem it = u.items[idx];
-        const UnevenSched& s = u.scheds[it.sched];
+        const UnevenSched s = u.scheds[it.sched];
         if (it.kind == kUnevenRow)
         {
             if (tid == 0)
@@ -109,34 +174,29 @@ __global__ void __launch_bounds__(kUnevenThreads, 1)
         }
         const float2* src = it.kind == kUnevenRow ? scratch : gin;
         float2* dst = it.kind == kUnevenCol ? scratch : gout;
-        const int pitch = line_pitch(s.n);
+        const int n = s.n;
+        const int pitch = line_pitch(n);
+        // per-line start offsets, once per item
+        for (int a = tid; a < it.lines; a += blockDim.x)
+        {
+            s_in[a] = it.line_table >= 0 ? u.line_off[it.line_table + a] : it.in_base + a * it.in_ldist;
+            s_out[a] = it.line_table >= 0 ? u.line_off[it.line_table + a] : it.out_base + a * it.out_ldist;
+        }
+        __syncthreads();
         // inverse: conjugate on the way into the first pass of each transform and out of the last
         const bool first_pass = it.kind != kUnevenRow;
         const bool last_pass = it.kind != kUnevenCol;
-        uneven_load(it, s, src, u.line_off, sm, pitch, first_pass ? in_im : 1.0f, it.kind == kUnevenRow);
+        uneven_load(n, it.lines, it.in_estride, s_in, src, sm, pitch, first_pass ? in_im : 1.0f,
+                    it.kind == kUnevenRow);
         __syncthreads();
-        const int T = (s.n + 15) / 16;
+        const int T = (n + 15) / 16;
         const int ll = tid / T;
-        Ctx c;
-        c.jt = tid - ll * T;
-        c.T = T;
-        c.ok = ll < it.lines;
-        c.q = 0;
-        c.in = nullptr;
-        c.out = nullptr;
-        c.in_im = 1.0f;
-        c.out_re = 1.0f;
-        c.out_im = 1.0f;
-        PassDesc d{};
-        d.n = s.n;
-        d.nstages = s.nstages;
-        for (int i = 0; i < kMaxStages; ++i)
-            d.radix[i] = s.radix[i];
-        d.tw = s.tw;
-        const LayRow<1> lay{sm + (ll < it.lines ? ll : 0) * pitch};
-        run_dynamic<16, false, false, Kind<PassMap::Row, false>>(d, c, lay, s.n);
-        uneven_store(it, s, u.tables, dst, u.line_off, sm, pitch, last_pass ? u.scale : 1.0f,
-                     last_pass ? out_im : 1.0f);
+        const bool ok = ll < it.lines;
+        uneven_stages(s, sm + (ok ? ll : 0) * pitch, tid - ll * T, T, ok);
+        const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_hi[it.ftw]) : nullptr;
+        const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_lo[it.ftw]) : nullptr;
+        uneven_store(n, it.lines, it.out_estride, s_out, it.q0, fh, fl, dst, sm, pitch,
+                     last_pass ? u.scale : 1.0f, last_pass ? out_im : 1.0f);
         if (it.kind == kUnevenCol)
         {
             __threadfence(); // release: this item's workspace writes before its completion count
