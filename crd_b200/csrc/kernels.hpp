@@ -6,6 +6,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <vector>
+
 namespace crdfft
 {
 
@@ -71,6 +74,13 @@ struct Arena
     size_t used;
 };
 void arena_bind(Arena* a);
+
+// Tensor-core line pass (tc_fft.cu): the first radix-16 stage as a tcgen05 GEMM. prec 1 = split-BF16 (3 terms),
+// 2 = FP16 with a per-line scale. Row-contiguous passes of n = 512 (16.8.4), 1024 (16.16.4), 4096 (16.16.16).
+bool tc_pass_supported(const PassDesc& d, int prec);
+void tc_build_a(int prec, std::vector<uint16_t>* out);
+cudaError_t launch_tc_pass(const PassDesc& d, int prec, const void* amat, const void* in, void* out,
+                           cudaStream_t stream);
 
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);

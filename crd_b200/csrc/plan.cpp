@@ -93,6 +93,7 @@ enum class StepKind : int
 {
     Line,
     Cluster,
+    TcLine,
     R2CPost,
     C2RPre,
     ChirpPre,
@@ -106,6 +107,8 @@ struct Step
     StepKind kind = StepKind::Line;
     PassDesc pass{};
     PassDesc pass2{}; // Cluster: the row phase
+    int prec = 0;     // TcLine: 1 split-BF16, 2 FP16 scaled
+    const void* amat = nullptr;
     PassShape shape{};
     RealRecombine real{};
     ChirpDesc chirp{};
@@ -232,6 +235,8 @@ struct Plan
     std::string algorithm;
     std::vector<long long> factors;
     int* err = nullptr; // device word the pipelined kernels flag a given-up wait in
+    const void* tc_amat = nullptr; // tensor-core DFT-16 operand image for the plan's precision
+    int tc_steps = 0;
     // FftPlan::execute_batched sub-plans, one per batch value used (element-major layout).
     std::map<long long, Plan*> batched;
     std::mutex batched_mu;
@@ -597,6 +602,31 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     }
     if (d.nstages == 0) // n == 1: no butterflies; the pass is a copy with the epilogue, staged through smem
         dl = ds = false;
+    const int prec = p.desc.precision;
+    if (prec != CRDFFT_PREC_FP32 && tc_pass_supported(d, prec))
+    {
+        // the first radix-16 stage on the tensor cores (tc_fft.cu); other passes of the plan stay FP32
+        if (p.tc_amat == nullptr)
+        {
+            std::vector<uint16_t> img;
+            tc_build_a(prec, &img);
+            std::vector<float> as_float(img.size() / 2);
+            std::memcpy(as_float.data(), img.data(), img.size() * sizeof(uint16_t));
+            void* dev = nullptr;
+            const crdfft_status st2 = upload_table(p, as_float, &dev);
+            if (st2 != CRDFFT_OK)
+                return st2;
+            p.tc_amat = dev;
+        }
+        s.kind = StepKind::TcLine;
+        s.prec = prec;
+        s.amat = p.tc_amat;
+        s.src = src;
+        s.dst = dst;
+        ++p.tc_steps;
+        *step = s;
+        return CRDFFT_OK;
+    }
     if (!choose_shape(d, map, dl, ds, &s.shape))
         return CRDFFT_UNSUPPORTED_SIZE;
     s.src = src;
@@ -684,7 +714,7 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     }
     long long n1 = 0, n2 = 0;
     if (istride == 1 && ostride == 1 && idist == n && odist == n && std::getenv("CRDFFT_NO_CLUSTER") == nullptr &&
-        cluster_split(n, &n1, &n2))
+        p.desc.precision == CRDFFT_PREC_FP32 && cluster_split(n, &n1, &n2))
     {
         // One cluster per transform: columns of n1, DSMEM transpose with the four-step twiddle, rows of n2. The
         // twiddle is one full table tw[k1 n2 + j] = W_n^{j k1} (FP64 roots, narrowed).
@@ -1309,8 +1339,6 @@ crdfft_status validate(const crdfft_desc& d)
         return CRDFFT_INVALID_DESC;
     if (d.kind != CRDFFT_C2C && d.rank != 1)
         return CRDFFT_UNSUPPORTED_SIZE;
-    if (d.precision != CRDFFT_PREC_FP32)
-        return CRDFFT_UNSUPPORTED_SIZE;
     return CRDFFT_OK;
 }
 
@@ -1354,6 +1382,8 @@ crdfft_status create(const crdfft_desc* desc, Plan** out)
         }
         p->ws_owned = true;
     }
+    if (p->tc_steps > 0)
+        p->algorithm += desc->precision == CRDFFT_PREC_SPLIT_BF16 ? "+tc-bf16x3" : "+tc-fp16";
     *out = p.release();
     return CRDFFT_OK;
 }
@@ -1425,6 +1455,7 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
         {
             case StepKind::Line: e = launch_line_pass(s.pass, s.shape, src, dst, stream); break;
             case StepKind::Cluster: e = launch_cluster_fft(s.pass, s.pass2, s.count, src, dst, stream); break;
+            case StepKind::TcLine: e = launch_tc_pass(s.pass, s.prec, s.amat, src, dst, stream); break;
             case StepKind::R2CPost: e = launch_r2c_post(s.real, src, dst, stream); break;
             case StepKind::C2RPre: e = launch_c2r_pre(s.real, src, dst, stream); break;
             case StepKind::ChirpPre: e = launch_chirp_pre(s.chirp, src, dst, stream); break;
