@@ -130,7 +130,23 @@ class ClockSampler:
 # one), its algorithmic HBM bytes, the number of kernel launches it issues, and a check that returns the rel-L2 of
 # its output against numpy's float64 FFT on a sample.
 
-WORKLOADS = ("mixed", "r2c", "uneven", "nd")
+WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision")
+
+
+WORKLOAD_CONFIGS = {
+    "mixed": {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward",
+              "l2": "inputs 2 GiB per size (> 126 MB L2), no flush needed"},
+    "n1024": {"workload": "c2c_fwd_fp32_N1024_batch4096", "sizes": [[1024, 4096]], "direction": "forward",
+              "l2": "8 input + 8 output buffers rotate (512 MiB)"},
+    "r2c": {"workload": "r2c_c2r_fp32_N1048576_batch512", "sizes": [[1 << 20, 512]],
+            "l2": "2 GiB real input, no flush needed", "flops": "2.5 N log2 N per real transform"},
+    "uneven": {"workload": "uneven_20000_7smooth_16_65536", "transforms": 20000,
+               "l2": "about 2.5 GB moved per step (> 126 MB L2)"},
+    "nd": {"workload": "nd_c2c_fp32_4096x4096_512x512x512", "inputs": "uniform[-1,1) + 1% x 1e4",
+           "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
+    "precision": {"workload": "nd_c2c_4096x4096_512x512x512_fp32_splitbf16_fp16", "inputs": "uniform[-1,1) + 1% x 1e4",
+                  "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
+}
 
 
 class Op:
@@ -149,7 +165,7 @@ def _rel(a, b):
 
 
 def build_mixed(dev, rank, cf):
-    """BASELINE configs[1], C2C part: forward C2C at N in {4096, 65536, 2^20, 107520}, batch filling 2 GiB."""
+    """Large and mixed-radix C2C: forward C2C at N in {4096, 65536, 2^20, 107520}, batch filling 2 GiB."""
     import numpy as np
     import torch
 
@@ -161,26 +177,63 @@ def build_mixed(dev, rank, cf):
     ops = []
     for n, b in SIZES:
         plan = cf.Plan([n], batch=b)
+        info = {"batch": b, "algorithm": plan.info()["algorithm"]}
 
-        def check(n=n, b=b, plan=plan):
+        def check(n=n, b=b, plan=plan, info=info):
             plan.execute(xin[: n * b], xout[: n * b], cf.FORWARD)  # the output buffer is shared: redo this op
             torch.cuda.synchronize()
-            worst = 0.0
+            # round trip of the first and last transforms: forward, then inverse scaled by 1/N
+            inv = cf.Plan([n], batch=1, norm=cf.NORM_INVERSE)
+            back = torch.empty(n, dtype=torch.complex64, device=dev)
+            worst, trip = 0.0, 0.0
             for t in (0, b - 1):
+                inv.execute(xout[t * n:(t + 1) * n], back, cf.INVERSE)
+                torch.cuda.synchronize()
                 x = xin[t * n:(t + 1) * n].cpu().numpy()
                 y = xout[t * n:(t + 1) * n].cpu().numpy()
                 worst = max(worst, _rel(y, np.fft.fft(x.astype(np.complex128))))
+                trip = max(trip, _rel(back.cpu().numpy(), x))
+            info["round_trip_rel_l2"] = trip
             return worst
 
         ops.append(Op(str(n), xin[: n * b], xout[: n * b],
                       lambda i, o, plan=plan: plan.execute(i, o, cf.FORWARD), flops(n, b), algorithmic_bytes(n, b),
-                      plan.info()["passes"], check, {"batch": b, "algorithm": plan.info()["algorithm"]}))
-    return ops, {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward",
-                 "l2": "inputs 2 GiB per size (> 126 MB L2), no flush needed"}
+                      plan.info()["passes"], check, info))
+    return ops, dict(WORKLOAD_CONFIGS["mixed"])
+
+
+def build_n1024(dev, rank, cf):
+    """Plain batched C2C: forward N = 1024, batch 4096, contiguous (64 MiB in + out per execute). Eight input and
+    eight output buffers rotate across steps (512 MiB, four times the 126 MB L2), so no execute finds its input in L2."""
+    import numpy as np
+    import torch
+
+    n, b, ring = 1024, 4096, 8
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED - 1 + rank)
+    ins = [(torch.rand(2 * n * b, generator=gen, device=dev, dtype=torch.float32) * 2 - 1).view(torch.complex64)
+           for _ in range(ring)]
+    outs = [torch.empty(n * b, dtype=torch.complex64, device=dev) for _ in range(ring)]
+    plan = cf.Plan([n], batch=b)
+    state = {"k": 0}
+
+    def run(i, o):
+        k = state["k"] % ring
+        plan.execute(ins[k], outs[k], cf.FORWARD)
+        state["k"] += 1
+
+    def check():
+        plan.execute(ins[0], outs[0], cf.FORWARD)
+        torch.cuda.synchronize()
+        x = ins[0].view(b, n)[:: b // 8].cpu().numpy().astype(np.complex128)
+        return _rel(outs[0].view(b, n)[:: b // 8].cpu().numpy(), np.fft.fft(x, axis=1))
+
+    return [Op("1024", ins[0], outs[0], run, flops(n, b), algorithmic_bytes(n, b), plan.info()["passes"], check,
+               {"batch": b, "algorithm": plan.info()["algorithm"]})], dict(WORKLOAD_CONFIGS["n1024"])
 
 
 def build_r2c(dev, rank, cf):
-    """BASELINE configs[1], real part: R2C and C2R at N = 2^20, batch 512 (2 GiB of real input)."""
+    """Real transforms: R2C and C2R at N = 2^20, batch 512 (2 GiB of real input)."""
     import numpy as np
     import torch
 
@@ -211,12 +264,11 @@ def build_r2c(dev, rank, cf):
               check_r2c, {"batch": b, "algorithm": r2c.info()["algorithm"]}),
            Op("c2r", spec, back, lambda i, o: c2r.execute(i, o, cf.INVERSE), fl, by, c2r.info()["passes"],
               check_c2r, {"batch": b, "algorithm": c2r.info()["algorithm"]})]
-    return ops, {"workload": "r2c_c2r_fp32_N1048576_batch512", "sizes": [[n, b]],
-                 "l2": "2 GiB real input, no flush needed", "flops": "2.5 N log2 N per real transform"}
+    return ops, dict(WORKLOAD_CONFIGS["r2c"])
 
 
 def build_uneven(dev, rank, cf):
-    """20,000 transforms, sizes log-uniform over the 7-smooth integers in [16, 65536], each at
+    """Uneven batch: 20,000 transforms, sizes log-uniform over the 7-smooth integers in [16, 65536], each at
     its own offset of a packed buffer, Gaussian inputs, one persistent graph-captured launch."""
     import numpy as np
     import torch
@@ -245,13 +297,15 @@ def build_uneven(dev, rank, cf):
 
     return [Op("uneven", xin, xout, lambda i, o: plan.execute(i, o, cf.FORWARD), fl, by, 1, check,
                {"transforms": len(sizes), "items": plan.info()["factors"][1], "algorithm": "uneven-batch"})], \
-        {"workload": "uneven_20000_7smooth_16_65536", "transforms": 20000, "size_classes": len(set(sizes)),
-         "l2": f"{by / 2**30:.2f} GiB moved per step (> 126 MB L2)"}
+        dict(WORKLOAD_CONFIGS["uneven"], size_classes=len(set(sizes)))
 
 
-def build_nd(dev, rank, cf):
-    """BASELINE configs[3], FP32 form: 2-D C2C 4096 x 4096 and 3-D C2C 512^3, uniform[-1,1) plus 1% of entries
-    scaled by 1e4. Four input buffers of each shape rotate across steps so the 128 MiB 2-D input is not L2-resident."""
+PRECISIONS = {"fp32": 0, "split-bf16": 1, "fp16-scaled": 2}
+
+
+def _build_nd_forms(dev, rank, cf, forms):
+    """2-D C2C 4096 x 4096 and 3-D C2C 512^3, uniform[-1,1) plus 1% of entries scaled by 1e4, at each precision form
+    in `forms`. Four input buffers of the 2-D shape rotate across steps so its 128 MiB input is not L2-resident."""
     import numpy as np
     import torch
 
@@ -267,27 +321,43 @@ def build_nd(dev, rank, cf):
             x[idx] *= 1e4
             bufs.append(x)
         out = torch.empty(total, dtype=torch.complex64, device=dev)
-        plan = cf.Plan(list(dims), batch=1)
-        state = {"k": 0}
+        want = {}
+        for form in forms:
+            plan = cf.Plan(list(dims), batch=1, precision=PRECISIONS[form])
+            state = {"k": 0}
 
-        def run(i, o, plan=plan, bufs=bufs, state=state):
-            plan.execute(bufs[state["k"] % len(bufs)], o, cf.FORWARD)
-            state["k"] += 1
+            def run(i, o, plan=plan, bufs=bufs, state=state):
+                plan.execute(bufs[state["k"] % len(bufs)], o, cf.FORWARD)
+                state["k"] += 1
 
-        def check(plan=plan, bufs=bufs, out=out, dims=dims):
-            plan.execute(bufs[0], out, cf.FORWARD)
-            torch.cuda.synchronize()
-            x = bufs[0].cpu().numpy().reshape(dims).astype(np.complex128)
-            return _rel(out.cpu().numpy().reshape(dims), np.fft.fftn(x))
+            def check(plan=plan, bufs=bufs, out=out, dims=dims, want=want):
+                plan.execute(bufs[0], out, cf.FORWARD)
+                torch.cuda.synchronize()
+                if "y" not in want:  # the FP64 answer, once per shape
+                    want["y"] = np.fft.fftn(bufs[0].cpu().numpy().reshape(dims).astype(np.complex128))
+                return _rel(out.cpu().numpy().reshape(dims), want["y"])
 
-        name = "x".join(str(d) for d in dims)
-        ops.append(Op(name, bufs[0], out, run, 5.0 * total * math.log2(total), 16 * total, plan.info()["passes"],
-                      check, {"algorithm": plan.info()["algorithm"]}))
-    return ops, {"workload": "nd_c2c_fp32_4096x4096_512x512x512", "inputs": "uniform[-1,1) + 1% x 1e4",
-                 "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"}
+            name = "x".join(str(d) for d in dims) + ("" if forms == ("fp32",) else f"/{form}")
+            ops.append(Op(name, bufs[0], out, run, 5.0 * total * math.log2(total), 16 * total,
+                          plan.info()["passes"], check, {"algorithm": plan.info()["algorithm"], "precision": form}))
+    return ops
 
 
-BUILDERS = {"mixed": build_mixed, "r2c": build_r2c, "uneven": build_uneven, "nd": build_nd}
+def build_nd(dev, rank, cf):
+    """Multi-dimensional C2C at FP32: 2-D 4096 x 4096 and 3-D 512^3."""
+    return _build_nd_forms(dev, rank, cf, ("fp32",)), \
+        dict(WORKLOAD_CONFIGS["nd"])
+
+
+def build_precision(dev, rank, cf):
+    """The same 2-D and 3-D transforms with the first radix-16 stage of each unit-stride pass on the tensor cores
+    (split-BF16: rel-L2 <= 1e-6 against FP64; FP16 with a per-line scale: reported), beside plain FP32."""
+    return _build_nd_forms(dev, rank, cf, tuple(PRECISIONS)), \
+        dict(WORKLOAD_CONFIGS["precision"])
+
+
+BUILDERS = {"mixed": build_mixed, "n1024": build_n1024, "r2c": build_r2c, "uneven": build_uneven, "nd": build_nd,
+            "precision": build_precision}
 
 
 # ---- the reference's CPU implementation (reference arm and cpu_baseline) -------------------------------------------
@@ -351,6 +421,21 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
 
             timed(run, flops(n, count), str(n), rs)
             sample.append(f"N={n} x{count} transforms")
+    elif workload == "n1024":
+        n, batch = 1024, 4096
+        buf = oracle.lcg_complex64(SEED - 1, n * batch)
+        ptr = buf.view(np.float32).ctypes.data_as(fp)
+        sc = np.float32(1.0 / math.sqrt(n))
+
+        def run():
+            if R.crdref_c2c_f32(n, batch, ptr, 0, threads) != 0:
+                raise RuntimeError("crdref_c2c_f32 failed for n=1024")
+
+        def rs():
+            buf[:] *= sc
+
+        timed(run, flops(n, batch), "1024", rs)
+        sample.append(f"N=1024 x{batch} transforms (the whole batch)")
     elif workload == "r2c":
         n = 1 << 20
         count = max(threads, min(512, budget_bytes // (4 * n)))
@@ -391,7 +476,7 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
         timed(run, fl, "uneven", rs)
         sample.append(f"first {len(sizes)} of 20000 transforms ({len(set(sizes))} sizes), per-thread plan cache "
                       "built in the warm-up pass")
-    elif workload == "nd":
+    elif workload in ("nd", "precision"):  # the reference has FP32 only
         for dims in ((4096, 4096), (512, 512, 512)):
             total = int(np.prod(dims))
             x = oracle.lcg_complex64(SEED + total, total)
@@ -424,8 +509,7 @@ def run_reference_arm(args) -> None:
     res = reference_cpu(args.workload, args.steps, args.warmup, budget_bytes=1 << 30)
     value = res["value"]
     ms_per_step = res["seconds"] / args.steps * 1e3
-    config = {"workload": WORKLOAD, "sizes": [[n, b] for n, b in SIZES], "direction": "forward"} \
-        if args.workload == "mixed" else {"workload": args.workload}
+    config = dict(WORKLOAD_CONFIGS[args.workload])
     config["parallelism"] = "host threads"
     line = {
         "impl": "reference",
@@ -603,8 +687,8 @@ def run_ours(args) -> None:
                    "sample": f"unavailable: {exc}"}
 
     if rank == 0:
-        config.update({"precision": "fp32", "placement": "out-of-place", "planner": args.planner,
-                       "parallelism": f"replicas{world}"})
+        config.update({"precision": "per op" if args.workload == "precision" else "fp32",
+                       "placement": "out-of-place", "planner": args.planner, "parallelism": f"replicas{world}"})
         line = {
             "metric": METRIC,
             "value": round(value, 2),
@@ -643,8 +727,9 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=WORKLOADS, default="mixed",
-                    help="mixed (default): configs[1] C2C sizes; r2c: R2C/C2R 2^20; uneven: configs[2]; "
-                         "nd: configs[3] FP32 2-D/3-D")
+                    help="mixed (default): C2C at N 4096/65536/2^20/107520; n1024: N 1024 x 4096; r2c: R2C/C2R 2^20; uneven: 20,000 "
+                         "7-smooth sizes; nd: FP32 2-D 4096^2 / 3-D 512^3; precision: the same 2-D/3-D at FP32, "
+                         "split-BF16 and FP16-scaled")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--planner", choices=["estimate", "measure"], default="measure",
