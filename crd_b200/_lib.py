@@ -32,6 +32,9 @@ C2R = 2
 PREC_FP32 = 0
 PREC_SPLIT_BF16 = 1
 PREC_FP16_SCALED = 2
+PLANNER_ESTIMATE = 0
+PLANNER_MEASURE = 1
+PLANNER_LEARNED = 2
 
 NORM_NONE = 0
 NORM_INVERSE = 1
@@ -69,6 +72,16 @@ EXPORTS = (
     "crdfft_execute_static_scratch",
     "crdfft_plan_create_uneven",
     "crdfft_uneven_offsets",
+    "crdfft_pass_feature_count",
+    "crdfft_learned_model_import",
+    "crdfft_learned_model_export",
+    "crdfft_learned_model_forget",
+    "crdfft_learned_predict",
+    "crdfft_mlp_param_count",
+    "crdfft_mlp_workspace_floats",
+    "crdfft_mlp_forward",
+    "crdfft_mlp_gradients",
+    "crdfft_mlp_adam",
 )
 
 
@@ -151,6 +164,17 @@ def lib():
         "crdfft_execute_static_scratch": ([vp, vp, i64, i64, i32, vp], i32),
         "crdfft_plan_create_uneven": ([ctypes.POINTER(i64), i64, ctypes.POINTER(i64), pp], i32),
         "crdfft_uneven_offsets": ([ctypes.POINTER(i64), i64, ctypes.POINTER(i64)], i64),
+        "crdfft_pass_feature_count": ([], i32),
+        "crdfft_learned_model_import": ([ctypes.c_char_p], i32),
+        "crdfft_learned_model_export": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
+        "crdfft_learned_model_forget": ([], None),
+        "crdfft_learned_predict": ([ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float)], i32),
+        "crdfft_mlp_param_count": ([i32, i32], ctypes.c_size_t),
+        "crdfft_mlp_workspace_floats": ([i32, i32, i64], ctypes.c_size_t),
+        "crdfft_mlp_forward": ([i32, i32, vp, vp, i64, vp, vp, vp], i32),
+        "crdfft_mlp_gradients": ([i32, i32, vp, vp, vp, i64, vp, vp, vp, vp], i32),
+        "crdfft_mlp_adam": ([vp, vp, vp, vp, i64, i32, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                             ctypes.c_float, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

@@ -19,6 +19,7 @@
 #include "kernels.hpp"
 #include "pass_desc.hpp"
 #include "tuner.hpp"
+#include "learned.hpp"
 #include "uneven.hpp"
 
 #include <cuda_runtime.h>
@@ -504,11 +505,42 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
             return true;
         }
     }
-    if (planner_mode() == kPlannerMeasure && t_arena == nullptr) // measuring allocates scratch: never from an arena
+    const int mode = planner_mode();
+    if (mode == kPlannerLearned && learned_ready())
+    {
+        // rank the candidates by predicted time; nothing is timed and nothing is remembered
+        const std::vector<PassShape> cands = candidate_shapes(d, map, dl, ds);
+        int best = -1;
+        float best_t = 0.0f;
+        for (size_t i = 0; i < cands.size(); ++i)
+        {
+            float f[kPassFeatures];
+            pass_features(d, cands[i], f);
+            const float t = learned_predict(f);
+            if (best < 0 || t < best_t)
+            {
+                best = static_cast<int>(i);
+                best_t = t;
+            }
+        }
+        if (best >= 0)
+        {
+            *out = cands[best];
+            return true;
+        }
+    }
+    if (mode == kPlannerMeasure && t_arena == nullptr) // measuring allocates scratch: never from an arena
     {
         const std::vector<PassShape> cands = candidate_shapes(d, map, dl, ds);
         std::vector<float> ms;
-        const int best = measure_shapes(d, key, cands, &ms);
+        int heur = -1;
+        PassShape hs;
+        if (heuristic_shape(d, map, dl, ds, &hs))
+            for (size_t i = 0; i < cands.size(); ++i)
+                if (cands[i].pipelined == hs.pipelined && cands[i].points_per_thread == hs.points_per_thread &&
+                    cands[i].lines_per_cta == hs.lines_per_cta)
+                    heur = static_cast<int>(i);
+        const int best = measure_shapes(d, key, cands, &ms, heur);
         if (best >= 0)
         {
             WisdomEntry e;
@@ -1033,8 +1065,33 @@ crdfft_status build_nd(Plan& p)
         total *= d.dims[i];
     const long long idist = d.idist ? d.idist : total;
     const long long odist = d.odist ? d.odist : total;
-    if (idist != total || odist != total || d.istride > 1 || d.ostride > 1)
+    if (idist < total || odist < total || d.istride > 1 || d.ostride > 1)
         return CRDFFT_UNSUPPORTED_SIZE;
+    // The lines of one axis as groups of lpg lines. Packed batches: the classic maps. Padded batches (a distance
+    // above the transform's size) need each group inside one batch member: the last axis (groups = batch members,
+    // lines n apart) and the first (groups = batch members, lines adjacent); a middle axis of a padded 3-D batch has
+    // no such map.
+    auto axis_map = [&](int ax, long long n, long long st_ax, long long dist, LineMap* m, long long* lpg) {
+        if (dist == total)
+        {
+            *m = st_ax == 1 ? LineMap{n, 0, 1} : LineMap{n * st_ax, 1, st_ax};
+            *lpg = st_ax == 1 ? 1 : st_ax;
+            return true;
+        }
+        if (st_ax == 1)
+        {
+            *m = LineMap{dist, n, 1};
+            *lpg = total / n;
+            return true;
+        }
+        if (ax == 0)
+        {
+            *m = LineMap{dist, 1, st_ax};
+            *lpg = st_ax;
+            return true;
+        }
+        return false;
+    };
     const float inv_scale =
         d.norm == CRDFFT_NORM_INVERSE ? static_cast<float>(1.0 / static_cast<double>(total)) : 1.0f;
     for (int dir = 0; dir < 2; ++dir)
@@ -1057,12 +1114,15 @@ crdfft_status build_nd(Plan& p)
             for (int j = ax + 1; j < rank; ++j)
                 st_ax *= d.dims[j];
             const long long lines = d.batch * (total / n);
-            LineMap m = st_ax == 1 ? LineMap{n, 0, 1} : LineMap{n * st_ax, 1, st_ax};
-            const long long lpg = st_ax == 1 ? 1 : st_ax;
+            LineMap mi, mo;
+            long long lpg = 1, lpg_o = 1;
+            if (!axis_map(ax, n, st_ax, first ? idist : odist, &mi, &lpg) ||
+                !axis_map(ax, n, st_ax, odist, &mo, &lpg_o) || lpg != lpg_o)
+                return CRDFFT_UNSUPPORTED_SIZE;
             const bool is_last = ax == last_axis;
             Step s;
             const crdfft_status st =
-                make_line_step(p, n, lines, lpg, m, m, first ? BufRef{Buf::In, 0} : BufRef{Buf::Out, 0},
+                make_line_step(p, n, lines, lpg, mi, mo, first ? BufRef{Buf::In, 0} : BufRef{Buf::Out, 0},
                                BufRef{Buf::Out, 0}, dir == 1 && first, dir == 1 && is_last,
                                (dir == 1 && is_last) ? inv_scale : 1.0f, &s);
             if (st != CRDFFT_OK)
@@ -1074,6 +1134,8 @@ crdfft_status build_nd(Plan& p)
         {
             // every axis has length 1: a copy with the inverse's scale
             Step s;
+            if (idist != total || odist != total)
+                return CRDFFT_UNSUPPORTED_SIZE;
             const crdfft_status st = make_line_step(p, 1, d.batch * total, 1, LineMap{1, 0, 1}, LineMap{1, 0, 1},
                                                     BufRef{Buf::In, 0}, BufRef{Buf::Out, 0}, false, false,
                                                     dir == 1 ? inv_scale : 1.0f, &s);
@@ -1854,6 +1916,32 @@ void crdfft_wisdom_forget(void) { wisdom_forget(); }
 crdfft_status crdfft_planner_log(char* buf, size_t cap, size_t* needed)
 {
     return copy_out(planner_log_export(), buf, cap, needed);
+}
+
+int32_t crdfft_pass_feature_count(void) { return kPassFeatures; }
+
+crdfft_status crdfft_learned_model_import(const char* text)
+{
+    if (text == nullptr)
+        return CRDFFT_INVALID_ARG;
+    return learned_import(text) < 0 ? CRDFFT_INVALID_ARG : CRDFFT_OK;
+}
+
+crdfft_status crdfft_learned_model_export(char* buf, size_t cap, size_t* needed)
+{
+    return copy_out(learned_export(), buf, cap, needed);
+}
+
+void crdfft_learned_model_forget(void) { learned_forget(); }
+
+crdfft_status crdfft_learned_predict(const float* features, float* out)
+{
+    if (features == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    if (!learned_ready())
+        return CRDFFT_INVALID_ARG;
+    *out = learned_predict(features);
+    return CRDFFT_OK;
 }
 
 crdfft_status crdfft_device_status(crdfft_plan* plan, void* stream)

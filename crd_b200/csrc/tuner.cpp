@@ -3,6 +3,7 @@
 #include "tuner.hpp"
 
 #include "kernels.hpp"
+#include "learned.hpp"
 
 #include <cuda_runtime.h>
 
@@ -65,13 +66,18 @@ int planner_mode()
     if (m < 0)
     {
         const char* e = std::getenv("CRDFFT_PLANNER");
-        m = (e != nullptr && std::strcmp(e, "measure") == 0) ? kPlannerMeasure : kPlannerEstimate;
+        m = (e != nullptr && std::strcmp(e, "measure") == 0)   ? kPlannerMeasure
+            : (e != nullptr && std::strcmp(e, "learned") == 0) ? kPlannerLearned
+                                                                : kPlannerEstimate;
         g_mode.store(m);
     }
     return m;
 }
 
-void set_planner_mode(int mode) { g_mode.store(mode == kPlannerMeasure ? kPlannerMeasure : kPlannerEstimate); }
+void set_planner_mode(int mode)
+{
+    g_mode.store(mode == kPlannerMeasure ? kPlannerMeasure : mode == kPlannerLearned ? kPlannerLearned : kPlannerEstimate);
+}
 
 std::string pass_key(const PassDesc& d, PassMap map, bool dl, bool ds)
 {
@@ -156,7 +162,7 @@ std::string planner_log_export()
 }
 
 int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector<PassShape>& cands,
-                   std::vector<float>* ms)
+                   std::vector<float>* ms, int heuristic)
 {
     ms->assign(cands.size(), -1.0f);
     if (cands.empty())
@@ -222,10 +228,23 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
         for (size_t i = 0; i < cands.size(); ++i)
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d lines=%lld ms=%.6f%s\n", key.c_str(),
+            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d lines=%lld ms=%.6f", key.c_str(),
                           cands[i].pipelined ? 1 : 0, cands[i].points_per_thread, cands[i].lines_per_cta, d0.lines,
-                          static_cast<double>((*ms)[i]), static_cast<int>(i) == best ? " best" : "");
+                          static_cast<double>((*ms)[i]));
             g_log += buf;
+            float f[kPassFeatures];
+            pass_features(d0, cands[i], f);
+            g_log += " feat=";
+            for (int k = 0; k < kPassFeatures; ++k)
+            {
+                std::snprintf(buf, sizeof(buf), k ? ",%.6g" : "%.6g", static_cast<double>(f[k]));
+                g_log += buf;
+            }
+            if (static_cast<int>(i) == best)
+                g_log += " best";
+            if (static_cast<int>(i) == heuristic)
+                g_log += " heur";
+            g_log += '\n';
         }
     }
     return best;

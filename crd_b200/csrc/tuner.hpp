@@ -18,6 +18,7 @@ enum PlannerMode : int
 {
     kPlannerEstimate = 0, // wisdom if present, else the heuristic
     kPlannerMeasure = 1,  // wisdom if present, else time every candidate and remember the fastest
+    kPlannerLearned = 2,  // wisdom if present, else the candidate the learned cost model ranks first
 };
 
 int planner_mode();
@@ -44,8 +45,9 @@ void wisdom_forget();
 // Times each candidate (1 warm-up, min of 3 launches, CUDA events) on scratch buffers sized for up to 64 MiB of
 // the pass's lines; returns the index of the fastest, or -1 if none could run. ms receives each candidate's time
 // (or a negative value when it failed). Appends every timing to the planner log.
+// `heuristic` is the index of the heuristic's own choice among the candidates (or -1), marked in the log.
 int measure_shapes(const PassDesc& d, const std::string& key, const std::vector<PassShape>& cands,
-                   std::vector<float>* ms);
+                   std::vector<float>* ms, int heuristic = -1);
 std::string planner_log_export();
 
 } // namespace crdfft

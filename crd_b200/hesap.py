@@ -293,12 +293,14 @@ def self_check() -> None:
 
 PLANNER_ESTIMATE = 0
 PLANNER_MEASURE = 1
+PLANNER_LEARNED = 2
 
 
 def set_planner(mode) -> None:
-    """CRDFFT_PLANNER_ESTIMATE (0, default) or CRDFFT_PLANNER_MEASURE (1); "estimate"/"measure" also accepted."""
+    """CRDFFT_PLANNER_ESTIMATE (0, default), CRDFFT_PLANNER_MEASURE (1) or CRDFFT_PLANNER_LEARNED (2);
+    "estimate"/"measure"/"learned" also accepted."""
     if isinstance(mode, str):
-        mode = {"estimate": PLANNER_ESTIMATE, "measure": PLANNER_MEASURE}[mode]
+        mode = {"estimate": PLANNER_ESTIMATE, "measure": PLANNER_MEASURE, "learned": PLANNER_LEARNED}[mode]
     lib().crdfft_set_planner_mode(int(mode))
 
 
@@ -324,6 +326,30 @@ def wisdom_forget() -> None:
 
 def planner_log() -> str:
     return _text(lib().crdfft_planner_log)
+
+
+def learned_model_import(text: str) -> None:
+    """Load the learned cost model (crdfft_learned_model_import); CRDFFT_PLANNER_LEARNED plans rank with it."""
+    check(lib().crdfft_learned_model_import(text.encode()), "learned_model_import")
+
+
+def learned_model_export() -> str:
+    return _text(lib().crdfft_learned_model_export)
+
+
+def learned_model_forget() -> None:
+    lib().crdfft_learned_model_forget()
+
+
+def learned_predict(features) -> float:
+    """The imported model's predicted log(ms) for one feature vector (host evaluation)."""
+    n = lib().crdfft_pass_feature_count()
+    if len(features) != n:
+        raise ValueError(f"expected {n} features")
+    arr = (ctypes.c_float * n)(*[float(v) for v in features])
+    out = ctypes.c_float(0.0)
+    check(lib().crdfft_learned_predict(arr, ctypes.byref(out)), "learned_predict")
+    return float(out.value)
 
 
 def device_status(plan: _Handle, stream=None) -> None:

@@ -183,6 +183,9 @@ int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offs
  * initial mode. Once a pass class has wisdom, every later plan of that class makes the same choice. */
 #define CRDFFT_PLANNER_ESTIMATE 0
 #define CRDFFT_PLANNER_MEASURE 1
+/*   CRDFFT_PLANNER_LEARNED   remembered wisdom, else the candidate with the lowest cost predicted by the imported
+ *                            learned model (crdfft_learned_model_import), else the heuristic. Nothing is timed. */
+#define CRDFFT_PLANNER_LEARNED 2
 void crdfft_set_planner_mode(int32_t mode);
 
 /* Wisdom as text ("crdfft-wisdom 1" then one line per pass class: key, pipelined, points a thread, lines a CTA,
@@ -193,8 +196,41 @@ crdfft_status crdfft_wisdom_import(const char* text);
 void crdfft_wisdom_forget(void);
 
 /* Every timing the measuring planner took in this process, one line per candidate ("<key> pipelined=.. P=.. lpc=..
- * lines=.. ms=..", the winner marked "best"): the training data of the learned cost model. */
+ * lines=.. ms=.. feat=f0,..,f31", the winner marked "best", the heuristic's own choice marked "heur"): the training
+ * data of the learned cost model. crdfft_wisdom_forget clears it too. */
 crdfft_status crdfft_planner_log(char* buf, size_t cap, size_t* needed);
+
+/* ---- Learned cost model -------------------------------------------------------------------------------------- */
+
+/* No counterpart in the reference (its planner reads a board of per-level winners measured offline,
+ * detail/level_plans_gen.hpp:33-148). A 3-layer MLP (FP32, ReLU) predicts the log-time of a pass under a candidate
+ * launch shape from a feature vector of crdfft_pass_feature_count() floats (the "feat=" field of the planner log).
+ * The model text is "crdfft-mlp 1", then "dims D H", "mean" and "std" (D feature normalisers each), "target m s"
+ * (log(ms) = m + s * output) and "params P" followed by the P parameters of crdfft_mlp_param_count's layout.
+ * Import rejects a malformed text (CRDFFT_INVALID_ARG) and keeps the current model. */
+int32_t crdfft_pass_feature_count(void);
+crdfft_status crdfft_learned_model_import(const char* text);
+crdfft_status crdfft_learned_model_export(char* buf, size_t cap, size_t* needed);
+void crdfft_learned_model_forget(void);
+/* Host evaluation of the imported model on one feature vector: predicted log(ms) in *out. */
+crdfft_status crdfft_learned_predict(const float* features, float* out);
+
+/* Device kernels that train the model (no library call, no floating-point atomics: bit-reproducible). Every pointer
+ * is device memory; parameters are one flat array [W1 (H x D)][b1 (H)][W2 (H x H)][b2 (H)][W3 (H)][b3 (1)],
+ * weights row-major (out x in); x is rows x D row-major (already normalised); workspace holds
+ * crdfft_mlp_workspace_floats(D, H, rows) floats. */
+size_t crdfft_mlp_param_count(int32_t in_dim, int32_t hidden);
+size_t crdfft_mlp_workspace_floats(int32_t in_dim, int32_t hidden, int64_t rows);
+/* y[rows] = W3 relu(W2 relu(W1 x + b1) + b2) + b3 */
+crdfft_status crdfft_mlp_forward(int32_t in_dim, int32_t hidden, const float* params, const float* x, int64_t rows,
+                                 float* y, float* workspace, void* stream);
+/* loss[0] = mean((y - target)^2) and grad = d loss / d params (same layout as params). */
+crdfft_status crdfft_mlp_gradients(int32_t in_dim, int32_t hidden, const float* params, const float* x,
+                                   const float* target, int64_t rows, float* grad, float* loss, float* workspace,
+                                   void* stream);
+/* One Adam step (bias-corrected moments, step >= 1) over count parameters. */
+crdfft_status crdfft_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t count, int32_t step,
+                              float lr, float beta1, float beta2, float eps, void* stream);
 
 /* ---- Without device allocation ----------------------------------------------------------------------------- */
 

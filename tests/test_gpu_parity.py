@@ -408,3 +408,23 @@ def test_uneven_dependency_wait_times_out():
     ys = y.cpu().numpy()
     for n, o in zip(sizes, good.offsets):
         _check(ys[o:o + n], oracle.fft64(xs[o:o + n]), n)
+
+
+@pytest.mark.parametrize("dims", [(24, 40), (375, 280), (64, 4096)])
+def test_nd_padded_batch_distances(dims):
+    """2-D batches whose members sit a padded distance apart (idist, odist above the transform size): each member
+    transforms on its own, and the padding of the output is left as it was."""
+    total = int(np.prod(dims))
+    batch, idist, odist = 3, total + 8, total + 12
+    x = oracle.lcg_complex64(0xADD ^ total, batch * idist)
+    for inverse in (False, True):
+        t = torch.from_numpy(x.copy()).cuda()
+        o = torch.full((batch * odist,), 7 + 7j, dtype=torch.complex64, device="cuda")
+        plan = cf.Plan(list(dims), batch=batch, idist=idist, odist=odist, norm=cf.NORM_INVERSE)
+        plan.execute(t, o, cf.INVERSE if inverse else cf.FORWARD)
+        torch.cuda.synchronize()
+        got = o.cpu().numpy()
+        for b in range(batch):
+            xb = x[b * idist:b * idist + total].reshape(dims)
+            _check(got[b * odist:b * odist + total].reshape(dims), oracle.nd64(xb, inverse), max(dims))
+            assert np.all(got[b * odist + total:(b + 1) * odist] == 7 + 7j)
