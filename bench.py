@@ -536,6 +536,24 @@ def run_reference_arm(args) -> None:
 # ---- our arm ---------------------------------------------------------------------------------------------------
 
 
+def max_over_ranks_of(v: float, world: int, device) -> float:
+    """The largest of a per-rank value over the job's ranks (the slowest rank's time is the job's time)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank_step: float, steps: int, world: int, total_ms: float) -> float:
+    """Whole-job rate per second: every rank runs its own replica of the per-GPU workload (weak scaling), so the job
+    processes world times one rank's units in the slowest rank's time."""
+    return units_per_rank_step * steps * world / (total_ms / 1e3)
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -558,11 +576,7 @@ def run_ours(args) -> None:
             dist.barrier()
 
     def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return max_over_ranks_of(v, world, dev)
 
     if args.wisdom and os.path.exists(args.wisdom):
         with open(args.wisdom) as f:
@@ -619,7 +633,7 @@ def run_ours(args) -> None:
               for i in range(len(ops))]
     step_flops = sum(op.flops for op in ops)
     step_bytes = sum(op.bytes for op in ops)
-    value = step_flops * args.steps * world / (total_ms / 1e3) / 1e9
+    value = job_rate(step_flops, args.steps, world, total_ms) / 1e9
     ms_per_step = total_ms / args.steps
 
     rel = {op.name: op.check() for op in ops}
@@ -672,7 +686,7 @@ def run_ours(args) -> None:
         e_ms = max_over_ranks(e0.elapsed_time(e1))
         h2d = sum(op.inp.numel() * op.inp.element_size() for op in ops)
         d2h = sum(op.out.numel() * op.out.element_size() for op in ops)
-        e2e = {"value": round(step_flops * e_steps * world / (e_ms / 1e3) / 1e9, 2), "unit": "GFLOP/s",
+        e2e = {"value": round(job_rate(step_flops, e_steps, world, e_ms) / 1e9, 2), "unit": "GFLOP/s",
                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e_steps,
                "ms_per_step": round(e_ms / e_steps, 3)}
 
