@@ -44,6 +44,7 @@ EXPORTS = (
     "crdfft_plan_create",
     "crdfft_plan_destroy",
     "crdfft_execute",
+    "crdfft_execute_host",
     "crdfft_plan_info_get",
     "crdfft_workspace_size",
     "crdfft_set_workspace",
@@ -136,6 +137,7 @@ def lib():
         "crdfft_plan_create": ([ctypes.POINTER(Desc), pp], i32),
         "crdfft_plan_destroy": ([vp], i32),
         "crdfft_execute": ([vp, vp, vp, i32, vp], i32),
+        "crdfft_execute_host": ([vp, vp, vp, i32, vp], i32),
         "crdfft_plan_info_get": ([vp, ctypes.POINTER(PlanInfo)], i32),
         "crdfft_workspace_size": ([vp], ctypes.c_size_t),
         "crdfft_set_workspace": ([vp, vp, ctypes.c_size_t], i32),

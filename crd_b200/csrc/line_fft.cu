@@ -13,6 +13,7 @@ namespace lfft
 {
 // The compile-time schedules (one translation unit each, sched_*.cu).
 KernelFn s_1024_classic(const PassDesc&, const PassShape&);
+KernelFn s_1024w_classic(const PassDesc&, const PassShape&);
 KernelFn s_256_classic(const PassDesc&, const PassShape&);
 KernelFn s_512_classic(const PassDesc&, const PassShape&);
 KernelFn s_4096_classic(const PassDesc&, const PassShape&);
@@ -27,8 +28,8 @@ PipeFn s_105_pipe(const PassDesc&, const PassShape&);
 
 KernelFn select_static(const PassDesc& d, const PassShape& sh)
 {
-    for (auto f : {s_1024_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic, s_16384_classic,
-                   s_105_classic})
+    for (auto f : {s_1024_classic, s_1024w_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic,
+                   s_16384_classic, s_105_classic})
         if (KernelFn k = f(d, sh))
             return k;
     return nullptr;

@@ -249,9 +249,40 @@ struct Plan
     int usmem = 0;
     std::map<std::tuple<const void*, void*, int>, cudaGraphExec_t> graphs;
     std::mutex graphs_mu;
+    // Host-buffer execute (crdfft_execute_host): chunk plans, staging buffers and streams, made by the first call.
+    struct HostPipe
+    {
+        long long chunk = 0;             // transforms a chunk
+        Plan* full = nullptr;            // plan of `chunk` transforms
+        Plan* tail = nullptr;            // plan of the last, shorter chunk (or null)
+        void* din[2] = {nullptr, nullptr};
+        void* dout[2] = {nullptr, nullptr};
+        cudaStream_t st[2] = {nullptr, nullptr};
+        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    };
+    HostPipe* host = nullptr;
+    std::mutex host_mu;
 
     ~Plan()
     {
+        if (host != nullptr)
+        {
+            for (int i = 0; i < 2; ++i)
+            {
+                if (host->st[i] != nullptr)
+                    cudaStreamSynchronize(host->st[i]);
+                cudaFree(host->din[i]);
+                cudaFree(host->dout[i]);
+                if (host->st[i] != nullptr)
+                    cudaStreamDestroy(host->st[i]);
+            }
+            for (cudaEvent_t e : host->ev)
+                if (e != nullptr)
+                    cudaEventDestroy(e);
+            delete host->full;
+            delete host->tail;
+            delete host;
+        }
         for (auto& kv : graphs)
             cudaGraphExecDestroy(kv.second);
         for (auto& kv : batched)
@@ -1600,6 +1631,125 @@ crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32
         (p.desc.kind == CRDFFT_C2R && direction != CRDFFT_INVERSE))
         return CRDFFT_INVALID_ARG;
     return run(p, in, out, direction, static_cast<cudaStream_t>(stream));
+}
+
+namespace
+{
+
+// Element sizes and per-transform extents (elements) of a plan's input and output, and its transform distances.
+struct HostLayout
+{
+    size_t in_elem, out_elem;
+    long long in_ext, out_ext, idist, odist;
+};
+
+bool host_layout(const crdfft_desc& d, HostLayout* L)
+{
+    if ((d.istride != 0 && d.istride != 1) || (d.ostride != 0 && d.ostride != 1))
+        return false;
+    long long total = 1;
+    for (int i = 0; i < d.rank; ++i)
+        total *= d.dims[i];
+    const long long half = total / 2 + 1;
+    L->in_elem = d.kind == CRDFFT_R2C ? 4 : 8;
+    L->out_elem = d.kind == CRDFFT_C2R ? 4 : 8;
+    L->in_ext = d.kind == CRDFFT_C2R ? half : total;
+    L->out_ext = d.kind == CRDFFT_R2C ? half : total;
+    L->idist = d.idist ? d.idist : L->in_ext;
+    L->odist = d.odist ? d.odist : L->out_ext;
+    return true;
+}
+
+crdfft_status host_pipe_setup(Plan& p, const HostLayout& L)
+{
+    std::unique_ptr<Plan::HostPipe> h(new Plan::HostPipe());
+    const long long per = std::max<long long>(1, static_cast<long long>(L.in_elem) * L.idist);
+    h->chunk = std::max<long long>(1, std::min<long long>(p.desc.batch, (64LL << 20) / per));
+    crdfft_desc cd = p.desc;
+    cd.batch = h->chunk;
+    crdfft_status st = create(&cd, &h->full);
+    if (st != CRDFFT_OK)
+        return st;
+    const long long rest = p.desc.batch % h->chunk;
+    if (rest != 0 && p.desc.batch > h->chunk)
+    {
+        cd.batch = rest;
+        st = create(&cd, &h->tail);
+        if (st != CRDFFT_OK)
+        {
+            delete h->full;
+            return st;
+        }
+    }
+    const size_t in_bytes = static_cast<size_t>((h->chunk - 1) * L.idist + L.in_ext) * L.in_elem;
+    const size_t out_bytes = static_cast<size_t>((h->chunk - 1) * L.odist + L.out_ext) * L.out_elem;
+    bool ok = true;
+    for (int i = 0; i < 2 && ok; ++i)
+        ok = dev_alloc(&h->din[i], in_bytes) == cudaSuccess && dev_alloc(&h->dout[i], out_bytes) == cudaSuccess &&
+             cudaStreamCreateWithFlags(&h->st[i], cudaStreamNonBlocking) == cudaSuccess;
+    for (int i = 0; i < 3 && ok; ++i)
+        ok = cudaEventCreateWithFlags(&h->ev[i], cudaEventDisableTiming) == cudaSuccess;
+    p.host = h.release();
+    return ok ? CRDFFT_OK : CRDFFT_OOM;
+}
+
+} // namespace
+
+crdfft_status crdfft_execute_host(crdfft_plan* plan, const void* in, void* out, int32_t direction, void* stream)
+{
+    if (plan == nullptr || in == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    if (direction != CRDFFT_FORWARD && direction != CRDFFT_INVERSE)
+        return CRDFFT_INVALID_ARG;
+    if ((p.desc.kind == CRDFFT_R2C && direction != CRDFFT_FORWARD) ||
+        (p.desc.kind == CRDFFT_C2R && direction != CRDFFT_INVERSE))
+        return CRDFFT_INVALID_ARG;
+    HostLayout L{};
+    if (p.uneven || !host_layout(p.desc, &L))
+        return CRDFFT_INVALID_ARG;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != p.device)
+        return CRDFFT_NO_DEVICE;
+    std::lock_guard<std::mutex> lk(p.host_mu);
+    if (p.host == nullptr)
+    {
+        const crdfft_status st = host_pipe_setup(p, L);
+        if (st != CRDFFT_OK)
+            return st;
+    }
+    Plan::HostPipe& h = *p.host;
+    if (h.st[1] == nullptr || h.ev[2] == nullptr)
+        return CRDFFT_OOM;
+    const cudaStream_t user = static_cast<cudaStream_t>(stream);
+    // the internal streams start after the work already on the caller's stream
+    if (cudaEventRecord(h.ev[2], user) != cudaSuccess || cudaStreamWaitEvent(h.st[0], h.ev[2], 0) != cudaSuccess ||
+        cudaStreamWaitEvent(h.st[1], h.ev[2], 0) != cudaSuccess)
+        return CRDFFT_LAUNCH;
+    const char* hin = static_cast<const char*>(in);
+    char* hout = static_cast<char*>(out);
+    int k = 0;
+    for (long long t0 = 0; t0 < p.desc.batch; t0 += h.chunk, k ^= 1)
+    {
+        const long long c = std::min(h.chunk, p.desc.batch - t0);
+        Plan* cp = c == h.chunk ? h.full : h.tail;
+        const size_t ib = static_cast<size_t>((c - 1) * L.idist + L.in_ext) * L.in_elem;
+        const size_t ob = static_cast<size_t>((c - 1) * L.odist + L.out_ext) * L.out_elem;
+        if (cudaMemcpyAsync(h.din[k], hin + static_cast<size_t>(t0 * L.idist) * L.in_elem, ib, cudaMemcpyHostToDevice,
+                            h.st[k]) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        const crdfft_status st = run(*cp, h.din[k], h.dout[k], direction, h.st[k]);
+        if (st != CRDFFT_OK)
+            return st;
+        if (cudaMemcpyAsync(hout + static_cast<size_t>(t0 * L.odist) * L.out_elem, h.dout[k], ob,
+                            cudaMemcpyDeviceToHost, h.st[k]) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+    }
+    // the caller's stream waits for both internal streams
+    for (int i = 0; i < 2; ++i)
+        if (cudaEventRecord(h.ev[i], h.st[i]) != cudaSuccess || cudaStreamWaitEvent(user, h.ev[i], 0) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+    return CRDFFT_OK;
 }
 
 crdfft_status crdfft_plan_info_get(const crdfft_plan* plan, crdfft_plan_info* info)

@@ -132,6 +132,18 @@ class Plan(_Handle):
         check(lib().crdfft_execute(self._h, pi, po, _dir(direction), _stream(stream)), "execute")
         return out
 
+    def execute_host(self, inp: torch.Tensor, out: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
+        """Run on HOST tensors (pinned for overlap; crdfft_execute_host): chunked copies in and out overlap the
+        transforms on the GPU. Synchronise `stream` (default: the current stream) before reading `out`."""
+        in_dtype = torch.float32 if self.kind == R2C else torch.complex64
+        out_dtype = torch.float32 if self.kind == C2R else torch.complex64
+        for t, dt, what in ((inp, in_dtype, "input"), (out, out_dtype, "output")):
+            if t.is_cuda or t.dtype != dt or not t.is_contiguous():
+                raise ValueError(f"{what} must be a contiguous host tensor of {dt}")
+        check(lib().crdfft_execute_host(self._h, inp.data_ptr(), out.data_ptr(), _dir(direction), _stream(stream)),
+              "execute_host")
+        return out
+
 
 class FftPlan(_Handle):
     """FftPlan<float>(alloc, n) - one size-n complex transform (fft.hpp:224)."""
