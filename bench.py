@@ -130,7 +130,7 @@ class ClockSampler:
 # one), its algorithmic HBM bytes, the number of kernel launches it issues, and a check that returns the rel-L2 of
 # its output against numpy's float64 FFT on a sample.
 
-WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision")
+WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision", "conv")
 
 
 WORKLOAD_CONFIGS = {
@@ -144,6 +144,8 @@ WORKLOAD_CONFIGS = {
                "l2": "about 2.5 GB moved per step (> 126 MB L2)"},
     "nd": {"workload": "nd_c2c_fp32_4096x4096_512x512x512", "inputs": "uniform[-1,1) + 1% x 1e4",
            "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
+    "conv": {"workload": "fused_conv_1d_N256_1024_4096_2^25_points", "filter": "one spectrum shared by the batch",
+             "l2": "256 MiB input per size (> 126 MB L2)", "flops": "10 N log2 N + 6 N per signal"},
     "precision": {"workload": "nd_c2c_4096x4096_512x512x512_fp32_splitbf16_fp16", "inputs": "uniform[-1,1) + 1% x 1e4",
                   "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
 }
@@ -157,6 +159,8 @@ class Op:
         # host(hin, hout): the same op on host buffers through the library's host-memory execute, or None (the
         # end-to-end leg then copies in, runs and copies out itself)
         self.host = host
+        # peer: (name, callable) running the vendor library's route for the same op on the same data, timed beside it
+        self.peer = None
 
 
 def _rel(a, b):
@@ -356,6 +360,42 @@ def build_nd(dev, rank, cf):
         dict(WORKLOAD_CONFIGS["nd"])
 
 
+CONV_SIZES = (256, 1024, 4096)
+CONV_POINTS = 1 << 25  # per size: 256 MiB of complex64 input (> 126 MB L2)
+
+
+def build_conv(dev, rank, cf):
+    """Fused FFT convolution, y = IFFT(FFT(x) * H) / N, batched 1-D at N in {256, 1024, 4096} over 2^25 points each,
+    one spectrum shared by the batch; beside it the vendor route (cuFFT through torch.fft: forward FFT, elementwise
+    product, inverse FFT: three global passes) on the same buffers."""
+    import numpy as np
+    import torch
+
+    ops = []
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 11 + rank)
+    xin = (torch.rand(2 * CONV_POINTS, generator=gen, device=dev, dtype=torch.float32) * 2 - 1).view(torch.complex64)
+    xout = torch.empty(CONV_POINTS, dtype=torch.complex64, device=dev)
+    for n in CONV_SIZES:
+        b = CONV_POINTS // n
+        plan = cf.ConvPlan([n], batch=b)
+        H = (torch.rand(2 * n, generator=gen, device=dev, dtype=torch.float32) * 2 - 1).view(torch.complex64)
+
+        def check(n=n, b=b, plan=plan, H=H):
+            plan.execute(xin, H, xout)
+            torch.cuda.synchronize()
+            x = xin.view(b, n)[:: b // 4].cpu().numpy().astype(np.complex128)
+            want = np.fft.ifft(np.fft.fft(x, axis=1) * H.cpu().numpy().astype(np.complex128), axis=1)
+            return _rel(xout.view(b, n)[:: b // 4].cpu().numpy(), want)
+
+        op = Op(f"conv{n}", xin, xout, lambda i, o, plan=plan, H=H: plan.execute(i, H, o),
+                b * (10.0 * n * math.log2(n) + 6.0 * n), 16 * n * b, 1, check,
+                {"batch": b, "algorithm": plan.info()["algorithm"]})
+        op.peer = ("cufft_3pass", lambda n=n, b=b, H=H: torch.fft.ifft(torch.fft.fft(xin.view(b, n)) * H))
+        ops.append(op)
+    return ops, dict(WORKLOAD_CONFIGS["conv"])
+
+
 def build_precision(dev, rank, cf):
     """The same 2-D and 3-D transforms with the first radix-16 stage of each unit-stride pass on the tensor cores
     (split-BF16: rel-L2 <= 1e-6 against FP64; FP16 with a per-line scale: reported), beside plain FP32."""
@@ -364,7 +404,7 @@ def build_precision(dev, rank, cf):
 
 
 BUILDERS = {"mixed": build_mixed, "n1024": build_n1024, "r2c": build_r2c, "uneven": build_uneven, "nd": build_nd,
-            "precision": build_precision}
+            "precision": build_precision, "conv": build_conv}
 
 
 # ---- the reference's CPU implementation (reference arm and cpu_baseline) -------------------------------------------
@@ -443,6 +483,23 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
 
         timed(run, flops(n, batch), "1024", rs)
         sample.append(f"N=1024 x{batch} transforms (the whole batch)")
+    elif workload == "conv":
+        # the reference's CPU route to the same result: FftPlan forward, the product, FftPlan inverse and 1/N
+        for n in CONV_SIZES:
+            count = max(threads, min(CONV_POINTS // n, budget_bytes // (8 * n)))
+            buf = oracle.lcg_complex64(SEED ^ (n + 11), n * count)
+            H = oracle.lcg_complex64(SEED ^ (n + 12), n)
+            ptr = buf.view(np.float32).ctypes.data_as(fp)
+
+            def run(n=n, count=count, buf=buf, ptr=ptr, H=H):
+                R.crdref_c2c_f32(n, count, ptr, 0, threads)
+                v = buf.reshape(count, n)
+                v *= H
+                R.crdref_c2c_f32(n, count, ptr, 1, threads)
+                v *= np.float32(1.0 / n)
+
+            timed(run, count * (10.0 * n * math.log2(n) + 6.0 * n), f"conv{n}")
+            sample.append(f"conv N={n} x{count}")
     elif workload == "r2c":
         n = 1 << 20
         count = max(threads, min(512, budget_bytes // (4 * n)))
@@ -662,6 +719,20 @@ def run_ours(args) -> None:
         per[op.name] = dict(op.info, launches=op.launches, ms=round(ms, 4),
                             gflops=round(op.flops / (ms / 1e3) / 1e9, 1), hbm_gbs=round(gbs, 1),
                             hbm_frac=round(gbs / peaks["hbm_gbs"], 4), rel_l2_vs_fp64=rel[op.name])
+        if op.peer is not None:
+            # the vendor route for the same op, same data, same event timing (untimed by the job's clock)
+            name, fn = op.peer
+            for _ in range(max(3, args.warmup)):
+                fn()
+            p0 = torch.cuda.Event(enable_timing=True)
+            p1 = torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            for _ in range(args.steps):
+                fn()
+            p1.record(stream)
+            torch.cuda.synchronize()
+            pms = p0.elapsed_time(p1) / args.steps
+            per[op.name].update({"peer": name, "peer_ms": round(pms, 4), "speedup_vs_peer": round(pms / ms, 2)})
 
     # End to end through the public API with host buffers: every step copies each op's input from pinned host
     # memory, runs it, and copies its whole output back (crdfft_execute_host where the op has it: the batch in chunks,
@@ -754,7 +825,7 @@ def main() -> None:
     ap.add_argument("--workload", choices=WORKLOADS, default="mixed",
                     help="mixed (default): C2C at N 4096/65536/2^20/107520; n1024: N 1024 x 4096; r2c: R2C/C2R 2^20; uneven: 20,000 "
                          "7-smooth sizes; nd: FP32 2-D 4096^2 / 3-D 512^3; precision: the same 2-D/3-D at FP32, "
-                         "split-BF16 and FP16-scaled")
+                         "split-BF16 and FP16-scaled; conv: fused FFT convolution beside cuFFT's three passes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--planner", choices=["estimate", "measure"], default="measure",

@@ -4,13 +4,13 @@ The compute runs in ``libcrdfft.so`` (hand-written CUDA kernels behind the C ABI
 package is the Python mirror of the reference's plan classes over that ABI (``crd_b200.hesap``).
 """
 
-from .hesap import (BluesteinPlan, FftPlan, Forward, Inverse, NdFftPlan, Plan, RealFftPlan, UnevenPlan, fft,
+from .hesap import (BluesteinPlan, ConvPlan, FftPlan, Forward, Inverse, NdFftPlan, Plan, RealFftPlan, UnevenPlan, fft,
                     ifft_normalized, self_check, uneven_offsets)
 from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP16_SCALED, PREC_FP32,
                    PREC_SPLIT_BF16, R2C, CrdFftError)
 
 __all__ = [
-    "BluesteinPlan", "FftPlan", "NdFftPlan", "Plan", "RealFftPlan", "UnevenPlan", "fft", "ifft_normalized",
+    "BluesteinPlan", "ConvPlan", "FftPlan", "NdFftPlan", "Plan", "RealFftPlan", "UnevenPlan", "fft", "ifft_normalized",
     "self_check", "uneven_offsets",
     "Forward", "Inverse", "C2C", "R2C", "C2R", "FORWARD", "INVERSE", "NORM_NONE", "NORM_INVERSE", "PREC_FP32",
     "PREC_SPLIT_BF16", "PREC_FP16_SCALED", "CrdFftError",

@@ -45,6 +45,8 @@ EXPORTS = (
     "crdfft_plan_destroy",
     "crdfft_execute",
     "crdfft_execute_host",
+    "crdfft_conv_plan_create",
+    "crdfft_conv_execute",
     "crdfft_plan_info_get",
     "crdfft_workspace_size",
     "crdfft_set_workspace",
@@ -138,6 +140,8 @@ def lib():
         "crdfft_plan_destroy": ([vp], i32),
         "crdfft_execute": ([vp, vp, vp, i32, vp], i32),
         "crdfft_execute_host": ([vp, vp, vp, i32, vp], i32),
+        "crdfft_conv_plan_create": ([ctypes.POINTER(Desc), i32, ctypes.c_double, pp], i32),
+        "crdfft_conv_execute": ([vp, vp, vp, vp, vp], i32),
         "crdfft_plan_info_get": ([vp, ctypes.POINTER(PlanInfo)], i32),
         "crdfft_workspace_size": ([vp], ctypes.c_size_t),
         "crdfft_set_workspace": ([vp, vp, ctypes.c_size_t], i32),

@@ -1,0 +1,146 @@
+// Fused FFT convolution: forward FFT -> multiply by a filter spectrum -> inverse FFT, one HBM read and one write per
+// point. The vendor route is three global passes (forward FFT, an elementwise multiply kernel, inverse FFT:
+// bench/gpu-fft/cufft_conv_bench.cu:3-5); the reference's own GPU kernel fuses them on chip
+// (engine/gpu/kir/include/crd/kir/ckir_fft.hpp:279-296): y = IFFT(FFT(x) * H) * scale, scale 1/N by default, one
+// filter spectrum shared by the batch or one per transform.
+//
+// Each CTA holds whole lines in shared memory: the forward stages leave the spectrum there in natural order (the
+// Stockham stages sort as they go); each thread multiplies its elements by H and conjugates them; the same forward
+// stages then run again and the last one stores conj(.) * scale, since IFFT(Z) = conj(FFT(conj(Z))). The line
+// stages are the line-FFT kernel's (line_fft.cuh). A row map serves 1-D batches; a column map serves the column
+// pass of a 2-D convolution (rows FFT, fused column convolution, inverse rows FFT).
+
+#include "kernels.hpp"
+#include "line_fft.cuh"
+
+namespace crdfft
+{
+namespace lfft
+{
+namespace
+{
+
+template <class S, int P, PassMap MAP>
+__global__ void __launch_bounds__(kMaxThreads)
+    conv_kernel(const PassDesc d, const float2* __restrict__ gin, const float2* __restrict__ spec,
+                const LineMap smap, float2* __restrict__ gout)
+{
+    extern __shared__ float2 sm[];
+    const int n = sched_n<S>(d);
+    const int T = (n + P - 1) / P;
+    const int lpc = blockDim.x / T;
+    const int tid = threadIdx.x;
+    const int pitch = line_pitch(n);
+    const long long line0 = static_cast<long long>(blockIdx.x) * lpc;
+    int ll, jt;
+    if constexpr (MAP == PassMap::Row)
+    {
+        ll = tid / T;
+        jt = tid - ll * T;
+    }
+    else
+    {
+        jt = tid / lpc;
+        ll = tid - jt * lpc;
+    }
+    const long long line = line0 + ll;
+    Ctx c;
+    c.ok = line < d.lines;
+    c.q = line % d.lines_per_group;
+    c.in = gin + line_offset(d.in, line, d.lines_per_group);
+    c.out = gout + line_offset(d.out, line, d.lines_per_group);
+    c.jt = jt;
+    c.T = T;
+    init_scales(d, c); // conj_out and the scale: the inverse's epilogue
+    c.in_im = 1.0f;
+    const LayRow<1> lay{sm + ll * pitch};
+
+    // forward FFT of the lines, read straight from global memory, result in shared memory
+    SchedRun<S>::template go<P, true, false, false, Kind<MAP, false>>(d, c, lay, n);
+    // Z = conj(X H), each thread on its own elements of its line
+    if (c.ok)
+    {
+        const float2* h = spec + line_offset(smap, line, d.lines_per_group);
+        for (int e = jt; e < n; e += T)
+        {
+            const float2 v = cmul(lay.at(e), __ldg(h + static_cast<long long>(e) * smap.estride));
+            lay.at(e) = make_float2(v.x, -v.y);
+        }
+    }
+    __syncthreads();
+    // conj(FFT(Z)) * scale = IFFT(X H) * scale, stored straight to global memory
+    SchedRun<S>::template go<P, false, true, false, Kind<MAP, true>>(d, c, lay, n);
+}
+
+using ConvFn = void (*)(const PassDesc, const float2*, const float2*, const LineMap, float2*);
+
+template <class S, int P> ConvFn conv_pick(PassMap map)
+{
+    return map == PassMap::Row ? conv_kernel<S, P, PassMap::Row> : conv_kernel<S, P, PassMap::Col>;
+}
+
+// The kernel for the pass at `P` points a thread: compile-time schedules for the common lengths, else the run-time
+// schedule (16 points a thread).
+ConvFn conv_select(const PassDesc& d, PassMap map, int P)
+{
+    if (P == 32)
+        return same_radices(d, {16, 16, 16}) && map == PassMap::Row ? conv_kernel<Sched<16, 16, 16>, 32, PassMap::Row>
+                                                                    : nullptr;
+    if (same_radices(d, {16, 16}))
+        return conv_pick<Sched<16, 16>, 16>(map);
+    if (same_radices(d, {16, 8, 4}))
+        return conv_pick<Sched<16, 8, 4>, 16>(map);
+    if (same_radices(d, {16, 16, 4}))
+        return conv_pick<Sched<16, 16, 4>, 16>(map);
+    return conv_pick<DynSched, 16>(map);
+}
+
+} // namespace
+} // namespace lfft
+
+bool conv_supported(const PassDesc& d)
+{
+    return d.nstages > 0 && (d.n + 15) / 16 <= lfft::kMaxThreads;
+}
+
+// Lines a CTA and points a thread: about 256 threads a CTA (the n = 4096 lines at 32 points a thread).
+void conv_shape(const PassDesc& d, PassMap map, int* P, int* lpc, int* smem)
+{
+    *P = (map == PassMap::Row && lfft::same_radices(d, {16, 16, 16})) ? 32 : 16;
+    const int T = (d.n + *P - 1) / *P;
+    int l = std::max(1, 256 / T);
+    if (map == PassMap::Col)
+        l = std::max(1, std::min(l, 16));
+    while (l > 1 && l * lfft::line_pitch(d.n) * 8 > 100 * 1024)
+        --l;
+    *lpc = l;
+    *smem = l * lfft::line_pitch(d.n) * 8;
+}
+
+cudaError_t launch_conv(const PassDesc& d, PassMap map, const LineMap& smap, const void* in, const void* spec,
+                        void* out, cudaStream_t stream)
+{
+    int P = 16, lpc = 1, smem = 0;
+    conv_shape(d, map, &P, &lpc, &smem);
+    lfft::ConvFn fn = lfft::conv_select(d, map, P);
+    if (fn == nullptr)
+        return cudaErrorInvalidConfiguration;
+    const int T = (d.n + P - 1) / P;
+    const long long groups = (d.lines + lpc - 1) / lpc;
+    if (groups <= 0)
+        return cudaSuccess;
+    if (groups > 0x7fffffffLL)
+        return cudaErrorInvalidConfiguration;
+    if (smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    fn<<<static_cast<unsigned>(groups), T * lpc, smem, stream>>>(d, static_cast<const float2*>(in),
+                                                                 static_cast<const float2*>(spec), smap,
+                                                                 static_cast<float2*>(out));
+    return cudaGetLastError();
+}
+
+} // namespace crdfft

@@ -14,6 +14,12 @@ namespace crdfft
 
 // One launch of the line-FFT kernel (line_fft.cu).
 cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void* in, void* out, cudaStream_t stream);
+
+// Fused FFT convolution of the lines of a pass (conv.cu): out = conj(FFT(conj(FFT(in) * H))) * scale, with H's
+// element e of line l at line_offset(smap, l) + e * smap.estride, the pass's conj_out set and its scale.
+bool conv_supported(const PassDesc& d);
+cudaError_t launch_conv(const PassDesc& d, PassMap map, const LineMap& smap, const void* in, const void* spec,
+                        void* out, cudaStream_t stream);
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
 int pass_threads_limit();

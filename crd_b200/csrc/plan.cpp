@@ -95,6 +95,7 @@ enum class StepKind : int
     Line,
     Cluster,
     TcLine,
+    Conv,
     R2CPost,
     C2RPre,
     ChirpPre,
@@ -111,6 +112,7 @@ struct Step
     int prec = 0;     // TcLine: 1 split-BF16, 2 FP16 scaled
     const void* amat = nullptr;
     PassShape shape{};
+    LineMap smap{};   // Conv: where each line's filter spectrum sits
     RealRecombine real{};
     ChirpDesc chirp{};
     BufRef src, dst;
@@ -262,6 +264,7 @@ struct Plan
     };
     HostPipe* host = nullptr;
     std::mutex host_mu;
+    bool conv = false; // fused convolution plan (crdfft_conv_plan_create): executes with a filter spectrum
 
     ~Plan()
     {
@@ -1181,6 +1184,83 @@ crdfft_status build_nd(Plan& p)
     return CRDFFT_OK;
 }
 
+// A fused-convolution request: one filter spectrum for the batch or one per transform, and the output scale
+// (negative: 1 / the transform size).
+struct ConvReq
+{
+    bool per_transform = false;
+    double scale = -1.0;
+};
+
+// The fused convolution (conv.cu): y = IFFT(FFT(x) * H) * scale. Rank 1: one launch, lines of the batch in shared
+// memory. Rank 2 (rows x cols): forward row FFTs, the fused convolution along the columns, inverse row FFTs with the
+// scale, as the reference's 2-D GPU convolution orders them (engine/gpu/kir/include/crd/kir/ckir_fft.hpp:2075-2090).
+crdfft_status build_conv(Plan& p, const ConvReq& req)
+{
+    const crdfft_desc& d = p.desc;
+    if (d.kind != CRDFFT_C2C || d.rank > 2 || d.istride > 1 || d.ostride > 1)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    long long total = 1;
+    for (int i = 0; i < d.rank; ++i)
+        total *= d.dims[i];
+    if ((d.idist != 0 && d.idist != total) || (d.odist != 0 && d.odist != total))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const float scale = static_cast<float>(req.scale < 0.0 ? 1.0 / static_cast<double>(total) : req.scale);
+    p.conv = true;
+    if (d.rank == 1)
+    {
+        const long long n = d.dims[0];
+        if (n < 2 || !single_pass_ok(n))
+            return CRDFFT_UNSUPPORTED_SIZE;
+        Step s;
+        s.kind = StepKind::Conv;
+        crdfft_status st = make_pass_desc(p, n, d.batch, 1, LineMap{n, 0, 1}, LineMap{n, 0, 1}, false, true, scale,
+                                          FourStepTw{}, &s.pass);
+        if (st != CRDFFT_OK)
+            return st;
+        if (!conv_supported(s.pass))
+            return CRDFFT_UNSUPPORTED_SIZE;
+        s.shape.map = PassMap::Row;
+        s.smap = LineMap{req.per_transform ? n : 0, 0, 1};
+        s.src = BufRef{Buf::In, 0};
+        s.dst = BufRef{Buf::Out, 0};
+        p.steps[0].push_back(s);
+        p.algorithm = "fused-conv";
+        p.factors = {n};
+        return CRDFFT_OK;
+    }
+    const long long rows = d.dims[0], cols = d.dims[1];
+    if (rows < 2 || cols < 2 || !single_pass_ok(rows) || !single_pass_ok(cols))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const long long lines = d.batch * rows;
+    Step r1;
+    crdfft_status st = make_line_step(p, cols, lines, 1, LineMap{cols, 0, 1}, LineMap{cols, 0, 1},
+                                      BufRef{Buf::In, 0}, BufRef{Buf::Out, 0}, false, false, 1.0f, &r1);
+    if (st != CRDFFT_OK)
+        return st;
+    Step cv;
+    cv.kind = StepKind::Conv;
+    st = make_pass_desc(p, rows, d.batch * cols, cols, LineMap{total, 1, cols}, LineMap{total, 1, cols}, false, true,
+                        1.0f, FourStepTw{}, &cv.pass);
+    if (st != CRDFFT_OK)
+        return st;
+    if (!conv_supported(cv.pass))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    cv.shape.map = PassMap::Col;
+    cv.smap = LineMap{req.per_transform ? total : 0, 1, cols};
+    cv.src = BufRef{Buf::Out, 0};
+    cv.dst = BufRef{Buf::Out, 0};
+    Step r2;
+    st = make_line_step(p, cols, lines, 1, LineMap{cols, 0, 1}, LineMap{cols, 0, 1}, BufRef{Buf::Out, 0},
+                        BufRef{Buf::Out, 0}, true, true, scale, &r2);
+    if (st != CRDFFT_OK)
+        return st;
+    p.steps[0] = {r1, cv, r2};
+    p.algorithm = "fused-conv-2d";
+    p.factors = {rows, cols};
+    return CRDFFT_OK;
+}
+
 // The split of a long uneven-batch transform: n = n1 * n2 with both halves at most `cap`, closest to square, n2
 // preferring a multiple of 16 (whole column tiles).
 bool uneven_split(long long n, long long cap, long long* n1, long long* n2)
@@ -1435,7 +1515,7 @@ crdfft_status validate(const crdfft_desc& d)
     return CRDFFT_OK;
 }
 
-crdfft_status create(const crdfft_desc* desc, Plan** out)
+crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = nullptr)
 {
     if (desc == nullptr || out == nullptr)
         return CRDFFT_INVALID_ARG;
@@ -1458,7 +1538,9 @@ crdfft_status create(const crdfft_desc* desc, Plan** out)
             return CRDFFT_LAUNCH;
         p->err = static_cast<int*>(e);
     }
-    if (desc->kind != CRDFFT_C2C)
+    if (conv != nullptr)
+        st = build_conv(*p, *conv);
+    else if (desc->kind != CRDFFT_C2C)
         st = build_real(*p);
     else if (desc->rank == 1)
         st = build_c2c_rank1(*p);
@@ -1530,7 +1612,7 @@ crdfft_status run_uneven(Plan& p, const void* in, void* out, int dir, cudaStream
     return cudaGraphLaunch(exec, stream) == cudaSuccess ? CRDFFT_OK : CRDFFT_LAUNCH;
 }
 
-crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stream)
+crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stream, const void* spec = nullptr)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev != p.device)
@@ -1549,6 +1631,11 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
             case StepKind::Line: e = launch_line_pass(s.pass, s.shape, src, dst, stream); break;
             case StepKind::Cluster: e = launch_cluster_fft(s.pass, s.pass2, s.count, src, dst, stream); break;
             case StepKind::TcLine: e = launch_tc_pass(s.pass, s.prec, s.amat, src, dst, stream); break;
+            case StepKind::Conv:
+                if (spec == nullptr)
+                    return CRDFFT_INVALID_ARG;
+                e = launch_conv(s.pass, s.shape.map, s.smap, src, spec, dst, stream);
+                break;
             case StepKind::R2CPost: e = launch_r2c_post(s.real, src, dst, stream); break;
             case StepKind::C2RPre: e = launch_c2r_pre(s.real, src, dst, stream); break;
             case StepKind::ChirpPre: e = launch_chirp_pre(s.chirp, src, dst, stream); break;
@@ -1620,11 +1707,40 @@ crdfft_status crdfft_plan_destroy(crdfft_plan* plan)
     return CRDFFT_OK;
 }
 
+crdfft_status crdfft_conv_plan_create(const crdfft_desc* desc, int32_t filter_per_transform, double scale,
+                                      crdfft_plan** plan)
+{
+    if (plan == nullptr)
+        return CRDFFT_INVALID_ARG;
+    *plan = nullptr;
+    ConvReq req;
+    req.per_transform = filter_per_transform != 0;
+    req.scale = scale;
+    Plan* p = nullptr;
+    const crdfft_status st = create(desc, &p, &req);
+    if (st != CRDFFT_OK)
+        return st;
+    *plan = reinterpret_cast<crdfft_plan*>(p);
+    return CRDFFT_OK;
+}
+
+crdfft_status crdfft_conv_execute(crdfft_plan* plan, const void* in, const void* spectrum, void* out, void* stream)
+{
+    if (plan == nullptr || in == nullptr || spectrum == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    if (!p.conv)
+        return CRDFFT_INVALID_ARG;
+    return run(p, in, out, 0, static_cast<cudaStream_t>(stream), spectrum);
+}
+
 crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32_t direction, void* stream)
 {
     if (plan == nullptr || in == nullptr || out == nullptr)
         return CRDFFT_INVALID_ARG;
     Plan& p = *as_plan(plan);
+    if (p.conv)
+        return CRDFFT_INVALID_ARG;
     if (direction != CRDFFT_FORWARD && direction != CRDFFT_INVERSE)
         return CRDFFT_INVALID_ARG;
     if ((p.desc.kind == CRDFFT_R2C && direction != CRDFFT_FORWARD) ||
@@ -1663,8 +1779,11 @@ bool host_layout(const crdfft_desc& d, HostLayout* L)
 crdfft_status host_pipe_setup(Plan& p, const HostLayout& L)
 {
     std::unique_ptr<Plan::HostPipe> h(new Plan::HostPipe());
+    // Chunks of an eighth of the batch, between 4 and 64 MiB of input: enough chunks for the copies in both
+    // directions to overlap, each large enough to run the copy engines at full rate.
     const long long per = std::max<long long>(1, static_cast<long long>(L.in_elem) * L.idist);
-    h->chunk = std::max<long long>(1, std::min<long long>(p.desc.batch, (64LL << 20) / per));
+    const long long target = std::min<long long>(64LL << 20, std::max<long long>(4LL << 20, per * p.desc.batch / 8));
+    h->chunk = std::max<long long>(1, std::min<long long>(p.desc.batch, target / per));
     crdfft_desc cd = p.desc;
     cd.batch = h->chunk;
     crdfft_status st = create(&cd, &h->full);
@@ -1706,7 +1825,7 @@ crdfft_status crdfft_execute_host(crdfft_plan* plan, const void* in, void* out, 
         (p.desc.kind == CRDFFT_C2R && direction != CRDFFT_INVERSE))
         return CRDFFT_INVALID_ARG;
     HostLayout L{};
-    if (p.uneven || !host_layout(p.desc, &L))
+    if (p.uneven || p.conv || !host_layout(p.desc, &L))
         return CRDFFT_INVALID_ARG;
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev != p.device)

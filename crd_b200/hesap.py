@@ -145,6 +145,34 @@ class Plan(_Handle):
         return out
 
 
+class ConvPlan(_Handle):
+    """Fused FFT convolution (crdfft_conv_plan_create): y = IFFT(FFT(x) * H) * scale over a batch of 1-D signals
+    (dims = [n]) or 2-D signals (dims = [rows, cols]); one spectrum H shared by the batch, or one per signal."""
+
+    def __init__(self, dims: Sequence[int], batch: int = 1, per_signal_filter: bool = False, scale: float = -1.0):
+        super().__init__()
+        dims = [int(v) for v in dims]
+        d = Desc()
+        d.rank = len(dims)
+        d.kind = C2C
+        d.precision = PREC_FP32
+        d.norm = NORM_NONE
+        for i, v in enumerate(dims):
+            d.dims[i] = v
+        d.batch = batch
+        self.dims = tuple(dims)
+        self.batch = batch
+        check(lib().crdfft_conv_plan_create(ctypes.byref(d), 1 if per_signal_filter else 0, float(scale),
+                                            ctypes.byref(self._h)), "conv_plan_create")
+
+    def execute(self, inp: torch.Tensor, spectrum: torch.Tensor, out: torch.Tensor, stream=None) -> torch.Tensor:
+        pi = _ptr(inp, torch.complex64, "input")
+        ps = _ptr(spectrum, torch.complex64, "spectrum")
+        po = _ptr(out, torch.complex64, "output")
+        check(lib().crdfft_conv_execute(self._h, pi, ps, po, _stream(stream)), "conv_execute")
+        return out
+
+
 class FftPlan(_Handle):
     """FftPlan<float>(alloc, n) - one size-n complex transform (fft.hpp:224)."""
 

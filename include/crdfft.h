@@ -116,9 +116,9 @@ crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32
 
 /* Run the plan on HOST buffers, the way the reference's plans are called (FftPlan::execute transforms a span of CPU
  * memory in place, fft.hpp:409-413): `in` and `out` are host memory laid out as the plan's descriptor says (element
- * stride 1; in == out allowed). The batch is cut into chunks of about 64 MiB; each chunk's copy to the device, its
- * transform and its copy back go on one of two internal streams in turn, so the copies in both directions and the
- * transforms of different chunks overlap. Use page-locked host memory (cudaHostAlloc / pinned tensors): with
+ * stride 1; in == out allowed). The batch is cut into chunks (an eighth of the batch, 4 to 64 MiB of input); each
+ * chunk's copy to the device, its transform and its copy back go on one of two internal streams in turn, so the
+ * copies in both directions and the transforms of different chunks overlap. Convolution plans are not supported. Use page-locked host memory (cudaHostAlloc / pinned tensors): with
  * pageable memory the result is the same but the copies do not overlap. The work is ordered after everything
  * already queued on `stream`, and `stream` waits for all of it: synchronise `stream` before reading `out`. The first
  * call on a plan allocates its device staging buffers (two chunks each way) and the chunk plans; calls on one plan
@@ -169,6 +169,23 @@ crdfft_status crdfft_nd_execute(crdfft_plan* plan, void* data, int32_t direction
  * plan, run it in place, release it (synchronises the stream before releasing). */
 crdfft_status crdfft_fft(void* data, int64_t n, int32_t direction, void* stream);
 crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream);
+
+/* ---- Fused FFT convolution ---------------------------------------------------------------------------------- */
+
+/* y = IFFT(FFT(x) * H) * scale for a batch of 1-D (rank 1) or 2-D (rank 2, rows x cols) complex signals: the circular
+ * convolution with the filter whose spectrum H = FFT(h) the caller supplies. No counterpart in crd-hesap-fft's CPU
+ * API; it follows the reference's GPU fused convolution (engine/gpu/kir/include/crd/kir/ckir_fft.hpp:279-296,
+ * 2075-2090: scale 1/N by default, one filter shared by the batch or one per signal), where the vendor route takes
+ * three global passes (bench/gpu-fft/cufft_conv_bench.cu:3-5). Rank 1 runs in one launch (each signal's forward
+ * FFT, product and inverse FFT in shared memory: one read and one write per point); rank 2 runs the row FFTs, the
+ * fused convolution along the columns, then the inverse row FFTs. desc: C2C, packed (element stride 1, distance
+ * the signal size), each dimension up to 8192 and 7-smooth. filter_per_transform: 0 for one spectrum (rank 1: n
+ * values; rank 2: rows x cols, row-major) shared by the batch, 1 for one per signal (batch times that). scale < 0
+ * means 1 / (number of points of one signal). */
+crdfft_status crdfft_conv_plan_create(const crdfft_desc* desc, int32_t filter_per_transform, double scale,
+                                      crdfft_plan** plan);
+/* in == out allowed. crdfft_execute rejects convolution plans (CRDFFT_INVALID_ARG). */
+crdfft_status crdfft_conv_execute(crdfft_plan* plan, const void* in, const void* spectrum, void* out, void* stream);
 
 /* ---- Uneven batches ---------------------------------------------------------------------------------------- */
 
