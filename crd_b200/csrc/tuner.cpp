@@ -50,6 +50,23 @@ int ilog2(long long v)
     return r;
 }
 
+// Reads a buffer larger than L2 so that the timed launch that follows finds its input in HBM, as a pass of a large
+// batch does. Reads only: the lines it leaves in L2 are clean, so no write-back competes with the timed launch.
+__global__ void l2_flush_kernel(const float4* __restrict__ p, long long n, float* sink)
+{
+    float acc = 0.0f;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+    {
+        const float4 v = __ldcg(p + i);
+        acc += v.x + v.y + v.z + v.w;
+    }
+    if (acc == 1.2345e-38f) // never, for finite zero-filled input: keeps the loads
+        *sink = acc;
+}
+
+constexpr size_t kFlushBytes = 256u << 20;
+
 // Largest element offset + 1 a line map reaches over the first `lines` lines.
 long long extent(const LineMap& m, long long lines, long long lpg, int n)
 {
@@ -192,6 +209,20 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaMemsetAsync(in, 0, static_cast<size_t>(in_ext) * 8, st);
+    // Cold-cache timing: an L2-sized read before every timed launch (skipped if the buffer cannot be had).
+    void* flush = nullptr;
+    if (cudaMalloc(&flush, kFlushBytes + 256) != cudaSuccess)
+    {
+        flush = nullptr;
+        cudaGetLastError();
+    }
+    else
+        cudaMemsetAsync(flush, 0, kFlushBytes + 256, st);
+    auto cold = [&]() {
+        if (flush != nullptr)
+            l2_flush_kernel<<<1184, 256, 0, st>>>(static_cast<const float4*>(flush), kFlushBytes / 16,
+                                                  reinterpret_cast<float*>(static_cast<char*>(flush) + kFlushBytes));
+    };
     int best = -1;
     for (size_t i = 0; i < cands.size(); ++i)
     {
@@ -201,6 +232,7 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
         bool ok = true;
         for (int r = 0; r < 3 && ok; ++r)
         {
+            cold();
             cudaEventRecord(e0, st);
             ok = launch_line_pass(d, cands[i], in, out, st) == cudaSuccess;
             cudaEventRecord(e1, st);
@@ -223,6 +255,8 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
     cudaStreamDestroy(st);
     cudaFree(in);
     cudaFree(out);
+    if (flush != nullptr)
+        cudaFree(flush);
     {
         std::lock_guard<std::mutex> lk(g_mu);
         for (size_t i = 0; i < cands.size(); ++i)

@@ -42,8 +42,8 @@ std::string wisdom_export();
 int wisdom_import(const std::string& text); // entries read, or -1 on a malformed line
 void wisdom_forget();
 
-// Times each candidate (1 warm-up, min of 3 launches, CUDA events) on scratch buffers sized for up to 64 MiB of
-// the pass's lines; returns the index of the fastest, or -1 if none could run. ms receives each candidate's time
+// Times each candidate (1 warm-up, min of 3 launches, CUDA events, each after an L2-sized read so that the input
+// comes from HBM as in a large batch) on scratch buffers sized for up to 64 MiB of the pass's lines; returns the index of the fastest, or -1 if none could run. ms receives each candidate's time
 // (or a negative value when it failed). Appends every timing to the planner log.
 // `heuristic` is the index of the heuristic's own choice among the candidates (or -1), marked in the log.
 int measure_shapes(const PassDesc& d, const std::string& key, const std::vector<PassShape>& cands,

@@ -205,7 +205,8 @@ int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offs
 /* How plan creation picks each pass's launch shape (kernel variant, points a thread, lines a CTA):
  *   CRDFFT_PLANNER_ESTIMATE  remembered wisdom for the pass's geometry class, else a fixed heuristic (default)
  *   CRDFFT_PLANNER_MEASURE   remembered wisdom, else time every candidate on the device (scratch buffers of up to
- *                            64 MiB per pass) and remember the fastest
+ *                            64 MiB per pass, each timed launch after an L2-sized read so that its input comes
+ *                            from HBM) and remember the fastest
  * The reference plans from the size alone from a board measured offline (detail/level_plans_gen.hpp:33-148); here
  * the board is measured on the device and kept as wisdom. The environment variable CRDFFT_PLANNER=measure sets the
  * initial mode. Once a pass class has wisdom, every later plan of that class makes the same choice. */
