@@ -19,6 +19,8 @@
 
 #include <cooperative_groups.h>
 
+#include <cstdlib>
+
 namespace cg = cooperative_groups;
 
 namespace crdfft
@@ -28,8 +30,10 @@ namespace lfft
 namespace
 {
 
+// Launched with a cluster of C CTAs (a launch attribute: 16 is above the portable size and needs the kernel's
+// non-portable opt-in). Two CTAs an SM at C = 8 (512 threads), four at C = 16 (256 threads).
 template <class S1, class S2, int C, int P, bool EPI>
-__global__ void __cluster_dims__(C, 1, 1) __launch_bounds__((S1::n * S2::n) / (P * C), 2)
+__global__ void __launch_bounds__((S1::n * S2::n) / (P * C), C >= 16 ? 4 : 2)
     cluster_fft_kernel(const PassDesc dA, const PassDesc dB, const float2* __restrict__ gin, float2* __restrict__ gout)
 {
     constexpr int N1 = S1::n;
@@ -135,12 +139,23 @@ template <class I> ClusterEntry entry(int n1, int n2, int c)
 const ClusterEntry* find(long long n1, long long n2)
 {
     static const ClusterEntry table[] = {
-        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 8, 16>>(256, 256, 8), // 65536
+        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 8, 16>>(256, 256, 8),   // 65536
+        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 16, 16>>(256, 256, 16), // 65536, 16-CTA clusters
     };
+    static const int want = [] {
+        const char* e = std::getenv("CRDFFT_CLUSTER_SIZE");
+        return e != nullptr ? std::atoi(e) : 16;
+    }();
+    const ClusterEntry* any = nullptr;
     for (const ClusterEntry& e : table)
         if (e.n1 == n1 && e.n2 == n2)
-            return &e;
-    return nullptr;
+        {
+            if (e.cluster == want)
+                return &e;
+            if (any == nullptr)
+                any = &e;
+        }
+    return any;
 }
 
 } // namespace
@@ -176,9 +191,25 @@ cudaError_t launch_cluster_fft(const PassDesc& a, const PassDesc& b, long long b
     const long long grid = batch * e->cluster;
     if (grid > 0x7fffffffLL)
         return cudaErrorInvalidConfiguration;
-    fn<<<static_cast<unsigned>(grid), e->threads, e->smem_bytes, stream>>>(a, b, static_cast<const float2*>(in),
-                                                                             static_cast<float2*>(out));
-    return cudaGetLastError();
+    if (e->cluster > 8)
+    {
+        const cudaError_t err = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (err != cudaSuccess)
+            return err;
+    }
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(static_cast<unsigned>(grid), 1, 1);
+    cfg.blockDim = dim3(static_cast<unsigned>(e->threads), 1, 1);
+    cfg.dynamicSmemBytes = static_cast<size_t>(e->smem_bytes);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(e->cluster);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, fn, a, b, static_cast<const float2*>(in), static_cast<float2*>(out));
 }
 
 } // namespace crdfft

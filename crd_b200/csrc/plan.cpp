@@ -113,6 +113,7 @@ struct Step
     const void* amat = nullptr;
     PassShape shape{};
     LineMap smap{};   // Conv: where each line's filter spectrum sits
+    int lane = 0;     // 0: the caller's stream; 1, 2: the plan's two internal streams (L2-sized four-step waves)
     RealRecombine real{};
     ChirpDesc chirp{};
     BufRef src, dst;
@@ -265,6 +266,10 @@ struct Plan
     HostPipe* host = nullptr;
     std::mutex host_mu;
     bool conv = false; // fused convolution plan (crdfft_conv_plan_create): executes with a filter spectrum
+    // Two internal streams for steps with lane 1 / 2, forked from and joined back to the caller's stream.
+    cudaStream_t lanes[2] = {nullptr, nullptr};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[2] = {nullptr, nullptr};
 
     ~Plan()
     {
@@ -288,6 +293,15 @@ struct Plan
         }
         for (auto& kv : graphs)
             cudaGraphExecDestroy(kv.second);
+        for (int i = 0; i < 2; ++i)
+        {
+            if (lanes[i] != nullptr)
+                cudaStreamDestroy(lanes[i]);
+            if (join[i] != nullptr)
+                cudaEventDestroy(join[i]);
+        }
+        if (fork != nullptr)
+            cudaEventDestroy(fork);
         for (auto& kv : batched)
             delete kv.second;
         if (arena_backed)
@@ -750,6 +764,18 @@ long long wave_bytes()
     return 512LL << 20;
 }
 
+// Four-step waves sized for L2 on two internal streams (CRDFFT_L2_WAVES=1) or one large wave at a time (=0).
+bool l2_waves()
+{
+    static const bool on = [] {
+        const char* e = std::getenv("CRDFFT_L2_WAVES");
+        return e == nullptr || std::atoi(e) != 0;
+    }();
+    return on;
+}
+
+long long l2_wave_bytes() { return 24LL << 20; }
+
 // A batch of 1-D complex transforms of length n: element j of transform t at base + t*dist + j*stride on each side.
 // Appends the steps of one direction; `ws_off` is where in the workspace this transform's scratch may start; the
 // scratch it needs is returned in *ws_need (complex elements).
@@ -826,12 +852,20 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     crdfft_status st = four_step_tables(p, n, n1, n2, &hi, &lo);
     if (st != CRDFFT_OK)
         return st;
-    long long wave = std::max(1LL, wave_bytes() / (n * 8));
+    // L2 waves: a wave small enough that pass 1's output is still in L2 when pass 2 reads it, two workspace slots,
+    // consecutive waves on the plan's two internal streams so that one wave's pass 2 overlaps the next one's pass 1
+    // (and fills its tail). Otherwise one large wave at a time on the caller's stream.
+    // (Transforms above 2 MiB are left to large waves: a 24 MiB wave of them is too few tiles to fill the GPU.)
+    const bool l2w = l2_waves() && t_arena == nullptr && n * 8 <= (2LL << 20) && batch * n * 8 > 2 * l2_wave_bytes();
+    long long wave = std::max(1LL, (l2w ? l2_wave_bytes() : wave_bytes()) / (n * 8));
     wave = std::min(wave, batch);
-    *ws_need = wave * n;
-    for (long long t0 = 0; t0 < batch; t0 += wave)
+    *ws_need = (l2w ? 2 : 1) * wave * n;
+    int wi = 0;
+    for (long long t0 = 0; t0 < batch; t0 += wave, ++wi)
     {
         const long long w = std::min(wave, batch - t0);
+        const long long slot_off = l2w ? (wi & 1) * wave * n : 0;
+        const int lane = l2w ? 1 + (wi & 1) : 0;
         // pass 1: columns n2' in [0, n2), elements n1' along stride n2 -> scratch Y[t][k1][n2']
         Step s1;
         FourStepTw ftw;
@@ -839,17 +873,20 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         ftw.hi = hi;
         ftw.lo = lo;
         st = make_line_step(p, n1, w * n2, n2, LineMap{idist, istride, n2 * istride}, LineMap{n, 1, n2},
-                            BufRef{src.b, src.off + t0 * idist}, BufRef{Buf::Ws, ws_off}, conj_in, false, 1.0f, &s1,
-                            ftw);
+                            BufRef{src.b, src.off + t0 * idist}, BufRef{Buf::Ws, ws_off + slot_off}, conj_in, false,
+                            1.0f, &s1, ftw);
         if (st != CRDFFT_OK)
             return st;
+        s1.lane = lane;
         steps.push_back(s1);
         // pass 2: rows k1 of length n2 -> X[t][k1 + n1 k2]
         Step s2;
         st = make_line_step(p, n2, w * n1, n1, LineMap{n, n2, 1}, LineMap{odist, ostride, n1 * ostride},
-                            BufRef{Buf::Ws, ws_off}, BufRef{dst.b, dst.off + t0 * odist}, false, conj_out, scale, &s2);
+                            BufRef{Buf::Ws, ws_off + slot_off}, BufRef{dst.b, dst.off + t0 * odist}, false, conj_out,
+                            scale, &s2);
         if (st != CRDFFT_OK)
             return st;
+        s2.lane = lane;
         steps.push_back(s2);
     }
     return CRDFFT_OK;
@@ -1621,8 +1658,39 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
         return CRDFFT_INVALID_ARG;
     if (p.uneven)
         return run_uneven(p, in, out, dir, stream);
+    // Steps on the plan's internal streams (lanes 1, 2) fork from the caller's stream and join back before the next
+    // step on the caller's stream, and at the end.
+    const cudaStream_t user = stream;
+    bool forked = false;
+    auto join = [&]() {
+        for (int i = 0; i < 2; ++i)
+            if (cudaEventRecord(p.join[i], p.lanes[i]) != cudaSuccess ||
+                cudaStreamWaitEvent(user, p.join[i], 0) != cudaSuccess)
+                return false;
+        forked = false;
+        return true;
+    };
     for (const Step& s : p.steps[dir])
     {
+        if (s.lane != 0 && !forked)
+        {
+            if (p.lanes[0] == nullptr)
+            {
+                for (int i = 0; i < 2; ++i)
+                    if (cudaStreamCreateWithFlags(&p.lanes[i], cudaStreamNonBlocking) != cudaSuccess ||
+                        cudaEventCreateWithFlags(&p.join[i], cudaEventDisableTiming) != cudaSuccess)
+                        return CRDFFT_LAUNCH;
+                if (cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming) != cudaSuccess)
+                    return CRDFFT_LAUNCH;
+            }
+            if (cudaEventRecord(p.fork, user) != cudaSuccess || cudaStreamWaitEvent(p.lanes[0], p.fork, 0) != cudaSuccess ||
+                cudaStreamWaitEvent(p.lanes[1], p.fork, 0) != cudaSuccess)
+                return CRDFFT_LAUNCH;
+            forked = true;
+        }
+        else if (s.lane == 0 && forked && !join())
+            return CRDFFT_LAUNCH;
+        stream = s.lane == 0 ? user : p.lanes[s.lane - 1];
         void* src = resolve(s.src, in, out, p.ws);
         void* dst = resolve(s.dst, in, out, p.ws);
         cudaError_t e = cudaSuccess;
@@ -1646,6 +1714,8 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
         if (e != cudaSuccess)
             return CRDFFT_LAUNCH;
     }
+    if (forked && !join())
+        return CRDFFT_LAUNCH;
     return CRDFFT_OK;
 }
 

@@ -428,3 +428,31 @@ def test_nd_padded_batch_distances(dims):
             xb = x[b * idist:b * idist + total].reshape(dims)
             _check(got[b * odist:b * odist + total].reshape(dims), oracle.nd64(xb, inverse), max(dims))
             assert np.all(got[b * odist + total:(b + 1) * odist] == 7 + 7j)
+
+
+@pytest.mark.parametrize("inverse", [False, True])
+def test_l2_sized_waves_on_two_streams(inverse):
+    """Batches larger than two L2-sized waves run the four-step waves alternately on the plan's two internal streams
+    (two workspace slots); every transform comes out right and the caller's stream sees all of it."""
+    n, batch = 1 << 17, 64
+    x, got, plan = _c2c(n, batch, inverse, seed=0x12AB)
+    assert plan.info()["algorithm"] == "four-step"
+    for t in (0, 23, 24, 47, 48, 63):  # across wave and slot boundaries
+        _check(got[t], oracle.fft64(x[t], inverse), n)
+
+
+def test_l2_waves_then_recombine_real():
+    """R2C: the half-length four-step waves on the internal streams, then the recombination on the caller's stream
+    (which must wait for both)."""
+    n, batch = 1 << 18, 100
+    x = oracle.lcg_float32(0x12AC, n * batch).reshape(batch, n)
+    t = torch.from_numpy(x).cuda()
+    spec = torch.empty(batch, n // 2 + 1, dtype=torch.complex64, device="cuda")
+    cf.Plan([n], batch=batch, kind=cf.R2C).execute(t, spec, cf.FORWARD)
+    back = torch.empty(batch, n, dtype=torch.float32, device="cuda")
+    cf.Plan([n], batch=batch, kind=cf.C2R, norm=cf.NORM_INVERSE).execute(spec, back, cf.INVERSE)
+    torch.cuda.synchronize()
+    s = spec.cpu().numpy()
+    for r in (0, 49, 99):
+        assert oracle.rel_l2(s[r], np.fft.rfft(x[r].astype(np.float64))) <= 1e-6
+    assert oracle.rel_l2(back.cpu().numpy(), x.astype(np.float64)) <= 1e-6
