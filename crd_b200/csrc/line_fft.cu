@@ -143,7 +143,12 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
     }
     lfft::KernelFn fn = lfft::select_static(d, cs);
     if (fn == nullptr)
+    {
+        // the run-time schedule kernel always stages its lines through shared memory (even a one-stage pass that
+        // a compile-time kernel runs register to register)
         fn = lfft::select_dynamic(d, cs);
+        cs.smem_bytes = sh.lines_per_cta * lfft::line_pitch(d.n) * 8;
+    }
     if (fn == nullptr || threads > lfft::kMaxThreads)
         return cudaErrorInvalidConfiguration;
     if (groups > 0x7fffffffLL)

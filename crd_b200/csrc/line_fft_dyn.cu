@@ -1,18 +1,89 @@
 // The line-FFT kernel with its radix schedule read from the descriptor at run time: every 7-smooth line length up to
-// 8192 that has no compile-time schedule (the uneven-size batches, Bluestein's inner lengths, odd N-D axes).
+// 8192 that has no compile-time schedule (2048, 8192, 1000, 6144, ..., the uneven batches' lengths, Bluestein's inner
+// lengths, odd N-D axes).
+//
+// The CTA stages its lines through shared memory with coalesced cooperative loads and stores (along whichever side
+// is unit-stride, with the epilogue on the way out), and runs the stages as out-of-line per-radix functions
+// (dyn_stage.cuh): a kernel that inlines every radix's stage variants spills heavily and ran ten times slower.
 
+#include "dyn_stage.cuh"
 #include "line_fft.cuh"
 
 namespace crdfft
 {
 namespace lfft
 {
+namespace
+{
+
+template <PassMap MAP, bool EPI>
+__global__ void __launch_bounds__(kMaxThreads) dyn_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
+                                                              float2* __restrict__ gout)
+{
+    extern __shared__ float2 sm[];
+    __shared__ long long s_in_off[kMaxLinesPerCta];
+    __shared__ long long s_out_off[kMaxLinesPerCta];
+    __shared__ int s_q[kMaxLinesPerCta];
+    __shared__ int s_radix[kMaxStages];
+
+    const int n = d.n;
+    const int T = (n + 15) / 16;
+    const int lpc = blockDim.x / T;
+    const int tid = threadIdx.x;
+    const int pitch = line_pitch(n);
+    const long long line0 = static_cast<long long>(blockIdx.x) * lpc;
+    int ll, jt;
+    if constexpr (MAP == PassMap::Row)
+    {
+        ll = tid / T;
+        jt = tid - ll * T;
+    }
+    else
+    {
+        jt = tid / lpc;
+        ll = tid - jt * lpc;
+    }
+    for (int i = tid; i < lpc; i += blockDim.x)
+    {
+        const long long line = line0 + i;
+        s_in_off[i] = line_offset(d.in, line, d.lines_per_group);
+        s_out_off[i] = line_offset(d.out, line, d.lines_per_group);
+        s_q[i] = static_cast<int>(line % d.lines_per_group);
+    }
+    if (tid < kMaxStages)
+        s_radix[tid] = d.radix[tid];
+    __syncthreads();
+
+    Ctx c;
+    init_scales(d, c);
+    const long long lines_here = d.lines - line0;
+    const long long ies = d.in.estride;
+    for_tile(n, lpc, ies == 1, [&](int a, int e) {
+        if (a < lines_here)
+            LayRow<1>{sm + a * pitch}.at(e) = load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * ies);
+    });
+    __syncthreads();
+
+    dyn_stages(s_radix, d.nstages, static_cast<const float2*>(d.tw), n, sm + ll * pitch, jt, T, ll < lines_here);
+
+    const long long oes = d.out.estride;
+    for_tile(n, lpc, oes == 1, [&](int a, int e) {
+        if (a < lines_here)
+            __stcs(gout + s_out_off[a] + static_cast<long long>(e) * oes,
+                   epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
+    });
+}
+
+} // namespace
 
 KernelFn select_dynamic(const PassDesc& d, const PassShape& sh)
 {
     if (sh.points_per_thread != 16)
         return nullptr;
-    return pick<DynSched, 16>(sh.map, sh.direct_load, sh.direct_store, pass_epi(d));
+    const bool epi = pass_epi(d);
+    if (sh.map == PassMap::Row)
+        return epi ? dyn_fft_kernel<PassMap::Row, true> : dyn_fft_kernel<PassMap::Row, false>;
+    return epi ? dyn_fft_kernel<PassMap::Col, true> : dyn_fft_kernel<PassMap::Col, false>;
 }
 
 } // namespace lfft

@@ -18,6 +18,7 @@
 #include "kernels.hpp"
 #include "line_fft.cuh"
 #include "uneven.hpp"
+#include "dyn_stage.cuh"
 
 namespace crdfft
 {
@@ -27,77 +28,6 @@ namespace
 {
 
 constexpr int kUnevenThreads = 256;
-
-// Shared-memory slot of element e of a line (the classic layout, line_fft.cuh LayRow<1>).
-__device__ __forceinline__ int spad(int e) { return e + (e >> 4); }
-
-// One stage of a run-time schedule, out of line so that each radix gets its own register allocation, with scalar
-// arguments only. j / L comes from a multiply-high by ceil(2^32 / L) (exact for j < 2^13 and L < 2^19).
-template <int R>
-__device__ __noinline__ void ustage(float2* sl, const float2* tw, int n, int L, unsigned magic, int jt, int T, bool ok)
-{
-    constexpr int B = (16 + R - 1) / R;
-    const int nb = n / R;
-    float2 v[B][R];
-#pragma unroll
-    for (int b = 0; b < B; ++b)
-    {
-        const int j = jt + b * T;
-        if (ok && j < nb)
-        {
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                v[b][r] = sl[spad(j + r * nb)];
-        }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int b = 0; b < B; ++b)
-    {
-        const int j = jt + b * T;
-        if (ok && j < nb)
-        {
-            const int q = L == 1 ? j : static_cast<int>(__umulhi(static_cast<unsigned>(j), magic));
-            const int k = j - q * L;
-            if (L > 1)
-            {
-#pragma unroll
-                for (int r = 1; r < R; ++r)
-                    v[b][r] = cmul(v[b][r], __ldg(tw + (r - 1) * L + k));
-            }
-            Dft<R>::run(v[b]);
-            const int base = q * L * R + k;
-#pragma unroll
-            for (int r = 0; r < R; ++r)
-                sl[spad(base + r * L)] = v[b][r];
-        }
-    }
-    __syncthreads();
-}
-
-__device__ __forceinline__ void uneven_stages(const UnevenSched& s, float2* sl, int jt, int T, bool ok)
-{
-    int L = 1;
-    const float2* tw = static_cast<const float2*>(s.tw);
-    for (int st = 0; st < s.nstages; ++st)
-    {
-        const int R = s.radix[st];
-        const unsigned magic = L == 1 ? 0u : (0xFFFFFFFFu / static_cast<unsigned>(L)) + 1u;
-        switch (R)
-        {
-            case 2: ustage<2>(sl, tw, s.n, L, magic, jt, T, ok); break;
-            case 3: ustage<3>(sl, tw, s.n, L, magic, jt, T, ok); break;
-            case 4: ustage<4>(sl, tw, s.n, L, magic, jt, T, ok); break;
-            case 5: ustage<5>(sl, tw, s.n, L, magic, jt, T, ok); break;
-            case 7: ustage<7>(sl, tw, s.n, L, magic, jt, T, ok); break;
-            case 8: ustage<8>(sl, tw, s.n, L, magic, jt, T, ok); break;
-            default: ustage<16>(sl, tw, s.n, L, magic, jt, T, ok); break;
-        }
-        if (L > 1)
-            tw += (R - 1) * L;
-        L *= R;
-    }
-}
 
 // Loads an item's lines into shared memory (row layout, one pad slot per 16), coalesced along whichever side of the
 // global layout is unit-stride; line a starts at base[a].
@@ -192,7 +122,8 @@ __global__ void __launch_bounds__(kUnevenThreads, 3)
         const int T = (n + 15) / 16;
         const int ll = tid / T;
         const bool ok = ll < it.lines;
-        uneven_stages(s, sm + (ok ? ll : 0) * pitch, tid - ll * T, T, ok);
+        dyn_stages(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n, sm + (ok ? ll : 0) * pitch, tid - ll * T,
+                   T, ok);
         const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_hi[it.ftw]) : nullptr;
         const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_lo[it.ftw]) : nullptr;
         uneven_store(n, it.lines, it.out_estride, s_out, it.q0, fh, fl, dst, sm, pitch,
