@@ -14,6 +14,13 @@ namespace lfft
 // The compile-time schedules (one translation unit each, sched_*.cu).
 KernelFn s_1024_classic(const PassDesc&, const PassShape&);
 KernelFn s_1024w_classic(const PassDesc&, const PassShape&);
+KernelFn s_16_classic(const PassDesc&, const PassShape&);
+KernelFn s_32_classic(const PassDesc&, const PassShape&);
+KernelFn s_64_classic(const PassDesc&, const PassShape&);
+KernelFn s_128_classic(const PassDesc&, const PassShape&);
+KernelFn s_2048_classic(const PassDesc&, const PassShape&);
+KernelFn s_8192_classic(const PassDesc&, const PassShape&);
+KernelFn s_8192w_classic(const PassDesc&, const PassShape&);
 KernelFn s_256_classic(const PassDesc&, const PassShape&);
 KernelFn s_512_classic(const PassDesc&, const PassShape&);
 KernelFn s_4096_classic(const PassDesc&, const PassShape&);
@@ -29,7 +36,8 @@ PipeFn s_105_pipe(const PassDesc&, const PassShape&);
 KernelFn select_static(const PassDesc& d, const PassShape& sh)
 {
     for (auto f : {s_1024_classic, s_1024w_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic,
-                   s_16384_classic, s_105_classic})
+                   s_16384_classic, s_105_classic, s_16_classic, s_32_classic, s_64_classic, s_128_classic,
+                   s_2048_classic, s_8192_classic, s_8192w_classic})
         if (KernelFn k = f(d, sh))
             return k;
     return nullptr;

@@ -682,6 +682,10 @@ crdfft_status make_line_step(Plan& p, long long n, long long lines, long long lp
     }
     if (d.nstages == 0) // n == 1: no butterflies; the pass is a copy with the epilogue, staged through smem
         dl = ds = false;
+    // Row lines of 32 points or fewer: one or two threads a line, so a direct load or store would touch a separate
+    // 128-byte line per thread; staged through shared memory the CTA's accesses are contiguous.
+    if (map == PassMap::Row && n <= 32)
+        dl = ds = false;
     const int prec = p.desc.precision;
     if (prec != CRDFFT_PREC_FP32 && tc_pass_supported(d, prec))
     {
