@@ -139,6 +139,59 @@ template <> struct Dft<16>
     }
 };
 
+// Multiply by the compile-time root W_32^J = cos(πJ/16) - i sin(πJ/16): the even J through W_16, the odd J from the
+// two first-octant pairs (cos, sin)(π/16) and (cos, sin)(3π/16) by the symmetries of the circle.
+template <int J> __device__ __forceinline__ float2 w32mul(float2 a)
+{
+    constexpr int j = J & 31;
+    if constexpr ((j & 1) == 0)
+        return w16mul<j / 2>(a);
+    else
+    {
+        constexpr float C1 = 0.98078528040323044913f; // cos(π/16)
+        constexpr float S1 = 0.19509032201612826785f; // sin(π/16)
+        constexpr float C3 = 0.83146961230254523708f; // cos(3π/16)
+        constexpr float S3 = 0.55557023301960222474f; // sin(3π/16)
+        // cos(πj/16), sin(πj/16) for odd j in [1, 31]
+        constexpr float c = j == 1 ? C1 : j == 3 ? C3 : j == 5 ? S3 : j == 7 ? S1 : j == 9 ? -S1 : j == 11 ? -S3
+                          : j == 13 ? -C3 : j == 15 ? -C1 : j == 17 ? -C1 : j == 19 ? -C3 : j == 21 ? -S3
+                          : j == 23 ? -S1 : j == 25 ? S1 : j == 27 ? S3 : j == 29 ? C3 : C1;
+        constexpr float s = j == 1 ? S1 : j == 3 ? S3 : j == 5 ? C3 : j == 7 ? C1 : j == 9 ? C1 : j == 11 ? C3
+                          : j == 13 ? S3 : j == 15 ? S1 : j == 17 ? -S1 : j == 19 ? -S3 : j == 21 ? -C3
+                          : j == 23 ? -C1 : j == 25 ? -C1 : j == 27 ? -C3 : j == 29 ? -S3 : -S1;
+        return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+    }
+}
+
+template <> struct Dft<32>
+{
+    // 32 = 2 x 16: E = DFT16 of the even points, O = DFT16 of the odd points, y[k] = E[k] + W_32^k O[k] and
+    // y[k + 16] = E[k] - W_32^k O[k] (k < 16).
+    template <int K> __device__ __forceinline__ static void combine(float2* v, const float2* e, const float2* o)
+    {
+        if constexpr (K < 16)
+        {
+            const float2 t = w32mul<K>(o[K]);
+            v[K] = cadd(e[K], t);
+            v[K + 16] = csub(e[K], t);
+            combine<K + 1>(v, e, o);
+        }
+    }
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        float2 e[16], o[16];
+#pragma unroll
+        for (int m = 0; m < 16; ++m)
+        {
+            e[m] = v[2 * m];
+            o[m] = v[2 * m + 1];
+        }
+        Dft<16>::run(e);
+        Dft<16>::run(o);
+        combine<0>(v, e, o);
+    }
+};
+
 // Odd prime radix p in {3, 5, 7}: with a_k = x_k + x_{p-k}, b_k = x_k - x_{p-k} (k = 1 .. h, h = (p-1)/2),
 //   y_m     = x_0 + sum_k cos(2πkm/p) a_k - i sum_k sin(2πkm/p) b_k
 //   y_{p-m} = x_0 + sum_k cos(2πkm/p) a_k + i sum_k sin(2πkm/p) b_k.

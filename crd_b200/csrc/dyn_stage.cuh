@@ -81,6 +81,7 @@ __device__ __forceinline__ void dyn_stages(const int* radix, int nstages, const 
             case 5: dstage<5>(sl, tw, n, L, magic, jt, T, ok); break;
             case 7: dstage<7>(sl, tw, n, L, magic, jt, T, ok); break;
             case 8: dstage<8>(sl, tw, n, L, magic, jt, T, ok); break;
+            case 32: dstage<32>(sl, tw, n, L, magic, jt, T, ok); break;
             default: dstage<16>(sl, tw, n, L, magic, jt, T, ok); break;
         }
         if (L > 1)

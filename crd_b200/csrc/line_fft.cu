@@ -14,6 +14,8 @@ namespace lfft
 // The compile-time schedules (one translation unit each, sched_*.cu).
 KernelFn s_1024_classic(const PassDesc&, const PassShape&);
 KernelFn s_1024w_classic(const PassDesc&, const PassShape&);
+KernelFn s_1024x_classic(const PassDesc&, const PassShape&);
+KernelFn s_8192x_classic(const PassDesc&, const PassShape&);
 KernelFn s_16_classic(const PassDesc&, const PassShape&);
 KernelFn s_32_classic(const PassDesc&, const PassShape&);
 KernelFn s_64_classic(const PassDesc&, const PassShape&);
@@ -37,7 +39,7 @@ KernelFn select_static(const PassDesc& d, const PassShape& sh)
 {
     for (auto f : {s_1024_classic, s_1024w_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic,
                    s_16384_classic, s_105_classic, s_16_classic, s_32_classic, s_64_classic, s_128_classic,
-                   s_2048_classic, s_8192_classic, s_8192w_classic})
+                   s_2048_classic, s_8192_classic, s_8192w_classic, s_1024x_classic, s_8192x_classic})
         if (KernelFn k = f(d, sh))
             return k;
     return nullptr;

@@ -122,11 +122,23 @@ struct Step
 };
 
 // 7-smooth test and the radix schedule: powers of two as 16s with an 8, 4 or 2 for the remainder, then 7s, 5s, 3s.
-bool radices_for(long long n, std::vector<int>& out)
+// With use32, the lengths where a radix-32 schedule measured faster as a unit-stride single pass take it (one
+// exchange through shared memory fewer): 1024 = 32 32 (66 -> 94 % of HBM), 8192 = 32 16 16. (512, 16384 and 32 were
+// slower with radix-32 stages, and so were the strided passes of the four-step.)
+bool radices_for(long long n, std::vector<int>& out, bool use32 = false)
 {
     out.clear();
     if (n < 1)
         return false;
+    if (use32)
+    {
+        switch (n)
+        {
+            case 1024: out = {32, 32}; return true;
+            case 8192: out = {32, 16, 16}; return true;
+            default: break;
+        }
+    }
     long long m = n;
     int twos = 0;
     while (m % 2 == 0)
@@ -176,17 +188,17 @@ bool is_smooth(long long n)
 // Line lengths one pass transforms: every 7-smooth n up to 8192, and 16384.
 bool single_pass_ok(long long n) { return n >= 1 && (n <= 8192 || n == 16384) && is_smooth(n); }
 
-bool has_static_schedule(long long n)
+bool has_static_schedule(long long n, bool use32 = false)
 {
     std::vector<int> rad;
-    if (!radices_for(n, rad) || static_cast<int>(rad.size()) > kMaxStages)
+    if (!radices_for(n, rad, use32) || static_cast<int>(rad.size()) > kMaxStages)
         return false;
     PassDesc d{};
     d.n = static_cast<int>(n);
     d.nstages = static_cast<int>(rad.size());
     for (size_t i = 0; i < rad.size(); ++i)
         d.radix[i] = rad[i];
-    return pass_has_static(d, 16);
+    return pass_has_static(d, 16) || pass_has_static(d, 32);
 }
 
 // The four-step split n = n1 * n2 (pass 1 transforms the n2 columns of length n1, pass 2 the n1 rows of length n2),
@@ -266,6 +278,9 @@ struct Plan
     HostPipe* host = nullptr;
     std::mutex host_mu;
     bool conv = false; // fused convolution plan (crdfft_conv_plan_create): executes with a filter spectrum
+    // Radix-32 schedules for the lengths that have them (FP32 line passes); off for the tensor-core precision forms,
+    // the fused convolution and the uneven batch, whose kernels take the radix-16 schedules.
+    bool use32 = true;
     // Two internal streams for steps with lane 1 / 2, forked from and joined back to the caller's stream.
     cudaStream_t lanes[2] = {nullptr, nullptr};
     cudaEvent_t fork = nullptr;
@@ -371,16 +386,17 @@ void root(long long k, long long n, double* re, double* im)
 // The stage-ordered twiddle table of a line length n with the planner's radix schedule: for each stage after the
 // first (radix R, after radices multiplying to L), W_{LR}^{r k} = W_n^{r k n/(L R)} at (r-1) L + k. Each entry is
 // computed in FP64 and narrowed once (fft.hpp:251-260).
-crdfft_status twiddle_table(Plan& p, long long n, const void** out)
+crdfft_status twiddle_table(Plan& p, long long n, const void** out, bool r32 = false)
 {
-    auto it = p.tw_by_n.find(n);
+    const long long key = r32 ? n | (1LL << 48) : n; // one table per (length, schedule family)
+    auto it = p.tw_by_n.find(key);
     if (it != p.tw_by_n.end())
     {
         *out = it->second;
         return CRDFFT_OK;
     }
     std::vector<int> rad;
-    if (!radices_for(n, rad))
+    if (!radices_for(n, rad, r32))
         return CRDFFT_UNSUPPORTED_SIZE;
     std::vector<float> h;
     long long L = 1;
@@ -403,7 +419,7 @@ crdfft_status twiddle_table(Plan& p, long long n, const void** out)
     const crdfft_status st = upload_table(p, h, &d);
     if (st != CRDFFT_OK)
         return st;
-    p.tw_by_n[n] = d;
+    p.tw_by_n[key] = d;
     *out = d;
     return CRDFFT_OK;
 }
@@ -495,11 +511,16 @@ bool heuristic_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape
             return true;
         }
     }
-    const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, 16);
-    if (sh.threads_per_line * sh.lines_per_cta > pass_threads_limit() || !pass_has_kernel(d, sh))
-        return false;
-    *out = sh;
-    return true;
+    for (int P : {16, 32}) // the radix-32 schedules exist at 32 points a thread only
+    {
+        const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, P);
+        if (sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit() && pass_has_kernel(d, sh))
+        {
+            *out = sh;
+            return true;
+        }
+    }
+    return false;
 }
 
 // Every launch shape the planner can measure for a pass: classic at 16 and 32 points a thread with one, two or
@@ -619,7 +640,9 @@ crdfft_status make_pass_desc(Plan& p, long long n, long long lines, long long lp
                              bool conj_in, bool conj_out, float scale, const FourStepTw& ftw, PassDesc* out_desc)
 {
     std::vector<int> rad;
-    if (!single_pass_ok(n) || !radices_for(n, rad) || static_cast<int>(rad.size()) > kMaxStages)
+    // radix-32 schedules for unit-stride passes only (the single passes)
+    const bool r32 = p.use32 && in.estride == 1 && out.estride == 1;
+    if (!single_pass_ok(n) || !radices_for(n, rad, r32) || static_cast<int>(rad.size()) > kMaxStages)
         return CRDFFT_UNSUPPORTED_SIZE;
     PassDesc d{};
     d.n = static_cast<int>(n);
@@ -630,7 +653,7 @@ crdfft_status make_pass_desc(Plan& p, long long n, long long lines, long long lp
     d.lines_per_group = lpg;
     d.in = in;
     d.out = out;
-    const crdfft_status st = twiddle_table(p, n, &d.tw);
+    const crdfft_status st = twiddle_table(p, n, &d.tw, r32);
     if (st != CRDFFT_OK)
         return st;
     d.ftw_M = ftw.M;
@@ -1346,6 +1369,7 @@ template <typename T> crdfft_status upload_vec(Plan& p, const std::vector<T>& v,
 // List order: every COL item (longest transforms first), then SMALL items (longest first), then ROW items.
 crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const int64_t* offsets)
 {
+    p.use32 = false; // the uneven kernel's stages run 16 points a thread
     const int threads = uneven_threads();
     const long long kUnevenSingle = 16LL * threads; // the longest line one item transforms (16 points a thread)
     std::map<long long, int> sched_of;
@@ -1570,6 +1594,7 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
     std::unique_ptr<Plan> p(new Plan());
     p->desc = *desc;
     p->device = dev;
+    p->use32 = desc->precision == CRDFFT_PREC_FP32 && conv == nullptr;
     {
         void* e = nullptr;
         if (dev_alloc(&e, 256) != cudaSuccess)

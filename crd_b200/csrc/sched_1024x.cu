@@ -1,0 +1,12 @@
+// Compile-time schedule 32 x 32 (n = 1024), 32 points a thread: the classic kernel (radix-32 stages, one
+// exchange through shared memory fewer than the radix-16 schedule of the same length).
+
+#include "line_fft.cuh"
+
+namespace crdfft
+{
+namespace lfft
+{
+CRDFFT_DEFINE_SCHEDULE(s_1024x, 32, 32,32)
+} // namespace lfft
+} // namespace crdfft

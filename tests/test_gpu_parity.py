@@ -284,7 +284,7 @@ def test_bounded_wait_reports_timeout(monkeypatch):
     completes) gives up after its iteration limit, reports CRDFFT_DEVICE_TIMEOUT, and leaves the context usable."""
     from crd_b200.hesap import device_status, stall_waits
 
-    n, batch = 1024, 64
+    n, batch = 256, 256  # a length with a pipelined instance
     x = torch.from_numpy(oracle.lcg_complex64(3, n * batch)).cuda()
     y = torch.empty_like(x)
     monkeypatch.setenv("CRDFFT_PIPELINE", "1")
@@ -308,7 +308,7 @@ def test_bounded_wait_reports_timeout(monkeypatch):
 
 def test_pipelined_and_classic_agree_bitwise(monkeypatch):
     """The pipelined kernel and the classic kernel run the same butterflies in the same order: same bits."""
-    for n, batch in ((1024, 33), (4096, 9), (65536, 2)):
+    for n, batch in ((256, 33), (4096, 9), (65536, 2)):
         x = torch.from_numpy(oracle.lcg_complex64(n + 1, n * batch)).cuda()
         a = torch.empty_like(x)
         b = torch.empty_like(x)
