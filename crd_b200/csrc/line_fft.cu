@@ -154,10 +154,12 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
     lfft::KernelFn fn = lfft::select_static(d, cs);
     if (fn == nullptr)
     {
-        // the run-time schedule kernel always stages its lines through shared memory (even a one-stage pass that
-        // a compile-time kernel runs register to register)
+        // the run-time schedule kernel always stages its lines through shared memory, in two buffers (even for a
+        // one-stage pass that a compile-time kernel runs register to register)
         fn = lfft::select_dynamic(d, cs);
-        cs.smem_bytes = sh.lines_per_cta * lfft::line_pitch(d.n) * 8;
+        cs.smem_bytes = 2 * sh.lines_per_cta * lfft::line_pitch(d.n) * 8; // two line buffers: out-of-place stages
+        if (cs.smem_bytes > 227 * 1024)
+            return cudaErrorInvalidConfiguration;
     }
     if (fn == nullptr || threads > lfft::kMaxThreads)
         return cudaErrorInvalidConfiguration;

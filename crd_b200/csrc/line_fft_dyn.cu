@@ -2,9 +2,10 @@
 // 8192 that has no compile-time schedule (2048, 8192, 1000, 6144, ..., the uneven batches' lengths, Bluestein's inner
 // lengths, odd N-D axes).
 //
-// The CTA stages its lines through shared memory with coalesced cooperative loads and stores (along whichever side
-// is unit-stride, with the epilogue on the way out), and runs the stages as out-of-line per-radix functions
-// (dyn_stage.cuh): a kernel that inlines every radix's stage variants spills heavily and ran ten times slower.
+// The CTA stages its lines through shared memory with coalesced cooperative loads (every load of a thread in flight
+// at once) and stores (along whichever side is unit-stride, with the epilogue on the way out), and runs the stages
+// as out-of-line per-radix functions that ping-pong between two halves of shared memory (dyn_stage.cuh): no register
+// spills, so no local-memory traffic.
 
 #include "dyn_stage.cuh"
 #include "line_fft.cuh"
@@ -58,19 +59,25 @@ __global__ void __launch_bounds__(kMaxThreads) dyn_fft_kernel(const PassDesc d, 
     init_scales(d, c);
     const long long lines_here = d.lines - line0;
     const long long ies = d.in.estride;
-    for_tile(n, lpc, ies == 1, [&](int a, int e) {
-        if (a < lines_here)
-            LayRow<1>{sm + a * pitch}.at(e) = load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * ies);
-    });
+    tile_load<16>(
+        n, lpc, ies == 1,
+        [&](int a, int e) {
+            return a < lines_here ? load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * ies)
+                                  : make_float2(0.f, 0.f);
+        },
+        [&](int a, int e, float2 x) { LayRow<1>{sm + a * pitch}.at(e) = x; });
     __syncthreads();
 
-    dyn_stages(s_radix, d.nstages, static_cast<const float2*>(d.tw), n, sm + ll * pitch, jt, T, ll < lines_here);
+    // out of place between the two halves of shared memory (lpc lines each)
+    const float2* res = dyn_stages_pp(s_radix, d.nstages, static_cast<const float2*>(d.tw), n, sm + ll * pitch,
+                                      sm + (lpc + ll) * pitch, jt, T, ll < lines_here);
+    float2* tile = const_cast<float2*>(res) - ll * pitch; // the half that holds the result
 
     const long long oes = d.out.estride;
     for_tile(n, lpc, oes == 1, [&](int a, int e) {
         if (a < lines_here)
             __stcs(gout + s_out_off[a] + static_cast<long long>(e) * oes,
-                   epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
+                   epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{tile + a * pitch}.at(e)));
     });
 }
 

@@ -13,7 +13,7 @@
 // which finish without waiting on anything: the ROW item's wait on the transform's completion counter always ends.
 // It is bounded anyway (spin_limit polls): a wait that runs out sets the plan's status word and skips the item.
 //
-// Each item's stages are the line-FFT kernel's run-time radix schedule (line_fft.cuh).
+// Each item runs the stages of its length's run-time radix schedule out of place (dyn_stage.cuh).
 
 #include "kernels.hpp"
 #include "line_fft.cuh"
@@ -34,6 +34,8 @@ constexpr int kUnevenThreads = 256;
 __device__ __forceinline__ void uneven_load(int n, int lines, long long estride, const long long* base,
                                             const float2* src, float2* sm, int pitch, float in_im, bool l2_only)
 {
+    // (one element at a time: holding a batch of loads in registers spills in this 80-register kernel, which
+    // measured slower)
     for_tile(n, lines, estride == 1, [&](int a, int e) {
         const float2* p = src + base[a] + static_cast<long long>(e) * estride;
         float2 x = l2_only ? __ldcg(p) : __ldcs(p);
@@ -122,11 +124,14 @@ __global__ void __launch_bounds__(kUnevenThreads, 3)
         const int T = (n + 15) / 16;
         const int ll = tid / T;
         const bool ok = ll < it.lines;
-        dyn_stages(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n, sm + (ok ? ll : 0) * pitch, tid - ll * T,
-                   T, ok);
+        // out of place between two buffers of the item's lines (the second right after the first)
+        const int lrow = ok ? ll : 0;
+        const float2* res = dyn_stages_pp(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
+                                          sm + lrow * pitch, sm + (it.lines + lrow) * pitch, tid - ll * T, T, ok);
+        const float2* tile = res - lrow * pitch;
         const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_hi[it.ftw]) : nullptr;
         const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_lo[it.ftw]) : nullptr;
-        uneven_store(n, it.lines, it.out_estride, s_out, it.q0, fh, fl, dst, sm, pitch,
+        uneven_store(n, it.lines, it.out_estride, s_out, it.q0, fh, fl, dst, tile, pitch,
                      last_pass ? u.scale : 1.0f, last_pass ? out_im : 1.0f);
         if (it.kind == kUnevenCol)
         {
