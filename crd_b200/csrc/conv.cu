@@ -84,8 +84,17 @@ template <class S, int P> ConvFn conv_pick(PassMap map)
 ConvFn conv_select(const PassDesc& d, PassMap map, int P)
 {
     if (P == 32)
-        return same_radices(d, {16, 16, 16}) && map == PassMap::Row ? conv_kernel<Sched<16, 16, 16>, 32, PassMap::Row>
-                                                                    : nullptr;
+    {
+        if (map != PassMap::Row)
+            return nullptr;
+        if (same_radices(d, {16, 16, 16}))
+            return conv_kernel<Sched<16, 16, 16>, 32, PassMap::Row>;
+        if (same_radices(d, {32, 32}))
+            return conv_kernel<Sched<32, 32>, 32, PassMap::Row>;
+        if (same_radices(d, {32, 16, 16}))
+            return conv_kernel<Sched<32, 16, 16>, 32, PassMap::Row>;
+        return nullptr;
+    }
     if (same_radices(d, {16, 16}))
         return conv_pick<Sched<16, 16>, 16>(map);
     if (same_radices(d, {16, 8, 4}))
@@ -103,10 +112,11 @@ bool conv_supported(const PassDesc& d)
     return d.nstages > 0 && (d.n + 15) / 16 <= lfft::kMaxThreads;
 }
 
-// Lines a CTA and points a thread: about 256 threads a CTA (the n = 4096 lines at 32 points a thread).
+// Lines a CTA and points a thread: about 256 threads a CTA (32 points a thread for the n = 4096 lines and the
+// radix-32 schedules).
 void conv_shape(const PassDesc& d, PassMap map, int* P, int* lpc, int* smem)
 {
-    *P = (map == PassMap::Row && lfft::same_radices(d, {16, 16, 16})) ? 32 : 16;
+    *P = (map == PassMap::Row && (lfft::same_radices(d, {16, 16, 16}) || d.radix[0] == 32)) ? 32 : 16;
     const int T = (d.n + *P - 1) / *P;
     int l = std::max(1, 256 / T);
     if (map == PassMap::Col)

@@ -278,8 +278,8 @@ struct Plan
     HostPipe* host = nullptr;
     std::mutex host_mu;
     bool conv = false; // fused convolution plan (crdfft_conv_plan_create): executes with a filter spectrum
-    // Radix-32 schedules for the lengths that have them (FP32 line passes); off for the tensor-core precision forms,
-    // the fused convolution and the uneven batch, whose kernels take the radix-16 schedules.
+    // Radix-32 schedules for the lengths that have them (FP32 unit-stride passes); off for the tensor-core precision
+    // forms and the uneven batch, whose kernels take the radix-16 schedules.
     bool use32 = true;
     // Two internal streams for steps with lane 1 / 2, forked from and joined back to the caller's stream.
     cudaStream_t lanes[2] = {nullptr, nullptr};
@@ -1594,7 +1594,7 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
     std::unique_ptr<Plan> p(new Plan());
     p->desc = *desc;
     p->device = dev;
-    p->use32 = desc->precision == CRDFFT_PREC_FP32 && conv == nullptr;
+    p->use32 = desc->precision == CRDFFT_PREC_FP32;
     {
         void* e = nullptr;
         if (dev_alloc(&e, 256) != cudaSuccess)
