@@ -10,6 +10,7 @@
 // stages are the line-FFT kernel's (line_fft.cuh). A row map serves 1-D batches; a column map serves the column
 // pass of a 2-D convolution (rows FFT, fused column convolution, inverse rows FFT).
 
+#include "dyn_stage.cuh"
 #include "kernels.hpp"
 #include "line_fft.cuh"
 
@@ -72,6 +73,83 @@ __global__ void __launch_bounds__(kMaxThreads)
     SchedRun<S>::template go<P, false, true, false, Kind<MAP, true>>(d, c, lay, n);
 }
 
+// The same convolution for lengths without a compile-time schedule: lines staged through shared memory with
+// coalesced loads and stores, both FFTs as out-of-place run-time stages between two line buffers (dyn_stage.cuh).
+template <PassMap MAP>
+__global__ void __launch_bounds__(kMaxThreads)
+    conv_dyn_kernel(const PassDesc d, const float2* __restrict__ gin, const float2* __restrict__ spec,
+                    const LineMap smap, float2* __restrict__ gout)
+{
+    extern __shared__ float2 sm[];
+    __shared__ long long s_in_off[kMaxLinesPerCta];
+    __shared__ long long s_out_off[kMaxLinesPerCta];
+    __shared__ int s_radix[kMaxStages];
+    const int n = d.n;
+    const int T = (n + 15) / 16;
+    const int lpc = blockDim.x / T;
+    const int tid = threadIdx.x;
+    const int pitch = line_pitch(n);
+    const long long line0 = static_cast<long long>(blockIdx.x) * lpc;
+    int ll, jt;
+    if constexpr (MAP == PassMap::Row)
+    {
+        ll = tid / T;
+        jt = tid - ll * T;
+    }
+    else
+    {
+        jt = tid / lpc;
+        ll = tid - jt * lpc;
+    }
+    for (int i = tid; i < lpc; i += blockDim.x)
+    {
+        s_in_off[i] = line_offset(d.in, line0 + i, d.lines_per_group);
+        s_out_off[i] = line_offset(d.out, line0 + i, d.lines_per_group);
+    }
+    if (tid < kMaxStages)
+        s_radix[tid] = d.radix[tid];
+    __syncthreads();
+    const long long lines_here = d.lines - line0;
+    const bool ok = ll < lines_here;
+    const long long ies = d.in.estride;
+    tile_load<16>(
+        n, lpc, ies == 1,
+        [&](int a, int e) {
+            return a < lines_here ? __ldcs(gin + s_in_off[a] + static_cast<long long>(e) * ies) : make_float2(0.f, 0.f);
+        },
+        [&](int a, int e, float2 x) { LayRow<1>{sm + a * pitch}.at(e) = x; });
+    __syncthreads();
+    const float2* tw = static_cast<const float2*>(d.tw);
+    float2* bufa = sm + ll * pitch;
+    float2* bufb = sm + (lpc + ll) * pitch;
+    // forward FFT
+    float2* x = dyn_stages_pp(s_radix, d.nstages, tw, n, bufa, bufb, jt, T, ok);
+    // Z = conj(X H)
+    if (ok)
+    {
+        const float2* h = spec + line_offset(smap, line0 + ll, d.lines_per_group);
+        for (int e = jt; e < n; e += T)
+        {
+            const float2 v = cmul(LayRow<1>{x}.at(e), __ldg(h + static_cast<long long>(e) * smap.estride));
+            LayRow<1>{x}.at(e) = make_float2(v.x, -v.y);
+        }
+    }
+    __syncthreads();
+    // conj(FFT(Z)) * scale
+    float2* y = dyn_stages_pp(s_radix, d.nstages, tw, n, x, x == bufa ? bufb : bufa, jt, T, ok);
+    float2* tile = y - ll * pitch;
+    const float re = d.scale;
+    const float im = d.conj_out ? -d.scale : d.scale;
+    const long long oes = d.out.estride;
+    for_tile(n, lpc, oes == 1, [&](int a, int e) {
+        if (a < lines_here)
+        {
+            const float2 v = LayRow<1>{tile + a * pitch}.at(e);
+            __stcs(gout + s_out_off[a] + static_cast<long long>(e) * oes, make_float2(v.x * re, v.y * im));
+        }
+    });
+}
+
 using ConvFn = void (*)(const PassDesc, const float2*, const float2*, const LineMap, float2*);
 
 template <class S, int P> ConvFn conv_pick(PassMap map)
@@ -101,7 +179,12 @@ ConvFn conv_select(const PassDesc& d, PassMap map, int P)
         return conv_pick<Sched<16, 8, 4>, 16>(map);
     if (same_radices(d, {16, 16, 4}))
         return conv_pick<Sched<16, 16, 4>, 16>(map);
-    return conv_pick<DynSched, 16>(map);
+    return map == PassMap::Row ? conv_dyn_kernel<PassMap::Row> : conv_dyn_kernel<PassMap::Col>;
+}
+
+bool conv_is_dynamic(const PassDesc& d, PassMap map, int P)
+{
+    return P == 16 && !same_radices(d, {16, 16}) && !same_radices(d, {16, 8, 4}) && !same_radices(d, {16, 16, 4});
 }
 
 } // namespace
@@ -135,6 +218,12 @@ cudaError_t launch_conv(const PassDesc& d, PassMap map, const LineMap& smap, con
     lfft::ConvFn fn = lfft::conv_select(d, map, P);
     if (fn == nullptr)
         return cudaErrorInvalidConfiguration;
+    if (lfft::conv_is_dynamic(d, map, P))
+    {
+        smem *= 2; // two line buffers
+        if (smem > 227 * 1024)
+            return cudaErrorInvalidConfiguration;
+    }
     const int T = (d.n + P - 1) / P;
     const long long groups = (d.lines + lpc - 1) / lpc;
     if (groups <= 0)
