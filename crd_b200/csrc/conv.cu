@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kMaxThreads)
     const long long line = line0 + ll;
     Ctx c;
     c.ok = line < d.lines;
-    c.q = line % d.lines_per_group;
+    c.q = (line % d.lines_per_group) / d.ftw_div;
     c.in = gin + line_offset(d.in, line, d.lines_per_group);
     c.out = gout + line_offset(d.out, line, d.lines_per_group);
     c.jt = jt;

@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
             const long long line = line0 + i;
             s_in_off[i] = line_offset(d.in, line, d.lines_per_group);
             s_out_off[i] = line_offset(d.out, line, d.lines_per_group);
-            s_q[i] = static_cast<int>(line % d.lines_per_group);
+            s_q[i] = static_cast<int>(line % d.lines_per_group) / d.ftw_div;
         }
         __syncthreads();
     }
@@ -416,7 +416,7 @@ __global__ void __launch_bounds__(kMaxThreads) line_fft_kernel(const PassDesc d,
     const long long line = line0 + ll;
     Ctx c;
     c.ok = line < d.lines;
-    c.q = line % d.lines_per_group;
+    c.q = (line % d.lines_per_group) / d.ftw_div;
     c.in = gin + line_offset(d.in, line, d.lines_per_group);
     c.out = gout + line_offset(d.out, line, d.lines_per_group);
     c.jt = jt;
@@ -635,12 +635,12 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
             {
                 const long long ln = grp * lpc + i;
                 s_out_off[i] = line_offset(d.out, ln, d.lines_per_group);
-                s_q[i] = static_cast<int>(ln % d.lines_per_group);
+                s_q[i] = static_cast<int>(ln % d.lines_per_group) / d.ftw_div;
             }
         }
         const long long line = grp * lpc + ll;
         c.ok = line < d.lines;
-        c.q = line % d.lines_per_group;
+        c.q = (line % d.lines_per_group) / d.ftw_div;
         c.in = gin;
         c.out = gout + line_offset(d.out, line, d.lines_per_group);
         if constexpr (MAP == PassMap::Row)

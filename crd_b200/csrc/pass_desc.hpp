@@ -37,12 +37,14 @@ struct PassDesc
                                  // radices multiplying to L), W_{LR}^{r k} at (r-1) L + k, stages back to back
     // Four-step twiddle, fused into the store: output element k of line q is multiplied by W_M^{q*k}
     // (q < n2, k < n1 = n) = hi[(q>>4) n + k] * lo[16 k + (q&15)] with hi = W_M^{16 a k}, lo = W_M^{b k}.
-    // Off when ftw_M == 0. (ftw_base / ftw_shift are unused by the kernels.)
+    // Off when ftw_M == 0. The twiddle row q of a line is (its index within its group) / ftw_div: 1 for a 1-D
+    // four-step (lines of a group are the columns), the column count for a split column pass of a 2-D array (the
+    // lines of a group are (q, column) pairs, column fastest).
     const void* ftw_hi;
     const void* ftw_lo;
     long long ftw_M;
-    int ftw_base;
-    int ftw_shift;
+    int ftw_div;
+    int ftw_unused;
     int conj_in;                 // conjugate every input element (inverse via conj(DFT(conj x)))
     int conj_out;                // conjugate every output element
     float scale;                 // multiply every output element (1 = off)

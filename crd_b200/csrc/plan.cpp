@@ -629,8 +629,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
 struct FourStepTw
 {
     long long M = 0;
-    int base = 0;
-    int shift = 0;
+    int div = 1; // twiddle row = (line index within its group) / div
     const void* hi = nullptr;
     const void* lo = nullptr;
 };
@@ -657,8 +656,8 @@ crdfft_status make_pass_desc(Plan& p, long long n, long long lines, long long lp
     if (st != CRDFFT_OK)
         return st;
     d.ftw_M = ftw.M;
-    d.ftw_base = ftw.base;
-    d.ftw_shift = ftw.shift;
+    d.ftw_div = ftw.div > 0 ? ftw.div : 1;
+    d.ftw_unused = 0;
     d.ftw_hi = ftw.hi;
     d.ftw_lo = ftw.lo;
     d.err = p.err;
@@ -1192,6 +1191,61 @@ crdfft_status build_nd(Plan& p)
     };
     const float inv_scale =
         d.norm == CRDFFT_NORM_INVERSE ? static_cast<float>(1.0 / static_cast<double>(total)) : 1.0f;
+    // Long columns of a packed 2-D batch (rows x cols, rows >= 2048): one column pass would hold only a few columns
+    // a CTA (32-byte runs). Instead the column FFT of length rows = n1 n2 runs as two strided passes of short lines,
+    // each CTA holding 64 or more adjacent columns (512-byte runs): C1 transforms the n1-point sub-columns j1 n2 + q
+    // in place with the four-step twiddle W_rows^{q k1}, C2 the n2-point sub-columns k1 n2 + q into rows
+    // k1 + n1 k2. The row pass writes the workspace, C1 works on it, C2 writes the output (one step per batch
+    // member, up to 8).
+    long long cn1 = 0, cn2 = 0;
+    const bool split_cols = rank == 2 && d.dims[0] >= 2048 && d.dims[1] >= 16 && idist == total && odist == total &&
+                            d.batch <= 8 && p.desc.precision == CRDFFT_PREC_FP32 &&
+                            std::getenv("CRDFFT_NO_SPLIT_COLUMNS") == nullptr &&
+                            four_step_split(d.dims[0], &cn1, &cn2) && single_pass_ok(d.dims[1]);
+    if (split_cols)
+    {
+        const long long rows = d.dims[0], cols = d.dims[1];
+        const void* hi = nullptr;
+        const void* lo = nullptr;
+        crdfft_status st = four_step_tables(p, rows, cn1, cn2, &hi, &lo);
+        if (st != CRDFFT_OK)
+            return st;
+        for (int dir = 0; dir < 2; ++dir)
+        {
+            Step r;
+            st = make_line_step(p, cols, d.batch * rows, 1, LineMap{cols, 0, 1}, LineMap{cols, 0, 1},
+                                BufRef{Buf::In, 0}, BufRef{Buf::Ws, 0}, dir == 1, false, 1.0f, &r);
+            if (st != CRDFFT_OK)
+                return st;
+            p.steps[dir].push_back(r);
+            FourStepTw ftw;
+            ftw.M = rows;
+            ftw.hi = hi;
+            ftw.lo = lo;
+            ftw.div = static_cast<int>(cols);
+            Step c1;
+            st = make_line_step(p, cn1, d.batch * cn2 * cols, cn2 * cols, LineMap{total, 1, cn2 * cols},
+                                LineMap{total, 1, cn2 * cols}, BufRef{Buf::Ws, 0}, BufRef{Buf::Ws, 0}, false, false,
+                                1.0f, &c1, ftw);
+            if (st != CRDFFT_OK)
+                return st;
+            p.steps[dir].push_back(c1);
+            for (long long b = 0; b < d.batch; ++b)
+            {
+                Step c2;
+                st = make_line_step(p, cn2, cn1 * cols, cols, LineMap{cn2 * cols, 1, cols},
+                                    LineMap{cols, 1, cn1 * cols}, BufRef{Buf::Ws, b * total},
+                                    BufRef{Buf::Out, b * total}, false, dir == 1, dir == 1 ? inv_scale : 1.0f, &c2);
+                if (st != CRDFFT_OK)
+                    return st;
+                p.steps[dir].push_back(c2);
+            }
+        }
+        p.ws_bytes = static_cast<size_t>(d.batch * total) * 8;
+        p.algorithm = "nd-axes-split-columns";
+        p.factors = {rows, cols, cn1, cn2};
+        return CRDFFT_OK;
+    }
     for (int dir = 0; dir < 2; ++dir)
     {
         // Axes from the last (unit stride) to the first; the first pass reads the input, later ones work in place
