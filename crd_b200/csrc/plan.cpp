@@ -1199,8 +1199,7 @@ crdfft_status build_nd(Plan& p)
     // member, up to 8).
     long long cn1 = 0, cn2 = 0;
     const bool split_cols = rank == 2 && d.dims[0] >= 2048 && d.dims[1] >= 16 && idist == total && odist == total &&
-                            d.batch <= 8 && p.desc.precision == CRDFFT_PREC_FP32 &&
-                            std::getenv("CRDFFT_NO_SPLIT_COLUMNS") == nullptr &&
+                            d.batch <= 8 && std::getenv("CRDFFT_NO_SPLIT_COLUMNS") == nullptr &&
                             four_step_split(d.dims[0], &cn1, &cn2) && single_pass_ok(d.dims[1]);
     if (split_cols)
     {
@@ -1242,7 +1241,7 @@ crdfft_status build_nd(Plan& p)
             }
         }
         p.ws_bytes = static_cast<size_t>(d.batch * total) * 8;
-        p.algorithm = "nd-axes-split-columns";
+        p.algorithm = "nd-axes-split-columns"; // (+tc-... appended by create() when the row pass is a TC pass)
         p.factors = {rows, cols, cn1, cn2};
         return CRDFFT_OK;
     }
