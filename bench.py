@@ -144,8 +144,10 @@ WORKLOAD_CONFIGS = {
                "l2": "about 2.5 GB moved per step (> 126 MB L2)"},
     "nd": {"workload": "nd_c2c_fp32_4096x4096_512x512x512", "inputs": "uniform[-1,1) + 1% x 1e4",
            "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
-    "conv": {"workload": "fused_conv_1d_N256_1024_4096_2^25_points", "filter": "one spectrum shared by the batch",
-             "l2": "256 MiB input per size (> 126 MB L2)", "flops": "10 N log2 N + 6 N per signal"},
+    "conv": {"workload": "fused_conv_1d_N256_1024_4096_2^25_points_real_N1024_4096_2^26_points_real2d_4096x4096x4",
+             "filter": "one spectrum shared by the batch",
+             "l2": "256 MiB input per size (> 126 MB L2)",
+             "flops": "complex: 10 N log2 N + 6 N per signal; real: 5 N log2 N + 3 N per signal"},
     "precision": {"workload": "nd_c2c_4096x4096_512x512x512_fp32_splitbf16_fp16", "inputs": "uniform[-1,1) + 1% x 1e4",
                   "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
 }
@@ -379,6 +381,7 @@ def build_nd(dev, rank, cf):
 
 CONV_SIZES = (256, 1024, 4096)
 CONV_POINTS = 1 << 25  # per size: 256 MiB of complex64 input (> 126 MB L2)
+REAL_CONV_DIMS = ((1024,), (4096,), (4096, 4096))  # real signals, 2^26 points (256 MiB of float32) each
 
 
 def build_conv(dev, rank, cf):
@@ -409,6 +412,38 @@ def build_conv(dev, rank, cf):
                 b * (10.0 * n * math.log2(n) + 6.0 * n), 16 * n * b, 1, check,
                 {"batch": b, "algorithm": plan.info()["algorithm"]})
         op.peer = ("cufft_3pass", lambda n=n, b=b, H=H: torch.fft.ifft(torch.fft.fft(xin.view(b, n)) * H))
+        ops.append(op)
+    # real signals: the half spectrum, one launch a batch (1-D) or R2C rows, half-width column convolution, C2R rows
+    # (2-D); the same 256 MiB buffers read as float32
+    rin, rout = xin.view(torch.float32), xout.view(torch.float32)
+    for dims in REAL_CONV_DIMS:
+        pts = int(np.prod(dims))
+        b = (2 * CONV_POINTS) // pts
+        hw = dims[-1] // 2 + 1
+        hshape = tuple(dims[:-1]) + (hw,)
+        plan = cf.ConvPlan(list(dims), batch=b, real=True)
+        H = (torch.rand(2 * int(np.prod(hshape)), generator=gen, device=dev, dtype=torch.float32) * 2 - 1)
+        H = H.view(torch.complex64).view(hshape)
+        name = "rconv" + "x".join(str(v) for v in dims)
+        axes = tuple(range(1, len(dims) + 1))
+
+        def rcheck(dims=dims, b=b, plan=plan, H=H, axes=axes):
+            plan.execute(rin, H, rout)
+            torch.cuda.synchronize()
+            x = rin.view((b,) + tuple(dims))[:: max(1, b // 4)].cpu().numpy().astype(np.float64)
+            want = np.fft.irfftn(np.fft.rfftn(x, axes=axes) * H.cpu().numpy().astype(np.complex128), s=dims,
+                                 axes=axes)
+            return _rel(rout.view((b,) + tuple(dims))[:: max(1, b // 4)].cpu().numpy(), want)
+
+        op = Op(name, rin, rout, lambda i, o, plan=plan, H=H: plan.execute(i, H, o),
+                b * (5.0 * pts * math.log2(pts) + 3.0 * pts), 8 * pts * b, plan.info()["passes"], rcheck,
+                {"batch": b, "algorithm": plan.info()["algorithm"]})
+        if len(dims) == 1:
+            op.peer = ("cufft_3pass", lambda n=dims[0], b=b, H=H: torch.fft.irfft(
+                torch.fft.rfft(rin.view(b, n)) * H, n))
+        else:
+            op.peer = ("cufft_3pass", lambda dims=dims, b=b, H=H: torch.fft.irfft2(
+                torch.fft.rfft2(rin.view((b,) + tuple(dims))) * H, s=dims))
         ops.append(op)
     return ops, dict(WORKLOAD_CONFIGS["conv"])
 
@@ -517,6 +552,25 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
 
             timed(run, count * (10.0 * n * math.log2(n) + 6.0 * n), f"conv{n}")
             sample.append(f"conv N={n} x{count}")
+        # real signals: RealFftPlan rfft, the product with the half spectrum, irfft (normalised: the 1/N)
+        for dims in REAL_CONV_DIMS:
+            if len(dims) != 1:
+                continue  # the reference's real plans are 1-D (real_fft.hpp)
+            n = dims[0]
+            count = max(threads, min((2 * CONV_POINTS) // n, budget_bytes // (4 * n)))
+            x = oracle.lcg_float32(SEED ^ (n + 13), n * count)
+            H = oracle.lcg_complex64(SEED ^ (n + 14), n // 2 + 1)
+            spec = np.empty(count * (n // 2 + 1), dtype=np.complex64)
+            back = np.empty(n * count, dtype=np.float32)
+
+            def rrun(n=n, count=count, x=x, H=H, spec=spec, back=back):
+                R.crdref_rfft_f32(n, count, x.ctypes.data_as(fp), spec.view(np.float32).ctypes.data_as(fp), threads)
+                spec.reshape(count, n // 2 + 1)[:] *= H
+                R.crdref_irfft_f32(n, count, spec.view(np.float32).ctypes.data_as(fp), back.ctypes.data_as(fp),
+                                   threads)
+
+            timed(rrun, count * (5.0 * n * math.log2(n) + 3.0 * n), f"rconv{n}")
+            sample.append(f"real conv N={n} x{count}")
     elif workload == "r2c":
         n = 1 << 20
         count = max(threads, min(512, budget_bytes // (4 * n)))

@@ -20,6 +20,27 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
 bool conv_supported(const PassDesc& d);
 cudaError_t launch_conv(const PassDesc& d, PassMap map, const LineMap& smap, const void* in, const void* spec,
                         void* out, cudaStream_t stream);
+// Lines a CTA, points a thread and shared memory of a fused convolution pass (conv.cu).
+void conv_shape(const PassDesc& d, PassMap map, int* P, int* lpc, int* smem);
+
+// Real-data line kernels (real_line.cu): the pass describes the M-point complex lines (n = 2M reals), row map,
+// unit stride. R2C: in = M real pairs a line, out = M + 1 complex. C2R: in = M + 1 complex, out = M real pairs,
+// conj_out set. Conv: real pairs in and out, the half spectrum (M + 1 values a line) at line_offset(smap, l),
+// conj_out set. wn holds W_n^k for k = 0 .. M/2 at least.
+enum : int
+{
+    kRealR2C = 0,
+    kRealC2R = 1,
+    kRealConv = 2,
+};
+struct RealLineAux
+{
+    const void* wn;
+    LineMap smap;
+};
+bool real_line_supported(const PassDesc& d);
+cudaError_t launch_real_line(const PassDesc& d, int mode, const RealLineAux& r, const void* in, const void* spec,
+                             void* out, cudaStream_t stream);
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
 int pass_threads_limit();

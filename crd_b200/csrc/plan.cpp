@@ -96,6 +96,7 @@ enum class StepKind : int
     Cluster,
     TcLine,
     Conv,
+    RealLine,
     R2CPost,
     C2RPre,
     ChirpPre,
@@ -113,6 +114,8 @@ struct Step
     const void* amat = nullptr;
     PassShape shape{};
     LineMap smap{};   // Conv: where each line's filter spectrum sits
+    int rmode = 0;    // RealLine: kRealR2C, kRealC2R or kRealConv
+    RealLineAux raux{};
     int lane = 0;     // 0: the caller's stream; 1, 2: the plan's two internal streams (L2-sized four-step waves)
     RealRecombine real{};
     ChirpDesc chirp{};
@@ -1109,6 +1112,34 @@ crdfft_status build_real(Plan& p)
     crdfft_status st = upload_table(p, wn, &dwn);
     if (st != CRDFFT_OK)
         return st;
+    // A half length that runs as a single pass: one launch, the recombination fused with the line FFT in shared
+    // memory (real_line.cu); the real data crosses HBM once each way.
+    if (single_pass_ok(h) && std::getenv("CRDFFT_NO_FUSED_REAL") == nullptr)
+    {
+        const bool r2c = d.kind == CRDFFT_R2C;
+        const long long idist = d.idist ? d.idist : (r2c ? n : h + 1);
+        const long long odist = d.odist ? d.odist : (r2c ? h + 1 : n);
+        if ((r2c ? idist : odist) % 2 != 0)
+            return CRDFFT_UNSUPPORTED_SIZE;
+        Step s;
+        s.kind = StepKind::RealLine;
+        s.rmode = r2c ? kRealR2C : kRealC2R;
+        s.raux = RealLineAux{dwn, LineMap{0, 0, 1}};
+        const LineMap in = r2c ? LineMap{idist / 2, 0, 1} : LineMap{idist, 0, 1};
+        const LineMap out = r2c ? LineMap{odist, 0, 1} : LineMap{odist / 2, 0, 1};
+        const float sc = (!r2c && d.norm == CRDFFT_NORM_INVERSE) ? static_cast<float>(1.0 / static_cast<double>(n))
+                                                                 : 1.0f;
+        st = make_pass_desc(p, h, d.batch, 1, in, out, false, !r2c, sc, FourStepTw{}, &s.pass);
+        if (st == CRDFFT_OK && real_line_supported(s.pass))
+        {
+            s.src = BufRef{Buf::In, 0};
+            s.dst = BufRef{Buf::Out, 0};
+            p.steps[r2c ? 0 : 1].push_back(s);
+            p.algorithm = "real-fused";
+            p.factors = {h};
+            return CRDFFT_OK;
+        }
+    }
     long long need = 0;
     if (d.kind == CRDFFT_R2C)
     {
@@ -1312,9 +1343,13 @@ struct ConvReq
 // The fused convolution (conv.cu): y = IFFT(FFT(x) * H) * scale. Rank 1: one launch, lines of the batch in shared
 // memory. Rank 2 (rows x cols): forward row FFTs, the fused convolution along the columns, inverse row FFTs with the
 // scale, as the reference's 2-D GPU convolution orders them (engine/gpu/kir/include/crd/kir/ckir_fft.hpp:2075-2090).
+crdfft_status build_real_conv(Plan& p, const ConvReq& req);
+
 crdfft_status build_conv(Plan& p, const ConvReq& req)
 {
     const crdfft_desc& d = p.desc;
+    if (d.kind == CRDFFT_R2C)
+        return build_real_conv(p, req);
     if (d.kind != CRDFFT_C2C || d.rank > 2 || d.istride > 1 || d.ostride > 1)
         return CRDFFT_UNSUPPORTED_SIZE;
     long long total = 1;
@@ -1375,6 +1410,103 @@ crdfft_status build_conv(Plan& p, const ConvReq& req)
     p.steps[0] = {r1, cv, r2};
     p.algorithm = "fused-conv-2d";
     p.factors = {rows, cols};
+    return CRDFFT_OK;
+}
+
+// The fused convolution of real signals (kind R2C): real input and output, the filter as the half spectrum
+// (n/2 + 1 values a row). Rank 1: one launch (real_line.cu, kRealConv). Rank 2 (rows x cols): R2C rows into the
+// workspace (rows x (cols/2 + 1)), the fused convolution along those half-width columns, C2R rows with the scale:
+// the three dispatches of the reference's real 2-D convolution (engine/gpu/kir/include/crd/kir/ckir_fft.hpp:
+// 2300-2308), here without its padding of the half width.
+crdfft_status build_real_conv(Plan& p, const ConvReq& req)
+{
+    const crdfft_desc& d = p.desc;
+    if (d.rank > 2 || d.istride > 1 || d.ostride > 1)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    long long total = 1;
+    for (int i = 0; i < d.rank; ++i)
+        total *= d.dims[i];
+    if ((d.idist != 0 && d.idist != total) || (d.odist != 0 && d.odist != total))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const long long n = d.dims[d.rank - 1]; // the real (last) axis
+    const long long h = n / 2;
+    if (n < 2 || (n & 1) != 0 || !single_pass_ok(h))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const float scale = static_cast<float>(req.scale < 0.0 ? 1.0 / static_cast<double>(total) : req.scale);
+    std::vector<float> wn(static_cast<size_t>(2 * (h + 1)));
+    for (long long k = 0; k <= h; ++k)
+    {
+        double re, im;
+        root(k, n, &re, &im);
+        wn[static_cast<size_t>(2 * k)] = static_cast<float>(re);
+        wn[static_cast<size_t>(2 * k + 1)] = static_cast<float>(im);
+    }
+    void* dwn = nullptr;
+    crdfft_status st = upload_table(p, wn, &dwn);
+    if (st != CRDFFT_OK)
+        return st;
+    p.conv = true;
+    const long long hw = h + 1;
+    if (d.rank == 1)
+    {
+        Step s;
+        s.kind = StepKind::RealLine;
+        s.rmode = kRealConv;
+        s.raux = RealLineAux{dwn, LineMap{req.per_transform ? hw : 0, 0, 1}};
+        st = make_pass_desc(p, h, d.batch, 1, LineMap{h, 0, 1}, LineMap{h, 0, 1}, false, true, scale, FourStepTw{},
+                            &s.pass);
+        if (st != CRDFFT_OK)
+            return st;
+        if (!real_line_supported(s.pass))
+            return CRDFFT_UNSUPPORTED_SIZE;
+        s.src = BufRef{Buf::In, 0};
+        s.dst = BufRef{Buf::Out, 0};
+        p.steps[0].push_back(s);
+        p.algorithm = "fused-real-conv";
+        p.factors = {n};
+        return CRDFFT_OK;
+    }
+    const long long rows = d.dims[0];
+    if (rows < 2 || !single_pass_ok(rows))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const long long lines = d.batch * rows;
+    const long long half_total = rows * hw;
+    Step r1;
+    r1.kind = StepKind::RealLine;
+    r1.rmode = kRealR2C;
+    r1.raux = RealLineAux{dwn, LineMap{0, 0, 1}};
+    st = make_pass_desc(p, h, lines, 1, LineMap{h, 0, 1}, LineMap{hw, 0, 1}, false, false, 1.0f, FourStepTw{},
+                        &r1.pass);
+    if (st != CRDFFT_OK)
+        return st;
+    Step cv;
+    cv.kind = StepKind::Conv;
+    st = make_pass_desc(p, rows, d.batch * hw, hw, LineMap{half_total, 1, hw}, LineMap{half_total, 1, hw}, false,
+                        true, 1.0f, FourStepTw{}, &cv.pass);
+    if (st != CRDFFT_OK)
+        return st;
+    Step r2;
+    r2.kind = StepKind::RealLine;
+    r2.rmode = kRealC2R;
+    r2.raux = RealLineAux{dwn, LineMap{0, 0, 1}};
+    st = make_pass_desc(p, h, lines, 1, LineMap{hw, 0, 1}, LineMap{h, 0, 1}, false, true, scale, FourStepTw{},
+                        &r2.pass);
+    if (st != CRDFFT_OK)
+        return st;
+    if (!real_line_supported(r1.pass) || !real_line_supported(r2.pass) || !conv_supported(cv.pass))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    cv.shape.map = PassMap::Col;
+    cv.smap = LineMap{req.per_transform ? half_total : 0, 1, hw};
+    r1.src = BufRef{Buf::In, 0};
+    r1.dst = BufRef{Buf::Ws, 0};
+    cv.src = BufRef{Buf::Ws, 0};
+    cv.dst = BufRef{Buf::Ws, 0};
+    r2.src = BufRef{Buf::Ws, 0};
+    r2.dst = BufRef{Buf::Out, 0};
+    p.steps[0] = {r1, cv, r2};
+    p.ws_bytes = static_cast<size_t>(d.batch * half_total) * 8;
+    p.algorithm = "fused-real-conv-2d";
+    p.factors = {rows, n};
     return CRDFFT_OK;
 }
 
@@ -1628,8 +1760,6 @@ crdfft_status validate(const crdfft_desc& d)
         return CRDFFT_INVALID_DESC;
     if (d.rank > 1 && (d.istride > 1 || d.ostride > 1))
         return CRDFFT_INVALID_DESC;
-    if (d.kind != CRDFFT_C2C && d.rank != 1)
-        return CRDFFT_UNSUPPORTED_SIZE;
     return CRDFFT_OK;
 }
 
@@ -1641,6 +1771,9 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
     crdfft_status st = validate(*desc);
     if (st != CRDFFT_OK)
         return st;
+    // real plans of rank > 1 exist only as convolutions (NdFftPlan is complex, nd_fft.hpp:28-194)
+    if (desc->kind != CRDFFT_C2C && desc->rank != 1 && conv == nullptr)
+        return CRDFFT_UNSUPPORTED_SIZE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess)
         return CRDFFT_NO_DEVICE;
@@ -1785,6 +1918,11 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
                 if (spec == nullptr)
                     return CRDFFT_INVALID_ARG;
                 e = launch_conv(s.pass, s.shape.map, s.smap, src, spec, dst, stream);
+                break;
+            case StepKind::RealLine:
+                if (s.rmode == kRealConv && spec == nullptr)
+                    return CRDFFT_INVALID_ARG;
+                e = launch_real_line(s.pass, s.rmode, s.raux, src, spec, dst, stream);
                 break;
             case StepKind::R2CPost: e = launch_r2c_post(s.real, src, dst, stream); break;
             case StepKind::C2RPre: e = launch_c2r_pre(s.real, src, dst, stream); break;

@@ -147,14 +147,17 @@ class Plan(_Handle):
 
 class ConvPlan(_Handle):
     """Fused FFT convolution (crdfft_conv_plan_create): y = IFFT(FFT(x) * H) * scale over a batch of 1-D signals
-    (dims = [n]) or 2-D signals (dims = [rows, cols]); one spectrum H shared by the batch, or one per signal."""
+    (dims = [n]) or 2-D signals (dims = [rows, cols]); one spectrum H shared by the batch, or one per signal.
+    real=True: real signals (float32) and the half spectrum H (complex64, cols/2 + 1 values a row)."""
 
-    def __init__(self, dims: Sequence[int], batch: int = 1, per_signal_filter: bool = False, scale: float = -1.0):
+    def __init__(self, dims: Sequence[int], batch: int = 1, per_signal_filter: bool = False, scale: float = -1.0,
+                 real: bool = False):
         super().__init__()
         dims = [int(v) for v in dims]
         d = Desc()
         d.rank = len(dims)
-        d.kind = C2C
+        d.kind = R2C if real else C2C
+        self.real = bool(real)
         d.precision = PREC_FP32
         d.norm = NORM_NONE
         for i, v in enumerate(dims):
@@ -166,9 +169,10 @@ class ConvPlan(_Handle):
                                             ctypes.byref(self._h)), "conv_plan_create")
 
     def execute(self, inp: torch.Tensor, spectrum: torch.Tensor, out: torch.Tensor, stream=None) -> torch.Tensor:
-        pi = _ptr(inp, torch.complex64, "input")
+        dt = torch.float32 if self.real else torch.complex64
+        pi = _ptr(inp, dt, "input")
         ps = _ptr(spectrum, torch.complex64, "spectrum")
-        po = _ptr(out, torch.complex64, "output")
+        po = _ptr(out, dt, "output")
         check(lib().crdfft_conv_execute(self._h, pi, ps, po, _stream(stream)), "conv_execute")
         return out
 

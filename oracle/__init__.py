@@ -243,12 +243,51 @@ def ref():
         R.crdref_nd_f64.argtypes = [_sz, ctypes.POINTER(ctypes.c_size_t), _dp, ctypes.c_int]
         R.crdref_uneven_f32.argtypes = [_sz, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64), _fp,
                                         ctypes.c_int, ctypes.c_int]
+        R.crdref_welch_f32.argtypes = [_sz, _sz, _fp, ctypes.c_double, _sz, _sz, _fp, ctypes.c_int]
+        R.crdref_welch_f64.argtypes = [_sz, _sz, _dp, ctypes.c_double, _sz, _sz, _dp, ctypes.c_int]
+        R.crdref_spectrogram_f64.argtypes = [_sz, _sz, _dp, ctypes.c_double, _sz, _sz, _dp, ctypes.c_int]
+        R.crdref_periodogram_f64.argtypes = [_sz, _sz, _dp, ctypes.c_double, _dp, ctypes.c_int]
         for f in ("crdref_c2c_f32", "crdref_c2c_f64", "crdref_execute_reference_f32", "crdref_execute_reference_f64",
                   "crdref_execute_batched_f32", "crdref_stockham_f32", "crdref_rfft_f32", "crdref_irfft_f32",
-                  "crdref_nd_f32", "crdref_nd_f64", "crdref_uneven_f32"):
+                  "crdref_nd_f32", "crdref_nd_f64", "crdref_uneven_f32", "crdref_welch_f32", "crdref_welch_f64",
+                  "crdref_spectrogram_f64", "crdref_periodogram_f64"):
             getattr(R, f).restype = ctypes.c_int
         _ref = R
     return _ref
+
+
+def ref_welch(x, fs: float, nperseg: int, noverlap: int, f32: bool = False, threads: int = 1) -> np.ndarray:
+    """The reference's dsp::welch_psd over the rows of x (spectral.hpp:141-172), in float or double."""
+    dt, fn = (np.float32, "crdref_welch_f32") if f32 else (np.float64, "crdref_welch_f64")
+    a = np.ascontiguousarray(x, dtype=dt)
+    n = a.shape[-1]
+    out = np.zeros(a.shape[:-1] + (nperseg // 2 + 1,), dtype=dt)
+    ptr = _ptr_f if f32 else _ptr_d
+    if getattr(ref(), fn)(n, a.size // n, ptr(a), fs, nperseg, noverlap, ptr(out), threads) != 0:
+        raise RuntimeError(f"{fn} failed")
+    return out
+
+
+def ref_spectrogram(x, fs: float, nperseg: int, noverlap: int, threads: int = 1) -> np.ndarray:
+    """The reference's dsp::spectrogram<double> over the rows of x (spectral.hpp:177-183): rows x nseg x nfreq."""
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    n = a.shape[-1]
+    hop = nperseg - noverlap
+    nseg = 0 if n < nperseg else (n - noverlap) // hop
+    out = np.zeros(a.shape[:-1] + (nseg, nperseg // 2 + 1))
+    if ref().crdref_spectrogram_f64(n, a.size // n, _ptr_d(a), fs, nperseg, noverlap, _ptr_d(out), threads) != 0:
+        raise RuntimeError("crdref_spectrogram_f64 failed")
+    return out
+
+
+def ref_periodogram(x, fs: float, threads: int = 1) -> np.ndarray:
+    """The reference's dsp::periodogram<double> over the rows of x (spectral.hpp:188-220)."""
+    a = np.ascontiguousarray(x, dtype=np.float64)
+    n = a.shape[-1]
+    out = np.zeros(a.shape[:-1] + (n // 2 + 1,))
+    if ref().crdref_periodogram_f64(n, a.size // n, _ptr_d(a), fs, _ptr_d(out), threads) != 0:
+        raise RuntimeError("crdref_periodogram_f64 failed")
+    return out
 
 
 def ref_c2c_f32(x, inverse: bool = False, threads: int = 1) -> np.ndarray:

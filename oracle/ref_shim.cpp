@@ -6,6 +6,7 @@
 // batch_arms.hpp:59-77).
 
 #include <crd/hesap/complex.hpp>
+#include <crd/hesap/dsp/spectral.hpp>
 #include <crd/hesap/fft/bluestein.hpp>
 #include <crd/hesap/fft/fft.hpp>
 #include <crd/hesap/fft/fft_dispatch.hpp>
@@ -118,6 +119,27 @@ template <typename T> int c2c(std::size_t n, std::size_t batch, T* data, int dir
     return 0;
 }
 
+} // namespace
+
+namespace
+{
+template <typename T, typename F> int spectral_rows(std::size_t n, std::size_t count, const T* x, T* out,
+                                                    std::size_t row, int threads, const F& one)
+{
+    fan_out(threads, count,
+            [&](std::size_t first, std::size_t last)
+            {
+                for (std::size_t g = first; g < last; ++g)
+                {
+                    const auto r = one(cont::ConstSpan<T>(x + g * n, n));
+                    for (std::size_t k = 0; k < row && k < r.size(); ++k)
+                    {
+                        out[g * row + k] = r[k];
+                    }
+                }
+            });
+    return 0;
+}
 } // namespace
 
 extern "C"
@@ -342,6 +364,58 @@ int crdref_nd_f64(std::size_t ndim, const std::size_t* dims, double* data, int d
     const fft::NdFftPlan<double> plan(&alloc(), cont::ConstSpan<std::size_t>(dims, ndim));
     plan.execute(cont::Span<Complex<double>>(reinterpret_cast<Complex<double>*>(data), total), dir_of(dir));
     return 0;
+}
+
+// hesap-dsp's spectral estimators over `count` signals of `n` samples each, one signal at a time per thread
+// (contiguous ranges, as above); each call runs the reference's own segment loop (spectral.hpp:44-120) on the
+// calling thread. welch_psd (spectral.hpp:141-172): out = count x (nperseg/2 + 1). spectrogram (spectral.hpp:177-183):
+// out = count x nseg x (nperseg/2 + 1). periodogram (spectral.hpp:188-220): out = count x (n/2 + 1).
+
+// RealFftPlan takes powers of two only (real_fft.hpp); other segment lengths are refused here, not aborted on.
+int crdref_welch_f32(std::size_t n, std::size_t count, const float* x, double fs, std::size_t nperseg,
+                     std::size_t noverlap, float* out, int threads)
+{
+    if (nperseg < 4 || !is_pow2(nperseg))
+        return -1;
+    return spectral_rows<float>(n, count, x, out, nperseg / 2 + 1, threads,
+                                [&](cont::ConstSpan<float> s)
+                                { return crd::hesap::dsp::welch_psd<float>(&alloc(), s, static_cast<float>(fs),
+                                                                           nperseg, noverlap); });
+}
+
+int crdref_welch_f64(std::size_t n, std::size_t count, const double* x, double fs, std::size_t nperseg,
+                     std::size_t noverlap, double* out, int threads)
+{
+    if (nperseg < 4 || !is_pow2(nperseg))
+        return -1;
+    return spectral_rows<double>(n, count, x, out, nperseg / 2 + 1, threads,
+                                 [&](cont::ConstSpan<double> s)
+                                 { return crd::hesap::dsp::welch_psd<double>(&alloc(), s, fs, nperseg, noverlap); });
+}
+
+int crdref_spectrogram_f64(std::size_t n, std::size_t count, const double* x, double fs, std::size_t nperseg,
+                           std::size_t noverlap, double* out, int threads)
+{
+    if (nperseg < 4 || !is_pow2(nperseg))
+        return -1;
+    const std::size_t hop = nperseg - noverlap;
+    const std::size_t nseg = n < nperseg ? 0 : (n - noverlap) / hop;
+    return spectral_rows<double>(n, count, x, out, nseg * (nperseg / 2 + 1), threads,
+                                 [&](cont::ConstSpan<double> s)
+                                 {
+                                     std::size_t ns = 0, nf = 0;
+                                     return crd::hesap::dsp::spectrogram<double>(&alloc(), s, fs, nperseg, noverlap,
+                                                                                 ns, nf);
+                                 });
+}
+
+int crdref_periodogram_f64(std::size_t n, std::size_t count, const double* x, double fs, double* out, int threads)
+{
+    if (n < 4 || !is_pow2(n))
+        return -1;
+    return spectral_rows<double>(n, count, x, out, n / 2 + 1, threads,
+                                 [&](cont::ConstSpan<double> s)
+                                 { return crd::hesap::dsp::periodogram<double>(&alloc(), s, fs); });
 }
 
 } // extern "C"
