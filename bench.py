@@ -130,7 +130,7 @@ class ClockSampler:
 # one), its algorithmic HBM bytes, the number of kernel launches it issues, and a check that returns the rel-L2 of
 # its output against numpy's float64 FFT on a sample.
 
-WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision", "conv")
+WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision", "conv", "welch")
 
 
 WORKLOAD_CONFIGS = {
@@ -148,6 +148,8 @@ WORKLOAD_CONFIGS = {
              "filter": "one spectrum shared by the batch",
              "l2": "256 MiB input per size (> 126 MB L2)",
              "flops": "complex: 10 N log2 N + 6 N per signal; real: 5 N log2 N + 3 N per signal"},
+    "welch": {"workload": "welch_spectrogram_64_signals_2^22_samples_nperseg1024_noverlap512_hann",
+              "l2": "1 GiB of float input (> 126 MB L2)", "flops": "2.5 N log2 N per segment (its real FFT)"},
     "precision": {"workload": "nd_c2c_4096x4096_512x512x512_fp32_splitbf16_fp16", "inputs": "uniform[-1,1) + 1% x 1e4",
                   "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
 }
@@ -455,8 +457,67 @@ def build_precision(dev, rank, cf):
         dict(WORKLOAD_CONFIGS["precision"])
 
 
+WELCH = (64, 1 << 22, 1024, 512)  # signals, samples a signal, nperseg, noverlap
+
+
+def _periodograms64(x, nper, nov):
+    """FP64 segment periodograms of the rows of x (fs 1, periodic Hann, mean removed): the result check."""
+    import numpy as np
+
+    hop = nper - nov
+    nseg = (x.shape[-1] - nov) // hop
+    w = 0.5 - 0.5 * np.cos(2 * np.pi * np.arange(nper) / nper)
+    idx = np.arange(nseg)[:, None] * hop + np.arange(nper)[None, :]
+    seg = x[..., idx]
+    seg = seg - seg.mean(axis=-1, keepdims=True)
+    p = np.abs(np.fft.rfft(seg * w, axis=-1)) ** 2 / np.sum(w * w)
+    p[..., 1:-1] *= 2
+    return p
+
+
+def build_welch(dev, rank, cf):
+    """hesap-dsp's spectral estimators on the device: Welch's PSD and the spectrogram of 64 signals of 2^22 samples
+    (1 GiB of float input), periodic Hann window, nperseg 1024, noverlap 512, fs 1; segment mean removed. One launch
+    over all 524,224 segments (plus the fixed-order average for Welch)."""
+    import numpy as np
+    import torch
+
+    count, ns, nper, nov = WELCH
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 21 + rank)
+    x = torch.randn(count * ns, generator=gen, device=dev, dtype=torch.float32) + 0.5
+    welch = cf.SpectralPlan(cf.SPECTRAL_WELCH, ns, count, 1.0, nper, nov)
+    spec = cf.SpectralPlan(cf.SPECTRAL_SPECTROGRAM, ns, count, 1.0, nper, nov)
+    pw = torch.empty(welch.out_shape(), dtype=torch.float32, device=dev)
+    ps = torch.empty(spec.out_shape(), dtype=torch.float32, device=dev)
+    nseg = welch.nseg
+    fl = count * nseg * 2.5 * nper * math.log2(nper)
+
+    def check_w():
+        welch.execute(x, pw)
+        torch.cuda.synchronize()
+        xs = x.view(count, ns)[:2, : 64 * nper].cpu().numpy().astype(np.float64)
+        want = _periodograms64(xs, nper, nov).mean(axis=-2)
+        got = cf.SpectralPlan(cf.SPECTRAL_WELCH, 64 * nper, 2, 1.0, nper, nov).execute(
+            x.view(count, ns)[:2, : 64 * nper].contiguous()).cpu().numpy()
+        return _rel(got, want)
+
+    def check_s():
+        spec.execute(x, ps)
+        torch.cuda.synchronize()
+        xs = x.view(count, ns)[0, : 33 * (nper - nov) + nov].cpu().numpy().astype(np.float64)
+        want = _periodograms64(xs, nper, nov)
+        return _rel(ps[0, :want.shape[0]].cpu().numpy(), want)
+
+    ops = [Op("welch", x, pw, lambda i, o: welch.execute(i, o), fl, 4 * count * ns + 4 * pw.numel(),
+              welch.info()["passes"], check_w, {"segments": count * nseg, "algorithm": welch.info()["algorithm"]}),
+           Op("spectrogram", x, ps, lambda i, o: spec.execute(i, o), fl, 4 * count * ns + 4 * ps.numel(),
+              spec.info()["passes"], check_s, {"segments": count * nseg, "algorithm": spec.info()["algorithm"]})]
+    return ops, dict(WORKLOAD_CONFIGS["welch"])
+
+
 BUILDERS = {"mixed": build_mixed, "n1024": build_n1024, "r2c": build_r2c, "uneven": build_uneven, "nd": build_nd,
-            "precision": build_precision, "conv": build_conv}
+            "precision": build_precision, "conv": build_conv, "welch": build_welch}
 
 
 # ---- the reference's CPU implementation (reference arm and cpu_baseline) -------------------------------------------
@@ -571,6 +632,21 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
 
             timed(rrun, count * (5.0 * n * math.log2(n) + 3.0 * n), f"rconv{n}")
             sample.append(f"real conv N={n} x{count}")
+    elif workload == "welch":
+        # the reference's dsp::welch_psd<float> over the signals, one signal at a time per thread
+        count, ns, nper, nov = WELCH
+        cnt = max(1, min(count, budget_bytes // (4 * ns)))
+        x = oracle.lcg_float32(SEED ^ 0x3E1C, cnt * ns)
+        out = np.empty(cnt * (nper // 2 + 1), dtype=np.float32)
+        nseg = (ns - nov) // (nper - nov)
+
+        def wrun():
+            if R.crdref_welch_f32(ns, cnt, x.ctypes.data_as(fp), 1.0, nper, nov, out.ctypes.data_as(fp),
+                                  threads) != 0:
+                raise RuntimeError("crdref_welch_f32 failed")
+
+        timed(wrun, cnt * nseg * 2.5 * nper * math.log2(nper), "welch")
+        sample.append(f"welch {cnt} signals x {ns} samples, nperseg {nper}, noverlap {nov}")
     elif workload == "r2c":
         n = 1 << 20
         count = max(threads, min(512, budget_bytes // (4 * n)))

@@ -39,6 +39,10 @@ PLANNER_LEARNED = 2
 NORM_NONE = 0
 NORM_INVERSE = 1
 
+SPECTRAL_WELCH = 0
+SPECTRAL_SPECTROGRAM = 1
+SPECTRAL_PERIODOGRAM = 2
+
 # Every function include/crdfft.h declares; the CPU tests check the library exports each of them.
 EXPORTS = (
     "crdfft_plan_create",
@@ -47,6 +51,9 @@ EXPORTS = (
     "crdfft_execute_host",
     "crdfft_conv_plan_create",
     "crdfft_conv_execute",
+    "crdfft_spectral_plan_create",
+    "crdfft_spectral_segments",
+    "crdfft_spectral_execute",
     "crdfft_plan_info_get",
     "crdfft_workspace_size",
     "crdfft_set_workspace",
@@ -110,6 +117,19 @@ class Desc(ctypes.Structure):
     ]
 
 
+class SpectralDesc(ctypes.Structure):
+    _fields_ = [
+        ("mode", ctypes.c_int32),
+        ("detrend", ctypes.c_int32),
+        ("nsamples", ctypes.c_int64),
+        ("count", ctypes.c_int64),
+        ("nperseg", ctypes.c_int64),
+        ("noverlap", ctypes.c_int64),
+        ("fs", ctypes.c_double),
+        ("window", ctypes.POINTER(ctypes.c_float)),
+    ]
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [
         ("algorithm", ctypes.c_char * 64),
@@ -142,6 +162,9 @@ def lib():
         "crdfft_execute_host": ([vp, vp, vp, i32, vp], i32),
         "crdfft_conv_plan_create": ([ctypes.POINTER(Desc), i32, ctypes.c_double, pp], i32),
         "crdfft_conv_execute": ([vp, vp, vp, vp, vp], i32),
+        "crdfft_spectral_plan_create": ([ctypes.POINTER(SpectralDesc), pp], i32),
+        "crdfft_spectral_segments": ([ctypes.POINTER(SpectralDesc)], i64),
+        "crdfft_spectral_execute": ([vp, vp, vp, vp], i32),
         "crdfft_plan_info_get": ([vp, ctypes.POINTER(PlanInfo)], i32),
         "crdfft_workspace_size": ([vp], ctypes.c_size_t),
         "crdfft_set_workspace": ([vp, vp, ctypes.c_size_t], i32),

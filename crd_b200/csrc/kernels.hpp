@@ -41,6 +41,28 @@ struct RealLineAux
 bool real_line_supported(const PassDesc& d);
 cudaError_t launch_real_line(const PassDesc& d, int mode, const RealLineAux& r, const void* in, const void* spec,
                              void* out, cudaStream_t stream);
+// Segment periodograms (spectral.cu): the pass describes the M-point complex lines of one segment (nperseg = 2M).
+// welch = 0: out = count x nseg x (M + 1) rows; welch = 1: out = count x ntiles per-CTA sums, then
+// launch_welch_finish adds them into count x (M + 1).
+struct SpectralDesc
+{
+    long long nsamples; // samples a signal (the distance between signals)
+    long long count;    // signals
+    long long nseg;     // segments a signal
+    long long hop;      // nperseg - noverlap
+    int nperseg;
+    int lpc;            // segments a CTA
+    int ntiles;         // CTAs a signal
+    int detrend;        // subtract each segment's mean
+    int welch;
+    float scale;        // 1 / (fs sum w^2)
+    const float* win;   // nperseg window values
+    const void* wn;     // float2 W_nperseg^k, k = 0 .. M/2 at least
+};
+bool spectral_shape(const PassDesc& d, int* P, int* lpc, int* threads, int* smem);
+cudaError_t launch_spectral(const PassDesc& d, const SpectralDesc& sd, int threads, int smem, const void* x,
+                            void* out, cudaStream_t stream);
+cudaError_t launch_welch_finish(const SpectralDesc& sd, const void* part, void* psd, cudaStream_t stream);
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
 int pass_threads_limit();

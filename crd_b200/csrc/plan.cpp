@@ -97,6 +97,9 @@ enum class StepKind : int
     TcLine,
     Conv,
     RealLine,
+    Spectral,
+    WelchFinish,
+    Zero,
     R2CPost,
     C2RPre,
     ChirpPre,
@@ -116,6 +119,8 @@ struct Step
     LineMap smap{};   // Conv: where each line's filter spectrum sits
     int rmode = 0;    // RealLine: kRealR2C, kRealC2R or kRealConv
     RealLineAux raux{};
+    SpectralDesc sdesc{}; // Spectral, WelchFinish
+    int sthreads = 0, ssmem = 0;
     int lane = 0;     // 0: the caller's stream; 1, 2: the plan's two internal streams (L2-sized four-step waves)
     RealRecombine real{};
     ChirpDesc chirp{};
@@ -281,6 +286,7 @@ struct Plan
     HostPipe* host = nullptr;
     std::mutex host_mu;
     bool conv = false; // fused convolution plan (crdfft_conv_plan_create): executes with a filter spectrum
+    bool spectral = false; // spectral estimator plan (crdfft_spectral_plan_create)
     // Radix-32 schedules for the lengths that have them (FP32 unit-stride passes); off for the tensor-core precision
     // forms and the uneven batch, whose kernels take the radix-16 schedules.
     bool use32 = true;
@@ -1184,6 +1190,110 @@ crdfft_status build_real(Plan& p)
     return CRDFFT_OK;
 }
 
+// 2-D and 3-D real transforms (the reference's NdFftPlan is complex only, nd_fft.hpp:28-194; the real plan is 1-D,
+// real_fft.hpp:18-101): the Hermitian half along the last axis, dims[0..rank-2] x (n/2 + 1) complex values a batch
+// member. R2C: fused R2C rows (real_line.cu) from the input into the output, then one in-place complex pass per
+// remaining axis. C2R: the complex axes inverse from the input into the workspace (the input stays untouched), then
+// fused C2R rows into the output. Unnormalised both ways unless norm = CRDFFT_NORM_INVERSE (1 / the real size on
+// C2R). Packed batches only.
+crdfft_status build_nd_real(Plan& p)
+{
+    const crdfft_desc& d = p.desc;
+    const int rank = d.rank;
+    const long long n = d.dims[rank - 1];
+    if (n < 2 || (n & 1) != 0 || !single_pass_ok(n / 2))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const long long h = n / 2, hw = h + 1;
+    long long outer = 1; // rows of the real axis in one batch member
+    for (int i = 0; i < rank - 1; ++i)
+        outer *= d.dims[i];
+    const long long rtotal = outer * n, ctotal = outer * hw;
+    const bool r2c = d.kind == CRDFFT_R2C;
+    if ((d.idist != 0 && d.idist != (r2c ? rtotal : ctotal)) || (d.odist != 0 && d.odist != (r2c ? ctotal : rtotal)))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    if ((d.istride != 0 && d.istride != 1) || (d.ostride != 0 && d.ostride != 1))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    std::vector<float> wn(static_cast<size_t>(2 * (h + 1)));
+    for (long long k = 0; k <= h; ++k)
+    {
+        double re, im;
+        root(k, n, &re, &im);
+        wn[static_cast<size_t>(2 * k)] = static_cast<float>(re);
+        wn[static_cast<size_t>(2 * k + 1)] = static_cast<float>(im);
+    }
+    void* dwn = nullptr;
+    crdfft_status st = upload_table(p, wn, &dwn);
+    if (st != CRDFFT_OK)
+        return st;
+    Step row;
+    row.kind = StepKind::RealLine;
+    row.rmode = r2c ? kRealR2C : kRealC2R;
+    row.raux = RealLineAux{dwn, LineMap{0, 0, 1}};
+    const float scale = (!r2c && d.norm == CRDFFT_NORM_INVERSE)
+                            ? static_cast<float>(1.0 / static_cast<double>(rtotal))
+                            : 1.0f;
+    st = make_pass_desc(p, h, d.batch * outer, 1, r2c ? LineMap{h, 0, 1} : LineMap{hw, 0, 1},
+                        r2c ? LineMap{hw, 0, 1} : LineMap{h, 0, 1}, false, !r2c, scale, FourStepTw{}, &row.pass);
+    if (st != CRDFFT_OK)
+        return st;
+    if (!real_line_supported(row.pass))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    // the complex axes of the half array, last to first
+    std::vector<int> axes;
+    for (int ax = rank - 2; ax >= 0; --ax)
+        if (d.dims[ax] > 1)
+            axes.push_back(ax);
+    std::vector<Step> cplx;
+    for (size_t i = 0; i < axes.size(); ++i)
+    {
+        const int ax = axes[i];
+        const long long m = d.dims[ax];
+        if (!single_pass_ok(m))
+            return CRDFFT_UNSUPPORTED_SIZE;
+        long long st_ax = hw;
+        for (int j = ax + 1; j < rank - 1; ++j)
+            st_ax *= d.dims[j];
+        const LineMap map{m * st_ax, 1, st_ax};
+        const bool first = i == 0, last = i + 1 == axes.size();
+        BufRef src, dst;
+        if (r2c)
+            src = dst = BufRef{Buf::Out, 0};
+        else
+        {
+            src = first ? BufRef{Buf::In, 0} : BufRef{Buf::Ws, 0};
+            dst = BufRef{Buf::Ws, 0};
+        }
+        Step s;
+        st = make_line_step(p, m, d.batch * (ctotal / m), st_ax, map, map, src, dst, !r2c && first, !r2c && last,
+                            1.0f, &s);
+        if (st != CRDFFT_OK)
+            return st;
+        cplx.push_back(s);
+    }
+    if (r2c)
+    {
+        row.src = BufRef{Buf::In, 0};
+        row.dst = BufRef{Buf::Out, 0};
+        p.steps[0].push_back(row);
+        for (const Step& s : cplx)
+            p.steps[0].push_back(s);
+    }
+    else
+    {
+        for (const Step& s : cplx)
+            p.steps[1].push_back(s);
+        row.src = cplx.empty() ? BufRef{Buf::In, 0} : BufRef{Buf::Ws, 0};
+        row.dst = BufRef{Buf::Out, 0};
+        p.steps[1].push_back(row);
+        if (!cplx.empty())
+            p.ws_bytes = static_cast<size_t>(d.batch * ctotal) * 8;
+    }
+    p.algorithm = "nd-real";
+    for (int i = 0; i < rank; ++i)
+        p.factors.push_back(d.dims[i]);
+    return CRDFFT_OK;
+}
+
 crdfft_status build_nd(Plan& p)
 {
     const crdfft_desc& d = p.desc;
@@ -1763,7 +1873,140 @@ crdfft_status validate(const crdfft_desc& d)
     return CRDFFT_OK;
 }
 
-crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = nullptr)
+// The segment geometry of a spectral descriptor (spectral.hpp:50-54, 146-149): the periodogram is one segment of
+// the whole signal; Welch reads noverlap 0 as nperseg / 2.
+struct SpecGeom
+{
+    long long nperseg = 0, noverlap = 0, hop = 0, nseg = 0;
+};
+
+bool spectral_geometry(const crdfft_spectral_desc& s, SpecGeom* g)
+{
+    if (s.nsamples < 1 || s.count < 1 || !(s.fs > 0.0) || s.mode < CRDFFT_SPECTRAL_WELCH ||
+        s.mode > CRDFFT_SPECTRAL_PERIODOGRAM)
+        return false;
+    if (s.mode == CRDFFT_SPECTRAL_PERIODOGRAM)
+    {
+        g->nperseg = s.nsamples;
+        g->noverlap = 0;
+    }
+    else
+    {
+        g->nperseg = s.nperseg;
+        g->noverlap = (s.mode == CRDFFT_SPECTRAL_WELCH && s.noverlap == 0) ? s.nperseg / 2 : s.noverlap;
+    }
+    if (g->nperseg < 4 || (g->nperseg & 1) != 0 || !single_pass_ok(g->nperseg / 2) || g->noverlap < 0 ||
+        g->noverlap >= g->nperseg)
+        return false;
+    g->hop = g->nperseg - g->noverlap;
+    g->nseg = s.nsamples < g->nperseg ? 0 : (s.nsamples - g->noverlap) / g->hop;
+    return true;
+}
+
+// The spectral estimators (spectral.cu): one launch over every segment of every signal, plus the fixed-order
+// average for Welch.
+crdfft_status build_spectral(Plan& p, const crdfft_spectral_desc& s)
+{
+    SpecGeom g;
+    if (!spectral_geometry(s, &g))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    const long long n = g.nperseg, M = n / 2, nfreq = M + 1;
+    // the window in FP64, narrowed (windows.hpp:56-124: the periodic Hann window, fac = -pi + 2 pi i / n); the
+    // density scale 1 / (fs sum w^2) over the narrowed values
+    std::vector<float> win(static_cast<size_t>(n));
+    double ss = 0.0;
+    for (long long i = 0; i < n; ++i)
+    {
+        double w;
+        if (s.mode == CRDFFT_SPECTRAL_PERIODOGRAM)
+            w = 1.0;
+        else if (s.window != nullptr)
+            w = s.window[i];
+        else
+            w = 0.5 + 0.5 * std::cos(-M_PI + 2.0 * M_PI * static_cast<double>(i) / static_cast<double>(n));
+        win[static_cast<size_t>(i)] = static_cast<float>(w);
+        ss += static_cast<double>(win[static_cast<size_t>(i)]) * win[static_cast<size_t>(i)];
+    }
+    if (!(ss > 0.0))
+        return CRDFFT_INVALID_ARG;
+    void* dwin = nullptr;
+    crdfft_status st = upload_table(p, win, &dwin);
+    if (st != CRDFFT_OK)
+        return st;
+    std::vector<float> wn(static_cast<size_t>(2 * (M + 1)));
+    for (long long k = 0; k <= M; ++k)
+    {
+        double re, im;
+        root(k, n, &re, &im);
+        wn[static_cast<size_t>(2 * k)] = static_cast<float>(re);
+        wn[static_cast<size_t>(2 * k + 1)] = static_cast<float>(im);
+    }
+    void* dwn = nullptr;
+    st = upload_table(p, wn, &dwn);
+    if (st != CRDFFT_OK)
+        return st;
+    p.spectral = true;
+    p.factors = {n, g.nseg};
+    const bool welch = s.mode == CRDFFT_SPECTRAL_WELCH;
+    p.algorithm = welch ? "spectral-welch" : s.mode == CRDFFT_SPECTRAL_SPECTROGRAM ? "spectral-spectrogram"
+                                                                                    : "spectral-periodogram";
+    if (g.nseg == 0)
+    {
+        if (welch)
+        {
+            Step z;
+            z.kind = StepKind::Zero;
+            z.count = s.count * nfreq * 4;
+            z.src = z.dst = BufRef{Buf::Out, 0};
+            p.steps[0].push_back(z);
+        }
+        return CRDFFT_OK;
+    }
+    Step sp;
+    sp.kind = StepKind::Spectral;
+    st = make_pass_desc(p, M, s.count * g.nseg, 1, LineMap{M, 0, 1}, LineMap{M, 0, 1}, false, false, 1.0f,
+                        FourStepTw{}, &sp.pass);
+    if (st != CRDFFT_OK)
+        return st;
+    int P = 16, lpc = 1, threads = 0, smem = 0;
+    if (!spectral_shape(sp.pass, &P, &lpc, &threads, &smem))
+        return CRDFFT_UNSUPPORTED_SIZE;
+    SpectralDesc sd{};
+    sd.nsamples = s.nsamples;
+    sd.count = s.count;
+    sd.nseg = g.nseg;
+    sd.hop = g.hop;
+    sd.nperseg = static_cast<int>(n);
+    sd.lpc = lpc;
+    sd.ntiles = static_cast<int>((g.nseg + lpc - 1) / lpc);
+    sd.detrend = s.detrend ? 1 : 0;
+    sd.welch = welch ? 1 : 0;
+    sd.scale = static_cast<float>(1.0 / (s.fs * ss));
+    sd.win = static_cast<const float*>(dwin);
+    sd.wn = dwn;
+    sp.sdesc = sd;
+    sp.sthreads = threads;
+    sp.ssmem = smem;
+    sp.src = BufRef{Buf::In, 0};
+    if (!welch)
+    {
+        sp.dst = BufRef{Buf::Out, 0};
+        p.steps[0].push_back(sp);
+        return CRDFFT_OK;
+    }
+    sp.dst = BufRef{Buf::Ws, 0};
+    Step fin;
+    fin.kind = StepKind::WelchFinish;
+    fin.sdesc = sd;
+    fin.src = BufRef{Buf::Ws, 0};
+    fin.dst = BufRef{Buf::Out, 0};
+    p.steps[0] = {sp, fin};
+    p.ws_bytes = static_cast<size_t>(s.count * sd.ntiles * nfreq) * 4 + 8;
+    return CRDFFT_OK;
+}
+
+crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = nullptr,
+                     const crdfft_spectral_desc* spec = nullptr)
 {
     if (desc == nullptr || out == nullptr)
         return CRDFFT_INVALID_ARG;
@@ -1771,9 +2014,6 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
     crdfft_status st = validate(*desc);
     if (st != CRDFFT_OK)
         return st;
-    // real plans of rank > 1 exist only as convolutions (NdFftPlan is complex, nd_fft.hpp:28-194)
-    if (desc->kind != CRDFFT_C2C && desc->rank != 1 && conv == nullptr)
-        return CRDFFT_UNSUPPORTED_SIZE;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess)
         return CRDFFT_NO_DEVICE;
@@ -1790,10 +2030,12 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
             return CRDFFT_LAUNCH;
         p->err = static_cast<int*>(e);
     }
-    if (conv != nullptr)
+    if (spec != nullptr)
+        st = build_spectral(*p, *spec);
+    else if (conv != nullptr)
         st = build_conv(*p, *conv);
     else if (desc->kind != CRDFFT_C2C)
-        st = build_real(*p);
+        st = desc->rank == 1 ? build_real(*p) : build_nd_real(*p);
     else if (desc->rank == 1)
         st = build_c2c_rank1(*p);
     else
@@ -1919,6 +2161,11 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
                     return CRDFFT_INVALID_ARG;
                 e = launch_conv(s.pass, s.shape.map, s.smap, src, spec, dst, stream);
                 break;
+            case StepKind::Spectral:
+                e = launch_spectral(s.pass, s.sdesc, s.sthreads, s.ssmem, src, dst, stream);
+                break;
+            case StepKind::WelchFinish: e = launch_welch_finish(s.sdesc, src, dst, stream); break;
+            case StepKind::Zero: e = cudaMemsetAsync(dst, 0, static_cast<size_t>(s.count), stream); break;
             case StepKind::RealLine:
                 if (s.rmode == kRealConv && spec == nullptr)
                     return CRDFFT_INVALID_ARG;
@@ -2014,6 +2261,48 @@ crdfft_status crdfft_conv_plan_create(const crdfft_desc* desc, int32_t filter_pe
     return CRDFFT_OK;
 }
 
+crdfft_status crdfft_spectral_plan_create(const crdfft_spectral_desc* desc, crdfft_plan** plan)
+{
+    if (plan == nullptr || desc == nullptr)
+        return CRDFFT_INVALID_ARG;
+    *plan = nullptr;
+    SpecGeom g;
+    if (!spectral_geometry(*desc, &g))
+        return CRDFFT_INVALID_DESC;
+    // the descriptor of the segment transforms, for the plan's bookkeeping (info, validation)
+    crdfft_desc d{};
+    d.rank = 1;
+    d.kind = CRDFFT_R2C;
+    d.precision = CRDFFT_PREC_FP32;
+    d.norm = CRDFFT_NORM_NONE;
+    d.dims[0] = g.nperseg;
+    d.batch = std::max<long long>(1, desc->count * g.nseg);
+    Plan* p = nullptr;
+    const crdfft_status st = create(&d, &p, nullptr, desc);
+    if (st != CRDFFT_OK)
+        return st;
+    *plan = reinterpret_cast<crdfft_plan*>(p);
+    return CRDFFT_OK;
+}
+
+int64_t crdfft_spectral_segments(const crdfft_spectral_desc* desc)
+{
+    SpecGeom g;
+    if (desc == nullptr || !spectral_geometry(*desc, &g))
+        return -1;
+    return g.nseg;
+}
+
+crdfft_status crdfft_spectral_execute(crdfft_plan* plan, const float* x, float* out, void* stream)
+{
+    if (plan == nullptr || x == nullptr || out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    if (!p.spectral)
+        return CRDFFT_INVALID_ARG;
+    return run(p, x, out, 0, static_cast<cudaStream_t>(stream));
+}
+
 crdfft_status crdfft_conv_execute(crdfft_plan* plan, const void* in, const void* spectrum, void* out, void* stream)
 {
     if (plan == nullptr || in == nullptr || spectrum == nullptr || out == nullptr)
@@ -2029,7 +2318,7 @@ crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32
     if (plan == nullptr || in == nullptr || out == nullptr)
         return CRDFFT_INVALID_ARG;
     Plan& p = *as_plan(plan);
-    if (p.conv)
+    if (p.conv || p.spectral)
         return CRDFFT_INVALID_ARG;
     if (direction != CRDFFT_FORWARD && direction != CRDFFT_INVERSE)
         return CRDFFT_INVALID_ARG;
@@ -2056,7 +2345,8 @@ bool host_layout(const crdfft_desc& d, HostLayout* L)
     long long total = 1;
     for (int i = 0; i < d.rank; ++i)
         total *= d.dims[i];
-    const long long half = total / 2 + 1;
+    const long long last = d.rank > 0 ? d.dims[d.rank - 1] : 1;
+    const long long half = (total / last) * (last / 2 + 1); // the Hermitian half along the last axis
     L->in_elem = d.kind == CRDFFT_R2C ? 4 : 8;
     L->out_elem = d.kind == CRDFFT_C2R ? 4 : 8;
     L->in_ext = d.kind == CRDFFT_C2R ? half : total;
@@ -2115,7 +2405,7 @@ crdfft_status crdfft_execute_host(crdfft_plan* plan, const void* in, void* out, 
         (p.desc.kind == CRDFFT_C2R && direction != CRDFFT_INVERSE))
         return CRDFFT_INVALID_ARG;
     HostLayout L{};
-    if (p.uneven || p.conv || !host_layout(p.desc, &L))
+    if (p.uneven || p.conv || p.spectral || !host_layout(p.desc, &L))
         return CRDFFT_INVALID_ARG;
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev != p.device)

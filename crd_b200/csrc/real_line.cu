@@ -19,6 +19,7 @@
 #include "dyn_stage.cuh"
 #include "kernels.hpp"
 #include "line_fft.cuh"
+#include "real_pair.cuh"
 
 namespace crdfft
 {
@@ -26,29 +27,6 @@ namespace lfft
 {
 namespace
 {
-
-__device__ __forceinline__ float2 conjf2(float2 v) { return make_float2(v.x, -v.y); }
-
-// X[k], X[M-k] from Z[k], Z[M-k] (0 < k <= M/2); w = W^k.
-__device__ __forceinline__ void r2c_pair(float2 zk, float2 zm, float2 w, float2& xk, float2& xm)
-{
-    const float2 e = make_float2(0.5f * (zk.x + zm.x), 0.5f * (zk.y - zm.y));
-    // (Z[k] - conj Z[M-k]) / 2i: (u + iv) / 2i = (v - iu) / 2
-    const float2 o = make_float2(0.5f * (zk.y + zm.y), -0.5f * (zk.x - zm.x));
-    const float2 t = cmul(w, o);
-    xk = make_float2(e.x + t.x, e.y + t.y);
-    xm = make_float2(e.x - t.x, t.y - e.y);
-}
-
-// Q[k], Q[M-k] from Y[k], Y[M-k] (0 < k <= M/2); w = W^k.
-__device__ __forceinline__ void c2r_pair(float2 yk, float2 ym, float2 w, float2& qk, float2& qm)
-{
-    const float2 a = make_float2(yk.x + ym.x, yk.y - ym.y);
-    const float2 b = make_float2(yk.x - ym.x, yk.y + ym.y);
-    const float2 bw = cmul(b, conjf2(w));
-    qk = make_float2(a.x - bw.y, a.y + bw.x);
-    qm = make_float2(a.x + bw.y, bw.x - a.y);
-}
 
 // The pairs of one line, handled by the line's T threads (thread jt takes k = jt, jt + T, ...). `get(i)` reads Z or
 // Y at i <= M; `put(i, v)` writes the result at i <= M.

@@ -27,7 +27,8 @@ from typing import Iterable, Optional, Sequence
 import torch
 
 from . import _lib
-from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP32, R2C, CrdFftError, Desc,
+from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP32, R2C, SPECTRAL_PERIODOGRAM,
+                   SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError, Desc, SpectralDesc,
                    PlanInfo, check, lib)
 
 Forward = FORWARD
@@ -175,6 +176,65 @@ class ConvPlan(_Handle):
         po = _ptr(out, dt, "output")
         check(lib().crdfft_conv_execute(self._h, pi, ps, po, _stream(stream)), "conv_execute")
         return out
+
+
+class SpectralPlan(_Handle):
+    """hesap-dsp's spectral estimators on the device (crdfft_spectral_plan_create) over `count` real signals of
+    `nsamples` samples: mode SPECTRAL_WELCH (welch_psd, spectral.hpp:141-172), SPECTRAL_SPECTROGRAM (spectrogram,
+    :177-183) or SPECTRAL_PERIODOGRAM (periodogram, :188-220). window: None for the periodic Hann window."""
+
+    def __init__(self, mode: int, nsamples: int, count: int = 1, fs: float = 1.0, nperseg: int = 256,
+                 noverlap: int = 0, window=None, detrend: bool = True):
+        super().__init__()
+        d = SpectralDesc()
+        d.mode, d.detrend = int(mode), 1 if detrend else 0
+        d.nsamples, d.count, d.nperseg, d.noverlap, d.fs = int(nsamples), int(count), int(nperseg), int(noverlap), fs
+        self._win = None
+        if window is not None:
+            import numpy as np
+
+            self._win = np.ascontiguousarray(window, dtype=np.float32)
+            d.window = self._win.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        self.mode, self.nsamples, self.count = int(mode), int(nsamples), int(count)
+        self.nperseg = int(nsamples) if mode == SPECTRAL_PERIODOGRAM else int(nperseg)
+        self.nfreq = self.nperseg // 2 + 1
+        self.nseg = int(lib().crdfft_spectral_segments(ctypes.byref(d)))
+        check(lib().crdfft_spectral_plan_create(ctypes.byref(d), ctypes.byref(self._h)), "spectral_plan_create")
+
+    def out_shape(self):
+        if self.mode == SPECTRAL_SPECTROGRAM:
+            return (self.count, self.nseg, self.nfreq)
+        return (self.count, self.nfreq)
+
+    def execute(self, x: torch.Tensor, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        if x.numel() != self.count * self.nsamples:
+            raise ValueError(f"x holds {x.numel()} samples, the plan {self.count} x {self.nsamples}")
+        if out is None:
+            out = torch.empty(self.out_shape(), dtype=torch.float32, device=x.device)
+        if out.numel() == 0:
+            return out  # a spectrogram of no segment
+        check(lib().crdfft_spectral_execute(self._h, _ptr(x, torch.float32, "x"), _ptr(out, torch.float32, "out"),
+                                            _stream(stream)), "spectral_execute")
+        return out
+
+
+def welch_psd(x: torch.Tensor, fs: float, nperseg: int, noverlap: int = 0) -> torch.Tensor:
+    """dsp::welch_psd over the rows of x (a 1-D tensor is one signal): the periodic Hann window, noverlap 0 means
+    nperseg / 2 (spectral.hpp:141-172)."""
+    plan = SpectralPlan(SPECTRAL_WELCH, x.shape[-1], x.numel() // x.shape[-1], fs, nperseg, noverlap)
+    return plan.execute(x).reshape(tuple(x.shape[:-1]) + (plan.nfreq,))
+
+
+def spectrogram(x: torch.Tensor, fs: float, nperseg: int, noverlap: int) -> torch.Tensor:
+    """dsp::spectrogram over the rows of x: (..., nseg, nfreq) (spectral.hpp:177-183)."""
+    plan = SpectralPlan(SPECTRAL_SPECTROGRAM, x.shape[-1], x.numel() // x.shape[-1], fs, nperseg, noverlap)
+    return plan.execute(x).reshape(tuple(x.shape[:-1]) + (plan.nseg, plan.nfreq))
+
+
+def periodogram(x: torch.Tensor, fs: float) -> torch.Tensor:
+    """dsp::periodogram over the rows of x (spectral.hpp:188-220)."""
+    plan = SpectralPlan(SPECTRAL_PERIODOGRAM, x.shape[-1], x.numel() // x.shape[-1], fs)
+    return plan.execute(x).reshape(tuple(x.shape[:-1]) + (plan.nfreq,))
 
 
 class FftPlan(_Handle):

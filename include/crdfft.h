@@ -69,7 +69,8 @@ typedef enum crdfft_norm
 } crdfft_norm;
 
 /* A plan descriptor. dims are row-major (dims[rank-1] varies fastest). For R2C/C2R, dims[rank-1] is the real
- * length n and the complex side holds n/2+1 values along that axis. Strides and distances count elements of the
+ * length n and the complex side holds n/2+1 values along that axis (rank 2 and 3 real plans: packed batches, n/2 at
+ * most 8192; the reference's real plan is 1-D and its NdFftPlan complex). Strides and distances count elements of the
  * side they describe (complex elements, or floats on the real side); 0 selects the packed layout:
  *   istride = 1, idist = prod(input dims).
  * The reference's element-major execute_batched (fft.hpp:462-470) is istride = ostride = batch, idist = odist = 1. */
@@ -181,11 +182,48 @@ crdfft_status crdfft_ifft_normalized(void* data, int64_t n, void* stream);
  * fused convolution along the columns, then the inverse row FFTs. desc: C2C, packed (element stride 1, distance
  * the signal size), each dimension up to 8192 and 7-smooth. filter_per_transform: 0 for one spectrum (rank 1: n
  * values; rank 2: rows x cols, row-major) shared by the batch, 1 for one per signal (batch times that). scale < 0
- * means 1 / (number of points of one signal). */
+ * means 1 / (number of points of one signal).
+ * desc.kind = CRDFFT_R2C: real signals (float in and out) and the half spectrum H (n/2 + 1 complex values along the
+ * last axis: rank 1 n/2 + 1, rank 2 rows x (cols/2 + 1)); the last dimension even with half at most 8192. Rank 1
+ * is one launch; rank 2 is R2C rows, the fused convolution along the half-width columns and C2R rows, the order of
+ * the reference's real 2-D convolution (ckir_fft.hpp:2300-2308). */
 crdfft_status crdfft_conv_plan_create(const crdfft_desc* desc, int32_t filter_per_transform, double scale,
                                       crdfft_plan** plan);
 /* in == out allowed. crdfft_execute rejects convolution plans (CRDFFT_INVALID_ARG). */
 crdfft_status crdfft_conv_execute(crdfft_plan* plan, const void* in, const void* spectrum, void* out, void* stream);
+
+/* ---- Spectral estimators ------------------------------------------------------------------------------------ */
+
+/* The segment periodograms of hesap-dsp (engine/numerics/hesap-dsp/include/crd/hesap/dsp/spectral.hpp) over `count`
+ * real signals of `nsamples` floats each (packed), in one launch: each segment minus its mean ('constant' detrend),
+ * times the window, real FFT, one-sided density |X|^2 / (fs sum w^2), doubled except at DC and Nyquist.
+ *   CRDFFT_SPECTRAL_WELCH        welch_psd (spectral.hpp:141-172): the average over segments, count x nfreq;
+ *                                noverlap 0 means nperseg / 2, as there
+ *   CRDFFT_SPECTRAL_SPECTROGRAM  spectrogram (spectral.hpp:177-183): count x nseg x nfreq, row s = segment s
+ *   CRDFFT_SPECTRAL_PERIODOGRAM  periodogram (spectral.hpp:188-220): one segment of the whole signal, boxcar
+ *                                window, count x nfreq (nperseg, noverlap and window ignored)
+ * nfreq = nperseg / 2 + 1, nseg = (nsamples - noverlap) / (nperseg - noverlap), 0 when nsamples < nperseg (Welch
+ * then writes zeros). nperseg even, at least 4, half at most 8192. The Welch average adds the segments in a fixed
+ * order, so its result is the same on every run. */
+#define CRDFFT_SPECTRAL_WELCH 0
+#define CRDFFT_SPECTRAL_SPECTROGRAM 1
+#define CRDFFT_SPECTRAL_PERIODOGRAM 2
+typedef struct crdfft_spectral_desc
+{
+    int32_t mode;
+    int32_t detrend;      /* 1: subtract each segment's mean (the reference's 'constant'); 0: none */
+    int64_t nsamples;
+    int64_t count;
+    int64_t nperseg;
+    int64_t noverlap;
+    double fs;
+    const float* window;  /* host, nperseg values; NULL: the periodic Hann window (windows.hpp:120-124) */
+} crdfft_spectral_desc;
+crdfft_status crdfft_spectral_plan_create(const crdfft_spectral_desc* desc, crdfft_plan** plan);
+/* Segments a signal under the descriptor (after the Welch noverlap default), or -1 for an invalid one. */
+int64_t crdfft_spectral_segments(const crdfft_spectral_desc* desc);
+/* x: count x nsamples floats on the device; out as above. crdfft_execute rejects spectral plans. */
+crdfft_status crdfft_spectral_execute(crdfft_plan* plan, const float* x, float* out, void* stream);
 
 /* ---- Uneven batches ---------------------------------------------------------------------------------------- */
 

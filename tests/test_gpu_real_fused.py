@@ -189,4 +189,55 @@ def test_real_conv_plan_errors():
     with pytest.raises(cf.CrdFftError):
         cf.ConvPlan([8, 8, 8], real=True)     # rank 3
     with pytest.raises(cf.CrdFftError):
-        cf.Plan([64, 64], kind=cf.R2C)       # real plans of rank 2 exist only as convolutions
+        cf.Plan([64, 63], kind=cf.R2C)       # odd real axis
+
+
+# ---- 2-D and 3-D real transforms -------------------------------------------------------------------------------
+
+
+@pytest.mark.parametrize("dims", [(64, 64), (16, 1024), (105, 96), (256, 2000), (8, 12, 16), (32, 16, 256), (4, 1, 6)])
+def test_nd_real_plans(dims):
+    batch = 3
+    total = int(np.prod(dims))
+    half = tuple(dims[:-1]) + (dims[-1] // 2 + 1,)
+    x = oracle.lcg_float32(0xF20 ^ total, batch * total).reshape((batch,) + tuple(dims))
+    r2c = cf.Plan(list(dims), batch=batch, kind=cf.R2C)
+    c2r = cf.Plan(list(dims), batch=batch, kind=cf.C2R, norm=cf.NORM_INVERSE)
+    assert r2c.info()["algorithm"] == "nd-real"
+    spec = torch.empty((batch,) + half, dtype=torch.complex64, device="cuda")
+    r2c.execute(torch.from_numpy(x).cuda(), spec, cf.FORWARD)
+    axes = tuple(range(1, len(dims) + 1))
+    y = oracle.lcg_complex64(0xF21 ^ total, batch * int(np.prod(half))).reshape((batch,) + half)
+    ty = torch.from_numpy(y).cuda()
+    back = torch.empty((batch,) + tuple(dims), dtype=torch.float32, device="cuda")
+    c2r.execute(ty, back, cf.INVERSE)
+    torch.cuda.synchronize()
+    want = np.fft.rfftn(x.astype(np.float64), axes=axes)
+    assert oracle.rel_l2(spec.cpu().numpy(), want) <= REL_L2
+    want_back = np.fft.irfftn(y.astype(np.complex128), s=dims, axes=axes)  # normalised, as numpy's
+    assert oracle.rel_l2(back.cpu().numpy(), want_back) <= REL_L2
+    assert np.array_equal(ty.cpu().numpy(), y)  # C2R leaves its input alone
+
+
+def test_nd_real_round_trip_unnormalised():
+    dims, batch = (128, 256), 2
+    x = oracle.lcg_float32(0xF22, batch * dims[0] * dims[1]).reshape(batch, *dims)
+    spec = torch.empty(batch, dims[0], dims[1] // 2 + 1, dtype=torch.complex64, device="cuda")
+    back = torch.empty(batch, *dims, dtype=torch.float32, device="cuda")
+    cf.Plan(list(dims), batch=batch, kind=cf.R2C).execute(torch.from_numpy(x).cuda(), spec, cf.FORWARD)
+    cf.Plan(list(dims), batch=batch, kind=cf.C2R).execute(spec, back, cf.INVERSE)
+    torch.cuda.synchronize()
+    assert oracle.rel_l2(back.cpu().numpy() / (dims[0] * dims[1]), x.astype(np.float64)) <= REL_L2
+
+
+def test_nd_real_host_execute_matches_device():
+    dims, batch = (64, 128), 16
+    x = oracle.lcg_float32(0xF23, batch * dims[0] * dims[1]).reshape(batch, *dims)
+    plan = cf.Plan(list(dims), batch=batch, kind=cf.R2C)
+    dev = torch.empty(batch, dims[0], dims[1] // 2 + 1, dtype=torch.complex64, device="cuda")
+    plan.execute(torch.from_numpy(x).cuda(), dev, cf.FORWARD)
+    hin = torch.from_numpy(x.copy()).pin_memory()
+    hout = torch.empty(dev.shape, dtype=torch.complex64).pin_memory()
+    plan.execute_host(hin, hout, cf.FORWARD)
+    torch.cuda.synchronize()
+    assert np.array_equal(hout.numpy(), dev.cpu().numpy())
