@@ -39,6 +39,7 @@ namespace lfft
 
 constexpr int kMaxLinesPerCta = 256;
 constexpr int kMaxThreads = 512;
+constexpr int kStaticThreads = 256; // the real-line and spectral kernels with a compile-time schedule
 constexpr int kPipeThreads = 256;
 
 // Classic layout: one pad slot every 16 complex (128 bytes) keeps the strided stage accesses spread over the banks.

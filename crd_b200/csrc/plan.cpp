@@ -809,7 +809,29 @@ bool l2_waves()
     return on;
 }
 
-long long l2_wave_bytes() { return 24LL << 20; }
+// The L2 wave size and the largest transform (bytes) that takes L2 waves; CRDFFT_L2_WAVE_BYTES and
+// CRDFFT_L2_WAVE_MAX_TRANSFORM override them.
+long long env_bytes(const char* name, long long dflt)
+{
+    const char* e = std::getenv(name);
+    if (e != nullptr)
+    {
+        const long long v = std::atoll(e);
+        if (v > 0)
+            return v;
+    }
+    return dflt;
+}
+long long l2_wave_bytes()
+{
+    static const long long v = env_bytes("CRDFFT_L2_WAVE_BYTES", 24LL << 20);
+    return v;
+}
+long long l2_wave_max_transform()
+{
+    static const long long v = env_bytes("CRDFFT_L2_WAVE_MAX_TRANSFORM", 2LL << 20);
+    return v;
+}
 
 // A batch of 1-D complex transforms of length n: element j of transform t at base + t*dist + j*stride on each side.
 // Appends the steps of one direction; `ws_off` is where in the workspace this transform's scratch may start; the
@@ -891,7 +913,8 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     // consecutive waves on the plan's two internal streams so that one wave's pass 2 overlaps the next one's pass 1
     // (and fills its tail). Otherwise one large wave at a time on the caller's stream.
     // (Transforms above 2 MiB are left to large waves: a 24 MiB wave of them is too few tiles to fill the GPU.)
-    const bool l2w = l2_waves() && t_arena == nullptr && n * 8 <= (2LL << 20) && batch * n * 8 > 2 * l2_wave_bytes();
+    const bool l2w = l2_waves() && t_arena == nullptr && n * 8 <= l2_wave_max_transform() &&
+                     batch * n * 8 > 2 * l2_wave_bytes();
     long long wave = std::max(1LL, (l2w ? l2_wave_bytes() : wave_bytes()) / (n * 8));
     wave = std::min(wave, batch);
     *ws_need = (l2w ? 2 : 1) * wave * n;

@@ -81,8 +81,10 @@ __device__ __forceinline__ void pair_pass(int M, int jt, int T, const float2* __
 }
 
 // Compile-time schedule of the M-point line. One CTA holds lpc whole lines (row map, unit stride on both sides).
+// At most 256 threads (the launch shapes of conv_shape for these schedules); 16 points a thread leave registers for
+// four CTAs an SM.
 template <class S, int P, int MODE>
-__global__ void __launch_bounds__(kMaxThreads)
+__global__ void __launch_bounds__(kStaticThreads, P == 16 ? 4 : 2)
     real_line_kernel(const PassDesc d, const float2* __restrict__ gin, const float2* __restrict__ spec,
                      const RealLineAux r, float2* __restrict__ gout)
 {
@@ -284,6 +286,8 @@ cudaError_t launch_real_line(const PassDesc& d, int mode, const RealLineAux& r, 
             return cudaErrorInvalidConfiguration;
     }
     const int T = (d.n + P - 1) / P;
+    if (!lfft::real_is_dynamic(d, P) && T * lpc > lfft::kStaticThreads)
+        return cudaErrorInvalidConfiguration;
     const long long groups = (d.lines + lpc - 1) / lpc;
     if (groups <= 0)
         return cudaSuccess;

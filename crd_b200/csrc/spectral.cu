@@ -25,8 +25,9 @@ namespace lfft
 namespace
 {
 
+// At most 256 threads with a compile-time schedule (four CTAs an SM at 16 points a thread), 512 with the run-time one.
 template <class S, int P, bool DYN>
-__global__ void __launch_bounds__(kMaxThreads)
+__global__ void __launch_bounds__(DYN ? kMaxThreads : kStaticThreads, DYN ? 1 : (P == 16 ? 4 : 2))
     spectral_kernel(const PassDesc d, const SpectralDesc sd, const float* __restrict__ x, float* __restrict__ out)
 {
     extern __shared__ float2 sm[];
@@ -50,55 +51,123 @@ __global__ void __launch_bounds__(kMaxThreads)
     if (DYN && tid < kMaxStages)
         s_radix[tid] = d.radix[tid];
 
-    // 1. the segment as real pairs, and its sum
-    float sum = 0.0f;
-    if (ok)
+    if constexpr (!DYN)
     {
-        const float* src = x + g * sd.nsamples + (seg0 + ll) * sd.hop;
-        const LayRow<1> lay{line};
-        if ((reinterpret_cast<uintptr_t>(src) & 7) == 0)
+        // 1-2 (compile-time schedule). Every pair of the thread in registers at once (all loads in flight), the
+        // segment's sum by warp shuffles (a line's T threads are consecutive lanes, or whole warps), then detrend
+        // and window applied in registers and one store to shared memory.
+        constexpr int TS = (S::n + P - 1) / P;
+        constexpr int ROUND = P < 16 ? P : 16;
+        static_assert(TS <= 32 ? (32 % TS == 0) : (TS % 32 == 0),
+                      "a line is a power-of-two part of a warp or whole warps");
+        const float* src = x + g * sd.nsamples + (seg0 + (ok ? ll : 0)) * sd.hop;
+        const bool al = (reinterpret_cast<uintptr_t>(src) & 7) == 0;
+        float2 v[P];
+        float sum = 0.0f;
+#pragma unroll
+        for (int r0 = 0; r0 < P; r0 += ROUND)
         {
-            const float2* s2 = reinterpret_cast<const float2*>(src);
-#pragma unroll 4
-            for (int m = jt; m < M; m += T)
+#pragma unroll
+            for (int r = r0; r < r0 + ROUND; ++r)
             {
-                const float2 v = __ldg(s2 + m);
-                lay.at(m) = v;
-                sum += v.x + v.y;
+                const int m = jt + r * TS;
+                v[r] = make_float2(0.0f, 0.0f);
+                if (ok && m < M)
+                    v[r] = al ? __ldg(reinterpret_cast<const float2*>(src) + m)
+                              : make_float2(__ldg(src + 2 * m), __ldg(src + 2 * m + 1));
             }
+        }
+#pragma unroll
+        for (int r = 0; r < P; ++r)
+            sum += v[r].x + v[r].y;
+        if constexpr (TS <= 32)
+        {
+#pragma unroll
+            for (int o = TS / 2; o > 0; o >>= 1)
+                sum += __shfl_xor_sync(0xffffffffu, sum, o);
         }
         else
         {
-#pragma unroll 4
-            for (int m = jt; m < M; m += T)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                sum += __shfl_xor_sync(0xffffffffu, sum, o);
+            if ((tid & 31) == 0)
+                red[tid >> 5] = sum;
+            __syncthreads();
+            sum = 0.0f;
+#pragma unroll
+            for (int i = 0; i < TS / 32; ++i)
+                sum += red[ll * (TS / 32) + i];
+        }
+        const float mean = sd.detrend ? sum / static_cast<float>(2 * M) : 0.0f;
+        const float2* w2 = reinterpret_cast<const float2*>(sd.win);
+        const LayRow<1> lay{line};
+        if (ok)
+        {
+#pragma unroll
+            for (int r = 0; r < P; ++r)
             {
-                const float2 v = make_float2(__ldg(src + 2 * m), __ldg(src + 2 * m + 1));
-                lay.at(m) = v;
-                sum += v.x + v.y;
+                const int m = jt + r * TS;
+                if (m < M)
+                {
+                    const float2 w = __ldg(w2 + m);
+                    lay.at(m) = make_float2((v[r].x - mean) * w.x, (v[r].y - mean) * w.y);
+                }
             }
         }
     }
-    red[tid] = sum;
-    __syncthreads();
-    if (ok && jt == 0)
+    else
     {
-        float s = 0.0f;
-        for (int t = 0; t < T; ++t)
-            s += red[ll * T + t];
-        s_mean[ll] = sd.detrend ? s / static_cast<float>(2 * M) : 0.0f;
-    }
-    __syncthreads();
-    // 2. detrend and window, each thread on the pairs it loaded
-    if (ok)
-    {
-        const float mean = s_mean[ll];
-        const float2* w2 = reinterpret_cast<const float2*>(sd.win);
-        const LayRow<1> lay{line};
-        for (int m = jt; m < M; m += T)
+        // 1. the segment as real pairs, and its sum
+        float sum = 0.0f;
+        if (ok)
         {
-            const float2 v = lay.at(m);
-            const float2 w = __ldg(w2 + m);
-            lay.at(m) = make_float2((v.x - mean) * w.x, (v.y - mean) * w.y);
+            const float* src = x + g * sd.nsamples + (seg0 + ll) * sd.hop;
+            const LayRow<1> lay{line};
+            if ((reinterpret_cast<uintptr_t>(src) & 7) == 0)
+            {
+                const float2* s2 = reinterpret_cast<const float2*>(src);
+#pragma unroll 4
+                for (int m = jt; m < M; m += T)
+                {
+                    const float2 v = __ldg(s2 + m);
+                    lay.at(m) = v;
+                    sum += v.x + v.y;
+                }
+            }
+            else
+            {
+#pragma unroll 4
+                for (int m = jt; m < M; m += T)
+                {
+                    const float2 v = make_float2(__ldg(src + 2 * m), __ldg(src + 2 * m + 1));
+                    lay.at(m) = v;
+                    sum += v.x + v.y;
+                }
+            }
+        }
+        red[tid] = sum;
+        __syncthreads();
+        if (ok && jt == 0)
+        {
+            float s = 0.0f;
+            for (int t = 0; t < T; ++t)
+                s += red[ll * T + t];
+            s_mean[ll] = sd.detrend ? s / static_cast<float>(2 * M) : 0.0f;
+        }
+        __syncthreads();
+        // 2. detrend and window, each thread on the pairs it loaded
+        if (ok)
+        {
+            const float mean = s_mean[ll];
+            const float2* w2 = reinterpret_cast<const float2*>(sd.win);
+            const LayRow<1> lay{line};
+            for (int m = jt; m < M; m += T)
+            {
+                const float2 v = lay.at(m);
+                const float2 w = __ldg(w2 + m);
+                lay.at(m) = make_float2((v.x - mean) * w.x, (v.y - mean) * w.y);
+            }
         }
     }
     // 3. the M-point FFT of the pairs
@@ -223,8 +292,11 @@ bool spectral_shape(const PassDesc& d, int* P, int* lpc, int* threads, int* smem
     const int line_bytes = (dyn ? 2 : 1) * pitch * 8;
     while (l > 1 && l * line_bytes + std::max(T * l, l * (d.n + 1)) * 4 > 200 * 1024)
         --l;
+    // whole warps (the compile-time path reduces a line's sum with warp shuffles)
+    if (!dyn && T < 32)
+        l = std::max(32 / T, l - l % (32 / T));
     const long long bytes = static_cast<long long>(l) * line_bytes + std::max(T * l, l * (d.n + 1)) * 4LL;
-    if (bytes > 227 * 1024 || T * l > lfft::kMaxThreads)
+    if (bytes > 227 * 1024 || T * l > (dyn ? lfft::kMaxThreads : lfft::kStaticThreads))
         return false;
     *P = p;
     *lpc = l;

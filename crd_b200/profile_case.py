@@ -1,9 +1,13 @@
 """One plan, executed a few times: the small, self-contained case that profilers capture.
 
     python -m crd_b200.profile_case N BATCH REPS [estimate|measure|learned] [WISDOM_FILE]
+    python -m crd_b200.profile_case r2c N BATCH REPS
+    python -m crd_b200.profile_case welch|spectrogram NPERSEG NOVERLAP COUNT NSAMPLES REPS
 
-Creates a forward C2C plan of BATCH transforms of length N (planner mode and optional wisdom as given), fills the
-input with uniform[-1, 1) values and runs REPS out-of-place executes on the current CUDA device.
+The first form creates a forward C2C plan of BATCH transforms of length N (planner mode and optional wisdom as
+given), fills the input with uniform[-1, 1) values and runs REPS out-of-place executes on the current CUDA device.
+The second runs a real-to-complex plan the same way; the third a spectral estimator over COUNT signals of NSAMPLES
+Gaussian samples (periodic Hann window, fs 1).
 """
 
 from __future__ import annotations
@@ -19,6 +23,29 @@ def main(argv=None) -> None:
     import crd_b200.hesap as F
 
     argv = sys.argv[1:] if argv is None else argv
+    if argv[0] == "r2c":
+        n, batch, reps = int(argv[1]), int(argv[2]), int(argv[3])
+        x = torch.rand(n * batch, device="cuda") * 2 - 1
+        y = torch.empty(batch * (n // 2 + 1), dtype=torch.complex64, device="cuda")
+        plan = cf.Plan([n], batch=batch, kind=cf.R2C)
+        print(plan.info())
+        for _ in range(reps):
+            plan.execute(x, y, cf.FORWARD)
+        torch.cuda.synchronize()
+        print("ok")
+        return
+    if argv[0] in ("welch", "spectrogram"):
+        nper, nov, count, ns, reps = (int(v) for v in argv[1:6])
+        mode = cf.SPECTRAL_WELCH if argv[0] == "welch" else cf.SPECTRAL_SPECTROGRAM
+        x = torch.randn(count * ns, device="cuda")
+        plan = cf.SpectralPlan(mode, ns, count, 1.0, nper, nov)
+        print(plan.info())
+        out = torch.empty(plan.out_shape(), dtype=torch.float32, device="cuda")
+        for _ in range(reps):
+            plan.execute(x, out)
+        torch.cuda.synchronize()
+        print("ok")
+        return
     n, batch, reps = int(argv[0]), int(argv[1]), int(argv[2])
     if len(argv) > 4 and os.path.exists(argv[4]):
         with open(argv[4]) as f:
