@@ -63,6 +63,9 @@ bool spectral_shape(const PassDesc& d, int* P, int* lpc, int* threads, int* smem
 cudaError_t launch_spectral(const PassDesc& d, const SpectralDesc& sd, int threads, int smem, const void* x,
                             void* out, cudaStream_t stream);
 cudaError_t launch_welch_finish(const SpectralDesc& sd, const void* part, void* psd, cudaStream_t stream);
+// The four-step column pass as a persistent kernel fed by 2-D tensor copies (tma_col.cu).
+bool tma_col_supported(const PassDesc& d);
+cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStream_t stream);
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
 int pass_threads_limit();

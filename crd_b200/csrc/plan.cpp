@@ -27,6 +27,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <cstdio>
 #include <complex>
 #include <cstdlib>
 #include <cstring>
@@ -99,6 +100,7 @@ enum class StepKind : int
     RealLine,
     Spectral,
     WelchFinish,
+    TmaCol,
     Zero,
     R2CPost,
     C2RPre,
@@ -799,6 +801,14 @@ long long wave_bytes()
     return 512LL << 20;
 }
 
+// The four-step column pass on the tensor-copy kernel (tma_col.cu) where it applies (1024- and 512-point columns:
+// 2^20 2.68 -> 2.39 ms, 2^19 2.54 -> 2.19 ms per 2 GiB); CRDFFT_TMA_COL=0 keeps the line kernel.
+bool tma_col_enabled()
+{
+    const char* e = std::getenv("CRDFFT_TMA_COL");
+    return e == nullptr || std::atoi(e) != 0;
+}
+
 // Four-step waves sized for L2 on two internal streams (CRDFFT_L2_WAVES=1) or one large wave at a time (=0).
 bool l2_waves()
 {
@@ -935,6 +945,8 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
                             1.0f, &s1, ftw);
         if (st != CRDFFT_OK)
             return st;
+        if (tma_col_enabled() && s1.kind == StepKind::Line && tma_col_supported(s1.pass))
+            s1.kind = StepKind::TmaCol;
         s1.lane = lane;
         steps.push_back(s1);
         // pass 2: rows k1 of length n2 -> X[t][k1 + n1 k2]
@@ -2188,6 +2200,7 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
                 e = launch_spectral(s.pass, s.sdesc, s.sthreads, s.ssmem, src, dst, stream);
                 break;
             case StepKind::WelchFinish: e = launch_welch_finish(s.sdesc, src, dst, stream); break;
+            case StepKind::TmaCol: e = launch_tma_col(s.pass, src, dst, stream); break;
             case StepKind::Zero: e = cudaMemsetAsync(dst, 0, static_cast<size_t>(s.count), stream); break;
             case StepKind::RealLine:
                 if (s.rmode == kRealConv && spec == nullptr)
@@ -2202,7 +2215,14 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
             case StepKind::Scale: e = launch_scale(dst, s.count, s.scale, stream); break;
         }
         if (e != cudaSuccess)
+        {
+            // CRDFFT_LOG_ERRORS=1: name the failing step and the CUDA error on stderr
+            static const bool log = std::getenv("CRDFFT_LOG_ERRORS") != nullptr;
+            if (log)
+                std::fprintf(stderr, "crdfft: step kind %d (n %d, lines %lld) failed: %s\n", static_cast<int>(s.kind),
+                             s.pass.n, s.pass.lines, cudaGetErrorString(e));
             return CRDFFT_LAUNCH;
+        }
     }
     if (forked && !join())
         return CRDFFT_LAUNCH;

@@ -1,0 +1,253 @@
+// The column pass of the four-step (n = n1 n2: n1-point DFTs down the columns of each transform's n1 x n2 matrix,
+// times the four-step twiddle) as a persistent kernel fed by the Tensor Memory Accelerator.
+//
+// A tile is 8 adjacent columns of one transform: an n1 x 8 box of the input seen as a [transforms * n1] x n2 matrix
+// of 8-byte elements, brought into shared memory by 2-D bulk tensor copies (cp.async.bulk.tensor, boxes of at most
+// 256 rows, completion counted in bytes on an mbarrier). Each CTA (one an SM) keeps `nbuf` tiles in flight: while it
+// transforms tile i from its buffer, tiles i+1 .. i+nbuf-1 are landing in the others, so the loads of the next
+// tiles overlap the arithmetic and the strided 64-byte runs of the column reads are always in flight. The stages are
+// the line kernels' (line_fft.cuh) on a column layout of pitch 8; the last stage writes the output straight to global
+// memory with the four-step twiddle. No cluster multicast: each CTA loads its own tiles.
+//
+// Every wait is bounded (the pass's spin limit): a wait that runs out sets the plan's status word, waits (bounded)
+// for the copies the CTA still has in flight and returns.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+
+#include "kernels.hpp"
+#include "line_fft.cuh"
+
+namespace crdfft
+{
+namespace lfft
+{
+namespace
+{
+
+constexpr int kTmaMaxRows = 256; // rows of one copy box
+constexpr int kTmaMaxBufs = 8;
+constexpr int kTmaSmemBudget = 200 * 1024;
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                 "[%4];" ::"r"(smem_addr(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+// Columns a tile: 8 (64-byte rows), so that two or three tiles of 512- or 1024-point columns fit in shared memory.
+__host__ __device__ constexpr int tma_cols(int) { return 8; }
+
+// Bytes between tile buffers: a tile rounded up to 1 KiB (copy destinations 128-byte aligned).
+__host__ __device__ constexpr int tma_tile_stride(int n) { return (n * tma_cols(n) * 8 + 1023) / 1024 * 1024; }
+
+template <class S, int P>
+__global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n), 1)
+    tma_col_kernel(const __grid_constant__ CUtensorMap map, const PassDesc d, float2* __restrict__ gout, int nbuf,
+                   int box_rows, long long tiles)
+{
+    constexpr int N = S::n;
+    constexpr int kTmaCols = tma_cols(N);
+    constexpr int T = (N + P - 1) / P;
+    constexpr int STRIDE = tma_tile_stride(N) / 8; // float2 elements between buffers
+    extern __shared__ unsigned char smraw[];
+    // the buffers from the first 1 KiB boundary of the dynamic shared memory, then the mbarriers and a flag
+    const uint32_t base = smem_addr(smraw);
+    unsigned char* aligned = smraw + ((1024u - (base & 1023u)) & 1023u);
+    float2* bufs = reinterpret_cast<float2*>(aligned);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(aligned + static_cast<size_t>(nbuf) * STRIDE * 8);
+    int& s_fail = *reinterpret_cast<int*>(bars + nbuf);
+    const int tid = threadIdx.x;
+    const int jt = tid / kTmaCols; // element group within the column
+    const int ll = tid - jt * kTmaCols;
+    const long long n2 = d.lines_per_group;
+    const long long tiles_per_group = n2 / kTmaCols;
+    const long long G = gridDim.x;
+    const uint32_t tile_bytes = static_cast<uint32_t>(N) * kTmaCols * 8u;
+
+    auto issue = [&](long long k, int b) {
+        const long long grp = k / tiles_per_group;
+        const int q0 = static_cast<int>(k - grp * tiles_per_group) * kTmaCols;
+        uint64_t* bar = bars + b;
+        mbar_expect_tx(bar, tile_bytes);
+        float2* dst = bufs + static_cast<size_t>(b) * STRIDE;
+        for (int r0 = 0; r0 < N; r0 += box_rows)
+            tma_load_2d(dst + static_cast<size_t>(r0) * kTmaCols, &map, q0, static_cast<int>(grp * N + r0), bar);
+    };
+
+    if (tid == 0)
+    {
+        s_fail = 0;
+        for (int b = 0; b < nbuf; ++b)
+            mbar_init(bars + b, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fence_proxy_async();
+        for (int b = 0; b < nbuf; ++b)
+        {
+            const long long k = blockIdx.x + b * G;
+            if (k < tiles)
+                issue(k, b);
+        }
+    }
+    __syncthreads();
+
+    int it = 0;
+    for (long long k = blockIdx.x; k < tiles; k += G, ++it)
+    {
+        const int b = it % nbuf;
+        const uint32_t parity = static_cast<uint32_t>(it / nbuf) & 1u;
+        const bool ready = mbar_wait_bounded(bars + b, parity, d.spin_limit);
+        if (!ready)
+            atomicExch(&s_fail, 1);
+        __syncthreads();
+        if (s_fail)
+        {
+            // the copies this CTA still has in flight: tiles k .. k + (nbuf-1) G, in buffers b, b+1, ...
+            if (tid == 0)
+            {
+                atomicOr(d.err, 1);
+                for (int j = 0; j < nbuf; ++j)
+                {
+                    const long long kk = k + j * G;
+                    if (kk >= tiles)
+                        break;
+                    const int itj = it + j;
+                    mbar_wait_bounded(bars + itj % nbuf, static_cast<uint32_t>(itj / nbuf) & 1u, d.spin_limit);
+                }
+            }
+            __syncthreads();
+            return;
+        }
+        const long long grp = k / tiles_per_group;
+        const long long q0 = (k - grp * tiles_per_group) * kTmaCols;
+        const long long line = grp * n2 + q0 + ll;
+        Ctx c;
+        c.ok = true;
+        c.q = (q0 + ll) / d.ftw_div;
+        c.in = nullptr;
+        c.out = gout + line_offset(d.out, line, n2);
+        c.jt = jt;
+        c.T = T;
+        init_scales(d, c);
+        const LayCol lay{bufs + static_cast<size_t>(b) * STRIDE + ll, kTmaCols};
+        // stages in shared memory (the first applies the input conjugation), the last one stores to global memory
+        SchedRun<S>::template go<P, false, true, true, Kind<PassMap::Col, true>>(d, c, lay, N);
+        __syncthreads(); // every thread has read buffer b
+        if (tid == 0)
+        {
+            const long long kn = k + nbuf * G;
+            if (kn < tiles)
+            {
+                fence_proxy_async(); // the stages' shared-memory accesses before the copy engine's writes
+                issue(kn, b);
+            }
+        }
+    }
+}
+
+using TmaFn = void (*)(const CUtensorMap, const PassDesc, float2*, int, int, long long);
+
+TmaFn tma_select(const PassDesc& d, int* P)
+{
+    // 1024- and 512-point columns at 16 points a thread (512 and 256 threads). Measured slower here, and left to the
+    // line kernel: radix-32 stages on this column layout (bank conflicts), 105-point columns (too little work a
+    // tile), 32 points a thread (half the warps).
+    if (same_radices(d, {16, 16, 4}))
+    {
+        *P = 16;
+        return tma_col_kernel<Sched<16, 16, 4>, 16>;
+    }
+    if (same_radices(d, {16, 8, 4}))
+    {
+        *P = 16;
+        return tma_col_kernel<Sched<16, 8, 4>, 16>;
+    }
+    return nullptr;
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return static_cast<PFN_cuTensorMapEncodeTiled_v12000>(nullptr);
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+} // namespace
+} // namespace lfft
+
+// The pass shapes this kernel takes: a column pass (elements n2 apart, adjacent lines adjacent) over packed groups
+// of n2 lines (n2 a multiple of 8, the input row of n2 elements a multiple of 16 bytes), a schedule it has, n1 a
+// multiple of its box rows.
+bool tma_col_supported(const PassDesc& d)
+{
+    int P = 0;
+    if (lfft::tma_select(d, &P) == nullptr)
+        return false;
+    const long long n2 = d.lines_per_group;
+    if (n2 % lfft::tma_cols(d.n) != 0 || d.in.ldist != 1 || d.in.estride != n2 || d.in.gdist != n2 * d.n)
+        return false;
+    if (d.n > lfft::kTmaMaxRows && d.n % lfft::kTmaMaxRows != 0)
+        return false;
+    if (d.lines % n2 != 0 || d.lines / n2 * d.n > 0x7fffffffLL)
+        return false;
+    if (2 * lfft::tma_tile_stride(d.n) > lfft::kTmaSmemBudget) // two tiles in flight at least
+        return false;
+    return lfft::encoder() != nullptr;
+}
+
+cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStream_t stream)
+{
+    int P = 0;
+    lfft::TmaFn fn = lfft::tma_select(d, &P);
+    if (fn == nullptr || lfft::encoder() == nullptr)
+        return cudaErrorInvalidConfiguration;
+    const long long n2 = d.lines_per_group;
+    const long long groups = d.lines / n2;
+    const int box_rows = d.n <= lfft::kTmaMaxRows ? d.n : lfft::kTmaMaxRows;
+    if ((reinterpret_cast<uintptr_t>(in) & 15) != 0)
+        return cudaErrorInvalidConfiguration;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(n2), static_cast<cuuint64_t>(groups * d.n)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(n2) * 8};
+    const int cols = lfft::tma_cols(d.n);
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(cols), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    if (lfft::encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(in), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue; // the tensor map was refused
+    const int tile_stride = lfft::tma_tile_stride(d.n);
+    int nbuf = lfft::kTmaSmemBudget / tile_stride;
+    if (nbuf > lfft::kTmaMaxBufs)
+        nbuf = lfft::kTmaMaxBufs;
+    if (nbuf < 2)
+        return cudaErrorInvalidConfiguration;
+    const int smem = 1024 + nbuf * tile_stride + nbuf * 8 + 16;
+    const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess)
+        return e;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = groups * (n2 / cols);
+    long long grid = sms;
+    if (grid > tiles)
+        grid = tiles;
+    if (grid < 1)
+        return cudaSuccess;
+    const int threads = ((d.n + P - 1) / P) * cols;
+    fn<<<static_cast<unsigned>(grid), threads, smem, stream>>>(map, d, static_cast<float2*>(out), nbuf, box_rows,
+                                                               tiles);
+    return cudaGetLastError();
+}
+
+} // namespace crdfft
