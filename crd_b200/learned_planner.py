@@ -86,10 +86,10 @@ class Problem:
 
 
 def problems(count: int, seed: int) -> list[Problem]:
-    """Seeded problems: a third each 1-D C2C, 1-D R2C and 2-D C2C. 1-D sizes log-uniform over the 7-smooth integers
-    in [64, 2^22] (R2C: the even ones); 2-D sides over those in [16, 4096] with at least 64 points; batch log-uniform
-    in [1, 65536], capped so the input stays within 2 GiB; half padded (+8 elements between transforms); half
-    split-BF16."""
+    """Seeded problems: a quarter each 1-D C2C, 1-D R2C, 2-D C2C and 2-D R2C. 1-D sizes log-uniform over the 7-smooth
+    integers in [64, 2^22] (R2C: the even ones); 2-D sides over those in [16, 4096] with at least 64 points (R2C: an
+    even last side); batch log-uniform in [1, 65536], capped so the input stays within 2 GiB; half padded (+8 elements
+    between transforms; 2-D R2C plans take packed batches only); half split-BF16."""
     rng = np.random.default_rng(seed)
     s1 = np.array(smooth7(64, 1 << 22))
     s1e = s1[s1 % 2 == 0]
@@ -101,23 +101,24 @@ def problems(count: int, seed: int) -> list[Problem]:
         return int(cands[min(i, len(cands) - 1)])
 
     out = []
+    s2e = s2[s2 % 2 == 0]
     for _ in range(count):
-        shape = int(rng.integers(0, 3))
+        shape = int(rng.integers(0, 4))
         if shape == 0:
             dims, kind = (pick(s1, 64, 1 << 22),), C2C
         elif shape == 1:
             dims, kind = (pick(s1e, 64, 1 << 22),), R2C
         else:
             while True:
-                dims = (pick(s2, 16, 4096), pick(s2, 16, 4096))
+                dims = (pick(s2, 16, 4096), pick(s2e if shape == 3 else s2, 16, 4096))
                 if dims[0] * dims[1] >= 64:
                     break
-            kind = C2C
+            kind = R2C if shape == 3 else C2C
         pts = int(np.prod(dims))
         elem = 4 if kind == R2C else 8
         batch = int(round(math.exp(rng.uniform(0.0, math.log(65536)))))
         batch = max(1, min(batch, MAX_INPUT_BYTES // ((pts + 8) * elem)))
-        padded = bool(rng.integers(0, 2))
+        padded = bool(rng.integers(0, 2)) and not (kind == R2C and len(dims) == 2)
         precision = PREC_SPLIT_BF16 if rng.integers(0, 2) else PREC_FP32
         out.append(Problem(dims, batch, kind, padded, precision))
     return out

@@ -60,11 +60,12 @@ def test_problem_generator_follows_its_contract():
         if len(pr.dims) == 1:
             assert 64 <= pts <= 1 << 22
         if pr.kind == R2C:
-            assert len(pr.dims) == 1 and pts % 2 == 0
+            assert pr.dims[-1] % 2 == 0
+            assert len(pr.dims) == 1 or not pr.padded  # 2-D real plans take packed batches
         elem = 4 if pr.kind == R2C else 8
         assert 1 <= pr.batch <= 65536 and pr.batch * (pts + 8) * elem <= MAX_INPUT_BYTES
     kinds = {(len(p.dims), p.kind) for p in probs}
-    assert len(kinds) == 3
+    assert len(kinds) == 4
     assert any(p.padded for p in probs) and any(not p.padded for p in probs)
 
 
