@@ -31,9 +31,9 @@ namespace
 {
 
 // Launched with a cluster of C CTAs (a launch attribute: 16 is above the portable size and needs the kernel's
-// non-portable opt-in). Two CTAs an SM at C = 8 (512 threads), four at C = 16 (256 threads).
-template <class S1, class S2, int C, int P, bool EPI>
-__global__ void __launch_bounds__((S1::n * S2::n) / (P * C), C >= 16 ? 4 : 2)
+// non-portable opt-in). Two CTAs an SM at C = 8 (512 threads), five at C = 16 (256 threads).
+template <class S1, class S2, int C, int P, bool EPI, int MINB>
+__global__ void __launch_bounds__((S1::n * S2::n) / (P * C), MINB)
     cluster_fft_kernel(const PassDesc dA, const PassDesc dB, const float2* __restrict__ gin, float2* __restrict__ gout)
 {
     constexpr int N1 = S1::n;
@@ -114,14 +114,16 @@ __global__ void __launch_bounds__((S1::n * S2::n) / (P * C), C >= 16 ? 4 : 2)
 
 using ClusterFn = void (*)(const PassDesc, const PassDesc, const float2*, float2*);
 
-template <class S1, class S2, int C, int P> struct ClusterInst
+// MINB: CTAs an SM the registers are sized for (the kernel is latency-bound: more resident clusters hide the cluster
+// barriers better).
+template <class S1, class S2, int C, int P, int MINB> struct ClusterInst
 {
     static constexpr int threads = (S1::n * S2::n) / (P * C);
     static constexpr int smem_elems =
         (S1::n * (S2::n / C + 1)) > (S2::n * (S1::n / C + 1)) ? (S1::n * (S2::n / C + 1)) : (S2::n * (S1::n / C + 1));
     static ClusterFn get(bool epi)
     {
-        return epi ? cluster_fft_kernel<S1, S2, C, P, true> : cluster_fft_kernel<S1, S2, C, P, false>;
+        return epi ? cluster_fft_kernel<S1, S2, C, P, true, MINB> : cluster_fft_kernel<S1, S2, C, P, false, MINB>;
     }
 };
 
@@ -129,28 +131,36 @@ struct ClusterEntry
 {
     int n1, n2, cluster, threads, smem_bytes;
     ClusterFn fn_epi, fn_plain;
+    int minb;
 };
 
-template <class I> ClusterEntry entry(int n1, int n2, int c)
+template <class I> ClusterEntry entry(int n1, int n2, int c, int minb)
 {
-    return ClusterEntry{n1, n2, c, I::threads, I::smem_elems * 8, I::get(true), I::get(false)};
+    return ClusterEntry{n1, n2, c, I::threads, I::smem_elems * 8, I::get(true), I::get(false), minb};
 }
 
 const ClusterEntry* find(long long n1, long long n2)
 {
     static const ClusterEntry table[] = {
-        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 8, 16>>(256, 256, 8),   // 65536
-        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 16, 16>>(256, 256, 16), // 65536, 16-CTA clusters
+        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 8, 16, 2>>(256, 256, 8, 2),    // 65536
+        // 65536, 16-CTA clusters at five CTAs an SM (48 registers, no spills; 1.68 -> 1.60 ms per 2 GiB over four;
+        // six spill and are slower), four kept for comparison (CRDFFT_CLUSTER_OCC=4)
+        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 16, 16, 5>>(256, 256, 16, 5),
+        entry<ClusterInst<Sched<16, 16>, Sched<16, 16>, 16, 16, 4>>(256, 256, 16, 4),
     };
     static const int want = [] {
         const char* e = std::getenv("CRDFFT_CLUSTER_SIZE");
         return e != nullptr ? std::atoi(e) : 16;
     }();
+    const int occ = [] {
+        const char* e = std::getenv("CRDFFT_CLUSTER_OCC");
+        return e != nullptr ? std::atoi(e) : 0;
+    }();
     const ClusterEntry* any = nullptr;
     for (const ClusterEntry& e : table)
         if (e.n1 == n1 && e.n2 == n2)
         {
-            if (e.cluster == want)
+            if (e.cluster == want && (occ == 0 || e.minb == occ))
                 return &e;
             if (any == nullptr)
                 any = &e;
