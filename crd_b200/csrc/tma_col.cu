@@ -15,6 +15,8 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <cstdlib>
+
 
 #include "kernels.hpp"
 #include "line_fft.cuh"
@@ -28,7 +30,11 @@ namespace
 
 constexpr int kTmaMaxRows = 256; // rows of one copy box
 constexpr int kTmaMaxBufs = 8;
-constexpr int kTmaSmemBudget = 200 * 1024;
+constexpr int kSmPerSm = 228 * 1024; // shared memory of an SM; each CTA also takes 1 KiB of it
+
+// Bytes a CTA may give to tile buffers when `ctas` CTAs share an SM (1 KiB reserved a CTA, 1 KiB of alignment slack,
+// the barriers).
+__host__ __device__ constexpr int tma_buffer_budget(int ctas) { return kSmPerSm / ctas - 2 * 1024 - 64; }
 
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar)
 {
@@ -38,14 +44,19 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
                  : "memory");
 }
 
-// Columns a tile: 8 (64-byte rows), so that two or three tiles of 512- or 1024-point columns fit in shared memory.
-__host__ __device__ constexpr int tma_cols(int) { return 8; }
+// Columns a tile: 8 (64-byte rows) for 512- and 1024-point columns, so that three tiles fit in shared memory; 32
+// (256-byte rows) for short columns, whose tiles are small.
+__host__ __device__ constexpr int tma_cols(int n) { return n <= 256 ? 32 : 8; }
+
+// CTAs an SM: one for long columns (three 64 KiB tiles), four for short columns (two tiles each), so that short
+// columns, with few threads a tile, still keep enough warps resident.
+__host__ __device__ constexpr int tma_ctas(int n) { return n <= 256 ? 4 : 1; }
 
 // Bytes between tile buffers: a tile rounded up to 1 KiB (copy destinations 128-byte aligned).
 __host__ __device__ constexpr int tma_tile_stride(int n) { return (n * tma_cols(n) * 8 + 1023) / 1024 * 1024; }
 
 template <class S, int P>
-__global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n), 1)
+__global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n), tma_ctas(S::n))
     tma_col_kernel(const __grid_constant__ CUtensorMap map, const PassDesc d, float2* __restrict__ gout, int nbuf,
                    int box_rows, long long tiles)
 {
@@ -153,8 +164,7 @@ using TmaFn = void (*)(const CUtensorMap, const PassDesc, float2*, int, int, lon
 TmaFn tma_select(const PassDesc& d, int* P)
 {
     // 1024- and 512-point columns at 16 points a thread (512 and 256 threads). Measured slower here, and left to the
-    // line kernel: radix-32 stages on this column layout (bank conflicts), 105-point columns (too little work a
-    // tile), 32 points a thread (half the warps).
+    // line kernel: radix-32 stages on this column layout (bank conflicts), 32 points a thread (half the warps).
     if (same_radices(d, {16, 16, 4}))
     {
         *P = 16;
@@ -164,6 +174,13 @@ TmaFn tma_select(const PassDesc& d, int* P)
     {
         *P = 16;
         return tma_col_kernel<Sched<16, 8, 4>, 16>;
+    }
+    // 105-point columns (32-column tiles, four CTAs an SM): faster for 3*5*7*4096 (2.86 -> 2.71 ms per 2 GiB),
+    // slower for 107520 (2.23 -> 2.36 ms), so only on request (CRDFFT_TMA_SHORT=1)
+    if (std::getenv("CRDFFT_TMA_SHORT") != nullptr && same_radices(d, {7, 5, 3}))
+    {
+        *P = 16;
+        return tma_col_kernel<Sched<7, 5, 3>, 16>;
     }
     return nullptr;
 }
@@ -199,7 +216,7 @@ bool tma_col_supported(const PassDesc& d)
         return false;
     if (d.lines % n2 != 0 || d.lines / n2 * d.n > 0x7fffffffLL)
         return false;
-    if (2 * lfft::tma_tile_stride(d.n) > lfft::kTmaSmemBudget) // two tiles in flight at least
+    if (2 * lfft::tma_tile_stride(d.n) > lfft::tma_buffer_budget(lfft::tma_ctas(d.n))) // two tiles in flight
         return false;
     return lfft::encoder() != nullptr;
 }
@@ -226,7 +243,7 @@ cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStr
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue; // the tensor map was refused
     const int tile_stride = lfft::tma_tile_stride(d.n);
-    int nbuf = lfft::kTmaSmemBudget / tile_stride;
+    int nbuf = lfft::tma_buffer_budget(lfft::tma_ctas(d.n)) / tile_stride;
     if (nbuf > lfft::kTmaMaxBufs)
         nbuf = lfft::kTmaMaxBufs;
     if (nbuf < 2)
@@ -239,7 +256,7 @@ cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStr
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = groups * (n2 / cols);
-    long long grid = sms;
+    long long grid = static_cast<long long>(sms) * lfft::tma_ctas(d.n);
     if (grid > tiles)
         grid = tiles;
     if (grid < 1)
