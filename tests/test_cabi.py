@@ -74,3 +74,30 @@ def test_invalid_descriptor_rejected_without_device():
     assert L.crdfft_plan_create(None, ctypes.byref(h)) == _lib.INVALID_ARG
     assert L.crdfft_execute(None, None, None, 0, None) == _lib.INVALID_ARG
     assert L.crdfft_plan_destroy(None) == _lib.OK
+
+
+def test_spectral_descriptor_and_segment_count_without_device():
+    """crdfft_spectral_desc layout (2 int32 + 4 int64 + double + pointer = 56 bytes) and the segment count rule of
+    the reference's spectral.hpp:50-54 (Welch reads noverlap 0 as nperseg / 2), evaluated on the host."""
+    from oracle import spectral as S
+
+    assert ctypes.sizeof(_lib.SpectralDesc) == 56
+    L = _lib.lib()
+
+    def segs(mode, ns, nper, nov, fs=1.0):
+        d = _lib.SpectralDesc()
+        d.mode, d.detrend, d.nsamples, d.count, d.nperseg, d.noverlap, d.fs = mode, 1, ns, 3, nper, nov, fs
+        return L.crdfft_spectral_segments(ctypes.byref(d))
+
+    for ns, nper, nov in ((512, 64, 32), (100000, 1024, 512), (63, 64, 0), (5000, 256, 255), (70000, 4096, 1024)):
+        want = S.segment_count(ns, nper, nov if nov else nper // 2)
+        assert segs(_lib.SPECTRAL_WELCH, ns, nper, nov) == want
+    assert segs(_lib.SPECTRAL_SPECTROGRAM, 512, 64, 0) == 8          # no overlap: 512 / 64
+    assert segs(_lib.SPECTRAL_PERIODOGRAM, 4096, 0, 0) == 1
+    assert segs(_lib.SPECTRAL_WELCH, 1000, 255, 0) == -1               # odd segment length
+    assert segs(_lib.SPECTRAL_WELCH, 1000, 256, 256) == -1             # no hop
+    assert segs(_lib.SPECTRAL_WELCH, 1000, 256, 0, fs=0.0) == -1       # fs
+    assert segs(_lib.SPECTRAL_WELCH, 10 ** 6, 2 * 30000, 0) == -1      # half length beyond one pass
+    h = ctypes.c_void_p()
+    assert L.crdfft_spectral_plan_create(None, ctypes.byref(h)) == _lib.INVALID_ARG
+    assert L.crdfft_spectral_execute(None, None, None, None) == _lib.INVALID_ARG
