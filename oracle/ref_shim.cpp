@@ -28,10 +28,12 @@ using crd::hesap::Complex;
 namespace
 {
 
+// Never destroyed: plans kept in the caches below deallocate through it, and static destructors at process exit
+// run in an order that could otherwise destroy the allocator first.
 crd::memory::MallocAllocator& alloc()
 {
-    static crd::memory::MallocAllocator a("crdref-shim");
-    return a;
+    static crd::memory::MallocAllocator* a = new crd::memory::MallocAllocator("crdref-shim");
+    return *a;
 }
 
 fft::FftDirection dir_of(int dir)
@@ -300,8 +302,9 @@ int crdref_uneven_f32(std::size_t count, const std::int64_t* sizes, const std::i
         std::map<std::size_t, std::unique_ptr<fft::FftPlan<float>>> pow2;
         std::map<std::size_t, std::unique_ptr<fft::BluesteinPlan<float>>> other;
     };
-    // One cache per range index (ranges are stable for a given count and thread count), kept across calls.
-    static std::map<std::size_t, Cache> caches;
+    // One cache per range index (ranges are stable for a given count and thread count), kept across calls and never
+    // destroyed (its plans would otherwise be freed at exit, after or during the allocator's own teardown).
+    static std::map<std::size_t, Cache>& caches = *new std::map<std::size_t, Cache>();
     const std::size_t nt = threads < 1 ? 1 : (static_cast<std::size_t>(threads) < count ? threads : count);
     for (std::size_t j = 0; j < nt; ++j)
         (void)caches[j]; // created here, on one thread; each range then touches only its own

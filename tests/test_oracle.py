@@ -8,6 +8,8 @@ re-derives the reference's published known-answer digests from them (src/fft_sel
 
 from __future__ import annotations
 
+import os
+
 import numpy as np
 import pytest
 
@@ -142,3 +144,27 @@ def test_reference_library_when_built():
     assert R.crdref_level() in (0, 3, 4)
     for level in (0, 3, 4):
         assert R.crdref_self_check_level(level) == 0
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+def test_reference_shim_exits_cleanly_after_cached_plans():
+    """The shim keeps per-thread plan caches across uneven-batch calls; a process that used them (the bench's CPU
+    baseline) must exit without crashing in static destructors."""
+    import subprocess
+    import sys
+
+    code = (
+        "import sys, ctypes, numpy as np\n"
+        f"sys.path.insert(0, {os.path.dirname(os.path.dirname(os.path.abspath(__file__)))!r})\n"
+        "import oracle\n"
+        "R = oracle.ref()\n"
+        "s = np.array([16, 48, 1024, 1000, 4096, 105], dtype=np.int64)\n"
+        "o = np.concatenate([[0], np.cumsum(s)[:-1]]).astype(np.int64)\n"
+        "d = oracle.lcg_complex64(1, int(s.sum()))\n"
+        "P = ctypes.POINTER(ctypes.c_int64)\n"
+        "for _ in range(2):\n"
+        "    R.crdref_uneven_f32(len(s), s.ctypes.data_as(P), o.ctypes.data_as(P),\n"
+        "                        d.view(np.float32).ctypes.data_as(ctypes.POINTER(ctypes.c_float)), 0, 4)\n"
+        "print('done')\n")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and "done" in r.stdout, (r.returncode, r.stderr[-500:])
