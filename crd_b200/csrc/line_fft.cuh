@@ -374,10 +374,11 @@ __device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
 
 // ---- classic kernel ---------------------------------------------------------------------------------------------
 
-// 16 points a thread: registers for two 512-thread CTAs (or four of 256) an SM.
+// 16 points a thread on lines of 256 points or more: registers for two 512-thread CTAs (or four of 256) an SM
+// (shorter lines keep the compiler's own choice, which used fewer registers).
 template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
-__global__ void __launch_bounds__(kMaxThreads, P <= 16 ? 2 : 0) line_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
-                                                               float2* __restrict__ gout)
+__global__ void __launch_bounds__(kMaxThreads, (P <= 16 && S::n >= 256) ? 2 : 0)
+    line_fft_kernel(const PassDesc d, const float2* __restrict__ gin, float2* __restrict__ gout)
 {
     extern __shared__ float2 sm[];
     __shared__ long long s_in_off[kMaxLinesPerCta];
