@@ -39,6 +39,22 @@ struct RealLineAux
     LineMap smap;
 };
 bool real_line_supported(const PassDesc& d);
+
+// The row pass of a half-length four-step (M = n1 n2 complex points of z[m] = x[2m] + i x[2m+1]) fused with the R2C
+// recombination (real_line.cu): a CTA transforms rows p and n1 - p of the column pass's output, which hold the
+// pairs Z[k], Z[M-k] (k = p + n1 k2), and writes the real input's spectrum X[k], k = 0 .. M, at out + t odist.
+struct RowR2CDesc
+{
+    long long M;      // half length
+    long long odist;  // complex elements between transforms of the output
+    long long batch;  // transforms of this launch
+    int n1, n2;       // column and row lengths of the four-step
+    const void* wn;   // float2 W_{2M}^k, k = 0 .. M
+    float scale;
+};
+bool row_r2c_supported(const PassDesc& row);
+cudaError_t launch_row_r2c(const PassDesc& row, const RowR2CDesc& r, const void* ws, void* out,
+                           cudaStream_t stream);
 cudaError_t launch_real_line(const PassDesc& d, int mode, const RealLineAux& r, const void* in, const void* spec,
                              void* out, cudaStream_t stream);
 // Segment periodograms (spectral.cu): the pass describes the M-point complex lines of one segment (nperseg = 2M).

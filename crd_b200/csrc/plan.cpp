@@ -98,6 +98,7 @@ enum class StepKind : int
     TcLine,
     Conv,
     RealLine,
+    RowR2C,
     Spectral,
     WelchFinish,
     TmaCol,
@@ -122,6 +123,7 @@ struct Step
     int rmode = 0;    // RealLine: kRealR2C, kRealC2R or kRealConv
     RealLineAux raux{};
     SpectralDesc sdesc{}; // Spectral, WelchFinish
+    RowR2CDesc rr{};      // RowR2C
     int sthreads = 0, ssmem = 0;
     int lane = 0;     // 0: the caller's stream; 1, 2: the plan's two internal streams (L2-sized four-step waves)
     RealRecombine real{};
@@ -846,10 +848,16 @@ long long l2_wave_max_transform()
 // A batch of 1-D complex transforms of length n: element j of transform t at base + t*dist + j*stride on each side.
 // Appends the steps of one direction; `ws_off` is where in the workspace this transform's scratch may start; the
 // scratch it needs is returned in *ws_need (complex elements).
+// r2c_wn: the half-length transform of an R2C plan (wn = W_{2n}^k, k = 0 .. n): where the four-step's row pass has a
+// fused form, it also recombines the pairs and writes the n + 1 values of each real transform's spectrum (odist
+// apart); *r2c_fused tells the caller whether it did.
 crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istride, long long idist,
                           long long ostride, long long odist, BufRef src, BufRef dst, bool conj_in, bool conj_out,
-                          float scale, long long ws_off, std::vector<Step>& steps, long long* ws_need)
+                          float scale, long long ws_off, std::vector<Step>& steps, long long* ws_need,
+                          const void* r2c_wn = nullptr, bool* r2c_fused = nullptr)
 {
+    if (r2c_fused != nullptr)
+        *r2c_fused = false;
     *ws_need = 0;
     if (single_pass_ok(n))
     {
@@ -956,6 +964,16 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
                             scale, &s2);
         if (st != CRDFFT_OK)
             return st;
+        if (r2c_wn != nullptr && ostride == 1 && !conj_out && std::getenv("CRDFFT_NO_FUSED_REAL") == nullptr &&
+            row_r2c_supported(s2.pass))
+        {
+            s2.kind = StepKind::RowR2C;
+            s2.rr = RowR2CDesc{n, odist, w, static_cast<int>(n1), static_cast<int>(n2), r2c_wn, scale};
+            if (r2c_fused != nullptr && t0 == 0)
+                *r2c_fused = true;
+        }
+        else if (r2c_fused != nullptr && *r2c_fused)
+            return CRDFFT_UNSUPPORTED_SIZE; // every wave takes the same form
         s2.lane = lane;
         steps.push_back(s2);
     }
@@ -1188,10 +1206,18 @@ crdfft_status build_real(Plan& p)
         const long long odist = d.odist ? d.odist : h + 1;   // complex
         if (idist % 2 != 0)
             return CRDFFT_UNSUPPORTED_SIZE;
+        bool fused = false;
         st = plan_c2c_1d(p, h, d.batch, 1, idist / 2, 1, odist, BufRef{Buf::In, 0}, BufRef{Buf::Out, 0}, false,
-                         false, 1.0f, 0, p.steps[0], &need);
+                         false, 1.0f, 0, p.steps[0], &need, dwn, &fused);
         if (st != CRDFFT_OK)
             return st;
+        if (fused)
+        {
+            p.ws_bytes = static_cast<size_t>(need) * 8;
+            p.algorithm = "real+four-step-fused";
+            p.factors = {h};
+            return CRDFFT_OK;
+        }
         Step post;
         post.kind = StepKind::R2CPost;
         post.real = RealRecombine{h, d.batch, odist, odist, dwn, 1.0f};
@@ -2202,6 +2228,7 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
             case StepKind::WelchFinish: e = launch_welch_finish(s.sdesc, src, dst, stream); break;
             case StepKind::TmaCol: e = launch_tma_col(s.pass, src, dst, stream); break;
             case StepKind::Zero: e = cudaMemsetAsync(dst, 0, static_cast<size_t>(s.count), stream); break;
+            case StepKind::RowR2C: e = launch_row_r2c(s.pass, s.rr, src, dst, stream); break;
             case StepKind::RealLine:
                 if (s.rmode == kRealConv && spec == nullptr)
                     return CRDFFT_INVALID_ARG;

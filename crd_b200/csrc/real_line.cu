@@ -225,6 +225,111 @@ __global__ void __launch_bounds__(kMaxThreads)
     });
 }
 
+// Row pass + R2C recombination. LP pair slots a CTA: slot j takes rows p = p0 + j (low) and (n1 - p) mod n1
+// (high); p runs over 0 .. n1/2 (p = 0 and p = n1/2 pair with themselves). For k = p + n1 k2 the partner is
+// M - k = (n1 - p) + n1 (n2 - 1 - k2) for 0 < p < n1/2; within row 0 it is n1 (n2 - k2), within row n1/2 it is
+// n1/2 + n1 (n2 - 1 - k2). Consecutive threads take consecutive p, so each store is a run of LP elements.
+template <class S, int P, int LP>
+__global__ void __launch_bounds__(kStaticThreads, 2)
+    row_r2c_kernel(const PassDesc d, const RowR2CDesc r, const float2* __restrict__ ws, float2* __restrict__ out)
+{
+    extern __shared__ float2 sm[];
+    constexpr int N2 = S::n;
+    constexpr int T = (N2 + P - 1) / P;
+    const int tid = threadIdx.x;
+    const int pitch = line_pitch(N2);
+    const int half1 = r.n1 / 2;
+    const long long blocks_per_t = (half1 + LP) / LP;
+    const long long t = blockIdx.x / blocks_per_t;
+    const int p0 = static_cast<int>(blockIdx.x - t * blocks_per_t) * LP;
+    const int ll = tid / T;
+    const int jt = tid - ll * T;
+    const int j = ll < LP ? ll : ll - LP;
+    const int pj = p0 + j;
+    const int row = ll < LP ? pj : (r.n1 - pj) % r.n1;
+    Ctx c;
+    c.ok = pj <= half1;
+    c.q = 0;
+    c.in = ws + t * r.M + static_cast<long long>(c.ok ? row : 0) * N2;
+    c.out = nullptr;
+    c.jt = jt;
+    c.T = T;
+    init_scales(d, c);
+    c.in_im = 1.0f;
+    SchedRun<S>::template go<P, true, false, false, Kind<PassMap::Row, false>>(d, c, LayRow<1>{sm + ll * pitch}, N2);
+    // the recombination (every line of the CTA is in shared memory)
+    float2* ot = out + t * r.odist;
+    const float2* wn = static_cast<const float2*>(r.wn);
+    const long long M = r.M;
+    const float s = r.scale;
+    for (int idx = tid; idx < LP * N2; idx += blockDim.x)
+    {
+        const int jj = idx % LP;
+        const int k2 = idx / LP;
+        const int p = p0 + jj;
+        if (p > half1)
+            continue;
+        const LayRow<1> lo{sm + jj * pitch};
+        const LayRow<1> hi{sm + (LP + jj) * pitch};
+        float2 zk, zm;
+        long long k;
+        if (p == 0)
+        {
+            if (2 * k2 > N2)
+                continue;
+            if (k2 == 0)
+            {
+                const float2 z0 = lo.at(0);
+                __stcs(ot, make_float2((z0.x + z0.y) * s, 0.0f));
+                __stcs(ot + M, make_float2((z0.x - z0.y) * s, 0.0f));
+                continue;
+            }
+            k = static_cast<long long>(r.n1) * k2;
+            zk = lo.at(k2);
+            zm = lo.at(N2 - k2);
+        }
+        else if (2 * p == r.n1)
+        {
+            if (2 * k2 > N2 - 1)
+                continue;
+            k = p + static_cast<long long>(r.n1) * k2;
+            zk = lo.at(k2);
+            zm = lo.at(N2 - 1 - k2);
+        }
+        else
+        {
+            k = p + static_cast<long long>(r.n1) * k2;
+            zk = lo.at(k2);
+            zm = hi.at(N2 - 1 - k2);
+        }
+        float2 xk, xm;
+        r2c_pair(zk, zm, __ldg(wn + k), xk, xm);
+        __stcs(ot + k, make_float2(xk.x * s, xk.y * s));
+        if (M - k != k)
+            __stcs(ot + (M - k), make_float2(xm.x * s, xm.y * s));
+    }
+}
+
+using RowR2CFn = void (*)(const PassDesc, const RowR2CDesc, const float2*, float2*);
+
+// The row schedules it has: 512-point rows (2^19 = 1024 x 512, R2C of 2^20) and 1024-point rows.
+RowR2CFn row_r2c_select(const PassDesc& d, int* P, int* LP)
+{
+    if (same_radices(d, {16, 8, 4}))
+    {
+        *P = 32;
+        *LP = 8;
+        return row_r2c_kernel<Sched<16, 8, 4>, 32, 8>;
+    }
+    if (same_radices(d, {16, 16, 4}))
+    {
+        *P = 32;
+        *LP = 4;
+        return row_r2c_kernel<Sched<16, 16, 4>, 32, 4>;
+    }
+    return nullptr;
+}
+
 using RealFn = void (*)(const PassDesc, const float2*, const float2*, const RealLineAux, float2*);
 
 template <int MODE> RealFn real_select(const PassDesc& d, int P)
@@ -267,6 +372,40 @@ bool real_line_supported(const PassDesc& d)
 {
     return d.nstages > 0 && d.n >= 2 && (d.n + 15) / 16 <= lfft::kMaxThreads && d.in.estride == 1 &&
            d.out.estride == 1;
+}
+
+bool row_r2c_supported(const PassDesc& row)
+{
+    int P = 0, LP = 0;
+    return lfft::row_r2c_select(row, &P, &LP) != nullptr;
+}
+
+cudaError_t launch_row_r2c(const PassDesc& row, const RowR2CDesc& r, const void* ws, void* out,
+                           cudaStream_t stream)
+{
+    int P = 0, LP = 0;
+    lfft::RowR2CFn fn = lfft::row_r2c_select(row, &P, &LP);
+    if (fn == nullptr || r.n2 != row.n || r.n1 < 2 || (r.n1 & 1) != 0 || r.M != static_cast<long long>(r.n1) * r.n2)
+        return cudaErrorInvalidConfiguration;
+    const int T = (row.n + P - 1) / P;
+    const int threads = T * 2 * LP;
+    if (threads > lfft::kStaticThreads)
+        return cudaErrorInvalidConfiguration;
+    const int smem = 2 * LP * lfft::line_pitch(row.n) * 8;
+    const long long blocks = r.batch * ((r.n1 / 2 + LP) / LP);
+    if (blocks <= 0)
+        return cudaSuccess;
+    if (blocks > 0x7fffffffLL)
+        return cudaErrorInvalidConfiguration;
+    if (smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    fn<<<static_cast<unsigned>(blocks), threads, smem, stream>>>(row, r, static_cast<const float2*>(ws),
+                                                                 static_cast<float2*>(out));
+    return cudaGetLastError();
 }
 
 cudaError_t launch_real_line(const PassDesc& d, int mode, const RealLineAux& r, const void* in, const void* spec,

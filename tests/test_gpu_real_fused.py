@@ -241,3 +241,28 @@ def test_nd_real_host_execute_matches_device():
     plan.execute_host(hin, hout, cf.FORWARD)
     torch.cuda.synchronize()
     assert np.array_equal(hout.numpy(), dev.cpu().numpy())
+
+
+# ---- R2C of long transforms: the half-length four-step's row pass fused with the recombination -----------------
+
+
+@pytest.mark.parametrize("n,batch,pad", [(1 << 20, 3, 0), (1 << 21, 2, 4), (1 << 20, 5, 3)])
+def test_long_r2c_fused_row_pass(n, batch, pad, monkeypatch):
+    h = n // 2 + 1
+    odist = h + pad
+    x = torch.from_numpy(oracle.lcg_float32(0xF30 ^ n ^ pad, batch * n)).cuda()
+    a = torch.full((batch * odist,), 3 + 3j, dtype=torch.complex64, device="cuda")
+    b = torch.full_like(a, 3 + 3j)
+    plan = cf.Plan([n], batch=batch, kind=cf.R2C, odist=odist)
+    assert plan.info()["algorithm"] == "real+four-step-fused"
+    plan.execute(x, a, cf.FORWARD)
+    monkeypatch.setenv("CRDFFT_NO_FUSED_REAL", "1")
+    ref = cf.Plan([n], batch=batch, kind=cf.R2C, odist=odist)
+    assert ref.info()["algorithm"] == "real+four-step"
+    ref.execute(x, b, cf.FORWARD)
+    torch.cuda.synchronize()
+    got = a.cpu().numpy().reshape(batch, odist)
+    assert np.array_equal(got, b.cpu().numpy().reshape(batch, odist))  # same arithmetic, fused or not
+    want = _spec64(x.cpu().numpy().reshape(batch, n)[[0, -1]])
+    assert oracle.rel_l2(got[[0, -1], :h], want) <= REL_L2
+    assert np.all(got[:, h:] == 3 + 3j)
