@@ -30,17 +30,26 @@ namespace
 constexpr int kUnevenThreads = 256;
 
 // Loads an item's lines into shared memory (row layout, one pad slot per 16), coalesced along whichever side of the
-// global layout is unit-stride; line a starts at base[a].
+// global layout is unit-stride; line a starts at base[a]. Asynchronous 8-byte copies (cp.async): every copy of a
+// thread is in flight at once without holding registers (a batch of loads in registers spilled in this 80-register
+// kernel). The caller waits for them and synchronises; an inverse's conjugation is applied after that
+// (uneven_conj).
 __device__ __forceinline__ void uneven_load(int n, int lines, long long estride, const long long* base,
-                                            const float2* src, float2* sm, int pitch, float in_im, bool l2_only)
+                                            const float2* src, float2* sm, int pitch)
 {
-    // (one element at a time: holding a batch of loads in registers spills in this 80-register kernel, which
-    // measured slower)
     for_tile(n, lines, estride == 1, [&](int a, int e) {
         const float2* p = src + base[a] + static_cast<long long>(e) * estride;
-        float2 x = l2_only ? __ldcg(p) : __ldcs(p);
-        x.y *= in_im;
-        LayRow<1>{sm + a * pitch}.at(e) = x;
+        float2* d = &LayRow<1>{sm + a * pitch}.at(e);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(d)), "l"(p) : "memory");
+    });
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+__device__ __forceinline__ void uneven_conj(int n, int lines, float2* sm, int pitch)
+{
+    for_tile(n, lines, true, [&](int a, int e) {
+        float2& x = LayRow<1>{sm + a * pitch}.at(e);
+        x.y = -x.y;
     });
 }
 
@@ -118,9 +127,13 @@ __global__ void __launch_bounds__(kUnevenThreads, 3)
         // inverse: conjugate on the way into the first pass of each transform and out of the last
         const bool first_pass = it.kind != kUnevenRow;
         const bool last_pass = it.kind != kUnevenCol;
-        uneven_load(n, it.lines, it.in_estride, s_in, src, sm, pitch, first_pass ? in_im : 1.0f,
-                    it.kind == kUnevenRow);
+        uneven_load(n, it.lines, it.in_estride, s_in, src, sm, pitch);
         __syncthreads();
+        if (first_pass && in_im < 0.0f)
+        {
+            uneven_conj(n, it.lines, sm, pitch); // each thread the elements it copied
+            __syncthreads();
+        }
         const int T = (n + 15) / 16;
         const int ll = tid / T;
         const bool ok = ll < it.lines;
