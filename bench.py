@@ -433,8 +433,10 @@ def build_conv(dev, rank, cf):
             plan.execute(rin, H, rout)
             torch.cuda.synchronize()
             x = rin.view((b,) + tuple(dims))[:: max(1, b // 4)].cpu().numpy().astype(np.float64)
-            want = np.fft.irfftn(np.fft.rfftn(x, axes=axes) * H.cpu().numpy().astype(np.complex128), s=dims,
-                                 axes=axes)
+            spec = np.fft.rfftn(x, axes=axes) * H.cpu().numpy().astype(np.complex128)
+            for ax in axes[:-1]:
+                spec = np.fft.ifft(spec, axis=ax)
+            want = _irfft_ref(spec, dims[-1])
             return _rel(rout.view((b,) + tuple(dims))[:: max(1, b // 4)].cpu().numpy(), want)
 
         op = Op(name, rin, rout, lambda i, o, plan=plan, H=H: plan.execute(i, H, o),
@@ -455,6 +457,20 @@ def build_precision(dev, rank, cf):
     (split-BF16: rel-L2 <= 1e-6 against FP64; FP16 with a per-line scale: reported), beside plain FP32."""
     return _build_nd_forms(dev, rank, cf, tuple(PRECISIONS)), \
         dict(WORKLOAD_CONFIGS["precision"])
+
+
+def _irfft_ref(y, n):
+    """The reference's normalised irfft over the last axis (real_fft.hpp:65-92), which the library's C2R follows:
+    numpy's irfft drops the imaginary parts of Y[0] and Y[n/2]; the reference's pair formula keeps them, which adds a
+    constant to the even and to the odd samples."""
+    import numpy as np
+
+    out = np.fft.irfft(y, n, axis=-1)
+    h = n // 2
+    im0, imh = y[..., 0].imag, y[..., h].imag
+    out[..., 0::2] += (-(im0 + imh) / 2 / h)[..., None]
+    out[..., 1::2] += ((im0 - imh) / 2 / h)[..., None]
+    return out
 
 
 WELCH = (64, 1 << 22, 1024, 512)  # signals, samples a signal, nperseg, noverlap

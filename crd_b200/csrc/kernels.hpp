@@ -53,6 +53,7 @@ struct RowR2CDesc
     float scale;
 };
 bool row_r2c_supported(const PassDesc& row);
+
 cudaError_t launch_row_r2c(const PassDesc& row, const RowR2CDesc& r, const void* ws, void* out,
                            cudaStream_t stream);
 cudaError_t launch_real_line(const PassDesc& d, int mode, const RealLineAux& r, const void* in, const void* spec,

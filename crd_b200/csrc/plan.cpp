@@ -1231,6 +1231,8 @@ crdfft_status build_real(Plan& p)
         const long long odist = d.odist ? d.odist : n;       // floats
         if (odist % 2 != 0)
             return CRDFFT_UNSUPPORTED_SIZE;
+        // (A column pass that formed the pairs itself, reading Y directly, measured no faster than this separate
+        // pass followed by the tensor-copy column pass: Y's odd transform distance rules the tensor copies out.)
         Step pre;
         pre.kind = StepKind::C2RPre;
         pre.real = RealRecombine{h, d.batch, odist / 2, idist, dwn, 1.0f};

@@ -11,10 +11,10 @@
 // With W = exp(-2 pi i / n), E = (Z[k] + conj Z[M-k]) / 2 and O = (Z[k] - conj Z[M-k]) / 2i:
 //   X[k] = E + W^k O,   X[M-k] = conj(E - W^k O),   X[0] = Re Z[0] + Im Z[0],   X[M] = Re Z[0] - Im Z[0];
 // and for the inverse, with a = Y[k] + conj Y[M-k], b = Y[k] - conj Y[M-k]:
-//   Q[k] = a + i b W^-k,   Q[M-k] = conj(a) + i conj(b W^-k),   Q[0] = (Y0 + YM) + i (Y0 - YM) on the real parts,
-// so that IFFT_M(Q) (unnormalised) = y[2m] + i y[2m+1] with y the unnormalised inverse real transform. The imaginary
-// parts of Y[0] and Y[M] are ignored, as every C2R does. IFFT(Q) is computed as conj(FFT(conj Q)), which runs the
-// forward stages again.
+//   Q[k] = a + i b W^-k,   Q[M-k] = conj(a) + i conj(b W^-k),
+// so that IFFT_M(Q) (unnormalised) = y[2m] + i y[2m+1] with y the unnormalised inverse real transform. Q[0] pairs
+// Y[0] with Y[M] by the same formula (W^0 = 1), imaginary parts included, as the reference's irfft does
+// (real_fft.hpp:72-84). IFFT(Q) is computed as conj(FFT(conj Q)), which runs the forward stages again.
 
 #include "dyn_stage.cuh"
 #include "kernels.hpp"
@@ -47,14 +47,18 @@ __device__ __forceinline__ void pair_pass(int M, int jt, int T, const float2* __
             }
             else if constexpr (MODE == kRealC2R)
             {
-                const float2 ym = get(M);
-                put(0, make_float2(z0.x + ym.x, z0.x - ym.x));
+                // the pair (0, M) with W^0 = 1, imaginary parts included, as the reference's irfft forms it
+                float2 q0, unused;
+                c2r_pair(z0, get(M), make_float2(1.0f, 0.0f), q0, unused);
+                put(0, q0);
             }
             else
             {
-                const float y0 = (z0.x + z0.y) * __ldg(h).x;
-                const float ym = (z0.x - z0.y) * __ldg(h + static_cast<long long>(M) * hes).x;
-                put(0, make_float2(y0 + ym, y0 - ym));
+                const float2 y0 = cmul(make_float2(z0.x + z0.y, 0.0f), __ldg(h));
+                const float2 ym = cmul(make_float2(z0.x - z0.y, 0.0f), __ldg(h + static_cast<long long>(M) * hes));
+                float2 q0, unused;
+                c2r_pair(y0, ym, make_float2(1.0f, 0.0f), q0, unused);
+                put(0, q0);
             }
             continue;
         }

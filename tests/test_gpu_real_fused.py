@@ -5,8 +5,9 @@
 * The real fused convolution (ConvPlan(real=True)): y = IRFFT(RFFT(x) * H) * scale, 1-D in one launch and 2-D as
   R2C rows, a half-width column convolution and C2R rows; rel-L2 <= 1e-6.
 
-C2R, as every inverse real transform, reads only the real parts of Y[0] and Y[n/2]; numpy's irfft does the same, so
-non-Hermitian test spectra check that too."""
+C2R follows the reference's irfft (real_fft.hpp:65-92), restated by the oracle (oracle.irfft64): Y[0] and Y[n/2] enter
+the pair recombination with their imaginary parts, where numpy's irfft drops them; the test spectra are not Hermitian
+at 0 and n/2, so they check that convention too."""
 
 from __future__ import annotations
 
@@ -39,7 +40,7 @@ def test_r2c_c2r_fused(n):
     assert r2c.info()["algorithm"] == "real-fused" and c2r.info()["algorithm"] == "real-fused"
     spec = torch.empty(batch, n // 2 + 1, dtype=torch.complex64, device="cuda")
     r2c.execute(torch.from_numpy(x).cuda(), spec, cf.FORWARD)
-    # a spectrum that is not Hermitian at 0 and n/2: only their real parts count
+    # a spectrum that is not Hermitian at 0 and n/2
     y = oracle.lcg_complex64(0xF01 ^ n, batch * (n // 2 + 1)).reshape(batch, n // 2 + 1)
     back = torch.empty(batch, n, dtype=torch.float32, device="cuda")
     c2r.execute(torch.from_numpy(y).cuda(), back, cf.INVERSE)
@@ -48,7 +49,7 @@ def test_r2c_c2r_fused(n):
     want = _spec64(x)
     assert oracle.rel_l2(got, want) <= REL_L2
     assert oracle.max_rel(got, want) <= oracle.f32_class(n)
-    want_back = np.fft.irfft(y.astype(np.complex128), n, axis=-1) * n  # unnormalised C2R
+    want_back = oracle.irfft64(y, n) * n  # unnormalised C2R, the reference's convention
     assert oracle.rel_l2(back.cpu().numpy(), want_back) <= REL_L2
 
 
@@ -87,7 +88,7 @@ def test_fused_padded_distances_leave_gaps_alone(n):
                                                                               cf.INVERSE)
     torch.cuda.synchronize()
     gb = back.cpu().numpy().reshape(batch, idist)
-    want_b = np.fft.irfft(y.reshape(batch, odist)[:, :h].astype(np.complex128), n, axis=-1) * n
+    want_b = oracle.irfft64(y.reshape(batch, odist)[:, :h], n) * n
     assert oracle.rel_l2(gb[:, :n], want_b) <= REL_L2
     assert np.all(gb[:, n:] == 9.0)
 
@@ -124,11 +125,17 @@ def test_fused_matches_two_launch_path(monkeypatch):
 # ---- real fused convolution ------------------------------------------------------------------------------------
 
 
+def _irfft_ref(yh, n):
+    """The reference's normalised irfft over the last axis (oracle restatement), any leading shape."""
+    return oracle.irfft64(np.ascontiguousarray(yh), n)
+
+
 def _rconv_want(x, hs, axes_shape, scale):
     if len(axes_shape) == 1:
-        y = np.fft.irfft(np.fft.rfft(x.astype(np.float64), axis=-1) * hs, axes_shape[0], axis=-1)
+        y = _irfft_ref(np.fft.rfft(x.astype(np.float64), axis=-1) * hs, axes_shape[0])
     else:
-        y = np.fft.irfft2(np.fft.rfft2(x.astype(np.float64), axes=(-2, -1)) * hs, s=axes_shape, axes=(-2, -1))
+        spec = np.fft.rfft2(x.astype(np.float64), axes=(-2, -1)) * hs
+        y = _irfft_ref(np.fft.ifft(spec, axis=-2), axes_shape[1])
     return y * np.prod(axes_shape) * scale
 
 
@@ -214,7 +221,11 @@ def test_nd_real_plans(dims):
     torch.cuda.synchronize()
     want = np.fft.rfftn(x.astype(np.float64), axes=axes)
     assert oracle.rel_l2(spec.cpu().numpy(), want) <= REL_L2
-    want_back = np.fft.irfftn(y.astype(np.complex128), s=dims, axes=axes)  # normalised, as numpy's
+    # normalised: the complex axes inverted (FP64), then the reference's irfft along the last axis
+    yc = y.astype(np.complex128)
+    for ax in range(1, len(dims)):
+        yc = np.fft.ifft(yc, axis=ax)
+    want_back = _irfft_ref(yc, dims[-1])
     assert oracle.rel_l2(back.cpu().numpy(), want_back) <= REL_L2
     assert np.array_equal(ty.cpu().numpy(), y)  # C2R leaves its input alone
 
@@ -266,3 +277,22 @@ def test_long_r2c_fused_row_pass(n, batch, pad, monkeypatch):
     want = _spec64(x.cpu().numpy().reshape(batch, n)[[0, -1]])
     assert oracle.rel_l2(got[[0, -1], :h], want) <= REL_L2
     assert np.all(got[:, h:] == 3 + 3j)
+
+
+
+@pytest.mark.parametrize("n,batch,pad,norm", [(1 << 20, 3, 0, 0), (1 << 21, 2, 5, 1)])
+def test_long_c2r_follows_reference_irfft(n, batch, pad, norm):
+    """C2R of long transforms (recombination kernel, then the half-length four-step) against the reference's irfft
+    restated by the oracle, on spectra that are not Hermitian at 0 and n/2; the input is only read."""
+    h = n // 2 + 1
+    idist = h + pad
+    nm = cf.NORM_INVERSE if norm else cf.NORM_NONE
+    y = oracle.lcg_complex64(0xF31 ^ n ^ pad, batch * idist)
+    ty = torch.from_numpy(y).cuda()
+    out = torch.empty(batch * n, dtype=torch.float32, device="cuda")
+    cf.Plan([n], batch=batch, kind=cf.C2R, idist=idist, norm=nm).execute(ty, out, cf.INVERSE)
+    torch.cuda.synchronize()
+    got = out.cpu().numpy().reshape(batch, n)
+    want = oracle.irfft64(y.reshape(batch, idist)[[0, -1], :h], n) * (1 if norm else n)
+    assert oracle.rel_l2(got[[0, -1]], want) <= REL_L2
+    assert np.array_equal(ty.cpu().numpy(), y)
