@@ -3,11 +3,13 @@
     python -m crd_b200.profile_case N BATCH REPS [estimate|measure|learned] [WISDOM_FILE]
     python -m crd_b200.profile_case r2c N BATCH REPS
     python -m crd_b200.profile_case welch|spectrogram NPERSEG NOVERLAP COUNT NSAMPLES REPS
+    python -m crd_b200.profile_case uneven COUNT REPS
 
 The first form creates a forward C2C plan of BATCH transforms of length N (planner mode and optional wisdom as
 given), fills the input with uniform[-1, 1) values and runs REPS out-of-place executes on the current CUDA device.
 The second runs a real-to-complex plan the same way; the third a spectral estimator over COUNT signals of NSAMPLES
-Gaussian samples (periodic Hann window, fs 1).
+Gaussian samples (periodic Hann window, fs 1); the fourth an uneven batch of COUNT transforms with the benchmark's size
+distribution (log-uniform over the 7-smooth lengths in [16, 65536]).
 """
 
 from __future__ import annotations
@@ -31,6 +33,19 @@ def main(argv=None) -> None:
         print(plan.info())
         for _ in range(reps):
             plan.execute(x, y, cf.FORWARD)
+        torch.cuda.synchronize()
+        print("ok")
+        return
+    if argv[0] == "uneven":
+        from crd_b200.workloads import uneven_sizes
+
+        count, reps = int(argv[1]), int(argv[2])
+        plan = cf.UnevenPlan(uneven_sizes(count))
+        x = torch.randn(2 * plan.total, device="cuda").view(torch.complex64)
+        y = torch.empty_like(x)
+        print(plan.info())
+        for _ in range(reps):
+            plan.execute(x, y)
         torch.cuda.synchronize()
         print("ok")
         return
