@@ -1,0 +1,129 @@
+// C++20 host code through include/crdfft.hpp: the crd-hesap-fft class names over the C ABI. Test infrastructure:
+// tests/test_cpp_binding.py compiles it with g++ against libcrdfft.so and runs it.
+//   abi_demo host            device-free paths (status codes, descriptor validation, the spectral segment rule)
+//   abi_demo device IN OUT   FftPlan(4096) forward of the complex64 file IN into OUT, RealFftPlan(4096) rfft of the
+//                            real parts of IN appended to OUT, and a 3-segment Welch PSD of them appended after that
+#include <crdfft.hpp>
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <vector>
+
+namespace
+{
+
+int host_checks()
+{
+    // an invalid descriptor is refused before any device is touched
+    crdfft_desc d{};
+    d.rank = 0;
+    d.batch = 1;
+    try
+    {
+        crdfft::Plan p(d);
+        std::puts("FAIL: rank 0 accepted");
+        return 1;
+    }
+    catch (const crdfft::Error& e)
+    {
+        if (e.status() != CRDFFT_INVALID_DESC)
+        {
+            std::printf("FAIL: status %d\n", static_cast<int>(e.status()));
+            return 1;
+        }
+    }
+    crdfft_spectral_desc s{};
+    s.mode = CRDFFT_SPECTRAL_WELCH;
+    s.detrend = 1;
+    s.nsamples = 512;
+    s.count = 1;
+    s.nperseg = 64;
+    s.noverlap = 0; // Welch reads 0 as nperseg / 2
+    s.fs = 100.0;
+    if (crdfft_spectral_segments(&s) != 15)
+    {
+        std::puts("FAIL: segments");
+        return 1;
+    }
+    std::printf("host ok: %s\n", crdfft_status_string(CRDFFT_OK));
+    return 0;
+}
+
+int device_run(const char* in_path, const char* out_path)
+{
+    constexpr int64_t n = 4096;
+    std::vector<crdfft::cfloat> x(n);
+    {
+        std::ifstream f(in_path, std::ios::binary);
+        f.read(reinterpret_cast<char*>(x.data()), static_cast<std::streamsize>(n * sizeof(crdfft::cfloat)));
+        if (!f)
+            return 2;
+    }
+    std::vector<float> xr(n);
+    for (int64_t i = 0; i < n; ++i)
+        xr[static_cast<size_t>(i)] = x[static_cast<size_t>(i)].real();
+    crdfft::cfloat* dx = nullptr;
+    crdfft::cfloat* ds = nullptr;
+    float* dr = nullptr;
+    float* dp = nullptr;
+    cudaMalloc(&dx, n * sizeof(crdfft::cfloat));
+    cudaMalloc(&ds, (n / 2 + 1) * sizeof(crdfft::cfloat));
+    cudaMalloc(&dr, n * sizeof(float));
+    cudaMalloc(&dp, 33 * sizeof(float));
+    cudaMemcpy(dx, x.data(), n * sizeof(crdfft::cfloat), cudaMemcpyHostToDevice);
+    cudaMemcpy(dr, xr.data(), n * sizeof(float), cudaMemcpyHostToDevice);
+    try
+    {
+        crdfft::FftPlan plan(n);
+        plan.execute(dx, crdfft::Direction::Forward);
+        crdfft::RealFftPlan real(n);
+        real.rfft(dr, ds);
+        crdfft_spectral_desc s{};
+        s.mode = CRDFFT_SPECTRAL_WELCH;
+        s.detrend = 1;
+        s.nsamples = 128;
+        s.count = 1;
+        s.nperseg = 64;
+        s.noverlap = 32;
+        s.fs = 1.0;
+        crdfft::SpectralPlan welch(s);
+        welch.execute(dr, dp);
+    }
+    catch (const crdfft::Error& e)
+    {
+        std::printf("FAIL: %s\n", e.what());
+        return 1;
+    }
+    if (cudaDeviceSynchronize() != cudaSuccess)
+        return 3;
+    std::vector<crdfft::cfloat> y(n), sp(n / 2 + 1);
+    std::vector<float> psd(33);
+    cudaMemcpy(y.data(), dx, n * sizeof(crdfft::cfloat), cudaMemcpyDeviceToHost);
+    cudaMemcpy(sp.data(), ds, (n / 2 + 1) * sizeof(crdfft::cfloat), cudaMemcpyDeviceToHost);
+    cudaMemcpy(psd.data(), dp, 33 * sizeof(float), cudaMemcpyDeviceToHost);
+    std::ofstream o(out_path, std::ios::binary);
+    o.write(reinterpret_cast<const char*>(y.data()), static_cast<std::streamsize>(y.size() * sizeof(crdfft::cfloat)));
+    o.write(reinterpret_cast<const char*>(sp.data()), static_cast<std::streamsize>(sp.size() * sizeof(crdfft::cfloat)));
+    o.write(reinterpret_cast<const char*>(psd.data()), static_cast<std::streamsize>(psd.size() * sizeof(float)));
+    cudaFree(dx);
+    cudaFree(ds);
+    cudaFree(dr);
+    cudaFree(dp);
+    std::puts("device ok");
+    return 0;
+}
+
+} // namespace
+
+int main(int argc, char** argv)
+{
+    if (argc >= 2 && std::strcmp(argv[1], "host") == 0)
+        return host_checks();
+    if (argc >= 4 && std::strcmp(argv[1], "device") == 0)
+        return device_run(argv[2], argv[3]);
+    std::puts("usage: abi_demo host | abi_demo device IN OUT");
+    return 2;
+}
