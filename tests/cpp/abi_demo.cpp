@@ -1,5 +1,5 @@
 // C++20 host code through include/crdfft.hpp: the crd-hesap-fft class names over the C ABI. Test infrastructure:
-// tests/test_cpp_binding.py compiles it with g++ against libcrdfft.so and runs it.
+// tests/test_zz_cpp_binding.py compiles it with g++ against libcrdfft.so and runs it.
 //   abi_demo host            device-free paths (status codes, descriptor validation, the spectral segment rule)
 //   abi_demo device IN OUT   FftPlan(4096) forward of the complex64 file IN into OUT, RealFftPlan(4096) rfft of the
 //                            real parts of IN appended to OUT, and a 3-segment Welch PSD of them appended after that
