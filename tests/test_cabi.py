@@ -101,3 +101,25 @@ def test_spectral_descriptor_and_segment_count_without_device():
     h = ctypes.c_void_p()
     assert L.crdfft_spectral_plan_create(None, ctypes.byref(h)) == _lib.INVALID_ARG
     assert L.crdfft_spectral_execute(None, None, None, None) == _lib.INVALID_ARG
+
+
+def test_wisdom_text_round_trip_without_device():
+    """Wisdom is host state: the committed file imports, exports the same entries, and malformed text is refused
+    without changing what is held."""
+    import crd_b200.hesap as H
+
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "profiles", "wisdom_b200.txt")
+    with open(path) as f:
+        text = f.read()
+    H.wisdom_forget()
+    try:
+        H.wisdom_import(text)
+        back = H.wisdom_export()
+        assert back.splitlines()[0] == "crdfft-wisdom 1"
+        entries = lambda t: sorted(ln.split()[0] for ln in t.splitlines()[1:] if ln.strip())  # noqa: E731
+        assert entries(back) == entries(text)
+        with pytest.raises(_lib.CrdFftError):
+            H.wisdom_import("not wisdom")
+        assert entries(H.wisdom_export()) == entries(text)
+    finally:
+        H.wisdom_forget()
