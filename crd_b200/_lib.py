@@ -54,6 +54,12 @@ EXPORTS = (
     "crdfft_spectral_plan_create",
     "crdfft_spectral_segments",
     "crdfft_spectral_execute",
+    "crdfft_cwt_plan_create",
+    "crdfft_cwt_plan_destroy",
+    "crdfft_cwt_execute",
+    "crdfft_cwt_frequencies",
+    "crdfft_cwt_fft_length",
+    "crdfft_cwt_plan_info",
     "crdfft_plan_info_get",
     "crdfft_workspace_size",
     "crdfft_set_workspace",
@@ -130,6 +136,19 @@ class SpectralDesc(ctypes.Structure):
     ]
 
 
+class CwtDesc(ctypes.Structure):
+    _fields_ = [
+        ("wavelet", ctypes.c_char_p),
+        ("scales", ctypes.POINTER(ctypes.c_double)),
+        ("nsamples", ctypes.c_int64),
+        ("count", ctypes.c_int64),
+        ("nscales", ctypes.c_int64),
+        ("sampling_period", ctypes.c_double),
+        ("precision", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [
         ("algorithm", ctypes.c_char * 64),
@@ -165,6 +184,12 @@ def lib():
         "crdfft_spectral_plan_create": ([ctypes.POINTER(SpectralDesc), pp], i32),
         "crdfft_spectral_segments": ([ctypes.POINTER(SpectralDesc)], i64),
         "crdfft_spectral_execute": ([vp, vp, vp, vp], i32),
+        "crdfft_cwt_plan_create": ([ctypes.POINTER(CwtDesc), pp], i32),
+        "crdfft_cwt_plan_destroy": ([vp], i32),
+        "crdfft_cwt_execute": ([vp, vp, vp, vp], i32),
+        "crdfft_cwt_frequencies": ([ctypes.POINTER(CwtDesc), ctypes.POINTER(ctypes.c_double)], i32),
+        "crdfft_cwt_fft_length": ([ctypes.POINTER(CwtDesc)], i64),
+        "crdfft_cwt_plan_info": ([vp, ctypes.POINTER(i64), ctypes.POINTER(i32)], i32),
         "crdfft_plan_info_get": ([vp, ctypes.POINTER(PlanInfo)], i32),
         "crdfft_workspace_size": ([vp], ctypes.c_size_t),
         "crdfft_set_workspace": ([vp, vp, ctypes.c_size_t], i32),

@@ -151,6 +151,19 @@ void tc_build_a(int prec, std::vector<uint16_t>* out);
 cudaError_t launch_tc_pass(const PassDesc& d, int prec, const void* amat, const void* in, void* out,
                            cudaStream_t stream);
 
+// The continuous wavelet transform's element-wise kernels (cwt.cu). CwtScale: one scale's epilogue parameters.
+struct CwtScale
+{
+    long long off; // (taps - 2) / 2: the first filtered sample a coefficient reads
+    float amp;     // -sqrt(scale)
+    int taps_ok;   // taps >= 2; otherwise the scale's coefficients are 0
+};
+cudaError_t launch_cwt_pad(const float* x, void* X, long long n, long long lfft, long long count, cudaStream_t stream);
+cudaError_t launch_cwt_product(const void* X, const void* K, void* W, long long lfft, long long nscales,
+                               cudaStream_t stream);
+cudaError_t launch_cwt_diff(const void* W, const CwtScale* scales, void* out, long long n, long long lfft,
+                            long long nscales, cudaStream_t stream);
+
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);
 

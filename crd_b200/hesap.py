@@ -28,7 +28,7 @@ import torch
 
 from . import _lib
 from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP32, R2C, SPECTRAL_PERIODOGRAM,
-                   SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError, Desc, SpectralDesc,
+                   SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError, CwtDesc, Desc, SpectralDesc,
                    PlanInfo, check, lib)
 
 Forward = FORWARD
@@ -235,6 +235,95 @@ def periodogram(x: torch.Tensor, fs: float) -> torch.Tensor:
     """dsp::periodogram over the rows of x (spectral.hpp:188-220)."""
     plan = SpectralPlan(SPECTRAL_PERIODOGRAM, x.shape[-1], x.numel() // x.shape[-1], fs)
     return plan.execute(x).reshape(tuple(x.shape[:-1]) + (plan.nfreq,))
+
+
+class CwtPlan:
+    """crd-hesap-wavelet's cwt (cwt.hpp:461-621) on the device over `count` real signals of `nsamples` samples:
+    coefficients (count, nscales, nsamples) complex64, row s of signal c = CwtResult::coeffs[s * n ...] of that
+    signal. wavelet: a pywt-style name ("mexh", "morl", "cmorB-C", "gausP", "cgauP", "shanB-C", "fbspM-B-C",
+    "paulM"; continuous_wavelet, cwt.hpp:300-407). The scales' kernels are built once, at plan time."""
+
+    def __init__(self, nsamples: int, scales, wavelet: str, count: int = 1, sampling_period: float = 1.0,
+                 precision: int = 12):
+        import numpy as np
+
+        self._h = ctypes.c_void_p()
+        self._scales = np.ascontiguousarray(scales, dtype=np.float64).reshape(-1)
+        self._name = str(wavelet).encode()
+        self.nsamples, self.count, self.nscales = int(nsamples), int(count), len(self._scales)
+        self._desc = self._make_desc(sampling_period, precision)
+        freqs = np.empty(self.nscales, dtype=np.float64)
+        check(lib().crdfft_cwt_frequencies(ctypes.byref(self._desc),
+                                           freqs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "cwt_frequencies")
+        self.frequencies = freqs
+        check(lib().crdfft_cwt_plan_create(ctypes.byref(self._desc), ctypes.byref(self._h)), "cwt_plan_create")
+        lfft, fused = ctypes.c_int64(), ctypes.c_int32()
+        check(lib().crdfft_cwt_plan_info(self._h, ctypes.byref(lfft), ctypes.byref(fused)), "cwt_plan_info")
+        self.fft_length, self.fused = int(lfft.value), bool(fused.value)
+
+    def _make_desc(self, sampling_period: float, precision: int) -> CwtDesc:
+        d = CwtDesc()
+        d.wavelet = self._name
+        d.scales = self._scales.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        d.nsamples, d.count, d.nscales = self.nsamples, self.count, self.nscales
+        d.sampling_period, d.precision = float(sampling_period), int(precision)
+        return d
+
+    def execute(self, x: torch.Tensor, out: Optional[torch.Tensor] = None, stream=None) -> torch.Tensor:
+        if x.numel() != self.count * self.nsamples:
+            raise ValueError(f"x holds {x.numel()} samples, the plan {self.count} x {self.nsamples}")
+        if out is None:
+            out = torch.empty((self.count, self.nscales, self.nsamples), dtype=torch.complex64, device=x.device)
+        if out.numel() != self.count * self.nscales * self.nsamples:
+            raise ValueError("out must hold count x nscales x nsamples values")
+        check(lib().crdfft_cwt_execute(self._h, _ptr(x, torch.float32, "x"), _ptr(out, torch.complex64, "out"),
+                                       _stream(stream)), "cwt_execute")
+        return out
+
+    def __del__(self):
+        try:
+            if self._h.value:
+                lib().crdfft_cwt_plan_destroy(self._h)
+                self._h = ctypes.c_void_p()
+        except Exception:
+            pass
+
+
+def cwt(x: torch.Tensor, scales, wavelet: str, sampling_period: float = 1.0, precision: int = 12):
+    """wavelet::cwt over the rows of x (a 1-D tensor is one signal): (coefficients (..., nscales, n) complex64 on
+    x's device, frequencies (nscales,) float64), the reference's CwtResult (cwt.hpp:446-456, 616-621)."""
+    n = x.shape[-1]
+    plan = CwtPlan(n, scales, wavelet, x.numel() // n, sampling_period, precision)
+    out = plan.execute(x.contiguous())
+    return out.reshape(tuple(x.shape[:-1]) + (plan.nscales, n)), plan.frequencies
+
+
+def cwt_fft_length(nsamples: int, scales, wavelet: str, precision: int = 12) -> int:
+    """The FFT length a CWT plan uses (no device needed): the power of two >= n + the longest kernel."""
+    import numpy as np
+
+    sc = np.ascontiguousarray(scales, dtype=np.float64).reshape(-1)
+    d = CwtDesc()
+    d.wavelet = str(wavelet).encode()
+    d.scales = sc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    d.nsamples, d.count, d.nscales, d.precision = int(nsamples), 1, len(sc), int(precision)
+    return int(lib().crdfft_cwt_fft_length(ctypes.byref(d)))
+
+
+def cwt_frequencies(scales, wavelet: str, sampling_period: float = 1.0, precision: int = 12):
+    """CwtResult::frequencies without a device: central_frequency / (scale * sampling_period) (cwt.hpp:410-444)."""
+    import numpy as np
+
+    sc = np.ascontiguousarray(scales, dtype=np.float64).reshape(-1)
+    d = CwtDesc()
+    d.wavelet = str(wavelet).encode()
+    d.scales = sc.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    d.nsamples, d.count, d.nscales = 1, 1, len(sc)
+    d.sampling_period, d.precision = float(sampling_period), int(precision)
+    out = np.empty(len(sc), dtype=np.float64)
+    check(lib().crdfft_cwt_frequencies(ctypes.byref(d), out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+          "cwt_frequencies")
+    return out
 
 
 class FftPlan(_Handle):

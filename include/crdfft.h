@@ -225,6 +225,43 @@ int64_t crdfft_spectral_segments(const crdfft_spectral_desc* desc);
 /* x: count x nsamples floats on the device; out as above. crdfft_execute rejects spectral plans. */
 crdfft_status crdfft_spectral_execute(crdfft_plan* plan, const float* x, float* out, void* stream);
 
+/* ---- Continuous wavelet transform ------------------------------------------------------------------------- */
+
+/* crd-hesap-wavelet's cwt (engine/numerics/hesap-wavelet/include/crd/hesap/wavelet/cwt.hpp:461-621) over `count`
+ * real signals of nsamples samples. The plan builds the wavelet's integral and each scale's kernel in FP64 on the
+ * host (sample_psi, cwt.hpp:149-280; the kernels at cwt.hpp:569-581) and keeps the kernels on the device; an execute
+ * zero-pads and transforms the signals, convolves every scale's kernel with each signal's spectrum in one fused
+ * launch (FFT x spectrum x inverse FFT; a spectrum product and an inverse FFT plan where the FFT length is beyond the
+ * fused kernel) and forms -sqrt(a) (w[t+1] - w[t]) / lfft (cwt.hpp:589-596). */
+typedef struct crdfft_cwt_desc
+{
+    const char* wavelet;    /* "mexh", "morl", "cmorB-C", "gausP", "cgauP", "shanB-C", "fbspM-B-C", "paulM"
+                             * (continuous_wavelet, cwt.hpp:300-407); a name matching none is "mexh", as there */
+    const double* scales;   /* host memory: nscales scales > 0 */
+    int64_t nsamples;       /* n >= 1 */
+    int64_t count;          /* signals >= 1 */
+    int64_t nscales;        /* 1 .. 65535 */
+    double sampling_period; /* for the frequencies only; 0 = 1 */
+    int32_t precision;      /* log2 of the wavelet grid, 1 .. 20; 0 = 12 (the reference's default) */
+    int32_t reserved;       /* 0 */
+} crdfft_cwt_desc;
+
+typedef struct crdfft_cwt_plan crdfft_cwt_plan;
+
+crdfft_status crdfft_cwt_plan_create(const crdfft_cwt_desc* desc, crdfft_cwt_plan** plan);
+crdfft_status crdfft_cwt_plan_destroy(crdfft_cwt_plan* plan);
+/* x: count x nsamples floats on the device; coeffs: count x nscales x nsamples complex values on the device, signal
+ * c's CwtResult::coeffs[s * n + i] (cwt.hpp:446-456) at coeffs[(c * nscales + s) * n + i]. Stream-ordered; the plan's
+ * scratch serves one execute at a time. */
+crdfft_status crdfft_cwt_execute(crdfft_cwt_plan* plan, const float* x, void* coeffs, void* stream);
+/* Host only, no device: CwtResult::frequencies, central_frequency / (scale * sampling_period) (cwt.hpp:410-444). */
+crdfft_status crdfft_cwt_frequencies(const crdfft_cwt_desc* desc, double* frequencies);
+/* Host only, no device: the FFT length, the power of two >= n + the longest kernel (cwt.hpp:479-506); -1 for an
+ * invalid descriptor. */
+int64_t crdfft_cwt_fft_length(const crdfft_cwt_desc* desc);
+/* The plan's FFT length and whether it runs the fused convolution (1) or the spectrum product + inverse FFT (0). */
+crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int32_t* fused);
+
 /* ---- Uneven batches ---------------------------------------------------------------------------------------- */
 
 /* `count` independent forward/inverse complex transforms of different lengths (7-smooth, 2 .. 8192^2), transform t
