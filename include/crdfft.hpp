@@ -223,6 +223,51 @@ private:
     Handle m_h;
 };
 
+// hesap-wavelet's cwt on the device (crdfft_cwt_plan_create): count x nscales x nsamples complex coefficients.
+class CwtPlan
+{
+public:
+    CwtPlan(const char* wavelet, std::span<const double> scales, int64_t nsamples, int64_t count = 1,
+            int32_t precision = 12)
+    {
+        crdfft_cwt_desc d{};
+        d.wavelet = wavelet;
+        d.scales = scales.data();
+        d.nsamples = nsamples;
+        d.count = count;
+        d.nscales = static_cast<int64_t>(scales.size());
+        d.precision = precision;
+        check(crdfft_cwt_plan_create(&d, &m_p), "CwtPlan");
+    }
+    CwtPlan(CwtPlan&& o) noexcept : m_p(std::exchange(o.m_p, nullptr)) {}
+    CwtPlan& operator=(CwtPlan&& o) noexcept
+    {
+        if (this != &o)
+        {
+            crdfft_cwt_plan_destroy(m_p);
+            m_p = std::exchange(o.m_p, nullptr);
+        }
+        return *this;
+    }
+    CwtPlan(const CwtPlan&) = delete;
+    CwtPlan& operator=(const CwtPlan&) = delete;
+    ~CwtPlan() { crdfft_cwt_plan_destroy(m_p); }
+
+    void execute(const float* device_x, cfloat* device_coeffs, void* stream = nullptr) const
+    {
+        check(crdfft_cwt_execute(m_p, device_x, device_coeffs, stream), "cwt_execute");
+    }
+    int64_t fft_length() const
+    {
+        int64_t n = 0;
+        check(crdfft_cwt_plan_info(m_p, &n, nullptr), "cwt_plan_info");
+        return n;
+    }
+
+private:
+    crdfft_cwt_plan* m_p = nullptr;
+};
+
 // One-shot helpers (fft.hpp:1006-1029).
 inline void fft(cfloat* device_data, int64_t n, Direction dir, void* stream = nullptr)
 {

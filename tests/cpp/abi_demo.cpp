@@ -48,6 +48,34 @@ int host_checks()
         std::puts("FAIL: segments");
         return 1;
     }
+    // the CWT's FFT length (the morl kernel at scale 16 has 257 taps) and a negative scale refused without a device
+    const double scales[2] = {1.0, 16.0};
+    crdfft_cwt_desc c{};
+    c.wavelet = "morl";
+    c.scales = scales;
+    c.nsamples = 100;
+    c.count = 1;
+    c.nscales = 2;
+    if (crdfft_cwt_fft_length(&c) != 512)
+    {
+        std::puts("FAIL: cwt fft length");
+        return 1;
+    }
+    const double bad[2] = {1.0, -2.0};
+    try
+    {
+        crdfft::CwtPlan p("morl", std::span<const double>(bad, 2), 100);
+        std::puts("FAIL: negative scale accepted");
+        return 1;
+    }
+    catch (const crdfft::Error& e)
+    {
+        if (e.status() != CRDFFT_INVALID_DESC)
+        {
+            std::printf("FAIL: cwt status %d\n", static_cast<int>(e.status()));
+            return 1;
+        }
+    }
     std::printf("host ok: %s\n", crdfft_status_string(CRDFFT_OK));
     return 0;
 }
