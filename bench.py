@@ -130,7 +130,7 @@ class ClockSampler:
 # one), its algorithmic HBM bytes, the number of kernel launches it issues, and a check that returns the rel-L2 of
 # its output against numpy's float64 FFT on a sample.
 
-WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision", "conv", "welch")
+WORKLOADS = ("mixed", "n1024", "r2c", "uneven", "nd", "precision", "conv", "welch", "cwt")
 
 
 WORKLOAD_CONFIGS = {
@@ -150,6 +150,9 @@ WORKLOAD_CONFIGS = {
              "flops": "complex: 10 N log2 N + 6 N per signal; real: 5 N log2 N + 3 N per signal"},
     "welch": {"workload": "welch_spectrogram_64_signals_2^22_samples_nperseg1024_noverlap512_hann",
               "l2": "1 GiB of float input (> 126 MB L2)", "flops": "2.5 N log2 N per segment (its real FFT)"},
+    "cwt": {"workload": "cwt_morl_64_signals_4096_samples_64_scales_1_to_128",
+            "l2": "128 MiB of coefficients written per step (> 126 MB L2)",
+            "flops": "the reference's steps: per signal 5 L log2 L + nscales (10 L log2 L + 6 L), L = 8192 (FFT length)"},
     "precision": {"workload": "nd_c2c_4096x4096_512x512x512_fp32_splitbf16_fp16", "inputs": "uniform[-1,1) + 1% x 1e4",
                   "l2": "2-D input rotates over 4 buffers (512 MiB); 3-D input 1 GiB"},
 }
@@ -532,8 +535,74 @@ def build_welch(dev, rank, cf):
     return ops, dict(WORKLOAD_CONFIGS["welch"])
 
 
+CWT = (64, 4096, 64, 128.0)  # signals, samples a signal, scales, largest scale (geometric from 1)
+
+
+def _cwt64_morl(x, scales):
+    """FP64 CWT of the rows of x with the real Morlet wavelet on 2^12 grid points over [-8, 8]: the integrated
+    wavelet sampled at floor(m / (a step)) and reversed, convolved with the signal through a zero-padded FFT,
+    -sqrt(a) (w[t+1] - w[t]) at t = (taps - 2) / 2 + i. The result check."""
+    import numpy as np
+
+    grid = 1 << 12
+    step = 16.0 / (grid - 1)
+    t = -8.0 + np.arange(grid) * step
+    ipsi = np.cumsum(np.exp(-t * t / 2) * np.cos(5 * t)) * step
+    n = x.shape[-1]
+    taps = []
+    for a in scales:
+        kk = 0
+        for m in range(int(math.ceil(a * 16.0 + 1.0))):
+            if int(m / (a * step)) >= grid:
+                break
+            kk += 1
+        taps.append(kk)
+    L = 1
+    while L < n + max(taps):
+        L <<= 1
+    X = np.fft.fft(x, L, axis=-1)
+    out = np.zeros(x.shape[:-1] + (len(scales), n), dtype=np.complex128)
+    for s, (a, kk) in enumerate(zip(scales, taps)):
+        m = kk - 1 - np.arange(kk)
+        kb = np.zeros(L)
+        kb[:kk] = ipsi[(m / (a * step)).astype(np.int64)]
+        w = np.fft.ifft(X * np.fft.fft(kb), axis=-1)
+        i = (kk - 2) // 2 + np.arange(n)
+        out[..., s, :] = -math.sqrt(a) * (w[..., i + 1] - w[..., i])
+    return out
+
+
+def build_cwt(dev, rank, cf):
+    """hesap-wavelet's cwt on the device: 64 signals of 4096 samples, 64 scales from 1 to 128, real Morlet (FFT
+    length 8192): one batched forward FFT, then per signal one fused convolution launch over the 64 scales' kernels and
+    the difference epilogue."""
+    import numpy as np
+    import torch
+
+    count, n, ns, top = CWT
+    scales = np.geomspace(1.0, top, ns)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(SEED + 31 + rank)
+    x = torch.randn(count * n, generator=gen, device=dev, dtype=torch.float32)
+    plan = cf.CwtPlan(n, scales, "morl", count)
+    out = torch.empty((count, ns, n), dtype=torch.complex64, device=dev)
+    L = plan.fft_length
+    fl = count * (5.0 * L * math.log2(L) + ns * (10.0 * L * math.log2(L) + 6.0 * L))
+    launches = 1 + cf.Plan([L], batch=count).info()["passes"] + count * (2 if plan.fused else 3)
+
+    def check():
+        plan.execute(x, out)
+        torch.cuda.synchronize()
+        xs = x.view(count, n)[:2].cpu().numpy().astype(np.float64)
+        return _rel(out[:2].cpu().numpy(), _cwt64_morl(xs, scales))
+
+    op = Op("cwt", x, out, lambda i, o: plan.execute(i, o), fl, 4 * count * n + 8 * count * ns * n, launches, check,
+            {"signals": count, "scales": ns, "fft_length": L, "fused": plan.fused})
+    return [op], dict(WORKLOAD_CONFIGS["cwt"])
+
+
 BUILDERS = {"mixed": build_mixed, "n1024": build_n1024, "r2c": build_r2c, "uneven": build_uneven, "nd": build_nd,
-            "precision": build_precision, "conv": build_conv, "welch": build_welch}
+            "precision": build_precision, "conv": build_conv, "welch": build_welch, "cwt": build_cwt}
 
 
 # ---- the reference's CPU implementation (reference arm and cpu_baseline) -------------------------------------------
@@ -663,6 +732,25 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
 
         timed(wrun, cnt * nseg * 2.5 * nper * math.log2(nper), "welch")
         sample.append(f"welch {cnt} signals x {ns} samples, nperseg {nper}, noverlap {nov}")
+    elif workload == "cwt":
+        # the reference's wavelet::cwt<float> over the signals, one signal at a time per thread
+        count, n, ns, top = CWT
+        scales = np.geomspace(1.0, top, ns).astype(np.float32)
+        cnt = max(threads, 1) if count > threads else count
+        x = oracle.lcg_float32(SEED ^ 0xC3, cnt * n)
+        out = np.empty(cnt * ns * n * 2, dtype=np.float32)
+        freqs = np.empty(ns)
+        L = 8192
+        fl = cnt * (5.0 * L * math.log2(L) + ns * (10.0 * L * math.log2(L) + 6.0 * L))
+
+        def crun():
+            if R.crdref_cwt_f32(n, cnt, x.ctypes.data_as(fp), scales.ctypes.data_as(fp), ns, b"morl",
+                                out.ctypes.data_as(fp), freqs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                threads) != 0:
+                raise RuntimeError("crdref_cwt_f32 failed")
+
+        timed(crun, fl, "cwt")
+        sample.append(f"cwt<float> morl {cnt} signals x {n} samples, {ns} scales")
     elif workload == "r2c":
         n = 1 << 20
         count = max(threads, min(512, budget_bytes // (4 * n)))

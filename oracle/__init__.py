@@ -247,10 +247,11 @@ def ref():
         R.crdref_welch_f64.argtypes = [_sz, _sz, _dp, ctypes.c_double, _sz, _sz, _dp, ctypes.c_int]
         R.crdref_spectrogram_f64.argtypes = [_sz, _sz, _dp, ctypes.c_double, _sz, _sz, _dp, ctypes.c_int]
         R.crdref_periodogram_f64.argtypes = [_sz, _sz, _dp, ctypes.c_double, _dp, ctypes.c_int]
+        R.crdref_cwt_f32.argtypes = [_sz, _sz, _fp, _fp, _sz, ctypes.c_char_p, _fp, _dp, ctypes.c_int]
         for f in ("crdref_c2c_f32", "crdref_c2c_f64", "crdref_execute_reference_f32", "crdref_execute_reference_f64",
                   "crdref_execute_batched_f32", "crdref_stockham_f32", "crdref_rfft_f32", "crdref_irfft_f32",
                   "crdref_nd_f32", "crdref_nd_f64", "crdref_uneven_f32", "crdref_welch_f32", "crdref_welch_f64",
-                  "crdref_spectrogram_f64", "crdref_periodogram_f64"):
+                  "crdref_spectrogram_f64", "crdref_periodogram_f64", "crdref_cwt_f32"):
             getattr(R, f).restype = ctypes.c_int
         _ref = R
     return _ref
@@ -266,6 +267,20 @@ def ref_welch(x, fs: float, nperseg: int, noverlap: int, f32: bool = False, thre
     if getattr(ref(), fn)(n, a.size // n, ptr(a), fs, nperseg, noverlap, ptr(out), threads) != 0:
         raise RuntimeError(f"{fn} failed")
     return out
+
+
+def ref_cwt(x, scales, wavelet: str, threads: int = 1):
+    """The reference's wavelet::cwt<float> over the rows of x (cwt.hpp:616-621): (coefficients rows x nscales x n
+    complex64, frequencies)."""
+    a = np.ascontiguousarray(x, dtype=np.float32)
+    sc = np.ascontiguousarray(scales, dtype=np.float32).reshape(-1)
+    n = a.shape[-1]
+    out = np.zeros(a.shape[:-1] + (len(sc), n), dtype=np.complex64)
+    freqs = np.zeros(len(sc))
+    if ref().crdref_cwt_f32(n, a.size // n, _ptr_f(a), _ptr_f(sc), len(sc), wavelet.encode(),
+                            out.ctypes.data_as(_fp), _ptr_d(freqs), threads) != 0:
+        raise RuntimeError("crdref_cwt_f32 failed")
+    return out, freqs
 
 
 def ref_spectrogram(x, fs: float, nperseg: int, noverlap: int, threads: int = 1) -> np.ndarray:

@@ -12,6 +12,7 @@
 #include <crd/hesap/fft/fft_dispatch.hpp>
 #include <crd/hesap/fft/nd_fft.hpp>
 #include <crd/hesap/fft/real_fft.hpp>
+#include <crd/hesap/wavelet/cwt.hpp>
 #include <crd/memory/allocators/malloc_allocator.hpp>
 
 #include <cstddef>
@@ -419,6 +420,35 @@ int crdref_periodogram_f64(std::size_t n, std::size_t count, const double* x, do
     return spectral_rows<double>(n, count, x, out, n / 2 + 1, threads,
                                  [&](cont::ConstSpan<double> s)
                                  { return crd::hesap::dsp::periodogram<double>(&alloc(), s, fs); });
+}
+
+// hesap-wavelet's cwt<float> (cwt.hpp:616-621) over `count` signals of `n` samples, one signal at a time per thread
+// (contiguous ranges, as above): out = count x nscales x n interleaved complex values, freqs = nscales values.
+int crdref_cwt_f32(std::size_t n, std::size_t count, const float* x, const float* scales, std::size_t nscales,
+                   const char* wavelet, float* out, double* freqs, int threads)
+{
+    if (n == 0 || nscales == 0 || wavelet == nullptr)
+        return -1;
+    const auto w = crd::hesap::wavelet::continuous_wavelet(wavelet);
+    fan_out(threads, count,
+            [&](std::size_t first, std::size_t last)
+            {
+                for (std::size_t g = first; g < last; ++g)
+                {
+                    const auto r = crd::hesap::wavelet::cwt<float>(&alloc(), cont::ConstSpan<float>(x + g * n, n),
+                                                                   cont::ConstSpan<float>(scales, nscales), w);
+                    float* o = out + g * nscales * n * 2;
+                    for (std::size_t k = 0; k < nscales * n; ++k)
+                    {
+                        o[2 * k] = r.coeffs[k].re;
+                        o[2 * k + 1] = r.coeffs[k].im;
+                    }
+                    if (g == 0 && freqs != nullptr)
+                        for (std::size_t s = 0; s < nscales; ++s)
+                            freqs[s] = r.frequencies[s];
+                }
+            });
+    return 0;
 }
 
 } // extern "C"
