@@ -5,14 +5,14 @@
 // cwt.hpp:149-280), its cumulative integral (conjugated for complex wavelets, cwt.hpp:470-477), each scale's tap
 // count (cwt.hpp:479-501), the FFT length lfft (the power of two >= n + the longest kernel, cwt.hpp:502-506), and
 // each scale's kernel: the integral sampled at floor(m / (a step)) and reversed, narrowed to FP32
-// (cwt.hpp:569-581). The kernels do not depend on the signal, so the device holds them for every execute.
+// (cwt.hpp:569-581). The kernels do not depend on the signal, so their spectra are computed once, on the device, and
+// kept for every execute (the reference transforms each kernel again on every call, cwt.hpp:582).
 //
-// Execute, all on the caller's stream: the signals zero-padded to lfft (cwt.cu) and transformed in one batched
-// FFT plan; then for each signal the fused convolution (conv.cu) of the nscales kernels with that signal's spectrum,
-// forward FFT x spectrum x unnormalised inverse in one launch (the reference's per-scale forward FFT, product and
-// inverse, cwt.hpp:582-588), and the epilogue -sqrt(a) (w[t+1] - w[t]) / lfft (cwt.cu, cwt.hpp:589-596). For FFT
-// lengths the fused convolution does not take, the kernels' spectra are computed once at plan time and each execute
-// runs the spectrum product (cwt.cu) and a batched inverse FFT plan instead.
+// Execute, all on the caller's stream: the signals zero-padded to lfft (cwt.cu) and transformed in one batched FFT
+// plan; then, over chunks of signals, the product of every signal's spectrum with every kernel spectrum as one grid
+// of (signal, scale) lines (cwt.cu, cwt.hpp:583-587), one batched unnormalised inverse FFT over those lines, and the
+// epilogue -sqrt(a) (w[t+1] - w[t]) / lfft (cwt.cu, cwt.hpp:589-596). A chunk's lines fill the GPU in each launch,
+// where a launch per signal would give one CTA per scale.
 #include "../../include/crdfft.h"
 #include "kernels.hpp"
 
@@ -29,21 +29,21 @@ struct crdfft_cwt_plan
 {
     int device = -1;
     long long n = 0, count = 0, nscales = 0, lfft = 0;
-    bool fused = false;
-    crdfft_plan* forward = nullptr; // the signals' FFTs (batch count, in place on X)
-    crdfft_plan* conv = nullptr;    // fused: the kernels convolved with one signal's spectrum (batch nscales)
-    crdfft_plan* inverse = nullptr; // otherwise: inverse FFTs of the spectrum products (batch nscales, in place on W)
-    void* kernels = nullptr;        // nscales x lfft complex: the reversed kernels (fused) or their spectra
-    void* X = nullptr;              // count x lfft complex: the signals' spectra
-    void* W = nullptr;              // nscales x lfft complex: one signal's filtered sequences
+    long long chunk = 0;                 // signals a product / inverse FFT / epilogue round takes
+    crdfft_plan* forward = nullptr;      // the signals' FFTs (batch count, in place on X)
+    crdfft_plan* inverse = nullptr;      // chunk x nscales inverse FFTs, in place on W
+    crdfft_plan* inverse_tail = nullptr; // (count mod chunk) x nscales, when the last chunk is shorter
+    void* spectra = nullptr;             // nscales x lfft complex: the kernels' spectra
+    void* X = nullptr;                   // count x lfft complex: the signals' spectra
+    void* W = nullptr;                   // chunk x nscales x lfft complex: the filtered sequences
     crdfft::CwtScale* scales = nullptr;
 
     ~crdfft_cwt_plan()
     {
-        for (crdfft_plan* p : {forward, conv, inverse})
+        for (crdfft_plan* p : {forward, inverse, inverse_tail})
             if (p != nullptr)
                 crdfft_plan_destroy(p);
-        for (void* b : {kernels, X, W, static_cast<void*>(scales)})
+        for (void* b : {spectra, X, W, static_cast<void*>(scales)})
             if (b != nullptr)
                 cudaFree(b);
     }
@@ -415,16 +415,21 @@ crdfft_status build(const crdfft_cwt_desc* d, const Geometry& g, crdfft_cwt_plan
         }
     }
 
-    const size_t kbytes = static_cast<size_t>(ns * lfft) * 8;
-    if (cudaMalloc(&p->kernels, kbytes) != cudaSuccess || cudaMalloc(&p->W, kbytes) != cudaSuccess ||
-        cudaMalloc(&p->X, static_cast<size_t>(d->count * lfft) * 8) != cudaSuccess ||
+    // signals a round: the filtered sequences within 512 MiB, the grid rows (signal x scale lines) within 65535
+    const long long line_bytes = lfft * 8;
+    p->chunk = std::max<long long>(
+        1, std::min<long long>({static_cast<long long>(d->count), (512LL << 20) / (ns * line_bytes), 65535 / ns}));
+    const size_t kbytes = static_cast<size_t>(ns * line_bytes);
+    if (cudaMalloc(&p->spectra, kbytes) != cudaSuccess ||
+        cudaMalloc(&p->W, static_cast<size_t>(p->chunk) * kbytes) != cudaSuccess ||
+        cudaMalloc(&p->X, static_cast<size_t>(d->count * line_bytes)) != cudaSuccess ||
         cudaMalloc(reinterpret_cast<void**>(&p->scales), sizeof(crdfft::CwtScale) * static_cast<size_t>(ns)) !=
             cudaSuccess)
     {
         cudaGetLastError();
         return CRDFFT_OOM;
     }
-    if (cudaMemcpy(p->kernels, table.data(), kbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
+    if (cudaMemcpy(p->spectra, table.data(), kbytes, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(p->scales, sc.data(), sizeof(crdfft::CwtScale) * static_cast<size_t>(ns),
                    cudaMemcpyHostToDevice) != cudaSuccess)
         return CRDFFT_LAUNCH;
@@ -433,26 +438,30 @@ crdfft_status build(const crdfft_cwt_desc* d, const Geometry& g, crdfft_cwt_plan
     crdfft_status st = crdfft_plan_create(&fd, &p->forward);
     if (st != CRDFFT_OK)
         return st;
+    // the kernels' spectra, once: a forward plan over the table in place
     crdfft_desc kd = line_desc(lfft, ns);
-    if (crdfft_conv_plan_create(&kd, 0, 1.0, &p->conv) == CRDFFT_OK)
-    {
-        p->fused = true;
-        return CRDFFT_OK;
-    }
-    p->conv = nullptr;
-    // the kernels' spectra, once: a forward plan over the table in place, then the inverse plan of each execute
     crdfft_plan* kf = nullptr;
     st = crdfft_plan_create(&kd, &kf);
     if (st != CRDFFT_OK)
         return st;
-    st = crdfft_execute(kf, p->kernels, p->kernels, CRDFFT_FORWARD, nullptr);
+    st = crdfft_execute(kf, p->spectra, p->spectra, CRDFFT_FORWARD, nullptr);
     const cudaError_t e = cudaStreamSynchronize(nullptr);
     crdfft_plan_destroy(kf);
     if (st != CRDFFT_OK)
         return st;
     if (e != cudaSuccess)
         return CRDFFT_LAUNCH;
-    return crdfft_plan_create(&kd, &p->inverse);
+    crdfft_desc id = line_desc(lfft, p->chunk * ns);
+    st = crdfft_plan_create(&id, &p->inverse);
+    if (st != CRDFFT_OK)
+        return st;
+    const long long tail = d->count % p->chunk;
+    if (tail != 0)
+    {
+        crdfft_desc td = line_desc(lfft, tail * ns);
+        st = crdfft_plan_create(&td, &p->inverse_tail);
+    }
+    return st;
 }
 
 } // namespace
@@ -508,19 +517,17 @@ crdfft_status crdfft_cwt_execute(crdfft_cwt_plan* plan, const float* x, void* co
     crdfft_status st = crdfft_execute(p.forward, p.X, p.X, CRDFFT_FORWARD, stream);
     if (st != CRDFFT_OK)
         return st;
-    for (long long c = 0; c < p.count; ++c)
+    for (long long c0 = 0; c0 < p.count; c0 += p.chunk)
     {
-        const void* spec = static_cast<const char*>(p.X) + static_cast<size_t>(c * p.lfft) * 8;
-        if (p.fused)
-            st = crdfft_conv_execute(p.conv, p.kernels, spec, p.W, stream);
-        else if (crdfft::launch_cwt_product(spec, p.kernels, p.W, p.lfft, p.nscales, s) != cudaSuccess)
-            st = CRDFFT_LAUNCH;
-        else
-            st = crdfft_execute(p.inverse, p.W, p.W, CRDFFT_INVERSE, stream);
+        const long long cc = std::min(p.chunk, p.count - c0);
+        const void* spec = static_cast<const char*>(p.X) + static_cast<size_t>(c0 * p.lfft) * 8;
+        if (crdfft::launch_cwt_product(spec, p.spectra, p.W, p.lfft, p.nscales, cc, s) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        st = crdfft_execute(cc == p.chunk ? p.inverse : p.inverse_tail, p.W, p.W, CRDFFT_INVERSE, stream);
         if (st != CRDFFT_OK)
             return st;
-        void* out = static_cast<char*>(coeffs) + static_cast<size_t>(c * p.nscales * p.n) * 8;
-        if (crdfft::launch_cwt_diff(p.W, p.scales, out, p.n, p.lfft, p.nscales, s) != cudaSuccess)
+        void* out = static_cast<char*>(coeffs) + static_cast<size_t>(c0 * p.nscales * p.n) * 8;
+        if (crdfft::launch_cwt_diff(p.W, p.scales, out, p.n, p.lfft, p.nscales, cc, s) != cudaSuccess)
             return CRDFFT_LAUNCH;
     }
     return CRDFFT_OK;
@@ -547,14 +554,14 @@ int64_t crdfft_cwt_fft_length(const crdfft_cwt_desc* desc)
     return geometry(desc, &g) == CRDFFT_OK ? g.lfft : -1;
 }
 
-crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int32_t* fused)
+crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int64_t* signals_per_round)
 {
     if (plan == nullptr)
         return CRDFFT_INVALID_ARG;
     if (fft_length != nullptr)
         *fft_length = plan->lfft;
-    if (fused != nullptr)
-        *fused = plan->fused ? 1 : 0;
+    if (signals_per_round != nullptr)
+        *signals_per_round = plan->chunk;
     return CRDFFT_OK;
 }
 

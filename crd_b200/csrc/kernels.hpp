@@ -159,10 +159,12 @@ struct CwtScale
     int taps_ok;   // taps >= 2; otherwise the scale's coefficients are 0
 };
 cudaError_t launch_cwt_pad(const float* x, void* X, long long n, long long lfft, long long count, cudaStream_t stream);
+// product: W (signals x nscales x lfft) = X (signals x lfft) times K (nscales x lfft), line by line;
+// diff: out (signals x nscales x n) from W.
 cudaError_t launch_cwt_product(const void* X, const void* K, void* W, long long lfft, long long nscales,
-                               cudaStream_t stream);
+                               long long signals, cudaStream_t stream);
 cudaError_t launch_cwt_diff(const void* W, const CwtScale* scales, void* out, long long n, long long lfft,
-                            long long nscales, cudaStream_t stream);
+                            long long nscales, long long signals, cudaStream_t stream);
 
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);

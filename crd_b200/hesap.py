@@ -241,7 +241,8 @@ class CwtPlan:
     """crd-hesap-wavelet's cwt (cwt.hpp:461-621) on the device over `count` real signals of `nsamples` samples:
     coefficients (count, nscales, nsamples) complex64, row s of signal c = CwtResult::coeffs[s * n ...] of that
     signal. wavelet: a pywt-style name ("mexh", "morl", "cmorB-C", "gausP", "cgauP", "shanB-C", "fbspM-B-C",
-    "paulM"; continuous_wavelet, cwt.hpp:300-407). The scales' kernels are built once, at plan time."""
+    "paulM"; continuous_wavelet, cwt.hpp:300-407). The scales' kernels and their spectra are built once, at plan
+    time."""
 
     def __init__(self, nsamples: int, scales, wavelet: str, count: int = 1, sampling_period: float = 1.0,
                  precision: int = 12):
@@ -257,9 +258,9 @@ class CwtPlan:
                                            freqs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "cwt_frequencies")
         self.frequencies = freqs
         check(lib().crdfft_cwt_plan_create(ctypes.byref(self._desc), ctypes.byref(self._h)), "cwt_plan_create")
-        lfft, fused = ctypes.c_int64(), ctypes.c_int32()
-        check(lib().crdfft_cwt_plan_info(self._h, ctypes.byref(lfft), ctypes.byref(fused)), "cwt_plan_info")
-        self.fft_length, self.fused = int(lfft.value), bool(fused.value)
+        lfft, rnd = ctypes.c_int64(), ctypes.c_int64()
+        check(lib().crdfft_cwt_plan_info(self._h, ctypes.byref(lfft), ctypes.byref(rnd)), "cwt_plan_info")
+        self.fft_length, self.signals_per_round = int(lfft.value), int(rnd.value)
 
     def _make_desc(self, sampling_period: float, precision: int) -> CwtDesc:
         d = CwtDesc()

@@ -229,10 +229,10 @@ crdfft_status crdfft_spectral_execute(crdfft_plan* plan, const float* x, float* 
 
 /* crd-hesap-wavelet's cwt (engine/numerics/hesap-wavelet/include/crd/hesap/wavelet/cwt.hpp:461-621) over `count`
  * real signals of nsamples samples. The plan builds the wavelet's integral and each scale's kernel in FP64 on the
- * host (sample_psi, cwt.hpp:149-280; the kernels at cwt.hpp:569-581) and keeps the kernels on the device; an execute
- * zero-pads and transforms the signals, convolves every scale's kernel with each signal's spectrum in one fused
- * launch (FFT x spectrum x inverse FFT; a spectrum product and an inverse FFT plan where the FFT length is beyond the
- * fused kernel) and forms -sqrt(a) (w[t+1] - w[t]) / lfft (cwt.hpp:589-596). */
+ * host (sample_psi, cwt.hpp:149-280; the kernels at cwt.hpp:569-581) and keeps the kernels' spectra on the device;
+ * an execute zero-pads and transforms the signals, multiplies every signal's spectrum by every kernel spectrum, runs
+ * one batched inverse FFT over those (signal, scale) lines and forms -sqrt(a) (w[t+1] - w[t]) / lfft
+ * (cwt.hpp:583-596), in rounds of as many signals as 512 MiB of scratch holds. */
 typedef struct crdfft_cwt_desc
 {
     const char* wavelet;    /* "mexh", "morl", "cmorB-C", "gausP", "cgauP", "shanB-C", "fbspM-B-C", "paulM"
@@ -259,8 +259,8 @@ crdfft_status crdfft_cwt_frequencies(const crdfft_cwt_desc* desc, double* freque
 /* Host only, no device: the FFT length, the power of two >= n + the longest kernel (cwt.hpp:479-506); -1 for an
  * invalid descriptor. */
 int64_t crdfft_cwt_fft_length(const crdfft_cwt_desc* desc);
-/* The plan's FFT length and whether it runs the fused convolution (1) or the spectrum product + inverse FFT (0). */
-crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int32_t* fused);
+/* The plan's FFT length and the signals one round of product, inverse FFT and epilogue takes. */
+crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int64_t* signals_per_round);
 
 /* ---- Uneven batches ---------------------------------------------------------------------------------------- */
 

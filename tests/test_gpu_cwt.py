@@ -1,4 +1,4 @@
-"""Device continuous wavelet transform (crdfft_cwt_*: cwt_plan.cpp, cwt.cu around the fused convolution) against
+"""Device continuous wavelet transform (crdfft_cwt_*: cwt_plan.cpp, cwt.cu around the batched FFT plans) against
 the FP64 oracle (oracle/wavelet.py, pinned to the reference tests' pywt vectors) and against those vectors
 directly. FP32 kernels and FFTs against FP64: rel-L2 <= 2e-5 over each signal's coefficients and <= 1e-4 over each
 scale (the epilogue differences neighbouring filtered samples, which costs up to about 30x the FFT's relative error
@@ -48,32 +48,45 @@ def test_reference_vectors(name, key, cplx):
     np.testing.assert_allclose(freqs, GOLD[key + "_freqs"], rtol=0, atol=1e-7)
 
 
-# (wavelet, n, scales, signals, fused): FFT lengths 512 .. 8192 run the fused convolution, 16384 and 32768 the
-# spectrum product and inverse FFT plan
+# (wavelet, n, scales, signals): FFT lengths 512 .. 32768, real and complex wavelets, a scale too small for two taps
 CASES = [
-    ("morl", 1000, np.geomspace(1.0, 128.0, 32), 3, True),
-    ("cmor1.5-1.0", 4096, np.geomspace(0.5, 64.0, 48), 2, True),
-    ("mexh", 3000, np.array([0.01, 0.3, 1.0, 2.0, 5.0, 20.0, 90.0]), 1, True),
-    ("gaus4", 5000, np.geomspace(1.0, 256.0, 24), 2, True),
-    ("paul4", 2048, np.geomspace(1.0, 100.0, 16), 1, True),
-    ("fbsp2-1.0-0.5", 100, np.array([1.0, 2.0, 4.0]), 5, True),
-    ("cgau2", 12000, np.geomspace(1.0, 64.0, 10), 1, False),
-    ("shan1.0-0.5", 20000, np.geomspace(1.0, 64.0, 20), 2, False),
+    ("morl", 1000, np.geomspace(1.0, 128.0, 32), 3),
+    ("cmor1.5-1.0", 4096, np.geomspace(0.5, 64.0, 48), 2),
+    ("mexh", 3000, np.array([0.01, 0.3, 1.0, 2.0, 5.0, 20.0, 90.0]), 1),
+    ("gaus4", 5000, np.geomspace(1.0, 256.0, 24), 2),
+    ("paul4", 2048, np.geomspace(1.0, 100.0, 16), 1),
+    ("fbsp2-1.0-0.5", 100, np.array([1.0, 2.0, 4.0]), 5),
+    ("cgau2", 12000, np.geomspace(1.0, 64.0, 10), 1),
+    ("shan1.0-0.5", 20000, np.geomspace(1.0, 64.0, 20), 2),
 ]
 
 
-@pytest.mark.parametrize("name,n,scales,count,fused", CASES)
-def test_against_oracle(name, n, scales, count, fused):
+@pytest.mark.parametrize("name,n,scales,count", CASES)
+def test_against_oracle(name, n, scales, count):
     rng = np.random.default_rng(n + count)
     x = rng.standard_normal((count, n)).astype(np.float32)
     plan = cf.CwtPlan(n, scales, name, count)
     assert plan.fft_length == W.geometry(n, scales, name)[0]
-    assert plan.fused == fused
+    assert plan.signals_per_round == count
     got = plan.execute(torch.from_numpy(x).cuda()).cpu().numpy().astype(np.complex128)
     for c in range(count):
         want, freqs = W.cwt(x[c].astype(np.float64), scales, name)
         _check(got[c], want)
     np.testing.assert_allclose(plan.frequencies, freqs, rtol=1e-14, atol=0)
+
+
+def test_signals_in_several_rounds():
+    """More signals than 512 MiB of filtered sequences hold: full rounds and a shorter last one (its own inverse
+    plan); signals at both ends of each round against the oracle."""
+    n, scales = 6000, np.geomspace(1.0, 200.0, 96)  # FFT length 16384: 12 MiB a signal, 42 signals a round
+    count = 45
+    x = np.random.default_rng(5).standard_normal((count, n)).astype(np.float32)
+    plan = cf.CwtPlan(n, scales, "morl", count)
+    assert plan.fft_length == 16384 and plan.signals_per_round == 42
+    got = plan.execute(torch.from_numpy(x).cuda()).cpu().numpy().astype(np.complex128)
+    for c in (0, 41, 42, 44):
+        want, _ = W.cwt(x[c].astype(np.float64), scales, "morl")
+        _check(got[c], want)
 
 
 def test_run_twice_bit_identical_and_stream_ordered():
