@@ -574,8 +574,9 @@ def _cwt64_morl(x, scales):
 
 def build_cwt(dev, rank, cf):
     """hesap-wavelet's cwt on the device: 64 signals of 4096 samples, 64 scales from 1 to 128, real Morlet (FFT
-    length 8192): one batched forward FFT of the signals, the product with the 64 kernel spectra (made at plan time)
-    over all 4096 (signal, scale) lines, one batched inverse FFT over them and the difference epilogue."""
+    length 8192): one batched forward FFT of the signals, then one kernel over all 4096 (signal, scale) lines: the
+    product with the kernel spectra (made at plan time), the inverse FFT in shared memory and the difference
+    epilogue."""
     import numpy as np
     import torch
 
@@ -589,8 +590,8 @@ def build_cwt(dev, rank, cf):
     L = plan.fft_length
     fl = count * (5.0 * L * math.log2(L) + ns * (10.0 * L * math.log2(L) + 6.0 * L))
     rounds = -(-count // plan.signals_per_round)
-    launches = 1 + cf.Plan([L], batch=count).info()["passes"] + rounds * (
-        2 + cf.Plan([L], batch=plan.signals_per_round * ns).info()["passes"])
+    launches = 1 + cf.Plan([L], batch=count).info()["passes"] + (1 if plan.fused else rounds * (
+        2 + cf.Plan([L], batch=plan.signals_per_round * ns).info()["passes"]))
 
     def check():
         plan.execute(x, out)
@@ -599,7 +600,8 @@ def build_cwt(dev, rank, cf):
         return _rel(out[:2].cpu().numpy(), _cwt64_morl(xs, scales))
 
     op = Op("cwt", x, out, lambda i, o: plan.execute(i, o), fl, 4 * count * n + 8 * count * ns * n, launches, check,
-            {"signals": count, "scales": ns, "fft_length": L, "signals_per_round": plan.signals_per_round})
+            {"signals": count, "scales": ns, "fft_length": L, "fused": plan.fused,
+             "signals_per_round": plan.signals_per_round})
     return [op], dict(WORKLOAD_CONFIGS["cwt"])
 
 

@@ -189,7 +189,7 @@ def lib():
         "crdfft_cwt_execute": ([vp, vp, vp, vp], i32),
         "crdfft_cwt_frequencies": ([ctypes.POINTER(CwtDesc), ctypes.POINTER(ctypes.c_double)], i32),
         "crdfft_cwt_fft_length": ([ctypes.POINTER(CwtDesc)], i64),
-        "crdfft_cwt_plan_info": ([vp, ctypes.POINTER(i64), ctypes.POINTER(i64)], i32),
+        "crdfft_cwt_plan_info": ([vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i32)], i32),
         "crdfft_plan_info_get": ([vp, ctypes.POINTER(PlanInfo)], i32),
         "crdfft_workspace_size": ([vp], ctypes.c_size_t),
         "crdfft_set_workspace": ([vp, vp, ctypes.c_size_t], i32),

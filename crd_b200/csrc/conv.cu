@@ -150,6 +150,91 @@ __global__ void __launch_bounds__(kMaxThreads)
     });
 }
 
+// The continuous wavelet transform's lines (crd-hesap-wavelet cwt.hpp:583-596) in one kernel: line l is signal
+// l / nscales at scale l mod nscales. Z = conj(X K) goes to shared memory, the forward stages leave FFT(Z) there in
+// natural order, and w = IFFT(X K) = conj(FFT(Z)) (unnormalised) is differenced on the way out:
+// out[l][i] = amp (w[off + i + 1] - w[off + i]) / lfft, or 0 for a scale with fewer than two taps. Only the n
+// coefficients of a line reach HBM; the spectra X (one line a signal) and K (one a scale) are read once a line.
+template <class S, int P>
+__global__ void __launch_bounds__(kMaxThreads)
+    cwt_line_kernel(const PassDesc d, const float2* __restrict__ X, const float2* __restrict__ K,
+                    const CwtScale* __restrict__ scales, long long nscales, long long nsamples, float inv_n,
+                    float2* __restrict__ gout)
+{
+    extern __shared__ float2 sm[];
+    constexpr int n = S::n;
+    constexpr int T = n / P;
+    const int lpc = blockDim.x / T;
+    const int tid = threadIdx.x;
+    const int ll = tid / T;
+    const int jt = tid - ll * T;
+    const long long line = static_cast<long long>(blockIdx.x) * lpc + ll;
+    Ctx c;
+    c.ok = line < d.lines;
+    c.q = 0;
+    c.in = X;
+    c.out = gout;
+    c.jt = jt;
+    c.T = T;
+    init_scales(d, c);
+    c.in_im = 1.0f;
+    const LayRow<1> lay{sm + ll * line_pitch(n)};
+    const long long sig = line / nscales, s = line - sig * nscales;
+    if (c.ok)
+    {
+        const float2* x = X + sig * n;
+        const float2* k = K + s * n;
+        for (int e = jt; e < n; e += T)
+        {
+            const float2 v = cmul(__ldg(x + e), __ldg(k + e));
+            lay.at(e) = make_float2(v.x, -v.y);
+        }
+    }
+    __syncthreads();
+    SchedRun<S>::template go<P, false, false, false, Kind<PassMap::Row, false>>(d, c, lay, n);
+    __syncthreads();
+    if (c.ok)
+    {
+        const CwtScale p = scales[s];
+        float2* o = gout + line * nsamples;
+        for (long long i = jt; i < nsamples; i += T)
+        {
+            float2 v = make_float2(0.0f, 0.0f);
+            if (p.taps_ok)
+            {
+                const float2 a = lay.at(static_cast<int>(p.off + i)), b = lay.at(static_cast<int>(p.off + i + 1));
+                v = make_float2(p.amp * (b.x - a.x) * inv_n, p.amp * (a.y - b.y) * inv_n);
+            }
+            __stcs(o + i, v);
+        }
+    }
+}
+
+using CwtFn = void (*)(const PassDesc, const float2*, const float2*, const CwtScale*, long long, long long, float,
+                       float2*);
+
+// Compile-time schedules only (the lengths conv_select runs statically on a row map).
+CwtFn cwt_select(const PassDesc& d, int P)
+{
+    if (P == 32)
+    {
+        if (same_radices(d, {16, 16, 16}))
+            return cwt_line_kernel<Sched<16, 16, 16>, 32>;
+        if (same_radices(d, {32, 32}))
+            return cwt_line_kernel<Sched<32, 32>, 32>;
+        if (same_radices(d, {32, 16, 16}))
+            return cwt_line_kernel<Sched<32, 16, 16>, 32>;
+        return nullptr;
+    }
+    if (same_radices(d, {16, 16}))
+        return cwt_line_kernel<Sched<16, 16>, 16>;
+    if (same_radices(d, {16, 8, 4}))
+        return cwt_line_kernel<Sched<16, 8, 4>, 16>;
+    if (same_radices(d, {16, 16, 4}))
+        return cwt_line_kernel<Sched<16, 16, 4>, 16>;
+    return nullptr;
+}
+
 using ConvFn = void (*)(const PassDesc, const float2*, const float2*, const LineMap, float2*);
 
 template <class S, int P> ConvFn conv_pick(PassMap map)
@@ -239,6 +324,39 @@ cudaError_t launch_conv(const PassDesc& d, PassMap map, const LineMap& smap, con
     fn<<<static_cast<unsigned>(groups), T * lpc, smem, stream>>>(d, static_cast<const float2*>(in),
                                                                  static_cast<const float2*>(spec), smap,
                                                                  static_cast<float2*>(out));
+    return cudaGetLastError();
+}
+
+bool cwt_lines_supported(const PassDesc& d)
+{
+    int P = 16, lpc = 1, smem = 0;
+    conv_shape(d, PassMap::Row, &P, &lpc, &smem);
+    return conv_supported(d) && lfft::cwt_select(d, P) != nullptr;
+}
+
+cudaError_t launch_cwt_lines(const PassDesc& d, const void* X, const void* K, const CwtScale* scales, long long nscales,
+                             long long n, void* out, cudaStream_t stream)
+{
+    int P = 16, lpc = 1, smem = 0;
+    conv_shape(d, PassMap::Row, &P, &lpc, &smem);
+    lfft::CwtFn fn = lfft::cwt_select(d, P);
+    if (fn == nullptr || n < 1 || n >= d.n)
+        return cudaErrorInvalidConfiguration;
+    const int T = d.n / P;
+    const long long groups = (d.lines + lpc - 1) / lpc;
+    if (groups <= 0)
+        return cudaSuccess;
+    if (groups > 0x7fffffffLL)
+        return cudaErrorInvalidConfiguration;
+    if (smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    fn<<<static_cast<unsigned>(groups), T * lpc, smem, stream>>>(
+        d, static_cast<const float2*>(X), static_cast<const float2*>(K), scales, nscales, n,
+        static_cast<float>(1.0 / static_cast<double>(d.n)), static_cast<float2*>(out));
     return cudaGetLastError();
 }
 

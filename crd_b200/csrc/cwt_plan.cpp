@@ -12,7 +12,9 @@
 // plan; then, over chunks of signals, the product of every signal's spectrum with every kernel spectrum as one grid
 // of (signal, scale) lines (cwt.cu, cwt.hpp:583-587), one batched unnormalised inverse FFT over those lines, and the
 // epilogue -sqrt(a) (w[t+1] - w[t]) / lfft (cwt.cu, cwt.hpp:589-596). A chunk's lines fill the GPU in each launch,
-// where a launch per signal would give one CTA per scale.
+// where a launch per signal would give one CTA per scale. Where the FFT length has a compile-time line schedule
+// (256 .. 8192), one kernel (conv.cu, cwt_line_kernel) does the product, the inverse FFT in shared memory and the
+// epilogue for every line, so only the coefficients are written.
 #include "../../include/crdfft.h"
 #include "kernels.hpp"
 
@@ -30,6 +32,9 @@ struct crdfft_cwt_plan
     int device = -1;
     long long n = 0, count = 0, nscales = 0, lfft = 0;
     long long chunk = 0;                 // signals a product / inverse FFT / epilogue round takes
+    bool fused = false;                  // one line kernel over all (signal, scale) lines (conv.cu)
+    crdfft_plan* lines_plan = nullptr;   // fused: the convolution plan whose line pass (stages, twiddles) it runs
+    crdfft::PassDesc pass{};             // fused: that line pass, lines = count x nscales
     crdfft_plan* forward = nullptr;      // the signals' FFTs (batch count, in place on X)
     crdfft_plan* inverse = nullptr;      // chunk x nscales inverse FFTs, in place on W
     crdfft_plan* inverse_tail = nullptr; // (count mod chunk) x nscales, when the last chunk is shorter
@@ -40,7 +45,7 @@ struct crdfft_cwt_plan
 
     ~crdfft_cwt_plan()
     {
-        for (crdfft_plan* p : {forward, inverse, inverse_tail})
+        for (crdfft_plan* p : {forward, inverse, inverse_tail, lines_plan})
             if (p != nullptr)
                 crdfft_plan_destroy(p);
         for (void* b : {spectra, X, W, static_cast<void*>(scales)})
@@ -415,13 +420,25 @@ crdfft_status build(const crdfft_cwt_desc* d, const Geometry& g, crdfft_cwt_plan
         }
     }
 
-    // signals a round: the filtered sequences within 512 MiB, the grid rows (signal x scale lines) within 65535
+    // the fused line kernel where the FFT length has a compile-time schedule: one launch, no filtered-sequence scratch
     const long long line_bytes = lfft * 8;
-    p->chunk = std::max<long long>(
-        1, std::min<long long>({static_cast<long long>(d->count), (512LL << 20) / (ns * line_bytes), 65535 / ns}));
+    crdfft_desc ld = line_desc(lfft, d->count * ns);
+    if (crdfft_conv_plan_create(&ld, 0, 1.0, &p->lines_plan) == CRDFFT_OK)
+    {
+        p->fused = crdfft::conv_line_pass(p->lines_plan, &p->pass) && crdfft::cwt_lines_supported(p->pass);
+        if (!p->fused)
+        {
+            crdfft_plan_destroy(p->lines_plan);
+            p->lines_plan = nullptr;
+        }
+    }
+    // otherwise signals a round: the filtered sequences within 512 MiB, the grid rows (lines) within 65535
+    p->chunk = p->fused ? d->count
+                        : std::max<long long>(1, std::min<long long>({static_cast<long long>(d->count),
+                                                                      (512LL << 20) / (ns * line_bytes), 65535 / ns}));
     const size_t kbytes = static_cast<size_t>(ns * line_bytes);
     if (cudaMalloc(&p->spectra, kbytes) != cudaSuccess ||
-        cudaMalloc(&p->W, static_cast<size_t>(p->chunk) * kbytes) != cudaSuccess ||
+        (!p->fused && cudaMalloc(&p->W, static_cast<size_t>(p->chunk) * kbytes) != cudaSuccess) ||
         cudaMalloc(&p->X, static_cast<size_t>(d->count * line_bytes)) != cudaSuccess ||
         cudaMalloc(reinterpret_cast<void**>(&p->scales), sizeof(crdfft::CwtScale) * static_cast<size_t>(ns)) !=
             cudaSuccess)
@@ -451,6 +468,8 @@ crdfft_status build(const crdfft_cwt_desc* d, const Geometry& g, crdfft_cwt_plan
         return st;
     if (e != cudaSuccess)
         return CRDFFT_LAUNCH;
+    if (p->fused)
+        return CRDFFT_OK;
     crdfft_desc id = line_desc(lfft, p->chunk * ns);
     st = crdfft_plan_create(&id, &p->inverse);
     if (st != CRDFFT_OK)
@@ -517,6 +536,10 @@ crdfft_status crdfft_cwt_execute(crdfft_cwt_plan* plan, const float* x, void* co
     crdfft_status st = crdfft_execute(p.forward, p.X, p.X, CRDFFT_FORWARD, stream);
     if (st != CRDFFT_OK)
         return st;
+    if (p.fused)
+        return crdfft::launch_cwt_lines(p.pass, p.X, p.spectra, p.scales, p.nscales, p.n, coeffs, s) == cudaSuccess
+                   ? CRDFFT_OK
+                   : CRDFFT_LAUNCH;
     for (long long c0 = 0; c0 < p.count; c0 += p.chunk)
     {
         const long long cc = std::min(p.chunk, p.count - c0);
@@ -554,7 +577,8 @@ int64_t crdfft_cwt_fft_length(const crdfft_cwt_desc* desc)
     return geometry(desc, &g) == CRDFFT_OK ? g.lfft : -1;
 }
 
-crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int64_t* signals_per_round)
+crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int64_t* signals_per_round,
+                                   int32_t* fused)
 {
     if (plan == nullptr)
         return CRDFFT_INVALID_ARG;
@@ -562,6 +586,8 @@ crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_len
         *fft_length = plan->lfft;
     if (signals_per_round != nullptr)
         *signals_per_round = plan->chunk;
+    if (fused != nullptr)
+        *fused = plan->fused ? 1 : 0;
     return CRDFFT_OK;
 }
 

@@ -3,6 +3,7 @@
 #pragma once
 
 #include "pass_desc.hpp"
+#include "../../include/crdfft.h"
 
 #include <cuda_runtime.h>
 
@@ -165,6 +166,13 @@ cudaError_t launch_cwt_product(const void* X, const void* K, void* W, long long 
                                long long signals, cudaStream_t stream);
 cudaError_t launch_cwt_diff(const void* W, const CwtScale* scales, void* out, long long n, long long lfft,
                             long long nscales, long long signals, cudaStream_t stream);
+// The CWT's lines in one kernel (conv.cu): load conj(X[c] K[s]) into shared memory, the forward stages of `d` (a
+// fused-convolution plan's line pass, conv_line_pass), and the differenced, conjugated, scaled store of n samples.
+// d.lines = signals x nscales lines of this launch. cwt_lines_supported: a compile-time schedule exists for d.
+bool conv_line_pass(crdfft_plan* plan, PassDesc* out);
+bool cwt_lines_supported(const PassDesc& d);
+cudaError_t launch_cwt_lines(const PassDesc& d, const void* X, const void* K, const CwtScale* scales, long long nscales,
+                             long long n, void* out, cudaStream_t stream);
 
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);

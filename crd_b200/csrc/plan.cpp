@@ -2289,6 +2289,20 @@ crdfft_desc desc_1d(long long n, int kind, int norm)
 Plan* as_plan(crdfft_plan* p) { return reinterpret_cast<Plan*>(p); }
 
 } // namespace
+
+// The line pass of a 1-D fused-convolution plan (its stages and forward twiddles), for kernels that run the same line
+// FFT with their own load and store (the CWT's (signal, scale) lines, cwt_plan.cpp).
+bool conv_line_pass(crdfft_plan* plan, PassDesc* out)
+{
+    if (plan == nullptr || out == nullptr)
+        return false;
+    const Plan& p = *as_plan(plan);
+    if (!p.conv || p.algorithm != "fused-conv" || p.steps[0].size() != 1)
+        return false;
+    *out = p.steps[0][0].pass;
+    return true;
+}
+
 } // namespace crdfft
 
 namespace crdfft

@@ -258,9 +258,10 @@ class CwtPlan:
                                            freqs.ctypes.data_as(ctypes.POINTER(ctypes.c_double))), "cwt_frequencies")
         self.frequencies = freqs
         check(lib().crdfft_cwt_plan_create(ctypes.byref(self._desc), ctypes.byref(self._h)), "cwt_plan_create")
-        lfft, rnd = ctypes.c_int64(), ctypes.c_int64()
-        check(lib().crdfft_cwt_plan_info(self._h, ctypes.byref(lfft), ctypes.byref(rnd)), "cwt_plan_info")
-        self.fft_length, self.signals_per_round = int(lfft.value), int(rnd.value)
+        lfft, rnd, fused = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32()
+        check(lib().crdfft_cwt_plan_info(self._h, ctypes.byref(lfft), ctypes.byref(rnd), ctypes.byref(fused)),
+              "cwt_plan_info")
+        self.fft_length, self.signals_per_round, self.fused = int(lfft.value), int(rnd.value), bool(fused.value)
 
     def _make_desc(self, sampling_period: float, precision: int) -> CwtDesc:
         d = CwtDesc()

@@ -230,9 +230,10 @@ crdfft_status crdfft_spectral_execute(crdfft_plan* plan, const float* x, float* 
 /* crd-hesap-wavelet's cwt (engine/numerics/hesap-wavelet/include/crd/hesap/wavelet/cwt.hpp:461-621) over `count`
  * real signals of nsamples samples. The plan builds the wavelet's integral and each scale's kernel in FP64 on the
  * host (sample_psi, cwt.hpp:149-280; the kernels at cwt.hpp:569-581) and keeps the kernels' spectra on the device;
- * an execute zero-pads and transforms the signals, multiplies every signal's spectrum by every kernel spectrum, runs
- * one batched inverse FFT over those (signal, scale) lines and forms -sqrt(a) (w[t+1] - w[t]) / lfft
- * (cwt.hpp:583-596), in rounds of as many signals as 512 MiB of scratch holds. */
+ * an execute zero-pads and transforms the signals, then for every (signal, scale) line multiplies the two spectra,
+ * inverse-transforms and forms -sqrt(a) (w[t+1] - w[t]) / lfft (cwt.hpp:583-596): in one kernel with the line in
+ * shared memory for FFT lengths 256 .. 8192 that have a compile-time schedule, else as a product kernel, a batched
+ * inverse FFT plan and an epilogue kernel in rounds of as many signals as 512 MiB of scratch holds. */
 typedef struct crdfft_cwt_desc
 {
     const char* wavelet;    /* "mexh", "morl", "cmorB-C", "gausP", "cgauP", "shanB-C", "fbspM-B-C", "paulM"
@@ -259,8 +260,10 @@ crdfft_status crdfft_cwt_frequencies(const crdfft_cwt_desc* desc, double* freque
 /* Host only, no device: the FFT length, the power of two >= n + the longest kernel (cwt.hpp:479-506); -1 for an
  * invalid descriptor. */
 int64_t crdfft_cwt_fft_length(const crdfft_cwt_desc* desc);
-/* The plan's FFT length and the signals one round of product, inverse FFT and epilogue takes. */
-crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int64_t* signals_per_round);
+/* The plan's FFT length, the signals one round takes, and whether one fused line kernel runs each execute (FFT
+ * lengths with a compile-time line schedule) or the product / inverse FFT / epilogue rounds. Any pointer may be NULL. */
+crdfft_status crdfft_cwt_plan_info(const crdfft_cwt_plan* plan, int64_t* fft_length, int64_t* signals_per_round,
+                                   int32_t* fused);
 
 /* ---- Uneven batches ---------------------------------------------------------------------------------------- */
 

@@ -260,7 +260,7 @@ public:
     int64_t fft_length() const
     {
         int64_t n = 0;
-        check(crdfft_cwt_plan_info(m_p, &n, nullptr), "cwt_plan_info");
+        check(crdfft_cwt_plan_info(m_p, &n, nullptr, nullptr), "cwt_plan_info");
         return n;
     }
 

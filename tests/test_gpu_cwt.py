@@ -1,4 +1,5 @@
-"""Device continuous wavelet transform (crdfft_cwt_*: cwt_plan.cpp, cwt.cu around the batched FFT plans) against
+"""Device continuous wavelet transform (crdfft_cwt_*: cwt_plan.cpp; the fused line kernel in conv.cu, or cwt.cu's
+product and epilogue around a batched inverse FFT plan) against
 the FP64 oracle (oracle/wavelet.py, pinned to the reference tests' pywt vectors) and against those vectors
 directly. FP32 kernels and FFTs against FP64: rel-L2 <= 2e-5 over each signal's coefficients and <= 1e-4 over each
 scale (the epilogue differences neighbouring filtered samples, which costs up to about 30x the FFT's relative error
@@ -48,26 +49,29 @@ def test_reference_vectors(name, key, cplx):
     np.testing.assert_allclose(freqs, GOLD[key + "_freqs"], rtol=0, atol=1e-7)
 
 
-# (wavelet, n, scales, signals): FFT lengths 512 .. 32768, real and complex wavelets, a scale too small for two taps
+# (wavelet, n, scales, signals, fused): FFT lengths 512 .. 32768, real and complex wavelets, a scale too small for two
+# taps; 4096 and 8192 run the fused line kernel, 16384 and 32768 the product / inverse FFT / epilogue rounds
 CASES = [
-    ("morl", 1000, np.geomspace(1.0, 128.0, 32), 3),
-    ("cmor1.5-1.0", 4096, np.geomspace(0.5, 64.0, 48), 2),
-    ("mexh", 3000, np.array([0.01, 0.3, 1.0, 2.0, 5.0, 20.0, 90.0]), 1),
-    ("gaus4", 5000, np.geomspace(1.0, 256.0, 24), 2),
-    ("paul4", 2048, np.geomspace(1.0, 100.0, 16), 1),
-    ("fbsp2-1.0-0.5", 100, np.array([1.0, 2.0, 4.0]), 5),
-    ("cgau2", 12000, np.geomspace(1.0, 64.0, 10), 1),
-    ("shan1.0-0.5", 20000, np.geomspace(1.0, 64.0, 20), 2),
+    ("morl", 1000, np.geomspace(1.0, 128.0, 32), 3, True),
+    ("cmor1.5-1.0", 4096, np.geomspace(0.5, 64.0, 48), 2, True),
+    ("mexh", 3000, np.array([0.01, 0.3, 1.0, 2.0, 5.0, 20.0, 90.0]), 1, True),
+    ("gaus4", 5000, np.geomspace(1.0, 256.0, 24), 2, True),
+    ("paul4", 2048, np.geomspace(1.0, 100.0, 16), 1, True),
+    ("fbsp2-1.0-0.5", 100, np.array([1.0, 2.0, 4.0]), 5, None),
+    ("cgau2", 12000, np.geomspace(1.0, 64.0, 10), 1, False),
+    ("shan1.0-0.5", 20000, np.geomspace(1.0, 64.0, 20), 2, False),
 ]
 
 
-@pytest.mark.parametrize("name,n,scales,count", CASES)
-def test_against_oracle(name, n, scales, count):
+@pytest.mark.parametrize("name,n,scales,count,fused", CASES)
+def test_against_oracle(name, n, scales, count, fused):
     rng = np.random.default_rng(n + count)
     x = rng.standard_normal((count, n)).astype(np.float32)
     plan = cf.CwtPlan(n, scales, name, count)
     assert plan.fft_length == W.geometry(n, scales, name)[0]
     assert plan.signals_per_round == count
+    if fused is not None:
+        assert plan.fused == fused
     got = plan.execute(torch.from_numpy(x).cuda()).cpu().numpy().astype(np.complex128)
     for c in range(count):
         want, freqs = W.cwt(x[c].astype(np.float64), scales, name)
@@ -82,7 +86,7 @@ def test_signals_in_several_rounds():
     count = 45
     x = np.random.default_rng(5).standard_normal((count, n)).astype(np.float32)
     plan = cf.CwtPlan(n, scales, "morl", count)
-    assert plan.fft_length == 16384 and plan.signals_per_round == 42
+    assert plan.fft_length == 16384 and plan.signals_per_round == 42 and not plan.fused
     got = plan.execute(torch.from_numpy(x).cuda()).cpu().numpy().astype(np.complex128)
     for c in (0, 41, 42, 44):
         want, _ = W.cwt(x[c].astype(np.float64), scales, "morl")
