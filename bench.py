@@ -338,14 +338,15 @@ def build_uneven(dev, rank, cf):
 PRECISIONS = {"fp32": 0, "split-bf16": 1, "fp16-scaled": 2}
 
 
-def _build_nd_forms(dev, rank, cf, forms):
+def _build_nd_forms(dev, rank, cf, forms, shapes=((4096, 4096), (512, 512, 512))):
     """2-D C2C 4096 x 4096 and 3-D C2C 512^3, uniform[-1,1) plus 1% of entries scaled by 1e4, at each precision form
     in `forms`. Four input buffers of the 2-D shape rotate across steps so its 128 MiB input is not L2-resident."""
     import numpy as np
     import torch
 
     ops = []
-    for dims, nbuf in (((4096, 4096), 4), ((512, 512, 512), 1)):
+    for dims in shapes:
+        nbuf = 4 if len(dims) == 2 else 1
         total = int(np.prod(dims))
         gen = torch.Generator(device=dev)
         gen.manual_seed(SEED + 4 + rank + total)
@@ -453,6 +454,35 @@ def build_conv(dev, rank, cf):
                 torch.fft.rfft2(rin.view((b,) + tuple(dims))) * H, s=dims))
         ops.append(op)
     return ops, dict(WORKLOAD_CONFIGS["conv"])
+
+
+def precision_contrast(dev, rank, cf, steps: int, warmup: int) -> dict:
+    """The metric's contrast on the 2-D 4096 x 4096 input of the precision configuration (uniform[-1,1) plus 1 % of
+    entries x 1e4): each precision form's ms per execute (CUDA events, four input buffers in turn so none is
+    L2-resident) and its rel-L2 against numpy's FP64 FFT. Timed outside the job's clock."""
+    import numpy as np
+    import torch
+
+    ops = [op for op in _build_nd_forms(dev, rank, cf, tuple(PRECISIONS), shapes=((4096, 4096),))]
+    out = {"shape": "4096x4096", "inputs": "uniform[-1,1) + 1% x 1e4", "bar": "rel-L2 <= 1e-6 vs FP64"}
+    stream = torch.cuda.current_stream()
+    for op in ops:
+        for _ in range(warmup):
+            op.run(op.inp, op.out)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            op.run(op.inp, op.out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[op.info["precision"]] = {"ms": round(ms, 4), "rel_l2_vs_fp64": op.check(),
+                                     "algorithm": op.info["algorithm"],
+                                     "hbm_frac": round(op.bytes / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"], 4)}
+    f32, bf = out["fp32"]["ms"], out["split-bf16"]["ms"]
+    out["split_bf16_speedup_vs_fp32"] = round(f32 / bf, 3)
+    return out
 
 
 def build_precision(dev, rank, cf):
@@ -619,7 +649,47 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> dict:
+def cpu_model() -> dict:
+    """The host CPU's model name and physical core count, from lscpu."""
+    info = {"model": None, "physical_cores": None, "threads": host_threads()}
+    try:
+        txt = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+    except (OSError, subprocess.TimeoutExpired):
+        return info
+    kv = {}
+    for ln in txt.splitlines():
+        if ":" in ln:
+            k, v = ln.split(":", 1)
+            kv[k.strip()] = v.strip()
+    info["model"] = kv.get("Model name")
+    try:
+        info["physical_cores"] = int(kv["Core(s) per socket"]) * int(kv.get("Socket(s)", "1"))
+    except (KeyError, ValueError):
+        pass
+    return info
+
+
+def cpu_rows(workload: str) -> list:
+    """Two more rows of the reference's CPU path, each in a child process (its kernel level is fixed at first use):
+    one host thread at the best level, and all threads with CRD_CPU_LEVEL=avx2."""
+    rows = []
+    for threads, level in ((1, None), (host_threads(), "avx2")):
+        env = dict(os.environ)
+        if level is not None:
+            env["CRD_CPU_LEVEL"] = level
+        try:
+            r = subprocess.run([sys.executable, os.path.abspath(__file__), "--impl", "reference", "--workload",
+                                workload, "--cpu-row", str(threads)], capture_output=True, text=True, env=env,
+                               timeout=300)
+            row = json.loads(r.stdout.strip().splitlines()[-1])
+        except Exception as exc:  # the main row stands; say why this one is missing
+            row = {"threads": threads, "value": None, "error": str(exc)[:200]}
+        row["level_request"] = level or "auto"
+        rows.append(row)
+    return rows
+
+
+def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int, threads: int | None = None) -> dict:
     """Time the reference's crd-hesap-fft (oracle/_ref/libcrdref.so: FftPlan<float> for powers of two,
     BluesteinPlan<float> otherwise, RealFftPlan<float>, NdFftPlan<float>; one plan per thread over contiguous
     ranges, detail/batch_arms.hpp:59-77) on this host, in place, over a bounded sample of the workload."""
@@ -630,7 +700,7 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
     if not oracle.ref_available():
         raise RuntimeError("oracle/_ref/libcrdref.so not built")
     R = oracle.ref()
-    threads = host_threads()
+    threads = threads or host_threads()
     total_flops = 0.0
     total_time = 0.0
     sample = []
@@ -821,7 +891,18 @@ def reference_cpu(workload: str, steps: int, warmup: int, budget_bytes: int) -> 
     }
 
 
+def run_cpu_row(args) -> None:
+    """One bounded CPU row (child of cpu_rows): 64 MiB per size at one thread, 256 MiB otherwise."""
+    budget = (64 << 20) if args.cpu_row == 1 else (256 << 20)
+    res = reference_cpu(args.workload, steps=2, warmup=1, budget_bytes=budget, threads=args.cpu_row)
+    print(json.dumps({"threads": res["cores"], "value": round(res["value"], 2), "unit": "GFLOP/s",
+                      "level": res["level"], "sample": res["sample"]}), flush=True)
+
+
 def run_reference_arm(args) -> None:
+    if getattr(args, "cpu_row", None) is not None:
+        run_cpu_row(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -846,7 +927,8 @@ def run_reference_arm(args) -> None:
         "data": "synthetic",
         "config": config,
         "cpu_baseline": {"value": round(value, 2), "unit": "GFLOP/s", "cores": res["cores"], "kind": "reference",
-                         "sample": res["sample"], "level": res["level"], "per_op_gflops": res["per_op_gflops"]},
+                         "sample": res["sample"], "level": res["level"], "per_op_gflops": res["per_op_gflops"],
+                         "host": cpu_model()},
         "e2e": {"value": round(value, 2), "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -959,16 +1041,26 @@ def run_ours(args) -> None:
     F.device_status(cf.Plan([16]))  # the library's status word path works (a fresh plan: OK)
 
     peaks = measured_peaks()
-    # Dominant kernel: the op with one launch per execute and the largest share of the step (for the default
-    # workload, the N = 65536 cluster kernel, whose one launch moves its whole 2 GiB batch in and out); when every op
-    # takes several launches, the longest op, per launch.
-    single = [i for i, op in enumerate(ops) if op.launches == 1] or list(range(len(ops)))
-    dom = max(single, key=lambda i: per_ms[i])
+    # Dominant op: the op with the largest share of the step's device time. Its achieved rate is its algorithmic
+    # bytes over its event-timed duration (for a multi-launch op, the four-step's passes and waves, that is the same
+    # as algorithmic bytes per launch over the average launch). Beside it, the longest single-launch kernel.
+    dom = max(range(len(ops)), key=lambda i: per_ms[i])
     dom_bytes = ops[dom].bytes / max(1, ops[dom].launches)
     dom_ms = per_ms[dom] / max(1, ops[dom].launches)
     achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    single = [i for i, op in enumerate(ops) if op.launches == 1]
+    one = max(single, key=lambda i: per_ms[i]) if single else None
     traffic_doc = profiled_traffic()
     traffic = traffic_doc.get(f"{args.workload}:{ops[dom].name}")
+    if traffic is not None:
+        traffic = round(traffic / max(1, ops[dom].launches))
+    single_roof = None
+    if one is not None and one != dom:
+        ach1 = ops[one].bytes / (per_ms[one] / 1e3) / 1e9
+        single_roof = {"kernel": f"{ops[one].name} ({ops[one].info.get('algorithm', '')})",
+                       "achieved": round(ach1, 1), "frac": round(ach1 / peaks["hbm_gbs"], 4),
+                       "traffic": traffic_doc.get(f"{args.workload}:{ops[one].name}"),
+                       "algorithmic_bytes_per_launch": ops[one].bytes}
     per = {}
     for op, ms in zip(ops, per_ms):
         gbs = op.bytes / (ms / 1e3) / 1e9
@@ -989,6 +1081,10 @@ def run_ours(args) -> None:
             torch.cuda.synchronize()
             pms = p0.elapsed_time(p1) / args.steps
             per[op.name].update({"peer": name, "peer_ms": round(pms, 4), "speedup_vs_peer": round(pms / ms, 2)})
+
+    precision = None
+    if args.workload == "mixed" and not args.no_precision:
+        precision = precision_contrast(dev, rank, cf, max(3, args.steps), max(3, args.warmup))
 
     # End to end through the public API with host buffers: every step copies each op's input from pinned host
     # memory, runs it, and copies its whole output back (crdfft_execute_host where the op has it: the batch in chunks,
@@ -1031,9 +1127,11 @@ def run_ours(args) -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            res = reference_cpu(args.workload, steps=2, warmup=1, budget_bytes=256 << 20)
+            # the reference arm's sample (1 GiB per size) with a few steps
+            res = reference_cpu(args.workload, steps=5, warmup=2, budget_bytes=1 << 30)
             cpu = {"value": round(res["value"], 2), "unit": "GFLOP/s", "cores": res["cores"], "kind": "reference",
-                   "sample": res["sample"], "level": res["level"], "per_op_gflops": res["per_op_gflops"]}
+                   "sample": res["sample"], "level": res["level"], "per_op_gflops": res["per_op_gflops"],
+                   "host": cpu_model(), "rows": cpu_rows(args.workload)}
         except Exception as exc:  # the GPU number stands; say why the baseline is missing
             cpu = {"value": None, "unit": "GFLOP/s", "cores": host_threads(), "kind": "reference",
                    "sample": f"unavailable: {exc}"}
@@ -1058,11 +1156,15 @@ def run_ours(args) -> None:
             "roofline": {"bound": "hbm", "kernel": f"{ops[dom].name} ({ops[dom].info.get('algorithm', '')})",
                          "achieved": round(achieved, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
                          "frac": round(achieved / peaks["hbm_gbs"], 4), "peak_source": peaks["source"],
-                         "traffic": traffic, "algorithmic_bytes_per_launch": round(dom_bytes)},
+                         "traffic": traffic, "algorithmic_bytes_per_launch": round(dom_bytes),
+                         "launches_per_execute": ops[dom].launches,
+                         "share_of_step": round(per_ms[dom] / sum(per_ms), 4),
+                         "single_launch_kernel": single_roof},
             "hbm_frac_step": round(step_bytes / (ms_per_step / 1e3) / 1e9 / peaks["hbm_gbs"], 4),
             "per_op": per,
             "rel_l2_vs_fp64_max": max(rel.values()),
             "gpu_launches": launches_per_step * args.steps,
+            "precision": precision,
             "clocks": clocks,
             "e2e": e2e,
             "cpu_baseline": cpu,
@@ -1084,6 +1186,9 @@ def main() -> None:
                          "split-BF16 and FP16-scaled; conv: fused FFT convolution beside cuFFT's three passes")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the split-BF16 vs FP32 contrast the default workload reports beside its line")
+    ap.add_argument("--cpu-row", type=int, default=None, help=argparse.SUPPRESS)  # one CPU row, in a child
     ap.add_argument("--planner", choices=["estimate", "measure"], default="measure",
                     help="measure: time each pass's candidate launch shapes at plan creation (outside the timed "
                          "region) and keep the fastest")

@@ -77,6 +77,8 @@ EXPORTS = (
     "crdfft_fft",
     "crdfft_ifft_normalized",
     "crdfft_self_check",
+    "crdfft_debug_self_check_mismatch",
+    "crdfft_debug_self_check_reset",
     "crdfft_debug_fail_alloc_after",
     "crdfft_device_status",
     "crdfft_debug_stall_waits",
@@ -207,6 +209,8 @@ def lib():
         "crdfft_fft": ([vp, i64, i32, vp], i32),
         "crdfft_ifft_normalized": ([vp, i64, vp], i32),
         "crdfft_self_check": ([], i32),
+        "crdfft_debug_self_check_mismatch": ([i32], None),
+        "crdfft_debug_self_check_reset": ([], None),
         "crdfft_debug_fail_alloc_after": ([i32], None),
         "crdfft_device_status": ([vp, vp], i32),
         "crdfft_debug_stall_waits": ([i32], None),

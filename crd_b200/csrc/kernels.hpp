@@ -137,6 +137,8 @@ cudaError_t launch_cluster_fft(const PassDesc& a, const PassDesc& b, long long b
 
 // A bump arena of device memory: while bound to the calling thread, plan creation takes every device allocation
 // (tables, status word, workspace) from it instead of cudaMalloc, and plans built so never free.
+crdfft_status first_use_self_check(int dev); // selfcheck.cpp
+
 struct Arena
 {
     char* base;

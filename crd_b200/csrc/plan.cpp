@@ -341,6 +341,12 @@ struct Plan
     }
 };
 
+// The tables are uploaded with cudaMemcpy and the status word cleared with cudaMemset, both on the legacy default
+// stream: a pageable-memory cudaMemcpy may return before its DMA lands and cudaMemset does not wait at all, and a
+// caller's non-blocking stream is not ordered after the legacy stream. So plan creation waits for the legacy stream
+// before it hands out a plan; an execute on any stream then reads finished tables.
+bool uploads_landed() { return cudaStreamSynchronize(cudaStreamLegacy) == cudaSuccess; }
+
 crdfft_status upload_table(Plan& p, const std::vector<float>& host, void** dev)
 {
     const size_t bytes = host.size() * sizeof(float);
@@ -2080,6 +2086,12 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess)
         return CRDFFT_NO_DEVICE;
+    if (t_arena == nullptr) // the static-scratch entry point allocates nothing, so it cannot run the check
+    {
+        st = first_use_self_check(dev);
+        if (st != CRDFFT_OK)
+            return st;
+    }
     std::unique_ptr<Plan> p(new Plan());
     p->desc = *desc;
     p->device = dev;
@@ -2116,6 +2128,8 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
     }
     if (p->tc_steps > 0)
         p->algorithm += desc->precision == CRDFFT_PREC_SPLIT_BF16 ? "+tc-bf16x3" : "+tc-fp16";
+    if (!uploads_landed())
+        return CRDFFT_LAUNCH;
     *out = p.release();
     return CRDFFT_OK;
 }
@@ -2784,6 +2798,9 @@ crdfft_status crdfft_plan_create_uneven(const int64_t* sizes, int64_t count, con
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess)
         return CRDFFT_NO_DEVICE;
+    const crdfft_status chk = first_use_self_check(dev);
+    if (chk != CRDFFT_OK)
+        return chk;
     std::vector<int64_t> packed;
     if (offsets == nullptr)
     {
@@ -2818,6 +2835,8 @@ crdfft_status crdfft_plan_create_uneven(const int64_t* sizes, int64_t count, con
         }
         p->ws_owned = true;
     }
+    if (!uploads_landed())
+        return CRDFFT_LAUNCH;
     *plan = reinterpret_cast<crdfft_plan*>(p.release());
     return CRDFFT_OK;
 }

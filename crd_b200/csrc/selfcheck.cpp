@@ -8,8 +8,12 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <complex>
+#include <cstdlib>
 #include <cstdint>
 #include <vector>
 
@@ -75,12 +79,16 @@ std::vector<cd> fft_pow2(std::vector<cd> a, int dir)
     return a;
 }
 
+std::atomic<int> g_plant_mismatch{0};
+
 bool close(const std::vector<float>& got, const std::vector<cd>& want, double scale)
 {
+    // test hook: a mistake planted in the host answer, on the CPU (crdfft_debug_self_check_mismatch)
+    const double planted = g_plant_mismatch.load() ? 1.0 : 0.0;
     double maxref = 0.0, maxerr = 0.0;
     for (std::size_t k = 0; k < want.size(); ++k)
     {
-        const cd w = want[k] * scale;
+        const cd w = want[k] * scale + cd(k == 0 ? planted : 0.0, 0.0);
         maxref = std::max(maxref, std::abs(w));
         maxerr = std::max(maxerr, std::abs(cd(got[2 * k], got[2 * k + 1]) - w));
     }
@@ -114,6 +122,52 @@ bool run_c2c(long long n, int dir, std::size_t salt, void* dbuf)
 }
 
 } // namespace
+
+namespace
+{
+// Per device: 0 not checked yet, 1 passed, 2 failed (plans on that device are refused from then on).
+std::mutex g_first_use_mu;
+std::map<int, int> g_first_use;
+thread_local bool t_in_self_check = false;
+} // namespace
+
+namespace crdfft
+{
+// The known-answer check at the first plan creation on each device, as the reference checks each kernel table
+// before its first use (src/fft_kernel_dispatch.cpp:48-52 through process_checked_kernel_level). The check itself
+// creates plans; those skip it (t_in_self_check). CRDFFT_SELF_CHECK=0 turns it off.
+crdfft_status first_use_self_check(int dev)
+{
+    static const bool off = [] {
+        const char* e = std::getenv("CRDFFT_SELF_CHECK");
+        return e != nullptr && std::atoi(e) == 0;
+    }();
+    if (off || t_in_self_check)
+        return CRDFFT_OK;
+    std::lock_guard<std::mutex> lk(g_first_use_mu);
+    int& state = g_first_use[dev];
+    if (state == 1)
+        return CRDFFT_OK;
+    if (state == 2)
+        return CRDFFT_NUMERIC_SELFCHECK;
+    t_in_self_check = true;
+    const crdfft_status st = crdfft_self_check();
+    t_in_self_check = false;
+    if (st == CRDFFT_OK)
+        state = 1;
+    else if (st == CRDFFT_NUMERIC_SELFCHECK)
+        state = 2;
+    return st; // other failures (out of memory, launch) leave the device unchecked: the next creation retries
+}
+} // namespace crdfft
+
+extern "C" void crdfft_debug_self_check_mismatch(int32_t on) { g_plant_mismatch.store(on ? 1 : 0); }
+
+extern "C" void crdfft_debug_self_check_reset(void)
+{
+    std::lock_guard<std::mutex> lk(g_first_use_mu);
+    g_first_use.clear();
+}
 
 extern "C" crdfft_status crdfft_self_check(void)
 {

@@ -9,11 +9,21 @@
 //
 // The array is kStaticScratchBytes (64 MiB) and lives on every GPU that loads the library until the process exits.
 // Half of it is available for the four-step intermediate, so a transform may hold at most 2^22 complex points
-// (32 MiB); larger n are rejected with CRDFFT_UNSUPPORTED_SIZE. Every call on a device shares the one array: the
-// most recent call's plan (its tables) stays in it, and two calls whose work overlaps on the GPU (different streams,
-// no ordering between them) race on it and may produce wrong results; order such calls on one stream. A call with
-// a new size or batch rebuilds the plan into the array on the host: the first call on a device also looks up the
-// array's device address, so make it before any stream capture.
+// (32 MiB); larger n are rejected with CRDFFT_UNSUPPORTED_SIZE. A length with a prime factor above 7 runs Bluestein
+// over a padded power-of-two length m >= 2n - 1, whose tables and padded sequences take about 8 m (batch + 3) bytes:
+// such n are accepted while that fits in the array (for one transform, n up to about 2^20) and are otherwise also
+// rejected with CRDFFT_UNSUPPORTED_SIZE.
+//
+// Every call on a device shares the one array: the most recent call's plan (its tables) stays in it, and two calls
+// whose work overlaps on the GPU (different streams, no ordering between them) race on it and may produce wrong
+// results; order such calls on one stream. A call with a new size or batch rebuilds the plan into the array: it first
+// waits until the device has finished all work queued so far (the previous call's kernels may still be reading the
+// old tables, on whatever stream they were queued), writes the new tables and waits for them to land, then queues the
+// transform. A call that would rebuild while its stream is being captured returns CRDFFT_INVALID_ARG and queues
+// nothing (the wait and the table uploads cannot be part of a capture); make the first call with each (n, batch)
+// outside the capture. Work captured from this entry point reads the array as it was when captured, so a graph
+// captured with one (n, batch) is valid only until a call with a different (n, batch) rebuilds the array. The first
+// call on a device also looks up the array's device address, so make it before any stream capture.
 
 #include "../../include/crdfft.h"
 #include "kernels.hpp"
@@ -70,6 +80,15 @@ extern "C" crdfft_status crdfft_execute_static_scratch(const void* in, void* out
     }
     if (s.plan == nullptr || s.n != n || s.batch != batch)
     {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(static_cast<cudaStream_t>(stream), &cap) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        if (cap != cudaStreamCaptureStatusNone)
+            return CRDFFT_INVALID_ARG; // a rebuild cannot be captured; the array is left as it was
+        // The previous call's kernels may still read the array (its tables, its intermediate) on any stream: let
+        // every queued kernel finish before the array is rewritten.
+        if (cudaDeviceSynchronize() != cudaSuccess)
+            return CRDFFT_LAUNCH;
         if (s.plan != nullptr)
         {
             crdfft_plan_destroy(s.plan); // arena-backed: releases host state only

@@ -346,9 +346,15 @@ crdfft_status crdfft_mlp_adam(float* params, const float* grad, float* m, float*
  * callbacks that must never enter an allocator, processes whose device memory belongs to a pool they do not own):
  * `batch` contiguous size-n complex transforms (FftPlan semantics: unnormalised both ways; in == out allowed), with
  * every table and intermediate taken from a 64 MiB device array that the library holds on each GPU it is loaded on.
- * Allocates no device memory. n up to 2^22 (larger: CRDFFT_UNSUPPORTED_SIZE). All calls on a device share the
- * array: the last call's plan stays in it, and calls whose GPU work overlaps race, so order them on one stream.
- * The first call on a device looks up the array's address; make it before any stream capture. */
+ * Allocates no device memory. n up to 2^22 (larger: CRDFFT_UNSUPPORTED_SIZE); a length with a prime factor above 7
+ * (Bluestein, padded length m >= 2n - 1) is accepted while its ~8 m (batch + 3) bytes fit the array, else also
+ * CRDFFT_UNSUPPORTED_SIZE. All calls on a device share the array: the last call's plan stays in it, and calls whose
+ * GPU work overlaps race, so order them on one stream. A call with a new (n, batch) rebuilds the array: it waits for
+ * all work queued on the device (cudaDeviceSynchronize), so the previous call's kernels finish first on any stream,
+ * and during a stream capture it returns CRDFFT_INVALID_ARG without queuing anything: make the first call with each
+ * (n, batch) outside the capture. A captured graph reads the array as it was when captured: it is valid only until
+ * a call with another (n, batch). The first call on a device looks up the array's address; make it before any
+ * stream capture. */
 crdfft_status crdfft_execute_static_scratch(const void* in, void* out, int64_t n, int64_t batch, int32_t direction,
                                             void* stream);
 
@@ -357,8 +363,16 @@ crdfft_status crdfft_execute_static_scratch(const void* in, void* out, int64_t n
 /* The device known-answer check (the role of the reference's fft_self_check, src/fft_self_check.cpp:153-211):
  * runs a set of small transforms (radices 2..16, 3, 5, 7, a four-step and a real transform) on the current device
  * and compares them with a host FP64 DFT: max|gpu - dft| <= 1e-5 (1 + max|dft|). CRDFFT_OK or
- * CRDFFT_NUMERIC_SELFCHECK. */
+ * CRDFFT_NUMERIC_SELFCHECK. The library also runs it once per device at the first plan creation there, as the
+ * reference checks its kernel table before first use (src/fft_kernel_dispatch.cpp:48-52): if it disagrees, that
+ * creation and every later one on the device return CRDFFT_NUMERIC_SELFCHECK. CRDFFT_SELF_CHECK=0 in the environment
+ * turns the first-use check off; crdfft_execute_static_scratch (which allocates nothing) does not run it. */
 crdfft_status crdfft_self_check(void);
+
+/* Test hooks for the first-use check: plant a mistake in the check's host FP64 answers (on: every comparison
+ * disagrees), and forget which devices were checked, so the next plan creation checks again. */
+void crdfft_debug_self_check_mismatch(int32_t on);
+void crdfft_debug_self_check_reset(void);
 
 /* Test hook: make the k-th device allocation from now fail (k >= 1), as if the device were out of memory; 0 turns
  * it off. The reference tests its out-of-memory paths with a refusing allocator in a child process

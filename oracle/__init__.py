@@ -188,6 +188,19 @@ def nd64(x, inverse: bool = False) -> np.ndarray:
     return a
 
 
+def nd64_axes(x) -> np.ndarray:
+    """Forward FP64 N-D FFT of a large array, axis by axis with the oracle's threaded batch FFT (fft64): the
+    row-column order of NdFftPlan::execute (nd_fft.hpp:105-182, one batch of lines per axis, last axis first),
+    for shapes whose strided single-threaded walk (nd64) would take minutes. Forward only, unnormalised."""
+    a = _c128(x)
+    for ax in range(a.ndim - 1, -1, -1):
+        if a.shape[ax] < 2:
+            continue
+        moved = np.ascontiguousarray(np.moveaxis(a, ax, -1))
+        a = np.moveaxis(fft64(moved), -1, ax)
+    return np.ascontiguousarray(a)
+
+
 # ---- metrics -----------------------------------------------------------------------------------------------------
 
 

@@ -17,7 +17,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit(f"usage: python {os.path.basename(__file__)} <reference checkout>")
+REF = sys.argv[1]
 SRC = os.path.join(REF, "tests", "numerics", "hesap-dsp", "spectral_refs.inc")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "spectral_refs.npz")
 

@@ -214,6 +214,31 @@ def test_device_self_check():
     cf.self_check()
 
 
+def test_self_check_gates_first_plan_creation():
+    """The known-answer check runs at the first plan creation on a device (the reference checks its kernel table
+    before first use, src/fft_kernel_dispatch.cpp:48-52). With a mistake planted in the check's host answers (on the
+    CPU), that creation and every later one on the device return CRDFFT_NUMERIC_SELFCHECK; once the device is
+    re-checked with correct answers, plans are created again."""
+    from crd_b200 import _lib
+
+    L = _lib.lib()
+    try:
+        L.crdfft_debug_self_check_reset()
+        L.crdfft_debug_self_check_mismatch(1)
+        with pytest.raises(_lib.CrdFftError) as e:
+            cf.Plan([1024], batch=2)
+        assert e.value.status == _lib.NUMERIC_SELFCHECK
+        L.crdfft_debug_self_check_mismatch(0)
+        with pytest.raises(_lib.CrdFftError) as e:  # the verdict sticks for the device
+            cf.Plan([64], batch=2)
+        assert e.value.status == _lib.NUMERIC_SELFCHECK
+    finally:
+        L.crdfft_debug_self_check_mismatch(0)
+        L.crdfft_debug_self_check_reset()
+    x, got, plan = _c2c(1024, 2, False)
+    _check(got, oracle.fft64(x), 1024)
+
+
 def test_run_twice_bit_identical_and_in_place():
     """Fixed schedules, no atomics: two runs give the same bits; in-place equals out-of-place."""
     for n, batch in ((1024, 64), (65536, 3), (107520, 2)):

@@ -126,6 +126,13 @@ def test_nd_restatement(golden):
         assert oracle.max_rel(golden[f"nd_{tag}_inv"], i) < 2e-4
 
 
+def test_nd_axes_matches_strided_oracle():
+    """The axis-by-axis N-D oracle used at the benchmark shapes agrees with the strided restatement (nd64)."""
+    for dims in ((8, 16), (4, 6, 5), (16, 12), (32, 8, 64)):
+        x = oracle.lcg_complex64(0xA0 + len(dims), int(np.prod(dims))).reshape(dims)
+        np.testing.assert_allclose(oracle.nd64_axes(x), oracle.nd64(x), rtol=0, atol=1e-10)
+
+
 def test_lcg_matches_reference_rule():
     """test_fft.cpp:31-44: first draws of the seed-0 stream, computed by hand."""
     s = 0
