@@ -5,15 +5,15 @@ package is the Python mirror of the reference's plan classes over that ABI (``cr
 """
 
 from .hesap import (BluesteinPlan, ConvPlan, CwtPlan, FftPlan, Forward, Inverse, NdFftPlan, Plan, RealFftPlan,
-                    SpectralPlan, UnevenPlan, cwt, cwt_fft_length, cwt_frequencies, fft, ifft_normalized, periodogram,
-                    self_check, spectrogram, uneven_offsets, welch_psd)
+                    SpectralPlan, UnevenPlan, cwt, cwt_fft_length, cwt_frequencies, fft, ifft_normalized,
+                    lower_tensor_fft, periodogram, self_check, spectrogram, uneven_offsets, welch_psd)
 from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP16_SCALED, PREC_FP32,
                    PREC_SPLIT_BF16, R2C, SPECTRAL_PERIODOGRAM, SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError)
 
 __all__ = [
     "BluesteinPlan", "ConvPlan", "FftPlan", "NdFftPlan", "Plan", "RealFftPlan", "SpectralPlan", "UnevenPlan", "fft",
     "ifft_normalized", "self_check", "uneven_offsets", "welch_psd", "spectrogram", "periodogram", "CwtPlan", "cwt",
-    "cwt_fft_length", "cwt_frequencies",
+    "cwt_fft_length", "cwt_frequencies", "lower_tensor_fft",
     "SPECTRAL_WELCH", "SPECTRAL_SPECTROGRAM", "SPECTRAL_PERIODOGRAM",
     "Forward", "Inverse", "C2C", "R2C", "C2R", "FORWARD", "INVERSE", "NORM_NONE", "NORM_INVERSE", "PREC_FP32",
     "PREC_SPLIT_BF16", "PREC_FP16_SCALED", "CrdFftError",

@@ -88,6 +88,8 @@ EXPORTS = (
     "crdfft_wisdom_forget",
     "crdfft_planner_log",
     "crdfft_execute_static_scratch",
+    "crdfft_execute_planar",
+    "crdfft_ceir_fft_desc",
     "crdfft_plan_create_uneven",
     "crdfft_uneven_offsets",
     "crdfft_pass_feature_count",
@@ -123,6 +125,25 @@ class Desc(ctypes.Structure):
         ("ostride", ctypes.c_int64),
         ("odist", ctypes.c_int64),
     ]
+
+
+class CeirFftOp(ctypes.Structure):
+    """crdfft_ceir_fft_op: what the reference's GPU provider knows about a CEIR tensor.fft op."""
+
+    _fields_ = [
+        ("num_operands", ctypes.c_int32),
+        ("num_results", ctypes.c_int32),
+        ("operand_is_tensor", ctypes.c_int32),
+        ("element_is_f32", ctypes.c_int32),
+        ("rank", ctypes.c_int32),
+        ("axis", ctypes.c_int32),
+        ("shape", ctypes.c_int64 * 8),
+        ("direction", ctypes.c_char_p),
+    ]
+
+
+CEIR_REJECT = {0: "none", 1: "op-not-supported", 2: "operand-not-tensor", 3: "element-not-f32",
+               4: "rank-unsupported", 5: "shape-not-static", 6: "direction-unknown", 7: "axis-unsupported"}
 
 
 class SpectralDesc(ctypes.Structure):
@@ -220,6 +241,9 @@ def lib():
         "crdfft_wisdom_forget": ([], None),
         "crdfft_planner_log": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
         "crdfft_execute_static_scratch": ([vp, vp, i64, i64, i32, vp], i32),
+        "crdfft_execute_planar": ([vp, vp, vp, vp, vp, i32, vp], i32),
+        "crdfft_ceir_fft_desc": ([ctypes.POINTER(CeirFftOp), ctypes.POINTER(Desc), ctypes.POINTER(i32),
+                                  ctypes.POINTER(i32)], i32),
         "crdfft_plan_create_uneven": ([ctypes.POINTER(i64), i64, ctypes.POINTER(i64), pp], i32),
         "crdfft_uneven_offsets": ([ctypes.POINTER(i64), i64, ctypes.POINTER(i64)], i64),
         "crdfft_pass_feature_count": ([], i32),

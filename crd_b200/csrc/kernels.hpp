@@ -178,5 +178,7 @@ cudaError_t launch_cwt_lines(const PassDesc& d, const void* X, const void* K, co
 
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);
+cudaError_t launch_planar_gather(const void* re, const void* im, void* out, long long count, cudaStream_t stream);
+cudaError_t launch_planar_scatter(const void* in, void* re, void* im, long long count, cudaStream_t stream);
 
 } // namespace crdfft

@@ -289,6 +289,9 @@ struct Plan
     };
     HostPipe* host = nullptr;
     std::mutex host_mu;
+    // Split-complex execute (crdfft_execute_planar): the interleaved staging buffer, made by the first call.
+    void* planar = nullptr;
+    std::mutex planar_mu;
     bool conv = false; // fused convolution plan (crdfft_conv_plan_create): executes with a filter spectrum
     bool spectral = false; // spectral estimator plan (crdfft_spectral_plan_create)
     // Radix-32 schedules for the lengths that have them (FP32 unit-stride passes); off for the tensor-core precision
@@ -330,6 +333,8 @@ struct Plan
         }
         if (fork != nullptr)
             cudaEventDestroy(fork);
+        if (planar != nullptr)
+            cudaFree(planar);
         for (auto& kv : batched)
             delete kv.second;
         if (arena_backed)
@@ -2426,6 +2431,52 @@ crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32
         (p.desc.kind == CRDFFT_C2R && direction != CRDFFT_INVERSE))
         return CRDFFT_INVALID_ARG;
     return run(p, in, out, direction, static_cast<cudaStream_t>(stream));
+}
+
+crdfft_status crdfft_execute_planar(crdfft_plan* plan, const float* re_in, const float* im_in, float* re_out,
+                                    float* im_out, int32_t direction, void* stream)
+{
+    if (plan == nullptr || re_in == nullptr || im_in == nullptr || re_out == nullptr || im_out == nullptr)
+        return CRDFFT_INVALID_ARG;
+    Plan& p = *as_plan(plan);
+    const crdfft_desc& d = p.desc;
+    if (p.conv || p.spectral || p.uneven || d.kind != CRDFFT_C2C)
+        return CRDFFT_INVALID_ARG;
+    if (direction != CRDFFT_FORWARD && direction != CRDFFT_INVERSE)
+        return CRDFFT_INVALID_ARG;
+    long long total = 1;
+    for (int i = 0; i < d.rank; ++i)
+        total *= d.dims[i];
+    // The planes are gathered and scattered whole, so the transforms must tile them exactly: packed batches
+    // (stride 1, distance prod(dims)) or, for rank 1, the element-major batch (stride batch, distance 1).
+    const bool packed = (d.istride == 0 || d.istride == 1) && (d.ostride == 0 || d.ostride == 1) &&
+                        (d.idist == 0 || d.idist == total) && (d.odist == 0 || d.odist == total);
+    const bool element_major = d.rank == 1 && d.istride == d.batch && d.ostride == d.batch && d.idist == 1 &&
+                               d.odist == 1;
+    if (!packed && !element_major)
+        return CRDFFT_INVALID_ARG;
+    const long long count = total * d.batch;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    {
+        std::lock_guard<std::mutex> lk(p.planar_mu);
+        if (p.planar == nullptr)
+        {
+            int dev = -1;
+            if (cudaGetDevice(&dev) != cudaSuccess || dev != p.device)
+                return CRDFFT_NO_DEVICE;
+            if (dev_alloc(&p.planar, static_cast<size_t>(count) * 8) != cudaSuccess)
+            {
+                p.planar = nullptr;
+                return CRDFFT_OOM;
+            }
+        }
+    }
+    if (launch_planar_gather(re_in, im_in, p.planar, count, s) != cudaSuccess)
+        return CRDFFT_LAUNCH;
+    const crdfft_status st = run(p, p.planar, p.planar, direction, s);
+    if (st != CRDFFT_OK)
+        return st;
+    return launch_planar_scatter(p.planar, re_out, im_out, count, s) == cudaSuccess ? CRDFFT_OK : CRDFFT_LAUNCH;
 }
 
 namespace

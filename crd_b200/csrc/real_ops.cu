@@ -213,6 +213,43 @@ cudaError_t launch_chirp_post(const ChirpDesc& p, const void* w, void* x, cudaSt
     return cudaGetLastError();
 }
 
+// Split-complex (planar) operands: the re and im planes of `count` complex values to interleaved pairs, and back.
+// Streaming, one element a thread per iteration, both sides coalesced.
+__global__ void planar_gather_kernel(const float* __restrict__ re, const float* __restrict__ im, float2* out,
+                                     long long count)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+        __stcs(out + i, make_float2(__ldcs(re + i), __ldcs(im + i)));
+}
+
+__global__ void planar_scatter_kernel(const float2* __restrict__ in, float* re, float* im, long long count)
+{
+    for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < count;
+         i += static_cast<long long>(gridDim.x) * blockDim.x)
+    {
+        const float2 v = __ldcs(in + i);
+        __stcs(re + i, v.x);
+        __stcs(im + i, v.y);
+    }
+}
+
+cudaError_t launch_planar_gather(const void* re, const void* im, void* out, long long count, cudaStream_t stream)
+{
+    planar_gather_kernel<<<grid_for(count, 256), 256, 0, stream>>>(static_cast<const float*>(re),
+                                                                    static_cast<const float*>(im),
+                                                                    static_cast<float2*>(out), count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planar_scatter(const void* in, void* re, void* im, long long count, cudaStream_t stream)
+{
+    planar_scatter_kernel<<<grid_for(count, 256), 256, 0, stream>>>(static_cast<const float2*>(in),
+                                                                     static_cast<float*>(re),
+                                                                     static_cast<float*>(im), count);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream)
 {
     scale_kernel<<<grid_for(count, 256), 256, 0, stream>>>(static_cast<float2*>(data), count, s);

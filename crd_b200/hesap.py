@@ -27,9 +27,9 @@ from typing import Iterable, Optional, Sequence
 import torch
 
 from . import _lib
-from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP32, R2C, SPECTRAL_PERIODOGRAM,
-                   SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError, CwtDesc, Desc, SpectralDesc,
-                   PlanInfo, check, lib)
+from ._lib import (C2C, C2R, CEIR_REJECT, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP32, R2C,
+                   SPECTRAL_PERIODOGRAM, SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CeirFftOp, CrdFftError, CwtDesc, Desc,
+                   SpectralDesc, PlanInfo, check, lib)
 
 Forward = FORWARD
 Inverse = INVERSE
@@ -133,6 +133,16 @@ class Plan(_Handle):
         check(lib().crdfft_execute(self._h, pi, po, _dir(direction), _stream(stream)), "execute")
         return out
 
+    def execute_planar(self, re_in: torch.Tensor, im_in: torch.Tensor, re_out: torch.Tensor, im_out: torch.Tensor,
+                       direction=FORWARD, stream=None):
+        """Run a C2C plan on split-complex planes (crdfft_execute_planar): float32 device tensors, one per part."""
+        if self.kind != C2C:
+            raise ValueError("planar operands are for complex-to-complex plans")
+        ptrs = [_ptr(t, torch.float32, what) for t, what in
+                ((re_in, "re_in"), (im_in, "im_in"), (re_out, "re_out"), (im_out, "im_out"))]
+        check(lib().crdfft_execute_planar(self._h, *ptrs, _dir(direction), _stream(stream)), "execute_planar")
+        return re_out, im_out
+
     def execute_host(self, inp: torch.Tensor, out: torch.Tensor, direction=FORWARD, stream=None) -> torch.Tensor:
         """Run on HOST tensors (pinned for overlap; crdfft_execute_host): chunked copies in and out overlap the
         transforms on the GPU. Synchronise `stream` (default: the current stream) before reading `out`."""
@@ -144,6 +154,29 @@ class Plan(_Handle):
         check(lib().crdfft_execute_host(self._h, inp.data_ptr(), out.data_ptr(), _dir(direction), _stream(stream)),
               "execute_host")
         return out
+
+
+def lower_tensor_fft(shape, direction, axis: int = -1, element_f32: bool = True, operand_is_tensor: bool = True,
+                     num_operands: int = 2, num_results: int = 2) -> dict:
+    """The CEIR tensor.fft lowering (crdfft_ceir_fft_desc): the plan descriptor fields and the direction for an op
+    on split-complex tensors of `shape` (a dynamic extent as -1). Raises CrdFftError with the reject reason in its
+    message when the op is outside the envelope; host only."""
+    op = CeirFftOp()
+    op.num_operands, op.num_results = num_operands, num_results
+    op.operand_is_tensor, op.element_is_f32 = int(operand_is_tensor), int(element_f32)
+    op.rank = len(shape)
+    op.axis = axis
+    for i, v in enumerate(list(shape)[:8]):
+        op.shape[i] = int(v)
+    op.direction = direction.encode() if isinstance(direction, str) else None
+    d = Desc()
+    dr = ctypes.c_int32()
+    why = ctypes.c_int32()
+    st = lib().crdfft_ceir_fft_desc(ctypes.byref(op), ctypes.byref(d), ctypes.byref(dr), ctypes.byref(why))
+    if st != 0:
+        raise CrdFftError(st, f"tensor.fft not lowered: {CEIR_REJECT.get(why.value, why.value)}")
+    return {"dims": [int(d.dims[0])], "batch": int(d.batch), "istride": int(d.istride), "idist": int(d.idist),
+            "ostride": int(d.ostride), "odist": int(d.odist), "norm": int(d.norm), "direction": int(dr.value)}
 
 
 class ConvPlan(_Handle):

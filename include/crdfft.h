@@ -126,6 +126,17 @@ crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32
  * must not overlap. Uneven-batch plans are not supported (CRDFFT_INVALID_ARG). */
 crdfft_status crdfft_execute_host(crdfft_plan* plan, const void* in, void* out, int32_t direction, void* stream);
 
+/* Run a C2C plan on split-complex (planar) operands: separate re and im planes of float, each laid out as the
+ * plan's descriptor says for complex elements (in == out planes allowed). The layouts whose transforms tile the
+ * planes exactly are accepted: packed batches, and the rank-1 element-major batch (istride = ostride = batch,
+ * idist = odist = 1); others return CRDFFT_INVALID_ARG. The split-complex tensors of the reference's CEIR
+ * `tensor.fft` op (operands re_in, im_in; results re_out, im_out; engine/execution/ceir-gpu/src/ckir_synth.cpp:331)
+ * and of its CKIR FFT kernels (engine/gpu/kir/include/crd/kir/ckir_fft.hpp:61-66) take this entry point. The planes
+ * are interleaved into a staging buffer the plan allocates at its first planar call (prod(dims) * batch * 8 bytes),
+ * transformed there in place and split again: two streaming passes around the plan's own. */
+crdfft_status crdfft_execute_planar(crdfft_plan* plan, const float* re_in, const float* im_in, float* re_out,
+                                    float* im_out, int32_t direction, void* stream);
+
 crdfft_status crdfft_plan_info_get(const crdfft_plan* plan, crdfft_plan_info* info);
 
 /* Bytes of scratch one execute of this plan uses (0 when it needs none). */
@@ -338,6 +349,48 @@ crdfft_status crdfft_mlp_gradients(int32_t in_dim, int32_t hidden, const float* 
 /* One Adam step (bias-corrected moments, step >= 1) over count parameters. */
 crdfft_status crdfft_mlp_adam(float* params, const float* grad, float* m, float* v, int64_t count, int32_t step,
                               float lr, float beta1, float beta2, float eps, void* stream);
+
+/* ---- The CEIR tensor.fft lowering -------------------------------------------------------------------------- */
+
+/* What the reference's GPU provider knows about a `tensor.fft` op when it lowers it (synth_fft,
+ * engine/execution/ceir-gpu/src/ckir_synth.cpp:318-366; the op contract, engine/execution/ceir/src/tensor.cpp:174-192,
+ * 344). The provider fills it from the op and its operand re_in. */
+#define CRDFFT_CEIR_MAX_RANK 8
+typedef struct crdfft_ceir_fft_op
+{
+    int32_t num_operands;      /* the op's operand count (re_in, im_in) */
+    int32_t num_results;       /* the op's result count (re_out, im_out) */
+    int32_t operand_is_tensor; /* re_in is Tensor-kinded */
+    int32_t element_is_f32;    /* re_in's element type is f32 */
+    int32_t rank;              /* rank of re_in's shape */
+    int32_t axis;              /* the `axis` attribute; -1 when absent (the innermost axis) */
+    int64_t shape[CRDFFT_CEIR_MAX_RANK]; /* static extents; a dynamic extent as -1 */
+    const char* direction;     /* the `direction` attribute's string, NULL when it is not a string */
+} crdfft_ceir_fft_op;
+
+/* Why an op was not lowered. The first six have the reference's SynthReject names (OpNotSupported,
+ * OperandNotTensor, ElementNotF32, FftRankUnsupported, ShapeNotStatic, FftDirectionUnknown); its FftLengthNotPow2
+ * does not occur here: every static length >= 1 is planned. */
+typedef enum crdfft_ceir_reject
+{
+    CRDFFT_CEIR_NONE = 0,
+    CRDFFT_CEIR_OP_NOT_SUPPORTED = 1,
+    CRDFFT_CEIR_OPERAND_NOT_TENSOR = 2,
+    CRDFFT_CEIR_ELEMENT_NOT_F32 = 3,
+    CRDFFT_CEIR_RANK_UNSUPPORTED = 4,
+    CRDFFT_CEIR_SHAPE_NOT_STATIC = 5,
+    CRDFFT_CEIR_DIRECTION_UNKNOWN = 6,
+    CRDFFT_CEIR_AXIS_UNSUPPORTED = 7
+} crdfft_ceir_reject;
+
+/* Map a tensor.fft op to a plan descriptor and a direction (host only, no device needed). The transform runs along
+ * `axis`: the innermost axis of any rank (batch = product of the other extents, packed) or axis 0 of a rank-2
+ * tensor (the element-major batch); FP32, unnormalised both ways like the op (the 1/N is the caller's,
+ * engine/gpu/kir/include/crd/kir/ckir_fft.hpp:21). The plan then runs with crdfft_execute_planar on the op's four
+ * planes. On a rejection *reject says why (the status is CRDFFT_INVALID_DESC or CRDFFT_UNSUPPORTED_SIZE) and the
+ * provider keeps its own path for the op. */
+crdfft_status crdfft_ceir_fft_desc(const crdfft_ceir_fft_op* op, crdfft_desc* desc, int32_t* direction,
+                                   int32_t* reject);
 
 /* ---- Without device allocation ----------------------------------------------------------------------------- */
 
