@@ -83,6 +83,7 @@ EXPORTS = (
     "crdfft_device_status",
     "crdfft_debug_stall_waits",
     "crdfft_set_planner_mode",
+    "crdfft_set_decomposition",
     "crdfft_wisdom_export",
     "crdfft_wisdom_import",
     "crdfft_wisdom_forget",
@@ -236,6 +237,7 @@ def lib():
         "crdfft_device_status": ([vp, vp], i32),
         "crdfft_debug_stall_waits": ([i32], None),
         "crdfft_set_planner_mode": ([i32], None),
+        "crdfft_set_decomposition": ([i64, i32, i64], i32),
         "crdfft_wisdom_export": ([ctypes.c_char_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)], i32),
         "crdfft_wisdom_import": ([ctypes.c_char_p], i32),
         "crdfft_wisdom_forget": ([], None),

@@ -4,6 +4,7 @@
 
 #include "kernels.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <mutex>
@@ -26,9 +27,12 @@ struct Model
     std::vector<float> params;      // [W1 H x D][b1 H][W2 H x H][b2 H][W3 H][b3]
 };
 
+// Two models: slot 0 ranks a pass's launch shapes ("crdfft-mlp 1"), slot 1 a transform's decompositions
+// ("crdfft-mlp-decomp 1").
 std::mutex g_mu;
-Model g_model;
-bool g_ready = false;
+Model g_models[2];
+bool g_ready[2] = {false, false};
+const char* const kTags[2] = {"crdfft-mlp", "crdfft-mlp-decomp"};
 
 size_t param_count(int d, int h) { return static_cast<size_t>(h) * d + h + static_cast<size_t>(h) * h + h + h + 1; }
 
@@ -91,12 +95,14 @@ void pass_features(const PassDesc& d, const PassShape& sh, float* f)
     f[31] = 1.0f;
 }
 
-int learned_import(const std::string& text)
+namespace
 {
-    std::istringstream in(text);
-    std::string tag;
+
+// Parses one model from `in` (its tag already read); 0 or -1.
+int parse_model(std::istream& in, Model* out)
+{
     int version = 0;
-    if (!(in >> tag >> version) || tag != "crdfft-mlp" || version != 1)
+    if (!(in >> version) || version != 1)
         return -1;
     Model m;
     std::string w;
@@ -124,36 +130,32 @@ int learned_import(const std::string& text)
     for (float& v : m.params)
         if (!(in >> v) || !std::isfinite(v))
             return -1;
-    std::lock_guard<std::mutex> lk(g_mu);
-    g_model = std::move(m);
-    g_ready = true;
+    *out = std::move(m);
     return 0;
 }
 
-std::string learned_export()
+std::string export_model(int slot)
 {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_ready)
-        return std::string();
+    const Model& m = g_models[slot];
     std::ostringstream o;
     char buf[32];
     auto put = [&](float v) {
         std::snprintf(buf, sizeof(buf), " %.9g", static_cast<double>(v));
         o << buf;
     };
-    o << "crdfft-mlp 1\ndims " << g_model.in_dim << ' ' << g_model.hidden << "\nmean";
-    for (float v : g_model.mean)
+    o << kTags[slot] << " 1\ndims " << m.in_dim << ' ' << m.hidden << "\nmean";
+    for (float v : m.mean)
         put(v);
     o << "\nstd";
-    for (float v : g_model.stdev)
+    for (float v : m.stdev)
         put(v);
     o << "\ntarget";
-    put(g_model.t_mean);
-    put(g_model.t_std);
-    o << "\nparams " << g_model.params.size() << '\n';
-    for (size_t i = 0; i < g_model.params.size(); ++i)
+    put(m.t_mean);
+    put(m.t_std);
+    o << "\nparams " << m.params.size() << '\n';
+    for (size_t i = 0; i < m.params.size(); ++i)
     {
-        put(g_model.params[i]);
+        put(m.params[i]);
         if (i % 8 == 7)
             o << '\n';
     }
@@ -161,28 +163,12 @@ std::string learned_export()
     return o.str();
 }
 
-bool learned_ready()
-{
-    std::lock_guard<std::mutex> lk(g_mu);
-    return g_ready;
-}
-
-void learned_forget()
-{
-    std::lock_guard<std::mutex> lk(g_mu);
-    g_ready = false;
-    g_model = Model{};
-}
-
 // The forward pass of the same network the device kernels train (mlp.cu), on the host: normalise, two ReLU layers,
 // one linear output, de-normalise.
-float learned_predict(const float* feat)
+float predict_model(const Model& m, const float* feat)
 {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_ready)
-        return 0.0f;
-    const int D = g_model.in_dim, H = g_model.hidden;
-    const float* W1 = g_model.params.data();
+    const int D = m.in_dim, H = m.hidden;
+    const float* W1 = m.params.data();
     const float* b1 = W1 + static_cast<size_t>(H) * D;
     const float* W2 = b1 + H;
     const float* b2 = W2 + static_cast<size_t>(H) * H;
@@ -190,7 +176,7 @@ float learned_predict(const float* feat)
     const float b3 = W3[H];
     std::vector<float> x(D), a1(H), a2(H);
     for (int k = 0; k < D; ++k)
-        x[k] = (feat[k] - g_model.mean[k]) / g_model.stdev[k];
+        x[k] = (feat[k] - m.mean[k]) / m.stdev[k];
     for (int o = 0; o < H; ++o)
     {
         float s = b1[o];
@@ -208,7 +194,133 @@ float learned_predict(const float* feat)
     float y = b3;
     for (int k = 0; k < H; ++k)
         y += W3[k] * a2[k];
-    return g_model.t_mean + g_model.t_std * y;
+    return m.t_mean + m.t_std * y;
+}
+
+} // namespace
+
+// A model text holds one or both models, each introduced by its tag; every model in it must parse, or nothing is
+// imported. A model replaces the one in its slot; the other slot is kept.
+int learned_import(const std::string& text)
+{
+    std::istringstream in(text);
+    std::string tag;
+    Model got[2];
+    bool have[2] = {false, false};
+    while (in >> tag)
+    {
+        int slot = -1;
+        for (int i = 0; i < 2; ++i)
+            if (tag == kTags[i])
+                slot = i;
+        if (slot < 0 || parse_model(in, &got[slot]) != 0)
+            return -1;
+        have[slot] = true;
+    }
+    if (!have[0] && !have[1])
+        return -1;
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (int i = 0; i < 2; ++i)
+        if (have[i])
+        {
+            g_models[i] = std::move(got[i]);
+            g_ready[i] = true;
+        }
+    return 0;
+}
+
+std::string learned_export()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    std::string out;
+    for (int i = 0; i < 2; ++i)
+        if (g_ready[i])
+            out += export_model(i);
+    return out;
+}
+
+bool learned_ready()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_ready[0];
+}
+
+bool learned_decomp_ready()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_ready[1];
+}
+
+void learned_forget()
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    for (int i = 0; i < 2; ++i)
+    {
+        g_ready[i] = false;
+        g_models[i] = Model{};
+    }
+}
+
+float learned_predict(const float* feat)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_ready[0] ? predict_model(g_models[0], feat) : 0.0f;
+}
+
+float learned_decomp_predict(const float* feat)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    return g_ready[1] ? predict_model(g_models[1], feat) : 0.0f;
+}
+
+// Features of a 1-D decomposition choice, all O(1) in magnitude:
+//   0 log2 n              1 log2 batch               2 log2 bytes of input     3-5 single pass / cluster / four-step
+//   6 log2 n1 (columns)   7 log2 n2 (rows)           8 |log2 (n1 / n2)|        9-10 n1, n2 have compile-time schedules
+//   11-17 stages of radix 16, 8, 4, 2, 3, 5, 7 in n1    18-24 the same for n2
+//   25 n2 a multiple of 16 (whole column tiles)      26 unit strides and packed  27 padded distances
+//   28 precision (0 FP32, 1 tensor-core form)        29 waves of the four-step at the default wave size (log2)
+//   30 the column pass takes the tensor-copy kernel  31 1 (bias feature, constant)
+void decomp_features(long long n, int kind, long long n1, long long batch, bool packed_unit, bool padded,
+                     int precision, const int* r1, int s1, const int* r2, int s2, bool stat1, bool stat2,
+                     bool tma_col, float* f)
+{
+    for (int i = 0; i < kPassFeatures; ++i)
+        f[i] = 0.0f;
+    const long long n2 = kind == 3 ? n / n1 : 1;
+    const long long a = kind == 3 ? n1 : n;
+    f[0] = lg2(static_cast<double>(n));
+    f[1] = lg2(static_cast<double>(batch));
+    f[2] = lg2(8.0 * static_cast<double>(n) * static_cast<double>(batch));
+    f[3 + (kind == 1 ? 0 : kind == 2 ? 1 : 2)] = 1.0f;
+    f[6] = lg2(static_cast<double>(a));
+    f[7] = lg2(static_cast<double>(n2));
+    f[8] = std::fabs(f[6] - f[7]);
+    f[9] = stat1 ? 1.0f : 0.0f;
+    f[10] = stat2 ? 1.0f : 0.0f;
+    auto count = [&](const int* r, int s, int at) {
+        for (int i = 0; i < s; ++i)
+            switch (r[i])
+            {
+                case 16: f[at + 0] += 1; break;
+                case 8: f[at + 1] += 1; break;
+                case 4: f[at + 2] += 1; break;
+                case 2: f[at + 3] += 1; break;
+                case 3: f[at + 4] += 1; break;
+                case 5: f[at + 5] += 1; break;
+                case 7: f[at + 6] += 1; break;
+                default: break;
+            }
+    };
+    count(r1, s1, 11);
+    count(r2, s2, 18);
+    f[25] = (kind == 3 && n2 % 16 == 0) ? 1.0f : 0.0f;
+    f[26] = packed_unit ? 1.0f : 0.0f;
+    f[27] = padded ? 1.0f : 0.0f;
+    f[28] = precision != 0 ? 1.0f : 0.0f;
+    f[29] = kind == 3 ? lg2(std::max(1.0, 8.0 * n * static_cast<double>(batch) / static_cast<double>(512 << 20)))
+                      : 0.0f;
+    f[30] = tma_col ? 1.0f : 0.0f;
+    f[31] = 1.0f;
 }
 
 } // namespace crdfft

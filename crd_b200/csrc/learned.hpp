@@ -26,4 +26,14 @@ void learned_forget();
 // Predicted log(ms) of the whole pass.
 float learned_predict(const float* feat);
 
+// The decomposition model (a second model in the same text, tag "crdfft-mlp-decomp"): the predicted log(ms) of a
+// whole 1-D transform batch under a decomposition (single pass, cluster four-step, or two-pass four-step n1 x n2).
+bool learned_decomp_ready();
+float learned_decomp_predict(const float* feat);
+// Feature vector of a decomposition (kind 1 single pass, 2 cluster, 3 four-step with columns of n1); radices of the
+// two line lengths r1[s1], r2[s2]; layout documented at the definition (learned.cpp).
+void decomp_features(long long n, int kind, long long n1, long long batch, bool packed_unit, bool padded,
+                     int precision, const int* r1, int s1, const int* r2, int s2, bool stat1, bool stat2,
+                     bool tma_col, float* f);
+
 } // namespace crdfft

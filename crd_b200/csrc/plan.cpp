@@ -581,6 +581,9 @@ std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl,
     return out;
 }
 
+int learned_top_k();
+bool tma_col_enabled();
+
 // The planner's choice of launch shape for a pass: remembered wisdom for its geometry class if any; else, in
 // measure mode, the fastest of the timed candidates (remembered); else the heuristic.
 bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* out)
@@ -601,24 +604,41 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
     const int mode = planner_mode();
     if (mode == kPlannerLearned && learned_ready())
     {
-        // rank the candidates by predicted time; nothing is timed and nothing is remembered
+        // The model ranks the candidates; its top proposals (learned_top_k) are then timed and the fastest is kept
+        // and remembered: the measuring planner judges what the model proposes. From an arena (nothing may be
+        // allocated) or with a top-k of 1, the model's first choice stands untimed.
         const std::vector<PassShape> cands = candidate_shapes(d, map, dl, ds);
-        int best = -1;
-        float best_t = 0.0f;
+        std::vector<std::pair<float, int>> ranked;
         for (size_t i = 0; i < cands.size(); ++i)
         {
             float f[kPassFeatures];
             pass_features(d, cands[i], f);
-            const float t = learned_predict(f);
-            if (best < 0 || t < best_t)
+            ranked.emplace_back(learned_predict(f), static_cast<int>(i));
+        }
+        std::sort(ranked.begin(), ranked.end());
+        const int k = std::min<int>(learned_top_k(), static_cast<int>(ranked.size()));
+        if (k >= 2 && t_arena == nullptr)
+        {
+            std::vector<PassShape> top;
+            for (int i = 0; i < k; ++i)
+                top.push_back(cands[ranked[i].second]);
+            std::vector<float> ms;
+            const int best = measure_shapes(d, key, top, &ms, 0);
+            if (best >= 0)
             {
-                best = static_cast<int>(i);
-                best_t = t;
+                WisdomEntry e;
+                e.pipelined = top[best].pipelined;
+                e.points_per_thread = top[best].points_per_thread;
+                e.lines_per_cta = top[best].lines_per_cta;
+                e.ms = ms[best];
+                wisdom_store(key, e);
+                *out = top[best];
+                return true;
             }
         }
-        if (best >= 0)
+        if (!ranked.empty())
         {
-            *out = cands[best];
+            *out = cands[ranked[0].second];
             return true;
         }
     }
@@ -647,6 +667,251 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
         }
     }
     return heuristic_shape(d, map, dl, ds, out);
+}
+
+// How many of the learned model's top proposals the measuring planner times (CRDFFT_LEARNED_TOP_K, default 2).
+int learned_top_k()
+{
+    static const int k = [] {
+        const char* e = std::getenv("CRDFFT_LEARNED_TOP_K");
+        const int v = e != nullptr ? std::atoi(e) : 2;
+        return v < 1 ? 1 : v;
+    }();
+    return k;
+}
+
+// ---- Decomposition of a 1-D transform --------------------------------------------------------------------------
+//
+// kind 1: one pass (n <= 8192, or 16384); 2: the cluster four-step (one launch, DSMEM transpose); 3: the two-pass
+// four-step with columns of n1 and rows of n / n1. The rule (estimate mode) is the size rule of the plan's header;
+// measure mode times every candidate on the device (a plan of a sample of the batch with that decomposition forced,
+// executed cold); learned mode ranks the candidates with the decomposition model and times only its top proposals.
+// The choice is remembered as decomposition wisdom.
+struct Decomp
+{
+    int kind = 0;
+    long long n1 = 0;
+};
+
+thread_local const Decomp* t_forced = nullptr; // the decomposition a timing plan is built with
+thread_local long long t_forced_n = 0;
+std::mutex g_hint_mu;
+std::map<long long, Decomp> g_hints; // crdfft_set_decomposition: per-length overrides
+
+bool cluster_ok(const Plan& p, long long n, long long istride, long long idist, long long ostride, long long odist)
+{
+    long long a = 0, b = 0;
+    return istride == 1 && ostride == 1 && idist == n && odist == n && std::getenv("CRDFFT_NO_CLUSTER") == nullptr &&
+           p.desc.precision == CRDFFT_PREC_FP32 && cluster_split(n, &a, &b);
+}
+
+Decomp rule_decomp(const Plan& p, long long n, long long istride, long long idist, long long ostride, long long odist)
+{
+    if (single_pass_ok(n))
+        return Decomp{1, 0};
+    if (cluster_ok(p, n, istride, idist, ostride, odist))
+        return Decomp{2, 0};
+    long long n1 = 0, n2 = 0;
+    if (four_step_split(n, &n1, &n2))
+        return Decomp{3, n1};
+    return Decomp{0, 0};
+}
+
+bool decomp_valid(const std::vector<Decomp>& cands, const Decomp& d)
+{
+    for (const Decomp& c : cands)
+        if (c.kind == d.kind && (c.kind != 3 || c.n1 == d.n1))
+            return true;
+    return false;
+}
+
+std::vector<Decomp> decomp_candidates(const Plan& p, long long n, long long istride, long long idist,
+                                      long long ostride, long long odist)
+{
+    std::vector<Decomp> out;
+    if (single_pass_ok(n))
+        out.push_back(Decomp{1, 0});
+    if (cluster_ok(p, n, istride, idist, ostride, odist))
+        out.push_back(Decomp{2, 0});
+    // Four-step splits: those whose two line lengths both have compile-time schedules (the run-time schedule is
+    // slower), and when there are fewer than two of those, also the four splits closest to square; the rule's own
+    // split is always among them.
+    if (n >= 2048 && n < (1LL << 31))
+    {
+        std::vector<std::pair<double, long long>> other;
+        for (long long a = 16; a * 16 <= n; ++a)
+        {
+            if (n % a != 0 || !single_pass_ok(a) || !single_pass_ok(n / a))
+                continue;
+            if (has_static_schedule(a) && has_static_schedule(n / a))
+                out.push_back(Decomp{3, a});
+            else
+                other.emplace_back(std::fabs(std::log(static_cast<double>(a) * a / static_cast<double>(n))), a);
+        }
+        std::sort(other.begin(), other.end());
+        const size_t nstat = out.size() - (single_pass_ok(n) ? 1 : 0);
+        if (nstat < 2)
+            for (size_t i = 0; i < other.size() && i < 4; ++i)
+                out.push_back(Decomp{3, other[i].second});
+        long long r1 = 0, r2 = 0;
+        if (four_step_split(n, &r1, &r2) && !decomp_valid(out, Decomp{3, r1}))
+            out.push_back(Decomp{3, r1});
+    }
+    return out;
+}
+
+void radix_list(long long n, std::vector<int>& r)
+{
+    r.clear();
+    radices_for(n, r);
+}
+
+void decomp_feature_vector(const Plan& p, long long n, const Decomp& c, long long batch, bool packed_unit,
+                           bool padded, float* f)
+{
+    std::vector<int> r1, r2;
+    const long long a = c.kind == 3 ? c.n1 : n;
+    const long long b = c.kind == 3 ? n / c.n1 : 1;
+    radix_list(a, r1);
+    if (b > 1)
+        radix_list(b, r2);
+    const bool tma = c.kind == 3 && tma_col_enabled() && b % 8 == 0 && (a == 1024 || a == 512);
+    decomp_features(n, c.kind, c.n1, batch, packed_unit, padded, p.desc.precision, r1.data(),
+                    static_cast<int>(r1.size()), r2.data(), static_cast<int>(r2.size()), has_static_schedule(a),
+                    b > 1 && has_static_schedule(b), tma, f);
+}
+
+struct ConvReq;
+crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv, const crdfft_spectral_desc* spec);
+void destroy_plan(Plan* p) { delete p; }
+crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stream, const void* spec);
+
+// Times one decomposition: a plan of `sample` transforms of the same layout with `c` forced, executed cold; the
+// time is scaled to the whole batch. Negative when the plan could not be built or run.
+float time_decomp(const Plan& p, long long n, const Decomp& c, long long batch, long long sample, long long istride,
+                  long long idist, long long ostride, long long odist)
+{
+    crdfft_desc d{};
+    d.rank = 1;
+    d.kind = CRDFFT_C2C;
+    d.precision = p.desc.precision;
+    d.norm = CRDFFT_NORM_NONE;
+    d.dims[0] = n;
+    d.batch = sample;
+    d.istride = istride;
+    d.idist = idist;
+    d.ostride = ostride;
+    d.odist = odist;
+    const Decomp* prev = t_forced;
+    const long long prev_n = t_forced_n;
+    t_forced = &c;
+    t_forced_n = n;
+    Plan* tp = nullptr;
+    const crdfft_status st = create(&d, &tp, nullptr, nullptr);
+    t_forced = prev;
+    t_forced_n = prev_n;
+    if (st != CRDFFT_OK)
+        return -1.0f;
+    const long long in_ext = (sample - 1) * idist + (n - 1) * istride + 1;
+    const long long out_ext = (sample - 1) * odist + (n - 1) * ostride + 1;
+    void* in = nullptr;
+    void* outb = nullptr;
+    float ms = -1.0f;
+    if (cudaMalloc(&in, static_cast<size_t>(in_ext) * 8) == cudaSuccess &&
+        cudaMalloc(&outb, static_cast<size_t>(out_ext) * 8) == cudaSuccess &&
+        cudaMemset(in, 0, static_cast<size_t>(in_ext) * 8) == cudaSuccess)
+    {
+        auto go = [&](cudaStream_t s) {
+            return run(*tp, in, outb, CRDFFT_FORWARD, s, nullptr) == CRDFFT_OK ? cudaSuccess : cudaErrorLaunchFailure;
+        };
+        ms = time_cold(go);
+        if (ms > 0.0f)
+            ms *= static_cast<float>(static_cast<double>(batch) / static_cast<double>(sample));
+    }
+    cudaGetLastError();
+    cudaFree(in);
+    cudaFree(outb);
+    destroy_plan(tp);
+    return ms;
+}
+
+Decomp choose_decomp(const Plan& p, long long n, long long batch, long long istride, long long idist,
+                     long long ostride, long long odist, bool fused_r2c)
+{
+    if (t_forced != nullptr && t_forced_n == n)
+        return *t_forced;
+    const Decomp rule = rule_decomp(p, n, istride, idist, ostride, odist);
+    const std::vector<Decomp> cands = decomp_candidates(p, n, istride, idist, ostride, odist);
+    {
+        std::lock_guard<std::mutex> lk(g_hint_mu);
+        auto it = g_hints.find(n);
+        if (it != g_hints.end() && decomp_valid(cands, it->second))
+            return it->second;
+    }
+    if (fused_r2c || p.desc.precision != CRDFFT_PREC_FP32 || cands.size() <= 1 || t_forced != nullptr)
+        return rule;
+    const bool packed_unit = istride == 1 && ostride == 1 && idist == n && odist == n;
+    const bool padded = (idist != n && idist % 16 != 0) || (odist != n && odist % 16 != 0);
+    const std::string key = decomp_key(n, batch, packed_unit, padded, p.desc.precision);
+    DecompEntry w;
+    if (decomp_lookup(key, &w) && decomp_valid(cands, Decomp{w.kind, w.n1}))
+        return Decomp{w.kind, w.n1};
+    const int mode = planner_mode();
+    if (mode == kPlannerEstimate || t_arena != nullptr)
+        return rule;
+    // the candidates to time: all of them (measure, or learned without a decomposition model), or the model's top k
+    std::vector<std::pair<float, Decomp>> order;
+    for (const Decomp& c : cands)
+    {
+        float f[kPassFeatures];
+        decomp_feature_vector(p, n, c, batch, packed_unit, padded, f);
+        order.emplace_back(mode == kPlannerLearned && learned_decomp_ready() ? learned_decomp_predict(f) : 0.0f, c);
+    }
+    size_t k = order.size();
+    if (mode == kPlannerLearned && learned_decomp_ready())
+    {
+        std::stable_sort(order.begin(), order.end(),
+                         [](const std::pair<float, Decomp>& a, const std::pair<float, Decomp>& b) {
+                             return a.first < b.first;
+                         });
+        k = std::min<size_t>(k, static_cast<size_t>(learned_top_k()));
+        if (k == 1)
+            return order[0].second;
+    }
+    const long long sample = std::max(1LL, std::min(batch, (256LL << 20) / (8 * n)));
+    int best = -1;
+    std::vector<float> ms(k, -1.0f);
+    for (size_t i = 0; i < k; ++i)
+    {
+        ms[i] = time_decomp(p, n, order[i].second, batch, sample, istride, idist, ostride, odist);
+        if (ms[i] > 0.0f && (best < 0 || ms[i] < ms[best]))
+            best = static_cast<int>(i);
+    }
+    for (size_t i = 0; i < k; ++i)
+    {
+        const Decomp& c = order[i].second;
+        float f[kPassFeatures];
+        decomp_feature_vector(p, n, c, batch, packed_unit, padded, f);
+        char buf[256];
+        std::snprintf(buf, sizeof(buf), "%s decomp kind=%d n1=%lld batch=%lld ms=%.6f", key.c_str(), c.kind, c.n1,
+                      batch, static_cast<double>(ms[i]));
+        std::string line = buf;
+        line += " feat=";
+        for (int j = 0; j < kPassFeatures; ++j)
+        {
+            std::snprintf(buf, sizeof(buf), j ? ",%.6g" : "%.6g", static_cast<double>(f[j]));
+            line += buf;
+        }
+        if (static_cast<int>(i) == best)
+            line += " best";
+        if (c.kind == rule.kind && c.n1 == (rule.kind == 3 ? rule.n1 : c.n1))
+            line += " heur";
+        planner_log_append(line);
+    }
+    if (best < 0)
+        return rule;
+    decomp_store(key, DecompEntry{order[best].second.kind, order[best].second.n1, ms[best]});
+    return order[best].second;
 }
 
 // Four-step twiddle of a pass (pass 1 of the four-step), or none.
@@ -870,7 +1135,10 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     if (r2c_fused != nullptr)
         *r2c_fused = false;
     *ws_need = 0;
-    if (single_pass_ok(n))
+    const Decomp dc = choose_decomp(p, n, batch, istride, idist, ostride, odist, r2c_wn != nullptr);
+    if (dc.kind == 0)
+        return CRDFFT_UNSUPPORTED_SIZE;
+    if (dc.kind == 1)
     {
         LineMap in{idist, 0, istride};
         LineMap out{odist, 0, ostride};
@@ -891,8 +1159,7 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         return CRDFFT_OK;
     }
     long long n1 = 0, n2 = 0;
-    if (istride == 1 && ostride == 1 && idist == n && odist == n && std::getenv("CRDFFT_NO_CLUSTER") == nullptr &&
-        p.desc.precision == CRDFFT_PREC_FP32 && cluster_split(n, &n1, &n2))
+    if (dc.kind == 2 && cluster_split(n, &n1, &n2))
     {
         // One cluster per transform: columns of n1, DSMEM transpose with the four-step twiddle, rows of n2. The
         // twiddle is one full table tw[k1 n2 + j] = W_n^{j k1} (FP64 roots, narrowed).
@@ -929,8 +1196,10 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         steps.push_back(s);
         return CRDFFT_OK;
     }
-    if (!four_step_split(n, &n1, &n2))
+    if (dc.kind != 3 || dc.n1 < 2 || n % dc.n1 != 0)
         return CRDFFT_UNSUPPORTED_SIZE;
+    n1 = dc.n1;
+    n2 = n / n1;
     const void* hi = nullptr;
     const void* lo = nullptr;
     if (n >= (1LL << 31))
@@ -2825,6 +3094,18 @@ void crdfft_debug_fail_alloc_after(int32_t k) { g_fail_alloc_after.store(k < 0 ?
 void crdfft_debug_stall_waits(int32_t on) { g_debug_stall.store(on ? 1 : 0); }
 
 void crdfft_set_planner_mode(int32_t mode) { set_planner_mode(mode); }
+
+crdfft_status crdfft_set_decomposition(int64_t n, int32_t kind, int64_t n1)
+{
+    if (kind < 0 || kind > 3 || n < 1 || (kind == 3 && (n1 < 2 || n % n1 != 0)))
+        return CRDFFT_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_hint_mu);
+    if (kind == 0)
+        g_hints.erase(n);
+    else
+        g_hints[n] = Decomp{kind, kind == 3 ? n1 : 0};
+    return CRDFFT_OK;
+}
 
 int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offsets)
 {

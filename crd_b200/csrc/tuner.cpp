@@ -24,6 +24,7 @@ namespace
 std::atomic<int> g_mode{-1};
 std::mutex g_mu;
 std::map<std::string, WisdomEntry> g_wisdom;
+std::map<std::string, DecompEntry> g_decomp;
 std::string g_log;
 
 std::string device_name()
@@ -133,6 +134,8 @@ std::string wisdom_export()
     for (const auto& kv : g_wisdom)
         o << kv.first << ' ' << (kv.second.pipelined ? 1 : 0) << ' ' << kv.second.points_per_thread << ' '
           << kv.second.lines_per_cta << ' ' << kv.second.ms << '\n';
+    for (const auto& kv : g_decomp)
+        o << kv.first << ' ' << kv.second.kind << ' ' << kv.second.n1 << ' ' << kv.second.ms << '\n';
     return o.str();
 }
 
@@ -143,12 +146,21 @@ int wisdom_import(const std::string& text)
     if (!std::getline(in, line) || line.rfind("crdfft-wisdom 1", 0) != 0)
         return -1;
     std::map<std::string, WisdomEntry> got;
+    std::map<std::string, DecompEntry> got_d;
     while (std::getline(in, line))
     {
         if (line.empty())
             continue;
         std::istringstream ls(line);
         std::string key;
+        if (line.rfind("D|", 0) == 0)
+        {
+            DecompEntry e;
+            if (!(ls >> key >> e.kind >> e.n1 >> e.ms) || e.kind < 1 || e.kind > 3 || (e.kind == 3 && e.n1 < 2))
+                return -1;
+            got_d[key] = e;
+            continue;
+        }
         int pipe = 0;
         WisdomEntry e;
         if (!(ls >> key >> pipe >> e.points_per_thread >> e.lines_per_cta >> e.ms))
@@ -162,14 +174,91 @@ int wisdom_import(const std::string& text)
     std::lock_guard<std::mutex> lk(g_mu);
     for (const auto& kv : got)
         g_wisdom[kv.first] = kv.second;
-    return static_cast<int>(got.size());
+    for (const auto& kv : got_d)
+        g_decomp[kv.first] = kv.second;
+    return static_cast<int>(got.size() + got_d.size());
 }
 
 void wisdom_forget()
 {
     std::lock_guard<std::mutex> lk(g_mu);
     g_wisdom.clear();
+    g_decomp.clear();
     g_log.clear();
+}
+
+bool decomp_lookup(const std::string& key, DecompEntry* e)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_decomp.find(key);
+    if (it == g_decomp.end())
+        return false;
+    *e = it->second;
+    return true;
+}
+
+void decomp_store(const std::string& key, const DecompEntry& e)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_decomp[key] = e;
+}
+
+// The class of a 1-D transform batch for decomposition wisdom: device, length, batch bucketed by powers of two,
+// layout (packed unit stride, padded distances) and precision form.
+std::string decomp_key(long long n, long long batch, bool packed_unit, bool padded, int precision)
+{
+    std::ostringstream k;
+    k << "D|" << device_name() << "|n" << n << ":b" << ilog2(batch) << ":u" << packed_unit << ":p" << padded
+      << ":x" << precision;
+    return k.str();
+}
+
+void planner_log_append(const std::string& line)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_log += line;
+    if (line.empty() || line.back() != '\n')
+        g_log += '\n';
+}
+
+float time_cold_fn(cudaError_t (*run)(void*, cudaStream_t), void* ctx)
+{
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+        return -1.0f;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    void* flush = nullptr;
+    if (cudaMalloc(&flush, kFlushBytes + 256) != cudaSuccess)
+    {
+        flush = nullptr;
+        cudaGetLastError();
+    }
+    else
+        cudaMemsetAsync(flush, 0, kFlushBytes + 256, st);
+    float best = -1.0f;
+    bool ok = run(ctx, st) == cudaSuccess; // warm-up
+    for (int r = 0; r < 3 && ok; ++r)
+    {
+        if (flush != nullptr)
+            l2_flush_kernel<<<1184, 256, 0, st>>>(static_cast<const float4*>(flush), kFlushBytes / 16,
+                                                  reinterpret_cast<float*>(static_cast<char*>(flush) + kFlushBytes));
+        cudaEventRecord(e0, st);
+        ok = run(ctx, st) == cudaSuccess;
+        cudaEventRecord(e1, st);
+        float t = 0.0f;
+        ok = ok && cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&t, e0, e1) == cudaSuccess;
+        if (ok && (best < 0.0f || t < best))
+            best = t;
+    }
+    cudaStreamSynchronize(st);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(st);
+    if (flush != nullptr)
+        cudaFree(flush);
+    return ok ? best : -1.0f;
 }
 
 std::string planner_log_export()

@@ -8,6 +8,8 @@
 
 #include "pass_desc.hpp"
 
+#include <cuda_runtime.h>
+
 #include <string>
 #include <vector>
 
@@ -49,5 +51,27 @@ void wisdom_forget();
 int measure_shapes(const PassDesc& d, const std::string& key, const std::vector<PassShape>& cands,
                    std::vector<float>* ms, int heuristic = -1);
 std::string planner_log_export();
+void planner_log_append(const std::string& line);
+
+// Decomposition wisdom: for a 1-D transform class (device, length, batch and layout class), the decomposition the
+// planner settled on (kind 1 single pass, 2 cluster four-step, 3 two-pass four-step with columns of n1) and its
+// measured time. Exported and imported with the pass wisdom (lines whose key starts with "D|").
+struct DecompEntry
+{
+    int kind = 0;
+    long long n1 = 0;
+    float ms = 0.0f;
+};
+bool decomp_lookup(const std::string& key, DecompEntry* e);
+void decomp_store(const std::string& key, const DecompEntry& e);
+std::string decomp_key(long long n, long long batch, bool packed_unit, bool padded, int precision);
+
+// Times `run` (which queues one execute on the stream it is given): 1 warm-up, then the minimum of 3 runs, each
+// after an L2-sized read so that inputs come from HBM. Milliseconds, or a negative value when a run failed.
+float time_cold_fn(cudaError_t (*run)(void*, cudaStream_t), void* ctx);
+template <class F> float time_cold(F& run)
+{
+    return time_cold_fn([](void* c, cudaStream_t s) { return (*static_cast<F*>(c))(s); }, &run);
+}
 
 } // namespace crdfft

@@ -296,15 +296,27 @@ int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offs
  *   CRDFFT_PLANNER_MEASURE   remembered wisdom, else time every candidate on the device (scratch buffers of up to
  *                            64 MiB per pass, each timed launch after an L2-sized read so that its input comes
  *                            from HBM) and remember the fastest
- * The reference plans from the size alone from a board measured offline (detail/level_plans_gen.hpp:33-148); here
- * the board is measured on the device and kept as wisdom. The environment variable CRDFFT_PLANNER=measure sets the
- * initial mode. Once a pass class has wisdom, every later plan of that class makes the same choice. */
+ * Two levels are planned this way: the decomposition of each 1-D transform length (one pass, the cluster four-step,
+ * or the two-pass four-step n1 x n2 for every split whose halves fit one CTA; timed as whole executes of a sample of
+ * the batch, up to 256 MiB) and the launch shape of each pass. The reference plans from the size alone from a board
+ * measured offline (detail/level_plans_gen.hpp:33-148); here the board is measured on the device and kept as wisdom.
+ * The environment variable CRDFFT_PLANNER=measure sets the initial mode. Once a class has wisdom, every later plan of
+ * that class makes the same choice. */
 #define CRDFFT_PLANNER_ESTIMATE 0
 #define CRDFFT_PLANNER_MEASURE 1
-/*   CRDFFT_PLANNER_LEARNED   remembered wisdom, else the candidate with the lowest cost predicted by the imported
- *                            learned model (crdfft_learned_model_import), else the heuristic. Nothing is timed. */
+/*   CRDFFT_PLANNER_LEARNED   remembered wisdom, else the imported learned models (crdfft_learned_model_import)
+ *                            rank the candidates (decompositions and launch shapes) and the measuring planner times
+ *                            only their top proposals (CRDFFT_LEARNED_TOP_K, default 2) and keeps the fastest: the
+ *                            model proposes, the measurement judges. Without a model for a level, that level is
+ *                            planned as in CRDFFT_PLANNER_MEASURE. */
 #define CRDFFT_PLANNER_LEARNED 2
 void crdfft_set_planner_mode(int32_t mode);
+
+/* Force the decomposition of 1-D transforms of length n in plans created from now on (whatever the planner mode):
+ * kind 1 one pass, 2 the cluster four-step, 3 the two-pass four-step with columns of n1 (rows of n / n1); kind 0
+ * removes the override. A decomposition the length does not admit is ignored at plan creation (the planner
+ * decides). Returns CRDFFT_INVALID_ARG for a kind outside 0..3. */
+crdfft_status crdfft_set_decomposition(int64_t n, int32_t kind, int64_t n1);
 
 /* Wisdom as text ("crdfft-wisdom 1" then one line per pass class: key, pipelined, points a thread, lines a CTA,
  * measured ms), keyed by device name. Export writes a NUL-terminated string into buf when cap suffices and reports
