@@ -136,13 +136,16 @@ class PassGroup:
 @dataclass
 class Measured:
     problem: Problem
-    groups: list = field(default_factory=list)
+    groups: list = field(default_factory=list)    # pass launch-shape candidates
+    dgroups: list = field(default_factory=list)   # decomposition candidates of the plan's 1-D lengths
     plan_ms: float = 0.0         # wall time of plan creation in measure mode (exhaustive planning)
+    wisdom: str = ""             # the wisdom the exhaustive planner left (its plan, re-created for the evaluation)
     error: str = ""
 
 
-def parse_log(text: str) -> list[PassGroup]:
-    """Group the planner log's candidate lines by pass (consecutive lines with one key); drop failed candidates."""
+def parse_log(text: str, decomp: bool = False) -> list[PassGroup]:
+    """Group the planner log's candidate lines by pass (consecutive lines with one key); drop failed candidates.
+    decomp: the decomposition lines (" decomp " entries) instead of the launch-shape lines."""
     groups: list[PassGroup] = []
     cur_key, rows = None, []
 
@@ -159,7 +162,7 @@ def parse_log(text: str) -> list[PassGroup]:
 
     for line in text.splitlines():
         parts = line.split()
-        if not parts:
+        if not parts or (len(parts) > 1 and parts[1] == "decomp") != decomp:
             continue
         key = parts[0]
         kv = dict(p.split("=", 1) for p in parts[1:] if "=" in p)
@@ -187,7 +190,10 @@ def collect(probs: list[Problem], progress: bool = False) -> list[Measured]:
             plan = F.Plan(list(pr.dims), **pr.desc_kwargs())
             m.plan_ms = (time.perf_counter() - t0) * 1e3
             del plan
-            m.groups = parse_log(F.planner_log())
+            log = F.planner_log()
+            m.groups = parse_log(log)
+            m.dgroups = parse_log(log, decomp=True)
+            m.wisdom = F.wisdom_export()
         except F.CrdFftError as exc:
             m.error = str(exc)
         out.append(m)
@@ -198,13 +204,20 @@ def collect(probs: list[Problem], progress: bool = False) -> list[Measured]:
     return out
 
 
-def dataset(measured: list[Measured]):
+def dataset(measured: list[Measured], decomp: bool = False):
+    """Feature rows and log(ms) targets of the launch-shape candidates (or, decomp, of the decompositions)."""
     xs, ys = [], []
     for m in measured:
-        for g in m.groups:
+        for g in (m.dgroups if decomp else m.groups):
             xs.append(g.feats)
             ys.append(np.log(g.ms))
+    if not xs:
+        return np.zeros((0, FEATURES), dtype=np.float32), np.zeros(0, dtype=np.float32)
     return np.concatenate(xs).astype(np.float32), np.concatenate(ys).astype(np.float32)
+
+
+PASS_TAG = "crdfft-mlp"
+DECOMP_TAG = "crdfft-mlp-decomp"
 
 
 @dataclass
@@ -215,10 +228,11 @@ class Model:
     t_std: float
     params: np.ndarray
     hidden: int = HIDDEN
+    tag: str = PASS_TAG          # which ranking the model serves: launch shapes or decompositions
 
     def text(self) -> str:
         f = lambda v: f"{float(v):.9g}"  # noqa: E731
-        lines = ["crdfft-mlp 1", f"dims {FEATURES} {self.hidden}",
+        lines = [f"{self.tag} 1", f"dims {FEATURES} {self.hidden}",
                  "mean " + " ".join(map(f, self.mean)), "std " + " ".join(map(f, self.std)),
                  f"target {f(self.t_mean)} {f(self.t_std)}", f"params {len(self.params)}"]
         for i in range(0, len(self.params), 8):
@@ -227,8 +241,24 @@ class Model:
 
     @staticmethod
     def parse(text: str) -> "Model":
+        """The first model of a model text."""
+        return Model.parse_all(text)[0]
+
+    @staticmethod
+    def parse_all(text: str) -> list:
+        """Every model of a model text, in order."""
         tok = text.split()
-        assert tok[0] == "crdfft-mlp" and tok[1] == "1" and tok[2] == "dims"
+        out = []
+        while tok:
+            m, used = Model._parse_tokens(tok)
+            out.append(m)
+            tok = tok[used:]
+        return out
+
+    @staticmethod
+    def _parse_tokens(tok: list) -> tuple:
+        assert tok[0] in (PASS_TAG, DECOMP_TAG) and tok[1] == "1" and tok[2] == "dims"
+        tag = tok[0]
         d, h = int(tok[3]), int(tok[4])
         i = 5
         assert tok[i] == "mean"
@@ -243,7 +273,7 @@ class Model:
         assert tok[i] == "params"
         n = int(tok[i + 1])
         params = np.array(tok[i + 2:i + 2 + n], dtype=np.float32)
-        return Model(mean, std, tm, ts, params, h)
+        return Model(mean, std, tm, ts, params, h, tag), i + 2 + n
 
 
 def init_params(d: int, h: int, seed: int) -> np.ndarray:
@@ -258,7 +288,7 @@ def init_params(d: int, h: int, seed: int) -> np.ndarray:
 
 
 def train(x: np.ndarray, y: np.ndarray, steps: int = 4000, lr: float = 3e-3, seed: int = 1,
-          hidden: int = HIDDEN, log_every: int = 0) -> tuple[Model, list]:
+          hidden: int = HIDDEN, log_every: int = 0, tag: str = PASS_TAG) -> tuple[Model, list]:
     """Full-batch Adam on mean-squared error of normalised log(ms), on the device with the library's kernels."""
     import torch
 
@@ -294,7 +324,7 @@ def train(x: np.ndarray, y: np.ndarray, steps: int = 4000, lr: float = 3e-3, see
             history.append((s, float(loss.item())))
     torch.cuda.synchronize()
     history.append((steps, float(loss.item())))
-    return Model(mean.astype(np.float32), std, t_mean, t_std, P.cpu().numpy(), hidden), history
+    return Model(mean.astype(np.float32), std, t_mean, t_std, P.cpu().numpy(), hidden, tag), history
 
 
 def predict_device(model: Model, x: np.ndarray) -> np.ndarray:
@@ -314,46 +344,85 @@ def predict_device(model: Model, x: np.ndarray) -> np.ndarray:
     return model.t_mean + model.t_std * out.cpu().numpy()
 
 
-def evaluate(model: Model, measured: list[Measured], replan: bool = True) -> dict:
-    """Achieved / optimal runtime on held-out problems: per problem, the summed measured time of the shapes the
-    model ranks first over the summed best measured times (and the same for the fixed heuristic); planning time
-    of the exhaustive planner (measured during collection) and of the learned one (re-planned here)."""
-    F.learned_model_import(model.text())
+def _exec_ms(plan, pr: Problem, bufs: dict) -> float:
+    """Cold-L2 device time of one forward execute of `plan` (min of 3 after a warm-up, CUDA events; a 256 MiB write
+    between runs evicts the inputs from L2)."""
+    import torch
+
+    pts = int(np.prod(pr.dims))
+    kw = pr.desc_kwargs()
+    half = pts // pr.dims[-1] * (pr.dims[-1] // 2 + 1)
+    idist = kw.get("idist", pts)
+    odist = kw.get("odist", pts if pr.kind != R2C else half)
+    in_dt = torch.float32 if pr.kind == R2C else torch.complex64
+    in_n = idist * (pr.batch - 1) + pts
+    out_n = odist * (pr.batch - 1) + (pts if pr.kind != R2C else half)
+    key = (in_n, in_dt, out_n)
+    if bufs.get("key") != key:
+        bufs.clear()
+        bufs["key"] = key
+        bufs["in"] = torch.zeros(in_n, dtype=in_dt, device="cuda")
+        bufs["out"] = torch.empty(out_n, dtype=torch.complex64, device="cuda")
+        bufs["flush"] = torch.empty(64 << 20, dtype=torch.float32, device="cuda")
+    best = None
+    for r in range(4):
+        bufs["flush"].zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.execute(bufs["in"], bufs["out"], F.FORWARD)
+        e1.record()
+        torch.cuda.synchronize()
+        if r > 0:
+            t = e0.elapsed_time(e1)
+            best = t if best is None else min(best, t)
+    return float(best)
+
+
+def evaluate(models: list, measured: list[Measured], replan: bool = True) -> dict:
+    """On held-out problems, each planner's plan is built and executed on the device at the problem's full size:
+    * exhaustive: the measuring planner's plan (its wisdom from the collection, re-created without timing);
+    * learned: the models rank the candidates (decompositions and launch shapes) and the measuring planner times
+      only their top proposals (planning time measured here, from empty wisdom);
+    * heuristic: the fixed rule, nothing timed.
+    achieved / optimal is the exhaustive plan's execute time over the learned plan's, per problem; every problem
+    whose plans could be built is scored (failures are counted and named)."""
+    for m in models:
+        F.learned_model_import(m.text())
     ratios, heur_ratios, optimal = [], [], 0
-    pass_hits = pass_total = 0
+    learned_ms, exhaustive_ms, failed = [], [], []
+    bufs: dict = {}
     for m in measured:
-        if not m.groups:
+        if m.error:
+            failed.append(f"{m.problem.label()}: {m.error}")
             continue
-        got = best = heur = 0.0
-        heur_ok = True
-        for g in m.groups:
-            pred = np.array([F.learned_predict(f) for f in g.feats])
-            pick = int(np.argmin(pred))
-            got += g.ms[pick]
-            best += g.ms[g.best]
-            pass_hits += int(pick == g.best)
-            pass_total += 1
-            if g.heur >= 0:
-                heur += g.ms[g.heur]
-            else:
-                heur_ok = False
-        ratios.append(best / got)
-        optimal += int(abs(got - best) <= 1e-12 * max(best, 1e-30))
-        if heur_ok:
-            heur_ratios.append(best / heur)
-    learned_ms = []
-    if replan:
-        F.set_planner("learned")
-        for m in measured:
-            if m.error:
-                continue
+        pr = m.problem
+        try:
             F.wisdom_forget()
+            F.wisdom_import(m.wisdom)
+            F.set_planner("estimate")
+            t_ex = _exec_ms(F.Plan(list(pr.dims), **pr.desc_kwargs()), pr, bufs)
+            F.wisdom_forget()
+            F.set_planner("learned")
             t0 = time.perf_counter()
-            plan = F.Plan(list(m.problem.dims), **m.problem.desc_kwargs())
+            lp = F.Plan(list(pr.dims), **pr.desc_kwargs())
             learned_ms.append((time.perf_counter() - t0) * 1e3)
-            del plan
-        F.set_planner("estimate")
-    exhaustive_ms = [m.plan_ms for m in measured if not m.error]
+            F.set_planner("estimate")
+            t_le = _exec_ms(lp, pr, bufs)
+            del lp
+            F.wisdom_forget()
+            t_he = _exec_ms(F.Plan(list(pr.dims), **pr.desc_kwargs()), pr, bufs)
+        except F.CrdFftError as exc:
+            F.set_planner("estimate")
+            failed.append(f"{pr.label()}: {exc}")
+            continue
+        exhaustive_ms.append(m.plan_ms)
+        ratios.append(t_ex / t_le)
+        heur_ratios.append(t_ex / t_he)
+        optimal += int(t_le <= t_ex * 1.02)
+    F.wisdom_forget()
+    F.set_planner("estimate")
+    bufs.clear()
 
     def summ(v):
         v = sorted(v)
@@ -363,12 +432,13 @@ def evaluate(model: Model, measured: list[Measured], replan: bool = True) -> dic
 
     return {
         "problems": len(ratios),
+        "problems_failed": failed,
         "achieved_over_optimal": summ(ratios),
         "heuristic_achieved_over_optimal": summ(heur_ratios),
-        "problems_at_optimum": optimal,
-        "passes_at_optimum": f"{pass_hits}/{pass_total}",
+        "problems_within_2pct_of_exhaustive": optimal,
         "planning_ms_exhaustive": summ(exhaustive_ms),
         "planning_ms_learned": summ(learned_ms),
+        "how": "each plan executed once warm then 3 times cold (CUDA events, min) at the problem's full size",
     }
 
 
@@ -388,26 +458,32 @@ def main() -> None:
     t2 = time.perf_counter()
     x, y = dataset(tr)
     model, hist = train(x, y, steps=args.steps, log_every=500)
+    xd, yd = dataset(tr, decomp=True)
+    dmodel, dhist = train(xd, yd, steps=args.steps, log_every=500, tag=DECOMP_TAG)
     t3 = time.perf_counter()
     xh, yh = dataset(ho)
     pred_h = predict_device(model, xh)
-    rep = evaluate(model, ho)
+    xdh, ydh = dataset(ho, decomp=True)
+    pred_dh = predict_device(dmodel, xdh) if xdh.shape[0] else np.zeros(0)
+    rep = evaluate([model, dmodel], ho)
     rep.update({
         "train_problems": args.train, "heldout_problems": args.heldout,
         "train_rows": int(x.shape[0]), "heldout_rows": int(xh.shape[0]),
+        "train_decomp_rows": int(xd.shape[0]), "heldout_decomp_rows": int(xdh.shape[0]),
         "train_failed": sum(1 for m in tr if m.error), "heldout_failed": sum(1 for m in ho if m.error),
-        "loss_history": hist,
+        "loss_history": hist, "decomp_loss_history": dhist,
         "heldout_rmse_log_ms": float(np.sqrt(np.mean((pred_h - yh) ** 2))),
+        "heldout_decomp_rmse_log_ms": float(np.sqrt(np.mean((pred_dh - ydh) ** 2))) if xdh.shape[0] else None,
         "seconds": {"collect_train": t1 - t0, "collect_heldout": t2 - t1, "train": t3 - t2},
         "hidden": HIDDEN, "features": FEATURES, "train_seed": hex(TRAIN_SEED), "heldout_seed": hex(HELDOUT_SEED),
     })
     os.makedirs(os.path.dirname(os.path.abspath(args.model)), exist_ok=True)
     with open(args.model, "w") as f:
-        f.write(model.text())
+        f.write(model.text() + dmodel.text())
     if args.report:
         with open(args.report, "w") as f:
             json.dump(rep, f, indent=1)
-    print(json.dumps({k: v for k, v in rep.items() if k != "loss_history"}, indent=1))
+    print(json.dumps({k: v for k, v in rep.items() if not k.endswith("loss_history")}, indent=1))
 
 
 if __name__ == "__main__":

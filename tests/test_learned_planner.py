@@ -83,6 +83,43 @@ def test_log_parser_groups_passes():
     assert g[1].heur == -1 and g[1].feats.shape == (1, D)
 
 
+def test_log_parser_separates_decompositions():
+    """Decomposition lines (" decomp ") and launch-shape lines of one log go to separate groups."""
+    from crd_b200.learned_planner import parse_log
+
+    f = ",".join(["1"] * D)
+    text = (f"D|dev|n1048576:b8:u1:p0:x0 decomp kind=3 n1=1024 batch=256 ms=2.5 feat={f} heur\n"
+            f"D|dev|n1048576:b8:u1:p0:x0 decomp kind=3 n1=512 batch=256 ms=2.25 feat={f} best\n"
+            f"k1 pipelined=0 P=16 lpc=1 lines=8 ms=0.5 feat={f} best\n")
+    d = parse_log(text, decomp=True)
+    p = parse_log(text)
+    assert len(d) == 1 and d[0].best == 1 and d[0].heur == 0 and d[0].ms.tolist() == [2.5, 2.25]
+    assert len(p) == 1 and p[0].key == "k1"
+
+
+def test_two_models_in_one_text():
+    """A model text may hold the launch-shape model and the decomposition model; the library imports both and
+    exports both, and the decomposition model alone keeps the shape model already loaded."""
+    import crd_b200.hesap as F
+    from crd_b200.learned_planner import DECOMP_TAG, Model
+
+    rng = np.random.default_rng(3)
+    p = _params().astype(np.float32)
+    a = Model(rng.normal(size=D).astype(np.float32), rng.uniform(0.5, 2, size=D).astype(np.float32), -1.0, 2.0, p)
+    b = Model(a.mean, a.std, 0.5, 1.5, (p * 0.5).astype(np.float32), tag=DECOMP_TAG)
+    try:
+        F.learned_model_import(a.text() + b.text())
+        got = Model.parse_all(F.learned_model_export())
+        assert [m.tag for m in got] == ["crdfft-mlp", DECOMP_TAG]
+        assert np.array_equal(got[1].params, b.params) and got[1].t_mean == b.t_mean
+        F.learned_model_forget()
+        F.learned_model_import(a.text())
+        F.learned_model_import(b.text())
+        assert [m.tag for m in Model.parse_all(F.learned_model_export())] == ["crdfft-mlp", DECOMP_TAG]
+    finally:
+        F.learned_model_forget()
+
+
 def test_model_text_round_trip_and_host_predict():
     """The library parses the model text, exports it unchanged, rejects malformed texts, and its host forward pass
     agrees with the FP64 oracle."""
