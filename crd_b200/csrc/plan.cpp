@@ -262,6 +262,7 @@ struct Plan
     bool ws_owned = false;
     std::string algorithm;
     std::vector<long long> factors;
+    long long split_n1 = 0; // the column length of the last two-pass four-step planned for this plan
     int* err = nullptr; // device word the pipelined kernels flag a given-up wait in
     const void* tc_amat = nullptr; // tensor-core DFT-16 operand image for the plan's precision
     int tc_steps = 0;
@@ -878,7 +879,7 @@ Decomp choose_decomp(const Plan& p, long long n, long long batch, long long istr
         if (k == 1)
             return order[0].second;
     }
-    const long long sample = std::max(1LL, std::min(batch, (256LL << 20) / (8 * n)));
+    const long long sample = std::max(1LL, std::min(batch, (64LL << 20) / (8 * n)));
     int best = -1;
     std::vector<float> ms(k, -1.0f);
     for (size_t i = 0; i < k; ++i)
@@ -928,8 +929,10 @@ crdfft_status make_pass_desc(Plan& p, long long n, long long lines, long long lp
                              bool conj_in, bool conj_out, float scale, const FourStepTw& ftw, PassDesc* out_desc)
 {
     std::vector<int> rad;
-    // radix-32 schedules for unit-stride passes only (the single passes)
-    const bool r32 = p.use32 && in.estride == 1 && out.estride == 1;
+    // radix-32 schedules for unit-stride passes only (the single passes); CRDFFT_R32_ROWS=1 also for passes that
+    // read unit-stride rows and store with a stride (the four-step's row pass)
+    static const bool r32_rows = std::getenv("CRDFFT_R32_ROWS") != nullptr && std::atoi(std::getenv("CRDFFT_R32_ROWS")) != 0;
+    const bool r32 = p.use32 && in.estride == 1 && (out.estride == 1 || r32_rows);
     if (!single_pass_ok(n) || !radices_for(n, rad, r32) || static_cast<int>(rad.size()) > kMaxStages)
         return CRDFFT_UNSUPPORTED_SIZE;
     PassDesc d{};
@@ -1200,6 +1203,7 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         return CRDFFT_UNSUPPORTED_SIZE;
     n1 = dc.n1;
     n2 = n / n1;
+    p.split_n1 = n1;
     const void* hi = nullptr;
     const void* lo = nullptr;
     if (n >= (1LL << 31))
@@ -1293,10 +1297,8 @@ crdfft_status build_c2c_rank1(Plan& p)
         }
         else
         {
-            long long n1, n2;
-            four_step_split(n, &n1, &n2);
             p.algorithm = "four-step";
-            p.factors = {n1, n2};
+            p.factors = {p.split_n1, n / p.split_n1};
         }
         return CRDFFT_OK;
     }
