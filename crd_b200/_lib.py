@@ -79,6 +79,7 @@ EXPORTS = (
     "crdfft_self_check",
     "crdfft_debug_self_check_mismatch",
     "crdfft_debug_self_check_reset",
+    "crdfft_debug_uneven_variant",
     "crdfft_debug_fail_alloc_after",
     "crdfft_device_status",
     "crdfft_debug_stall_waits",
@@ -233,6 +234,7 @@ def lib():
         "crdfft_self_check": ([], i32),
         "crdfft_debug_self_check_mismatch": ([i32], None),
         "crdfft_debug_self_check_reset": ([], None),
+        "crdfft_debug_uneven_variant": ([i32], None),
         "crdfft_debug_fail_alloc_after": ([i32], None),
         "crdfft_device_status": ([vp, vp], i32),
         "crdfft_debug_stall_waits": ([i32], None),

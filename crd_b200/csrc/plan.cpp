@@ -1977,7 +1977,11 @@ bool uneven_split(long long n, long long cap, long long* n1, long long* n2)
         for (int o = 0; o < 2; ++o)
         {
             const long long a = o ? d : n / d, b = o ? n / d : d;
-            const double score = (b % 16 != 0 ? 10.0 : 0.0) + std::fabs(std::log(static_cast<double>(a) / b));
+            // halves the kernel has as compile-time stages first, then whole 16-column tiles, then near square
+            const double stat = (uneven_static_ok(static_cast<int>(a)) ? 1.0 : 0.0) +
+                                (uneven_static_ok(static_cast<int>(b)) ? 1.0 : 0.0);
+            const double score = -3.0 * stat + (b % 16 != 0 ? 10.0 : 0.0) +
+                                 std::fabs(std::log(static_cast<double>(a) / b));
             if (score < best)
             {
                 best = score;
@@ -1987,6 +1991,76 @@ bool uneven_split(long long n, long long cap, long long* n1, long long* n2)
         }
     }
     return best < 1e299;
+}
+
+// The uneven kernel's variant for items of line length n: its compile-time stages (1) or the run-time stages (0).
+// CRDFFT_UNEVEN_STATIC=0/1 forces it; otherwise wisdom, else in measure and learned mode a timed choice (an uneven
+// plan of that length alone, each variant executed cold) that is remembered, else the compile-time stages.
+thread_local int t_uneven_force = -1;
+std::atomic<int> g_uneven_force{-1}; // crdfft_debug_uneven_variant
+
+crdfft_status create_uneven(const int64_t* sizes, int64_t count, const int64_t* offsets, Plan** out);
+
+int uneven_variant(long long n)
+{
+    if (!uneven_static_ok(static_cast<int>(n)))
+        return 0;
+    if (t_uneven_force >= 0)
+        return t_uneven_force;
+    if (g_uneven_force.load() >= 0)
+        return g_uneven_force.load();
+    static const int env = [] {
+        const char* e = std::getenv("CRDFFT_UNEVEN_STATIC");
+        return e != nullptr ? (std::atoi(e) != 0 ? 1 : 0) : -1;
+    }();
+    if (env >= 0)
+        return env;
+    std::ostringstream k;
+    k << "D|uneven|n" << n;
+    const std::string key = k.str();
+    DecompEntry w;
+    if (decomp_lookup(key, &w))
+        return w.kind == 2 ? 1 : 0;
+    const int mode = planner_mode();
+    if (mode == kPlannerEstimate || t_arena != nullptr)
+        return 1;
+    const long long count = std::max(1LL, std::min(8192LL, (64LL << 20) / (8 * n)));
+    std::vector<int64_t> sz(static_cast<size_t>(count), n);
+    float ms[2] = {-1.0f, -1.0f};
+    for (int v = 0; v < 2; ++v)
+    {
+        t_uneven_force = v;
+        Plan* tp = nullptr;
+        const crdfft_status st = create_uneven(sz.data(), count, nullptr, &tp);
+        t_uneven_force = -1;
+        if (st != CRDFFT_OK)
+            continue;
+        void* in = nullptr;
+        void* outb = nullptr;
+        if (cudaMalloc(&in, static_cast<size_t>(count * n) * 8) == cudaSuccess &&
+            cudaMalloc(&outb, static_cast<size_t>(count * n) * 8) == cudaSuccess &&
+            cudaMemset(in, 0, static_cast<size_t>(count * n) * 8) == cudaSuccess)
+        {
+            auto go = [&](cudaStream_t s) {
+                return run(*tp, in, outb, CRDFFT_FORWARD, s, nullptr) == CRDFFT_OK ? cudaSuccess
+                                                                                     : cudaErrorLaunchFailure;
+            };
+            ms[v] = time_cold(go);
+        }
+        cudaGetLastError();
+        cudaFree(in);
+        cudaFree(outb);
+        destroy_plan(tp);
+    }
+    if (ms[0] < 0.0f && ms[1] < 0.0f)
+        return 1;
+    const int pick = (ms[1] > 0.0f && (ms[0] < 0.0f || ms[1] <= ms[0])) ? 1 : 0;
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "%s uneven-variant run-time=%.6f compile-time=%.6f pick=%d", key.c_str(),
+                  static_cast<double>(ms[0]), static_cast<double>(ms[1]), pick);
+    planner_log_append(buf);
+    decomp_store(key, DecompEntry{pick ? 2 : 1, 0, ms[pick]});
+    return pick;
 }
 
 template <typename T> crdfft_status upload_vec(Plan& p, const std::vector<T>& v, const T** out)
@@ -2026,6 +2100,7 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
             return CRDFFT_UNSUPPORTED_SIZE;
         UnevenSched sc{};
         sc.n = static_cast<int>(n);
+        sc.variant = uneven_variant(n);
         sc.nstages = static_cast<int>(rad.size());
         for (size_t i = 0; i < rad.size(); ++i)
             sc.radix[i] = rad[i];
@@ -2197,6 +2272,61 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
     // one launch per execute (counter reset + the persistent kernel)
     p.steps[0].assign(1, Step{});
     p.steps[1].assign(1, Step{});
+    return CRDFFT_OK;
+}
+
+// The uneven-batch plan (crdfft_plan_create_uneven); also the timing plans of uneven_variant.
+crdfft_status create_uneven(const int64_t* sizes, int64_t count, const int64_t* offsets, Plan** out)
+{
+    *out = nullptr;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return CRDFFT_NO_DEVICE;
+    const crdfft_status chk = first_use_self_check(dev);
+    if (chk != CRDFFT_OK)
+        return chk;
+    std::vector<int64_t> packed;
+    if (offsets == nullptr)
+    {
+        packed.resize(static_cast<size_t>(count));
+        long long off = 0;
+        for (int64_t t = 0; t < count; ++t) // packed, each transform 16-byte aligned (crdfft_uneven_offsets)
+        {
+            packed[static_cast<size_t>(t)] = off;
+            off += (sizes[t] + 1) / 2 * 2;
+        }
+        offsets = packed.data();
+    }
+    std::unique_ptr<Plan> p(new Plan());
+    p->desc = crdfft_desc{};
+    p->desc.rank = 1;
+    p->desc.kind = CRDFFT_C2C;
+    p->desc.batch = count;
+    p->device = dev;
+    {
+        void* e = nullptr;
+        if (dev_alloc(&e, 256) != cudaSuccess)
+            return CRDFFT_OOM;
+        p->tables.push_back(e);
+        if (cudaMemset(e, 0, 256) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        p->err = static_cast<int*>(e);
+    }
+    crdfft_status st = build_uneven(*p, sizes, count, offsets);
+    if (st != CRDFFT_OK)
+        return st;
+    if (p->ws_bytes > 0)
+    {
+        if (dev_alloc(&p->ws, p->ws_bytes) != cudaSuccess)
+        {
+            p->ws = nullptr;
+            return CRDFFT_OOM;
+        }
+        p->ws_owned = true;
+    }
+    if (!uploads_landed())
+        return CRDFFT_LAUNCH;
+    *out = p.release();
     return CRDFFT_OK;
 }
 
@@ -3097,6 +3227,8 @@ void crdfft_debug_stall_waits(int32_t on) { g_debug_stall.store(on ? 1 : 0); }
 
 void crdfft_set_planner_mode(int32_t mode) { set_planner_mode(mode); }
 
+void crdfft_debug_uneven_variant(int32_t variant) { g_uneven_force.store(variant < 0 ? -1 : (variant ? 1 : 0)); }
+
 crdfft_status crdfft_set_decomposition(int64_t n, int32_t kind, int64_t n1)
 {
     if (kind < 0 || kind > 3 || n < 1 || (kind == 3 && (n1 < 2 || n % n1 != 0)))
@@ -3129,50 +3261,11 @@ crdfft_status crdfft_plan_create_uneven(const int64_t* sizes, int64_t count, con
     if (plan == nullptr || sizes == nullptr || count < 1)
         return CRDFFT_INVALID_ARG;
     *plan = nullptr;
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess)
-        return CRDFFT_NO_DEVICE;
-    const crdfft_status chk = first_use_self_check(dev);
-    if (chk != CRDFFT_OK)
-        return chk;
-    std::vector<int64_t> packed;
-    if (offsets == nullptr)
-    {
-        packed.resize(static_cast<size_t>(count));
-        crdfft_uneven_offsets(sizes, count, packed.data());
-        offsets = packed.data();
-    }
-    std::unique_ptr<Plan> p(new Plan());
-    p->desc = crdfft_desc{};
-    p->desc.rank = 1;
-    p->desc.kind = CRDFFT_C2C;
-    p->desc.batch = count;
-    p->device = dev;
-    {
-        void* e = nullptr;
-        if (dev_alloc(&e, 256) != cudaSuccess)
-            return CRDFFT_OOM;
-        p->tables.push_back(e);
-        if (cudaMemset(e, 0, 256) != cudaSuccess)
-            return CRDFFT_LAUNCH;
-        p->err = static_cast<int*>(e);
-    }
-    crdfft_status st = build_uneven(*p, sizes, count, offsets);
-    if (st != CRDFFT_OK)
-        return st;
-    if (p->ws_bytes > 0)
-    {
-        if (dev_alloc(&p->ws, p->ws_bytes) != cudaSuccess)
-        {
-            p->ws = nullptr;
-            return CRDFFT_OOM;
-        }
-        p->ws_owned = true;
-    }
-    if (!uploads_landed())
-        return CRDFFT_LAUNCH;
-    *plan = reinterpret_cast<crdfft_plan*>(p.release());
-    return CRDFFT_OK;
+    Plan* p = nullptr;
+    const crdfft_status st = create_uneven(sizes, count, offsets, &p);
+    if (st == CRDFFT_OK)
+        *plan = reinterpret_cast<crdfft_plan*>(p);
+    return st;
 }
 
 static crdfft_status copy_out(const std::string& s, char* buf, size_t cap, size_t* needed)

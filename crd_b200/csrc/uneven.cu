@@ -68,6 +68,83 @@ __device__ __forceinline__ void uneven_store(int n, int lines, long long estride
     });
 }
 
+// A line length's compile-time schedule on the item's tile, in place: the Stockham stages of the line-FFT kernel
+// (line_fft.cuh) with the radix, the stage's L and the line length known at compile time, 16 points a thread, the
+// padded row layout (spad), one barrier between a stage's reads and its writes. Only the twiddle table, the line and
+// the thread's place are run-time values, so the index arithmetic folds away. Out of line, so that its registers do
+// not add to the persistent kernel's.
+template <int R, int L, int N>
+__device__ __forceinline__ void ustage(const float2* __restrict__ tw, float2* line, int jt, int T, bool ok)
+{
+    constexpr int nb = N / R;
+    constexpr int B = (16 + R - 1) / R;
+    float2 v[B][R];
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+    {
+        const int j = jt + b * T;
+        if (ok && j < nb)
+        {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                v[b][r] = line[spad(j + r * nb)];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < B; ++b)
+    {
+        const int j = jt + b * T;
+        if (ok && j < nb)
+        {
+            const int k = j % L;
+            if constexpr (L > 1)
+            {
+#pragma unroll
+                for (int r = 1; r < R; ++r)
+                    v[b][r] = cmul(v[b][r], __ldg(tw + (r - 1) * L + k));
+            }
+            Dft<R>::run(v[b]);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                line[spad(base + r * L)] = v[b][r];
+        }
+    }
+    __syncthreads();
+}
+
+template <int N, int L, int OFF, int R, int... Rest>
+__device__ __forceinline__ void ustages(const float2* tw, float2* line, int jt, int T, bool ok)
+{
+    ustage<R, L, N>(tw + OFF, line, jt, T, ok);
+    if constexpr (sizeof...(Rest) > 0)
+        ustages<N, L * R, OFF + (L > 1 ? (R - 1) * L : 0), Rest...>(tw, line, jt, T, ok);
+}
+
+template <int... Rs>
+__device__ __noinline__ void static_item(const float2* tw, float2* line, int jt, int T, bool ok)
+{
+    ustages<(Rs * ... * 1), 1, 0, Rs...>(tw, line, jt, T, ok);
+}
+
+// The compile-time schedules by log2 n (16 .. 4096; the radix order of the planner's rule), reached through one
+// indirect call site: a call site saves the caller's live registers, and one site keeps that to one save area.
+using StaticFn = void (*)(const float2*, float2*, int, int, bool);
+__device__ StaticFn const kStaticItems[13] = {nullptr,
+                                              nullptr,
+                                              nullptr,
+                                              nullptr,
+                                              static_item<16>,
+                                              static_item<8, 4>,
+                                              static_item<16, 4>,
+                                              static_item<16, 8>,
+                                              static_item<16, 16>,
+                                              static_item<16, 8, 4>,
+                                              static_item<16, 16, 4>,
+                                              static_item<16, 16, 8>,
+                                              static_item<16, 16, 16>};
+
 __global__ void __launch_bounds__(kUnevenThreads, 3)
     uneven_kernel(const UnevenDesc u, const float2* __restrict__ gin, float2* __restrict__ gout, float2* scratch)
 {
@@ -139,9 +216,18 @@ __global__ void __launch_bounds__(kUnevenThreads, 3)
         const bool ok = ll < it.lines;
         // out of place between two buffers of the item's lines (the second right after the first)
         const int lrow = ok ? ll : 0;
-        const float2* res = dyn_stages_pp(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
-                                          sm + lrow * pitch, sm + (it.lines + lrow) * pitch, tid - ll * T, T, ok);
-        const float2* tile = res - lrow * pitch;
+        const float2* tile;
+        if (s.variant == 1) // a power of two 16 .. 4096 (the planner sets the variant only then)
+        {
+            kStaticItems[31 - __clz(n)](static_cast<const float2*>(s.tw), sm + lrow * pitch, tid - ll * T, T, ok);
+            tile = sm; // in place
+        }
+        else
+        {
+            const float2* res = dyn_stages_pp(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
+                                              sm + lrow * pitch, sm + (it.lines + lrow) * pitch, tid - ll * T, T, ok);
+            tile = res - lrow * pitch;
+        }
         const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_hi[it.ftw]) : nullptr;
         const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_lo[it.ftw]) : nullptr;
         uneven_store(n, it.lines, it.out_estride, s_out, it.q0, fh, fl, dst, tile, pitch,
@@ -161,6 +247,8 @@ __global__ void __launch_bounds__(kUnevenThreads, 3)
 } // namespace lfft
 
 int uneven_threads() { return lfft::kUnevenThreads; }
+
+bool uneven_static_ok(int n) { return n >= 16 && n <= 4096 && (n & (n - 1)) == 0; }
 
 cudaError_t launch_uneven(const UnevenDesc& u, int smem_bytes, const void* in, void* out, void* scratch,
                           cudaStream_t stream)

@@ -23,6 +23,7 @@ struct UnevenSched
     int nstages;
     int radix[kMaxStages];
     const void* tw;
+    int variant; // 0: the run-time stages (every length); 1: the length's compile-time schedule (uneven_static_ok)
 };
 
 struct UnevenItem
@@ -62,6 +63,8 @@ struct UnevenDesc
 };
 
 int uneven_threads();
+// Line lengths the persistent kernel also has as compile-time stage sequences (the powers of two 16 .. 4096).
+bool uneven_static_ok(int n);
 cudaError_t launch_uneven(const UnevenDesc& u, int smem_bytes, const void* in, void* out, void* scratch,
                           cudaStream_t stream);
 

@@ -439,6 +439,10 @@ crdfft_status crdfft_self_check(void);
 void crdfft_debug_self_check_mismatch(int32_t on);
 void crdfft_debug_self_check_reset(void);
 
+/* Test hook: uneven-batch plans created from now on run their power-of-two line lengths on the run-time stages (0)
+ * or on the compile-time stages (1); -1 returns the choice to the planner. */
+void crdfft_debug_uneven_variant(int32_t variant);
+
 /* Test hook: make the k-th device allocation from now fail (k >= 1), as if the device were out of memory; 0 turns
  * it off. The reference tests its out-of-memory paths with a refusing allocator in a child process
  * (tests/numerics/hesap-fft/CMakeLists.txt:26-36); here plan creation returns CRDFFT_OOM instead. */

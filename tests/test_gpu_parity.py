@@ -409,6 +409,30 @@ def test_uneven_batch(inverse):
         _check(gs, oracle.fft64(xs, inverse), n, f"uneven n={n}")
 
 
+@pytest.mark.parametrize("variant", [0, 1])
+def test_uneven_stage_variants(variant):
+    """The uneven kernel runs power-of-two line lengths (the small transforms and the halves of long ones) on their
+    compile-time stages or on the run-time stages; both against the FP64 oracle, with every power of two from 16 to
+    65536 in the batch."""
+    from crd_b200 import _lib
+
+    sizes = [1 << k for k in range(4, 17)] * 3 + [105, 3000, 45927]
+    L = _lib.lib()
+    L.crdfft_debug_uneven_variant(variant)
+    try:
+        plan = cf.UnevenPlan(sizes)
+    finally:
+        L.crdfft_debug_uneven_variant(-1)
+    x = oracle.gauss_complex64(0x5EED0033 + variant, plan.total)
+    tin = torch.from_numpy(x).cuda()
+    tout = torch.empty_like(tin)
+    plan.execute(tin, tout, cf.FORWARD)
+    torch.cuda.synchronize()
+    got = tout.cpu().numpy()
+    for n, o in zip(sizes, plan.offsets):
+        _check(got[o:o + n], oracle.fft64(x[o:o + n]), n, f"uneven variant {variant} n={n}")
+
+
 def test_uneven_dependency_wait_times_out():
     """A ROW item waiting for a COL item that never comes (the test hook adds one to its count) gives up after its
     bounded wait, the plan reports CRDFFT_DEVICE_TIMEOUT, and the context stays usable."""
