@@ -263,6 +263,7 @@ struct Plan
     std::string algorithm;
     std::vector<long long> factors;
     long long split_n1 = 0; // the column length of the last two-pass four-step planned for this plan
+    int split_kind = 0;     // the last 1-D decomposition planned: 1 one pass, 2 cluster, 3 two-pass four-step
     int* err = nullptr; // device word the pipelined kernels flag a given-up wait in
     const void* tc_amat = nullptr; // tensor-core DFT-16 operand image for the plan's precision
     int tc_steps = 0;
@@ -583,6 +584,7 @@ std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl,
 }
 
 int learned_top_k();
+int learned_top_k_shapes();
 bool tma_col_enabled();
 
 // The planner's choice of launch shape for a pass: remembered wisdom for its geometry class if any; else, in
@@ -617,7 +619,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
             ranked.emplace_back(learned_predict(f), static_cast<int>(i));
         }
         std::sort(ranked.begin(), ranked.end());
-        const int k = std::min<int>(learned_top_k(), static_cast<int>(ranked.size()));
+        const int k = std::min<int>(learned_top_k_shapes(), static_cast<int>(ranked.size()));
         if (k >= 2 && t_arena == nullptr)
         {
             std::vector<PassShape> top;
@@ -670,14 +672,24 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
     return heuristic_shape(d, map, dl, ds, out);
 }
 
-// How many of the learned model's top proposals the measuring planner times (CRDFFT_LEARNED_TOP_K, default 2).
+// How many of the learned models' top proposals the measuring planner times: decompositions (whole executes,
+// CRDFFT_LEARNED_TOP_K, default 2) and launch shapes (single passes, CRDFFT_LEARNED_TOP_K_SHAPES, default 1: the
+// shape model's first choice is taken untimed, its error is small and a pass timing costs as much as the ranking
+// saves).
+int env_top_k(const char* name, int dflt)
+{
+    const char* e = std::getenv(name);
+    const int v = e != nullptr ? std::atoi(e) : dflt;
+    return v < 1 ? 1 : v;
+}
 int learned_top_k()
 {
-    static const int k = [] {
-        const char* e = std::getenv("CRDFFT_LEARNED_TOP_K");
-        const int v = e != nullptr ? std::atoi(e) : 2;
-        return v < 1 ? 1 : v;
-    }();
+    static const int k = env_top_k("CRDFFT_LEARNED_TOP_K", 2);
+    return k;
+}
+int learned_top_k_shapes()
+{
+    static const int k = env_top_k("CRDFFT_LEARNED_TOP_K_SHAPES", 1);
     return k;
 }
 
@@ -846,8 +858,16 @@ Decomp choose_decomp(const Plan& p, long long n, long long batch, long long istr
     {
         std::lock_guard<std::mutex> lk(g_hint_mu);
         auto it = g_hints.find(n);
-        if (it != g_hints.end() && decomp_valid(cands, it->second))
-            return it->second;
+        if (it != g_hints.end())
+        {
+            const Decomp& h = it->second;
+            const bool ok = (h.kind == 1 && single_pass_ok(n)) ||
+                            (h.kind == 2 && cluster_ok(p, n, istride, idist, ostride, odist)) ||
+                            (h.kind == 3 && h.n1 >= 2 && n % h.n1 == 0 && single_pass_ok(h.n1) &&
+                             single_pass_ok(n / h.n1));
+            if (ok)
+                return h;
+        }
     }
     if (fused_r2c || p.desc.precision != CRDFFT_PREC_FP32 || cands.size() <= 1 || t_forced != nullptr)
         return rule;
@@ -1141,6 +1161,7 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     const Decomp dc = choose_decomp(p, n, batch, istride, idist, ostride, odist, r2c_wn != nullptr);
     if (dc.kind == 0)
         return CRDFFT_UNSUPPORTED_SIZE;
+    p.split_kind = dc.kind;
     if (dc.kind == 1)
     {
         LineMap in{idist, 0, istride};
@@ -1248,8 +1269,9 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
                             scale, &s2);
         if (st != CRDFFT_OK)
             return st;
-        if (r2c_wn != nullptr && ostride == 1 && !conj_out && std::getenv("CRDFFT_NO_FUSED_REAL") == nullptr &&
-            row_r2c_supported(s2.pass))
+        // the fused row pass pairs rows p and n1 - p in one CTA: even n1 only
+        if (r2c_wn != nullptr && ostride == 1 && !conj_out && n1 % 2 == 0 &&
+            std::getenv("CRDFFT_NO_FUSED_REAL") == nullptr && row_r2c_supported(s2.pass))
         {
             s2.kind = StepKind::RowR2C;
             s2.rr = RowR2CDesc{n, odist, w, static_cast<int>(n1), static_cast<int>(n2), r2c_wn, scale};
@@ -1285,12 +1307,12 @@ crdfft_status build_c2c_rank1(Plan& p)
         if (st != CRDFFT_OK)
             return st;
         p.ws_bytes = static_cast<size_t>(std::max(ws_f, ws_i)) * 8;
-        if (single_pass_ok(n))
+        if (p.split_kind == 1)
         {
             p.algorithm = "single-pass";
             p.factors = {n};
         }
-        else if (!p.steps[0].empty() && p.steps[0][0].kind == StepKind::Cluster)
+        else if (p.split_kind == 2)
         {
             p.algorithm = "cluster-four-step";
             p.factors = {p.steps[0][0].pass.n, p.steps[0][0].pass2.n};

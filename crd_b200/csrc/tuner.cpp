@@ -68,6 +68,31 @@ __global__ void l2_flush_kernel(const float4* __restrict__ p, long long n, float
 
 constexpr size_t kFlushBytes = 256u << 20;
 
+// The L2-flush buffer of the measuring planner: allocated (zeroed) at its first timing on a device and kept, so that
+// each timed candidate does not pay a 256 MiB allocation. Null when it cannot be had (timings then run warm).
+void* flush_buffer()
+{
+    static std::mutex mu;
+    static std::map<int, void*> bufs;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess)
+        return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = bufs.find(dev);
+    if (it != bufs.end())
+        return it->second;
+    void* p = nullptr;
+    if (cudaMalloc(&p, kFlushBytes + 256) != cudaSuccess || cudaMemset(p, 0, kFlushBytes + 256) != cudaSuccess)
+    {
+        cudaGetLastError();
+        if (p != nullptr)
+            cudaFree(p);
+        p = nullptr;
+    }
+    bufs[dev] = p;
+    return p;
+}
+
 // Largest element offset + 1 a line map reaches over the first `lines` lines.
 long long extent(const LineMap& m, long long lines, long long lpg, int n)
 {
@@ -229,14 +254,7 @@ float time_cold_fn(cudaError_t (*run)(void*, cudaStream_t), void* ctx)
         return -1.0f;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    void* flush = nullptr;
-    if (cudaMalloc(&flush, kFlushBytes + 256) != cudaSuccess)
-    {
-        flush = nullptr;
-        cudaGetLastError();
-    }
-    else
-        cudaMemsetAsync(flush, 0, kFlushBytes + 256, st);
+    void* flush = flush_buffer();
     float best = -1.0f;
     bool ok = run(ctx, st) == cudaSuccess; // warm-up
     for (int r = 0; r < 3 && ok; ++r)
@@ -256,8 +274,6 @@ float time_cold_fn(cudaError_t (*run)(void*, cudaStream_t), void* ctx)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaStreamDestroy(st);
-    if (flush != nullptr)
-        cudaFree(flush);
     return ok ? best : -1.0f;
 }
 
@@ -299,14 +315,7 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
     cudaEventCreate(&e1);
     cudaMemsetAsync(in, 0, static_cast<size_t>(in_ext) * 8, st);
     // Cold-cache timing: an L2-sized read before every timed launch (skipped if the buffer cannot be had).
-    void* flush = nullptr;
-    if (cudaMalloc(&flush, kFlushBytes + 256) != cudaSuccess)
-    {
-        flush = nullptr;
-        cudaGetLastError();
-    }
-    else
-        cudaMemsetAsync(flush, 0, kFlushBytes + 256, st);
+    void* flush = flush_buffer();
     auto cold = [&]() {
         if (flush != nullptr)
             l2_flush_kernel<<<1184, 256, 0, st>>>(static_cast<const float4*>(flush), kFlushBytes / 16,
@@ -344,8 +353,6 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
     cudaStreamDestroy(st);
     cudaFree(in);
     cudaFree(out);
-    if (flush != nullptr)
-        cudaFree(flush);
     {
         std::lock_guard<std::mutex> lk(g_mu);
         for (size_t i = 0; i < cands.size(); ++i)

@@ -205,12 +205,15 @@ def collect(probs: list[Problem], progress: bool = False) -> list[Measured]:
 
 
 def dataset(measured: list[Measured], decomp: bool = False):
-    """Feature rows and log(ms) targets of the launch-shape candidates (or, decomp, of the decompositions)."""
+    """Feature rows and targets: log(ms) of the launch-shape candidates; for the decompositions (decomp), log(ms)
+    relative to the mean over the same transform's candidates, because the planner only ranks the decompositions
+    of one transform against each other and their times differ far less than across transforms."""
     xs, ys = [], []
     for m in measured:
         for g in (m.dgroups if decomp else m.groups):
             xs.append(g.feats)
-            ys.append(np.log(g.ms))
+            lg = np.log(g.ms)
+            ys.append(lg - lg.mean() if decomp else lg)
     if not xs:
         return np.zeros((0, FEATURES), dtype=np.float32), np.zeros(0, dtype=np.float32)
     return np.concatenate(xs).astype(np.float32), np.concatenate(ys).astype(np.float32)

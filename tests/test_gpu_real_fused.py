@@ -296,3 +296,21 @@ def test_long_c2r_follows_reference_irfft(n, batch, pad, norm):
     want = oracle.irfft64(y.reshape(batch, idist)[[0, -1], :h], n) * (1 if norm else n)
     assert oracle.rel_l2(got[[0, -1]], want) <= REL_L2
     assert np.array_equal(ty.cpu().numpy(), y)
+
+
+@pytest.mark.parametrize("n,batch", [(107520, 3), (2 * 105 * 512, 2)])
+def test_r2c_c2r_with_odd_column_count(n, batch):
+    """R2C/C2R whose half-length four-step has an odd number of columns (53760 = 105 x 512): the row pass cannot
+    pair rows p and n1 - p in one CTA, so the recombination runs as its own step; both directions against the
+    oracle."""
+    h = n // 2 + 1
+    x = torch.from_numpy(oracle.lcg_float32(0xF32 ^ n, batch * n)).cuda()
+    spec = torch.empty(batch * h, dtype=torch.complex64, device="cuda")
+    r2c = cf.Plan([n], batch=batch, kind=cf.R2C)
+    r2c.execute(x, spec, cf.FORWARD)
+    back = torch.empty_like(x)
+    cf.Plan([n], batch=batch, kind=cf.C2R, norm=cf.NORM_INVERSE).execute(spec, back, cf.INVERSE)
+    torch.cuda.synchronize()
+    got = spec.cpu().numpy().reshape(batch, h)
+    assert oracle.rel_l2(got, oracle.rfft64(x.cpu().numpy().reshape(batch, n))) <= REL_L2
+    assert oracle.rel_l2(back.cpu().numpy(), x.cpu().numpy()) <= 2 * REL_L2
