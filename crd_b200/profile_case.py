@@ -4,12 +4,14 @@
     python -m crd_b200.profile_case r2c N BATCH REPS
     python -m crd_b200.profile_case welch|spectrogram NPERSEG NOVERLAP COUNT NSAMPLES REPS
     python -m crd_b200.profile_case uneven COUNT REPS
+    python -m crd_b200.profile_case nd PREC REPS DIM0 DIM1 [DIM2]
 
 The first form creates a forward C2C plan of BATCH transforms of length N (planner mode and optional wisdom as
 given), fills the input with uniform[-1, 1) values and runs REPS out-of-place executes on the current CUDA device.
 The second runs a real-to-complex plan the same way; the third a spectral estimator over COUNT signals of NSAMPLES
 Gaussian samples (periodic Hann window, fs 1); the fourth an uneven batch of COUNT transforms with the benchmark's size
-distribution (log-uniform over the 7-smooth lengths in [16, 65536]).
+distribution (log-uniform over the 7-smooth lengths in [16, 65536]); the fifth a 2-D or 3-D C2C transform at precision
+form PREC (0 FP32, 1 split-BF16, 2 FP16 scaled) with uniform[-1, 1) inputs plus 1 % of entries scaled by 1e4.
 """
 
 from __future__ import annotations
@@ -43,6 +45,23 @@ def main(argv=None) -> None:
         plan = cf.UnevenPlan(uneven_sizes(count))
         x = torch.randn(2 * plan.total, device="cuda").view(torch.complex64)
         y = torch.empty_like(x)
+        print(plan.info())
+        for _ in range(reps):
+            plan.execute(x, y)
+        torch.cuda.synchronize()
+        print("ok")
+        return
+    if argv[0] == "nd":
+        prec, reps = int(argv[1]), int(argv[2])
+        dims = [int(v) for v in argv[3:]]
+        total = 1
+        for v in dims:
+            total *= v
+        x = (torch.rand(2 * total, device="cuda") * 2 - 1).view(torch.complex64)
+        idx = torch.randperm(total, device="cuda")[: total // 100]
+        x[idx] *= 1e4
+        y = torch.empty_like(x)
+        plan = cf.Plan(dims, batch=1, precision=prec)
         print(plan.info())
         for _ in range(reps):
             plan.execute(x, y)
