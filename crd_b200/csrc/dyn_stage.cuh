@@ -162,8 +162,8 @@ __device__ __forceinline__ void tile_load(int n, int lpc, bool along_e, Load&& l
 // form must hold all of a thread's butterflies across a barrier, and the call convention then saves the excess in
 // local memory, which the many stages of a transform turn into DRAM traffic).
 template <int R>
-__device__ __noinline__ void pstage(const float2* src, float2* dst, const float2* tw, int n, int L, unsigned magic,
-                                    int jt, int T, bool ok)
+__device__ __forceinline__ void pstage_body(const float2* src, float2* dst, const float2* tw, int n, int L,
+                                            unsigned magic, int jt, int T, bool ok)
 {
     constexpr int B = (16 + R - 1) / R;
     const int nb = n / R;
@@ -194,8 +194,28 @@ __device__ __noinline__ void pstage(const float2* src, float2* dst, const float2
     }
 }
 
+template <int R>
+__device__ __noinline__ void pstage(const float2* src, float2* dst, const float2* tw, int n, int L, unsigned magic,
+                                    int jt, int T, bool ok)
+{
+    pstage_body<R>(src, dst, tw, n, L, magic, jt, T, ok);
+}
+
+// One stage, out of line (its own register allocation) or, INL, inlined into a caller with registers to spare (a
+// call site saves the caller's live registers in local memory at every call).
+template <int R, bool INL>
+__device__ __forceinline__ void pstage_at(const float2* src, float2* dst, const float2* tw, int n, int L,
+                                          unsigned magic, int jt, int T, bool ok)
+{
+    if constexpr (INL)
+        pstage_body<R>(src, dst, tw, n, L, magic, jt, T, ok);
+    else
+        pstage<R>(src, dst, tw, n, L, magic, jt, T, ok);
+}
+
 // All stages of a schedule, alternating between the line buffers a and b (a holds the input); returns the buffer
 // with the result. Every thread of the CTA calls it (one barrier a stage).
+template <bool INL = false>
 __device__ __forceinline__ float2* dyn_stages_pp(const int* radix, int nstages, const float2* tw, int n, float2* a,
                                                  float2* b, int jt, int T, bool ok)
 {
@@ -206,14 +226,14 @@ __device__ __forceinline__ float2* dyn_stages_pp(const int* radix, int nstages, 
         const unsigned magic = L == 1 ? 0u : (0xFFFFFFFFu / static_cast<unsigned>(L)) + 1u;
         switch (R)
         {
-            case 2: pstage<2>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 3: pstage<3>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 4: pstage<4>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 5: pstage<5>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 7: pstage<7>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 8: pstage<8>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 32: pstage<32>(a, b, tw, n, L, magic, jt, T, ok); break;
-            default: pstage<16>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 2: pstage_at<2, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 3: pstage_at<3, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 4: pstage_at<4, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 5: pstage_at<5, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 7: pstage_at<7, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 8: pstage_at<8, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 32: pstage_at<32, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            default: pstage_at<16, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
         }
         __syncthreads();
         float2* t = a;

@@ -2286,7 +2286,9 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
     u.spin_limit = g_debug_stall.load() ? (1 << 10) : (1 << 24);
     u.conj = 0;
     u.scale = 1.0f;
-    p.usmem = std::max(2 * maxsmem, 1024); // two buffers: the stages run out of place
+    // two item slots (one transformed while the next one's loads land) and the run-time stages' second buffer
+    u.slot_elems = (std::max(maxsmem, 1024) + 127) / 128 * 128 / 8;
+    p.usmem = 3 * u.slot_elems * 8;
     p.ws_bytes = static_cast<size_t>(scratch) * 8;
     p.uneven = true;
     p.algorithm = "uneven-batch";

@@ -8,12 +8,14 @@
 //          written to the transform's region of the workspace
 //   ROW    a tile of rows of that transform's workspace region: length-n2 DFTs, transposed store to the output
 //
-// CTAs (as many as fit on the GPU at once) take items in list order from an atomic counter. The list holds every
-// COL item before any ROW item, so a ROW item's transform has all of its COL items already taken by running CTAs,
-// which finish without waiting on anything: the ROW item's wait on the transform's completion counter always ends.
-// It is bounded anyway (spin_limit polls): a wait that runs out sets the plan's status word and skips the item.
+// CTAs (as many as fit on the GPU at once, G of them) take items in list order, CTA c the items c, c + G, ...; each
+// keeps two item slots in shared memory and issues the next item's loads before it transforms the current one. The
+// list holds every COL item before any ROW item, so the COL items a ROW item waits for belong to CTAs that reach them
+// without waiting on anything: the ROW item's wait on its transform's completion counter always ends. It is bounded
+// anyway (spin_limit polls): a wait that runs out sets the plan's status word and skips the item.
 //
-// Each item runs the stages of its length's run-time radix schedule out of place (dyn_stage.cuh).
+// Each item runs its length's compile-time stages in place where the kernel has them (powers of two) and the planner
+// chose them, else the stages of the length's run-time radix schedule out of place (dyn_stage.cuh).
 
 #include "kernels.hpp"
 #include "line_fft.cuh"
@@ -29,20 +31,20 @@ namespace
 
 constexpr int kUnevenThreads = 256;
 
-// Loads an item's lines into shared memory (row layout, one pad slot per 16), coalesced along whichever side of the
-// global layout is unit-stride; line a starts at base[a]. Asynchronous 8-byte copies (cp.async): every copy of a
-// thread is in flight at once without holding registers (a batch of loads in registers spilled in this 80-register
-// kernel). The caller waits for them and synchronises; an inverse's conjugation is applied after that
-// (uneven_conj).
-__device__ __forceinline__ void uneven_load(int n, int lines, long long estride, const long long* base,
-                                            const float2* src, float2* sm, int pitch)
+// Issues the loads of an item's lines into shared memory (row layout, one pad slot per 16), coalesced along
+// whichever side of the global layout is unit-stride; line a starts at base[a]. Asynchronous 8-byte copies
+// (cp.async) committed as one group: every copy of a thread is in flight at once without holding registers, and the
+// CTA transforms the previous item while they land. The caller waits for the group (cp.async.wait_all) and
+// synchronises; an inverse's conjugation is applied after that (uneven_conj).
+__device__ __forceinline__ void uneven_issue(int n, int lines, long long estride, const long long* base,
+                                             const float2* src, float2* sm, int pitch)
 {
     for_tile(n, lines, estride == 1, [&](int a, int e) {
         const float2* p = src + base[a] + static_cast<long long>(e) * estride;
         float2* d = &LayRow<1>{sm + a * pitch}.at(e);
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(d)), "l"(p) : "memory");
     });
-    asm volatile("cp.async.wait_all;" ::: "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
 }
 
 __device__ __forceinline__ void uneven_conj(int n, int lines, float2* sm, int pitch)
@@ -145,102 +147,142 @@ __device__ StaticFn const kStaticItems[13] = {nullptr,
                                               static_item<16, 16, 8>,
                                               static_item<16, 16, 16>};
 
-__global__ void __launch_bounds__(kUnevenThreads, 3)
+// The persistent loop, software-pipelined over two item slots: CTA c takes items c, c + G, c + 2G, ... (G CTAs, all
+// resident). While it transforms item i from one slot, the loads of item i + G land in the other. A ROW item is
+// prefetched only once its transform's COL items are all done (checked without waiting); otherwise its loads are
+// issued after the current item, behind a bounded wait. Every COL item precedes every ROW item in the list, and a CTA
+// takes its items in list order, so the COL items a ROW item waits for are never behind a wait themselves.
+struct SlotState
+{
+    int idx;  // item index, or -1
+    int go;   // its dependencies were met and its loads issued
+};
+
+__global__ void __launch_bounds__(kUnevenThreads, 2)
     uneven_kernel(const UnevenDesc u, const float2* __restrict__ gin, float2* __restrict__ gout, float2* scratch)
 {
     extern __shared__ float2 sm[];
-    __shared__ int s_item;
-    __shared__ int s_go;
+    __shared__ UnevenItem s_it[2];
     __shared__ long long s_in[kMaxLinesPerCta];
-    __shared__ long long s_out[kMaxLinesPerCta];
+    __shared__ long long s_out[2][kMaxLinesPerCta];
+    __shared__ int s_flag;
     const int tid = threadIdx.x;
     const float in_im = u.conj ? -1.0f : 1.0f;
     const float out_im = u.conj ? -u.scale : u.scale;
-    for (;;)
-    {
+    const int G = gridDim.x;
+    float2* const tmp = sm + 2 * u.slot_elems; // the run-time stages' second buffer
+
+    // Reads item idx into slot `slot` and issues its loads. wait: for a ROW item, wait (bounded) for its COL items;
+    // else only check them, and return 0 without issuing when they are not all done. Every thread calls it.
+    auto prepare = [&](int idx, int slot, bool wait) -> int {
         if (tid == 0)
-            s_item = atomicAdd(u.counter, 1);
-        __syncthreads();
-        const int idx = s_item;
-        if (idx >= u.nitems)
-            break;
-        const UnevenItem it = u.items[idx];
-        const UnevenSched s = u.scheds[it.sched];
-        if (it.kind == kUnevenRow)
         {
-            if (tid == 0)
+            s_it[slot] = u.items[idx];
+            const UnevenItem& it = s_it[slot];
+            int go = 1;
+            if (it.kind == kUnevenRow)
             {
-                int go = 1;
                 const volatile int* done = u.done + it.transform;
-                int i = 0;
-                while (*done < it.need)
+                if (!wait)
+                    go = *done >= it.need ? 1 : 0;
+                else
                 {
-                    if (++i > u.spin_limit)
+                    int i = 0;
+                    while (*done < it.need)
                     {
-                        go = 0;
-                        atomicOr(u.err, 1);
-                        break;
+                        if (++i > u.spin_limit)
+                        {
+                            go = -1; // gave up: the item is skipped
+                            atomicOr(u.err, 1);
+                            break;
+                        }
+                        __nanosleep(64);
                     }
-                    __nanosleep(64);
                 }
                 __threadfence(); // acquire: the COL items' workspace writes are visible from here on
-                s_go = go;
             }
-            __syncthreads();
-            if (!s_go)
-                continue;
+            s_flag = go;
         }
-        const float2* src = it.kind == kUnevenRow ? scratch : gin;
-        float2* dst = it.kind == kUnevenCol ? scratch : gout;
-        const int n = s.n;
-        const int pitch = line_pitch(n);
-        // per-line start offsets, once per item
+        __syncthreads();
+        const int go = s_flag;
+        if (go != 1)
+            return go;
+        const UnevenItem& it = s_it[slot];
         for (int a = tid; a < it.lines; a += blockDim.x)
         {
             s_in[a] = it.line_table >= 0 ? u.line_off[it.line_table + a] : it.in_base + a * it.in_ldist;
-            s_out[a] = it.line_table >= 0 ? u.line_off[it.line_table + a] : it.out_base + a * it.out_ldist;
+            s_out[slot][a] = it.line_table >= 0 ? u.line_off[it.line_table + a] : it.out_base + a * it.out_ldist;
         }
         __syncthreads();
-        // inverse: conjugate on the way into the first pass of each transform and out of the last
-        const bool first_pass = it.kind != kUnevenRow;
-        const bool last_pass = it.kind != kUnevenCol;
-        uneven_load(n, it.lines, it.in_estride, s_in, src, sm, pitch);
-        __syncthreads();
-        if (first_pass && in_im < 0.0f)
+        const int n = u.scheds[it.sched].n;
+        uneven_issue(n, it.lines, it.in_estride, s_in, it.kind == kUnevenRow ? scratch : gin, sm + slot * u.slot_elems,
+                     line_pitch(n));
+        return 1;
+    };
+
+    SlotState cur{static_cast<int>(blockIdx.x), 0};
+    if (cur.idx >= u.nitems)
+        return;
+    cur.go = prepare(cur.idx, 0, true);
+    for (int i = 0; cur.idx < u.nitems; ++i)
+    {
+        const int slot = i & 1;
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads(); // this item's lines are in its slot; the other slot is free
+        SlotState nxt{cur.idx + G, 0};
+        if (nxt.idx < u.nitems)
+            nxt.go = prepare(nxt.idx, slot ^ 1, false); // 0: a ROW item not ready yet, prepared after this one
+        if (cur.go == 1)
         {
-            uneven_conj(n, it.lines, sm, pitch); // each thread the elements it copied
-            __syncthreads();
+            const UnevenItem& it = s_it[slot];
+            const UnevenSched& s = u.scheds[it.sched];
+            float2* const buf = sm + slot * u.slot_elems;
+            float2* dst = it.kind == kUnevenCol ? scratch : gout;
+            const int n = s.n;
+            const int pitch = line_pitch(n);
+            // inverse: conjugate on the way into the first pass of each transform and out of the last
+            const bool first_pass = it.kind != kUnevenRow;
+            const bool last_pass = it.kind != kUnevenCol;
+            if (first_pass && in_im < 0.0f)
+            {
+                uneven_conj(n, it.lines, buf, pitch); // each thread the elements it copied
+                __syncthreads();
+            }
+            const int T = (n + 15) / 16;
+            const int ll = tid / T;
+            const bool ok = ll < it.lines;
+            const int lrow = ok ? ll : 0;
+            const float2* tile;
+            if (s.variant == 1) // a power of two 16 .. 4096 (the planner sets the variant only then)
+            {
+                kStaticItems[31 - __clz(n)](static_cast<const float2*>(s.tw), buf + lrow * pitch, tid - ll * T, T,
+                                            ok);
+                tile = buf; // in place
+            }
+            else
+            {
+                const float2* res = dyn_stages_pp<true>(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
+                                                  buf + lrow * pitch, tmp + lrow * pitch, tid - ll * T, T, ok);
+                tile = res - lrow * pitch;
+            }
+            const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_hi[it.ftw]) : nullptr;
+            const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_lo[it.ftw]) : nullptr;
+            uneven_store(n, it.lines, it.out_estride, s_out[slot], it.q0, fh, fl, dst, tile, pitch,
+                         last_pass ? u.scale : 1.0f, last_pass ? out_im : 1.0f);
+            if (it.kind == kUnevenCol)
+            {
+                __threadfence(); // release: this item's workspace writes before its completion count
+                __syncthreads();
+                if (tid == 0)
+                    atomicAdd(u.done + it.transform, 1);
+            }
         }
-        const int T = (n + 15) / 16;
-        const int ll = tid / T;
-        const bool ok = ll < it.lines;
-        // out of place between two buffers of the item's lines (the second right after the first)
-        const int lrow = ok ? ll : 0;
-        const float2* tile;
-        if (s.variant == 1) // a power of two 16 .. 4096 (the planner sets the variant only then)
-        {
-            kStaticItems[31 - __clz(n)](static_cast<const float2*>(s.tw), sm + lrow * pitch, tid - ll * T, T, ok);
-            tile = sm; // in place
-        }
-        else
-        {
-            const float2* res = dyn_stages_pp(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
-                                              sm + lrow * pitch, sm + (it.lines + lrow) * pitch, tid - ll * T, T, ok);
-            tile = res - lrow * pitch;
-        }
-        const float2* fh = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_hi[it.ftw]) : nullptr;
-        const float2* fl = it.ftw >= 0 ? static_cast<const float2*>(u.tables.ftw_lo[it.ftw]) : nullptr;
-        uneven_store(n, it.lines, it.out_estride, s_out, it.q0, fh, fl, dst, tile, pitch,
-                     last_pass ? u.scale : 1.0f, last_pass ? out_im : 1.0f);
-        if (it.kind == kUnevenCol)
-        {
-            __threadfence(); // release: this item's workspace writes before its completion count
-            __syncthreads();
-            if (tid == 0)
-                atomicAdd(u.done + it.transform, 1);
-        }
-        __syncthreads(); // shared memory and s_item are reused by the next item
+        __syncthreads(); // this slot and the stage buffer are free again
+        if (nxt.idx < u.nitems && nxt.go == 0)
+            nxt.go = prepare(nxt.idx, slot ^ 1, true);
+        cur = nxt;
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 } // namespace

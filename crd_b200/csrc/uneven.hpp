@@ -58,6 +58,7 @@ struct UnevenDesc
     int nitems;
     int ntransforms;
     int spin_limit;
+    int slot_elems; // float2 elements of one item slot of shared memory (two slots, then the stages' buffer)
     int conj;       // inverse: conjugate in and out
     float scale;
 };
