@@ -338,7 +338,7 @@ def build_uneven(dev, rank, cf):
         dict(WORKLOAD_CONFIGS["uneven"], size_classes=len(set(sizes)))
 
 
-PRECISIONS = {"fp32": 0, "split-bf16": 1, "fp16-scaled": 2}
+PRECISIONS = {"fp32": 0, "split-bf16": 1, "fp16-scaled": 2, "split-bf16-hilo": 3, "split-fp16-hilo": 4}
 
 
 def _build_nd_forms(dev, rank, cf, forms, shapes=((4096, 4096), (512, 512, 512))):
@@ -485,6 +485,10 @@ def precision_contrast(dev, rank, cf, steps: int, warmup: int) -> dict:
                                      "hbm_frac": round(op.bytes / (ms / 1e3) / 1e9 / measured_peaks()["hbm_gbs"], 4)}
     f32, bf = out["fp32"]["ms"], out["split-bf16"]["ms"]
     out["split_bf16_speedup_vs_fp32"] = round(f32 / bf, 3)
+    ok = [k for k in PRECISIONS if k != "fp32" and out[k]["rel_l2_vs_fp64"] <= 1e-6]
+    best = min(ok, key=lambda k: out[k]["ms"]) if ok else None
+    out["fastest_tensor_core_form_at_1e-6"] = best
+    out["its_speedup_vs_fp32"] = round(f32 / out[best]["ms"], 3) if best else None
     return out
 
 

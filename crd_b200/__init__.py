@@ -8,7 +8,7 @@ from .hesap import (BluesteinPlan, ConvPlan, CwtPlan, FftPlan, Forward, Inverse,
                     SpectralPlan, UnevenPlan, cwt, cwt_fft_length, cwt_frequencies, fft, ifft_normalized,
                     lower_tensor_fft, periodogram, self_check, spectrogram, uneven_offsets, welch_psd)
 from ._lib import (C2C, C2R, FORWARD, INVERSE, NORM_INVERSE, NORM_NONE, PREC_FP16_SCALED, PREC_FP32,
-                   PREC_SPLIT_BF16, R2C, SPECTRAL_PERIODOGRAM, SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError)
+                   PREC_SPLIT_BF16, PREC_SPLIT_BF16_2, PREC_SPLIT_FP16_2, R2C, SPECTRAL_PERIODOGRAM, SPECTRAL_SPECTROGRAM, SPECTRAL_WELCH, CrdFftError)
 
 __all__ = [
     "BluesteinPlan", "ConvPlan", "FftPlan", "NdFftPlan", "Plan", "RealFftPlan", "SpectralPlan", "UnevenPlan", "fft",
@@ -16,5 +16,5 @@ __all__ = [
     "cwt_fft_length", "cwt_frequencies", "lower_tensor_fft",
     "SPECTRAL_WELCH", "SPECTRAL_SPECTROGRAM", "SPECTRAL_PERIODOGRAM",
     "Forward", "Inverse", "C2C", "R2C", "C2R", "FORWARD", "INVERSE", "NORM_NONE", "NORM_INVERSE", "PREC_FP32",
-    "PREC_SPLIT_BF16", "PREC_FP16_SCALED", "CrdFftError",
+    "PREC_SPLIT_BF16", "PREC_FP16_SCALED", "PREC_SPLIT_BF16_2", "PREC_SPLIT_FP16_2", "CrdFftError",
 ]

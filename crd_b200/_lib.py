@@ -32,6 +32,8 @@ C2R = 2
 PREC_FP32 = 0
 PREC_SPLIT_BF16 = 1
 PREC_FP16_SCALED = 2
+PREC_SPLIT_BF16_2 = 3
+PREC_SPLIT_FP16_2 = 4
 PLANNER_ESTIMATE = 0
 PLANNER_MEASURE = 1
 PLANNER_LEARNED = 2

@@ -2360,7 +2360,7 @@ crdfft_status validate(const crdfft_desc& d)
         return CRDFFT_INVALID_DESC;
     if (d.kind < CRDFFT_C2C || d.kind > CRDFFT_C2R || d.norm < 0 || d.norm > 1)
         return CRDFFT_INVALID_DESC;
-    if (d.precision < 0 || d.precision > 2)
+    if (d.precision < 0 || d.precision > 4)
         return CRDFFT_INVALID_DESC;
     for (int i = 0; i < d.rank; ++i)
         if (d.dims[i] < 1)
@@ -2557,7 +2557,10 @@ crdfft_status create(const crdfft_desc* desc, Plan** out, const ConvReq* conv = 
         p->ws_owned = true;
     }
     if (p->tc_steps > 0)
-        p->algorithm += desc->precision == CRDFFT_PREC_SPLIT_BF16 ? "+tc-bf16x3" : "+tc-fp16";
+    {
+        static const char* const kForm[5] = {"", "+tc-bf16x3", "+tc-fp16", "+tc-bf16x2", "+tc-fp16x2"};
+        p->algorithm += kForm[desc->precision];
+    }
     if (!uploads_landed())
         return CRDFFT_LAUNCH;
     *out = p.release();

@@ -11,6 +11,12 @@
 //  * FP16 with a per-line scale: X scaled by a power of two that puts its largest component near 2^14, one term
 //    each of F and X in fp16, one MMA (2 instructions); the result is scaled back. About 11 bits: reported, not a
 //    1e-6 form.
+//  * split-BF16 hi+lo, three products (the two-term form): X = X1 + X2, F = F1 + F2 in bf16, products F1X1, F1X2,
+//    F2X1 (3 MMAs of K = 32). About 16 significant bits of the data: reported, not a 1e-6 form.
+//  * split-FP16 hi+lo with a per-line scale, three products: X scaled as in the FP16 form, X = X1 + X2 and
+//    F = F1 + F2 in fp16 (each second term the fp16 rounding of what the first leaves, about 22 bits together),
+//    products F1X1, F1X2, F2X1 in one accumulator. Values more than 2^17 below the line's largest lose bits of their
+//    second term to fp16's subnormal range; relative to the line's norm that is below 1e-7.
 //
 // A (M = 128) holds the same 32 rows four times, so every 32-lane slice of the accumulator holds the whole result and
 // each warp drains its own slice (tcgen05.ld): no cross-warp reduction. Operands are K-major, no swizzle: 8 x 16-byte
@@ -99,7 +105,12 @@ template <int... Rs> struct PeelOf<Sched<Rs...>>
     using type = Peel<Rs...>;
 };
 
-// PREC 1: split-BF16 (3 terms), PREC 2: FP16 with a per-line power-of-two scale.
+// Terms of each operand and the products of a precision form (CRDFFT_PREC_*: 1 split-BF16 three terms, 2 FP16
+// scaled, 3 split-BF16 two terms, 4 split-FP16 two terms scaled).
+__host__ __device__ constexpr int tc_terms(int prec) { return prec == 1 ? 3 : prec == 2 ? 1 : 2; }
+__host__ __device__ constexpr int tc_products(int prec) { return prec == 1 ? 6 : prec == 2 ? 1 : 3; }
+__host__ __device__ constexpr bool tc_fp16(int prec) { return prec == 2 || prec == 4; }
+
 template <class S, int PREC, bool EPI>
 __global__ void __launch_bounds__(kTcThreads, 2)
     tc_line_kernel(const PassDesc d, const float2* __restrict__ gin, float2* __restrict__ gout,
@@ -112,7 +123,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     constexpr int LPC = kTcCols / M;    // lines per CTA
     constexpr int T = N / 16;           // FP32 stages: 16 points a thread
     static_assert(T * LPC == kTcThreads, "one GEMM column per thread, one line tile per CTA");
-    constexpr int NTERMS = PREC == 1 ? 3 : 1;
+    constexpr int NTERMS = tc_terms(PREC);
     constexpr int A_BYTES = 128 * 32 * 2; // one A operand
     constexpr int B_BYTES = kTcCols * 32 * 2;
 
@@ -163,7 +174,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     }
     __shared__ float s_back[kTcCols];
     float scale_back = 1.0f;
-    if constexpr (PREC == 2)
+    if constexpr (tc_fp16(PREC))
     {
         // per-line power-of-two scale: the line's largest component near 2^14 (fp16 max 65504)
         float mx = 0.f;
@@ -204,7 +215,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 float v0 = k0 < 16 ? x[k0].x : x[k0 - 16].y;
                 float v1 = (k0 + 1) < 16 ? x[k0 + 1].x : x[k0 + 1 - 16].y;
                 uint32_t lo, hi;
-                if constexpr (PREC == 1)
+                if constexpr (!tc_fp16(PREC))
                 {
                     const __nv_bfloat16 b0 = __float2bfloat16_rn(v0);
                     const __nv_bfloat16 b1 = __float2bfloat16_rn(v1);
@@ -216,8 +227,12 @@ __global__ void __launch_bounds__(kTcThreads, 2)
                 }
                 else
                 {
-                    lo = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(v0)));
-                    hi = static_cast<uint32_t>(__half_as_ushort(__float2half_rn(v1)));
+                    const __half h0 = __float2half_rn(v0);
+                    const __half h1 = __float2half_rn(v1);
+                    lo = static_cast<uint32_t>(__half_as_ushort(h0));
+                    hi = static_cast<uint32_t>(__half_as_ushort(h1));
+                    v0 -= __half2float(h0);
+                    v1 -= __half2float(h1);
                 }
                 w[h] = lo | (hi << 16);
                 // store the remainders back for the next term
@@ -243,9 +258,9 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     {
         const uint32_t a0 = smem_addr(a_s);
         const uint32_t b0 = smem_addr(b_s);
-        const uint32_t idesc = umma_idesc(PREC == 1 ? 1u : 0u, kTcCols);
-        // (A term, B term) products: split-BF16 the six that matter at FP32 accuracy; FP16 the one
-        constexpr int np = PREC == 1 ? 6 : 1;
+        const uint32_t idesc = umma_idesc(tc_fp16(PREC) ? 0u : 1u, kTcCols);
+        // (A term, B term) products: three terms the six that matter at FP32 accuracy, two terms the three, one the one
+        constexpr int np = tc_products(PREC);
         const int pa[6] = {0, 0, 1, 0, 1, 2};
         const int pb[6] = {0, 1, 0, 2, 1, 0};
         bool acc = false;
@@ -319,7 +334,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
 // Shared memory of a tensor-core pass: barrier/slot page, A and B operand images, the line tile.
 int tc_smem_bytes(int n, int prec)
 {
-    const int terms = prec == 1 ? 3 : 1;
+    const int terms = tc_terms(prec);
     const int lpc = kTcCols / (n / 16);
     return 1024 + terms * (128 * 32 * 2) + terms * (kTcCols * 32 * 2) + lpc * line_pitch(n) * 8;
 }
@@ -328,9 +343,13 @@ using TcFn = void (*)(const PassDesc, const float2*, float2*, const uint4*);
 
 template <class S> TcFn tc_pick(int prec, bool epi)
 {
-    if (prec == 1)
-        return epi ? tc_line_kernel<S, 1, true> : tc_line_kernel<S, 1, false>;
-    return epi ? tc_line_kernel<S, 2, true> : tc_line_kernel<S, 2, false>;
+    switch (prec)
+    {
+        case 1: return epi ? tc_line_kernel<S, 1, true> : tc_line_kernel<S, 1, false>;
+        case 3: return epi ? tc_line_kernel<S, 3, true> : tc_line_kernel<S, 3, false>;
+        case 4: return epi ? tc_line_kernel<S, 4, true> : tc_line_kernel<S, 4, false>;
+        default: return epi ? tc_line_kernel<S, 2, true> : tc_line_kernel<S, 2, false>;
+    }
 }
 
 TcFn tc_select(const PassDesc& d, int prec)
@@ -348,14 +367,14 @@ TcFn tc_select(const PassDesc& d, int prec)
 
 bool tc_pass_supported(const PassDesc& d, int prec)
 {
-    return (prec == 1 || prec == 2) && d.in.estride == 1 && d.out.estride == 1 && lfft::tc_select(d, prec) != nullptr;
+    return prec >= 1 && prec <= 4 && d.in.estride == 1 && d.out.estride == 1 && lfft::tc_select(d, prec) != nullptr;
 }
 
 // The A operand images of the real-ified DFT-16 matrix, in the K-major shared-memory layout the kernel copies as is:
 // term t of A at bytes [t*8192, (t+1)*8192), rows r (0..127) holding real row r % 32 of [[Fr, -Fi], [Fi, Fr]].
 void tc_build_a(int prec, std::vector<uint16_t>* out)
 {
-    const int terms = prec == 1 ? 3 : 1;
+    const int terms = lfft::tc_terms(prec);
     out->assign(static_cast<size_t>(terms) * 128 * 32, 0);
     for (int row = 0; row < 128; ++row)
         for (int k = 0; k < 32; ++k)
@@ -375,7 +394,7 @@ void tc_build_a(int prec, std::vector<uint16_t>* out)
             {
                 uint16_t bits;
                 double q;
-                if (prec == 1)
+                if (!lfft::tc_fp16(prec))
                 {
                     const __nv_bfloat16 b = __float2bfloat16_rn(static_cast<float>(rem));
                     bits = __bfloat16_as_ushort(b);

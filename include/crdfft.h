@@ -58,8 +58,11 @@ typedef enum crdfft_kind
 typedef enum crdfft_precision
 {
     CRDFFT_PREC_FP32 = 0,       /* FP32 butterflies, FP32 data */
-    CRDFFT_PREC_SPLIT_BF16 = 1, /* radix-16 stages as tensor-core GEMM on bf16 hi+lo splits, FP32 accumulate */
-    CRDFFT_PREC_FP16_SCALED = 2 /* radix-16 stages on fp16 with a per-transform scale, FP32 accumulate */
+    CRDFFT_PREC_SPLIT_BF16 = 1,   /* first radix-16 stage as a tensor-core GEMM on three-term bf16 splits, six
+                                     products, FP32 accumulate (rel-L2 about 4e-7) */
+    CRDFFT_PREC_FP16_SCALED = 2,  /* the same on fp16 with a per-line power-of-two scale, one term (about 2e-4) */
+    CRDFFT_PREC_SPLIT_BF16_2 = 3, /* bf16 hi+lo, three products (about 16 bits of the data: above 1e-6) */
+    CRDFFT_PREC_SPLIT_FP16_2 = 4  /* fp16 hi+lo with a per-line scale, three products (about 22 bits) */
 } crdfft_precision;
 
 typedef enum crdfft_norm

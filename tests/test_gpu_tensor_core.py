@@ -4,6 +4,11 @@
 * FP16 with a per-line power-of-two scale (CRDFFT_PREC_FP16_SCALED): about 11 significant bits in the first stage;
   rel-L2 against FP64 <= 2e-3 here, and it is reported as a low-precision form, not held to 1e-6.
 
+* split-FP16 hi+lo with a per-line scale, three products (CRDFFT_PREC_SPLIT_FP16_2): about 22 significant bits;
+  rel-L2 against FP64 <= 1e-6, also on lines of very different magnitude and with 1 % of entries scaled by 1e4.
+* split-BF16 hi+lo, three products (CRDFFT_PREC_SPLIT_BF16_2, the two-term form): about 16 significant bits of the
+  data; reported, held to 2e-5 here (it cannot reach 1e-6).
+
 Passes the tensor-core kernel cannot take (strided loads, other radix schedules) run on the FP32 kernels within the
 same plan; the plan's algorithm string says when a tensor-core pass is present.
 """
@@ -112,3 +117,42 @@ def test_split_bf16_matches_fp32_closely():
     cf.Plan([n], batch=batch, precision=cf.PREC_SPLIT_BF16).execute(t, otc)
     torch.cuda.synchronize()
     assert oracle.rel_l2(otc.cpu().numpy(), o32.cpu().numpy().astype(np.complex128)) <= 1e-6
+
+
+HILO_BF16_REL_L2 = 2e-5
+
+
+@pytest.mark.parametrize("n", [512, 1024, 4096])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_split_fp16_hilo_1d(n, inverse):
+    got, want, plan = _run([n], 37, cf.PREC_SPLIT_FP16_2, inverse, 0x7C7 ^ n)
+    assert plan.info()["algorithm"].endswith("+tc-fp16x2")
+    rl2 = oracle.rel_l2(got, want)
+    assert rl2 <= SPLIT_REL_L2, f"n={n}: rel-L2 {rl2:.3e}"
+
+
+@pytest.mark.parametrize("n", [512, 4096])
+def test_split_bf16_hilo_1d_reported(n):
+    got, want, plan = _run([n], 37, cf.PREC_SPLIT_BF16_2, False, 0x7C8 ^ n)
+    assert plan.info()["algorithm"].endswith("+tc-bf16x2")
+    rl2 = oracle.rel_l2(got, want)
+    print(f"split-BF16 hi+lo n={n}: rel-L2 {rl2:.3e}")
+    assert rl2 <= HILO_BF16_REL_L2, f"n={n}: rel-L2 {rl2:.3e}"
+
+
+def test_split_fp16_hilo_scale_and_outliers():
+    """Lines of very different magnitude, and 1 % of entries scaled by 1e4: each line keeps rel-L2 <= 1e-6."""
+    n, batch = 4096, 16
+    x = oracle.lcg_complex64(0x7C9, n * batch).reshape(batch, n)
+    mags = (2.0 ** np.arange(-24, 24, 3)).astype(np.float32)
+    x = (x * mags[:, None]).astype(np.complex64)
+    idx = np.random.default_rng(7).choice(x.size, size=x.size // 100, replace=False)
+    x.reshape(-1)[idx] *= np.float32(1e4)
+    t = torch.from_numpy(x).cuda()
+    o = torch.empty_like(t)
+    cf.Plan([n], batch=batch, precision=cf.PREC_SPLIT_FP16_2).execute(t, o)
+    torch.cuda.synchronize()
+    got = o.cpu().numpy()
+    want = np.fft.fft(x.astype(np.complex128), axis=1)
+    for b in range(batch):
+        assert oracle.rel_l2(got[b], want[b]) <= SPLIT_REL_L2, f"line {b} (scale {mags[b]:.1e})"
