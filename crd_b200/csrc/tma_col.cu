@@ -44,26 +44,38 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
                  : "memory");
 }
 
-// Columns a tile: 8 (64-byte rows) for 512- and 1024-point columns, so that three tiles fit in shared memory; 32
-// (256-byte rows) for short columns, whose tiles are small.
-__host__ __device__ constexpr int tma_cols(int n) { return n <= 256 ? 32 : 8; }
-
-// CTAs an SM: one for long columns (three 64 KiB tiles), four for short columns (two tiles each), so that short
-// columns, with few threads a tile, still keep enough warps resident.
-__host__ __device__ constexpr int tma_ctas(int n) { return n <= 256 ? 4 : 1; }
+// Tile geometry. G = 0: columns a tile 8 (64-byte rows) for 512- and 1024-point columns, so that three tiles fit in
+// shared memory, one CTA an SM; 32 columns (256-byte rows) for short columns, whose tiles are small, four CTAs an SM
+// so that short columns, with few threads a tile, still keep enough warps resident. G = 1 (CRDFFT_TMA_GEOM=1, long
+// columns only): 4 columns a tile (32-byte rows), two CTAs an SM with three tiles each, so that a CTA's barriers stall
+// only half the SM's warps.
+__host__ __device__ constexpr int tma_cols(int n, int g = 0) { return n <= 256 ? 32 : (g == 1 ? 4 : 8); }
+__host__ __device__ constexpr int tma_ctas(int n, int g = 0) { return n <= 256 ? 4 : (g == 1 ? 2 : 1); }
 
 // Bytes between tile buffers: a tile rounded up to 1 KiB (copy destinations 128-byte aligned).
-__host__ __device__ constexpr int tma_tile_stride(int n) { return (n * tma_cols(n) * 8 + 1023) / 1024 * 1024; }
+__host__ __device__ constexpr int tma_tile_stride(int n, int g = 0)
+{
+    return (n * tma_cols(n, g) * 8 + 1023) / 1024 * 1024;
+}
 
-template <class S, int P>
-__global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n), tma_ctas(S::n))
+int tma_geom()
+{
+    static const int g = [] {
+        const char* e = std::getenv("CRDFFT_TMA_GEOM");
+        return e != nullptr && std::atoi(e) == 1 ? 1 : 0;
+    }();
+    return g;
+}
+
+template <class S, int P, int GEOM>
+__global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n, GEOM), tma_ctas(S::n, GEOM))
     tma_col_kernel(const __grid_constant__ CUtensorMap map, const PassDesc d, float2* __restrict__ gout, int nbuf,
                    int box_rows, long long tiles)
 {
     constexpr int N = S::n;
-    constexpr int kTmaCols = tma_cols(N);
+    constexpr int kTmaCols = tma_cols(N, GEOM);
     constexpr int T = (N + P - 1) / P;
-    constexpr int STRIDE = tma_tile_stride(N) / 8; // float2 elements between buffers
+    constexpr int STRIDE = tma_tile_stride(N, GEOM) / 8; // float2 elements between buffers
     extern __shared__ unsigned char smraw[];
     // the buffers from the first 1 KiB boundary of the dynamic shared memory, then the mbarriers and a flag
     const uint32_t base = smem_addr(smraw);
@@ -165,22 +177,23 @@ TmaFn tma_select(const PassDesc& d, int* P)
 {
     // 1024- and 512-point columns at 16 points a thread (512 and 256 threads). Measured slower here, and left to the
     // line kernel: radix-32 stages on this column layout (bank conflicts), 32 points a thread (half the warps).
+    const bool narrow = tma_geom() == 1;
     if (same_radices(d, {16, 16, 4}))
     {
         *P = 16;
-        return tma_col_kernel<Sched<16, 16, 4>, 16>;
+        return narrow ? tma_col_kernel<Sched<16, 16, 4>, 16, 1> : tma_col_kernel<Sched<16, 16, 4>, 16, 0>;
     }
     if (same_radices(d, {16, 8, 4}))
     {
         *P = 16;
-        return tma_col_kernel<Sched<16, 8, 4>, 16>;
+        return narrow ? tma_col_kernel<Sched<16, 8, 4>, 16, 1> : tma_col_kernel<Sched<16, 8, 4>, 16, 0>;
     }
     // 105-point columns (32-column tiles, four CTAs an SM): faster for 3*5*7*4096 (2.86 -> 2.71 ms per 2 GiB),
     // slower for 107520 (2.23 -> 2.36 ms), so only on request (CRDFFT_TMA_SHORT=1)
     if (std::getenv("CRDFFT_TMA_SHORT") != nullptr && same_radices(d, {7, 5, 3}))
     {
         *P = 16;
-        return tma_col_kernel<Sched<7, 5, 3>, 16>;
+        return tma_col_kernel<Sched<7, 5, 3>, 16, 0>;
     }
     return nullptr;
 }
@@ -210,13 +223,14 @@ bool tma_col_supported(const PassDesc& d)
     if (lfft::tma_select(d, &P) == nullptr)
         return false;
     const long long n2 = d.lines_per_group;
-    if (n2 % lfft::tma_cols(d.n) != 0 || d.in.ldist != 1 || d.in.estride != n2 || d.in.gdist != n2 * d.n)
+    const int g = lfft::tma_geom();
+    if (n2 % lfft::tma_cols(d.n, g) != 0 || d.in.ldist != 1 || d.in.estride != n2 || d.in.gdist != n2 * d.n)
         return false;
     if (d.n > lfft::kTmaMaxRows && d.n % lfft::kTmaMaxRows != 0)
         return false;
     if (d.lines % n2 != 0 || d.lines / n2 * d.n > 0x7fffffffLL)
         return false;
-    if (2 * lfft::tma_tile_stride(d.n) > lfft::tma_buffer_budget(lfft::tma_ctas(d.n))) // two tiles in flight
+    if (2 * lfft::tma_tile_stride(d.n, g) > lfft::tma_buffer_budget(lfft::tma_ctas(d.n, g))) // two tiles in flight
         return false;
     return lfft::encoder() != nullptr;
 }
@@ -235,15 +249,16 @@ cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStr
     CUtensorMap map;
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(n2), static_cast<cuuint64_t>(groups * d.n)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(n2) * 8};
-    const int cols = lfft::tma_cols(d.n);
+    const int g = lfft::tma_geom();
+    const int cols = lfft::tma_cols(d.n, g);
     const cuuint32_t box[2] = {static_cast<cuuint32_t>(cols), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
     if (lfft::encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(in), dims, strides, box, estr,
                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue; // the tensor map was refused
-    const int tile_stride = lfft::tma_tile_stride(d.n);
-    int nbuf = lfft::tma_buffer_budget(lfft::tma_ctas(d.n)) / tile_stride;
+    const int tile_stride = lfft::tma_tile_stride(d.n, g);
+    int nbuf = lfft::tma_buffer_budget(lfft::tma_ctas(d.n, g)) / tile_stride;
     if (nbuf > lfft::kTmaMaxBufs)
         nbuf = lfft::kTmaMaxBufs;
     if (nbuf < 2)
@@ -256,7 +271,7 @@ cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStr
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const long long tiles = groups * (n2 / cols);
-    long long grid = static_cast<long long>(sms) * lfft::tma_ctas(d.n);
+    long long grid = static_cast<long long>(sms) * lfft::tma_ctas(d.n, g);
     if (grid > tiles)
         grid = tiles;
     if (grid < 1)
