@@ -104,12 +104,35 @@ public:
     {
         check(crdfft_execute_host(m_h.get(), in, out, static_cast<int32_t>(dir), stream), "execute_host");
     }
+    // split-complex planes (C2C plans whose transforms tile the planes: packed, or rank-1 element-major)
+    void execute_planar(const float* re_in, const float* im_in, float* re_out, float* im_out, Direction dir,
+                        void* stream = nullptr) const
+    {
+        check(crdfft_execute_planar(m_h.get(), re_in, im_in, re_out, im_out, static_cast<int32_t>(dir), stream),
+              "execute_planar");
+    }
     crdfft_plan_info info() const { return m_h.info(); }
     crdfft_plan* handle() const noexcept { return m_h.get(); }
 
 private:
     Handle m_h;
 };
+
+// The CEIR tensor.fft lowering (crdfft_ceir_fft_desc): a plan and a direction for the op, or nullopt-like `ok` false
+// with the reject reason when the op is outside the envelope (the provider keeps its own path then).
+struct TensorFftLowering
+{
+    bool ok = false;
+    int32_t reject = 0;
+    int32_t direction = 0;
+    crdfft_desc desc{};
+};
+inline TensorFftLowering lower_tensor_fft(const crdfft_ceir_fft_op& op)
+{
+    TensorFftLowering l;
+    l.ok = crdfft_ceir_fft_desc(&op, &l.desc, &l.direction, &l.reject) == CRDFFT_OK;
+    return l;
+}
 
 // FftPlan<float>(alloc, n): one size-n complex transform, in place, unnormalised both ways (fft.hpp:224, 409-413).
 class FftPlan

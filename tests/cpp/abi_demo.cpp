@@ -2,7 +2,8 @@
 // tests/test_zz_cpp_binding.py compiles it with g++ against libcrdfft.so and runs it.
 //   abi_demo host            device-free paths (status codes, descriptor validation, the spectral segment rule)
 //   abi_demo device IN OUT   FftPlan(4096) forward of the complex64 file IN into OUT, RealFftPlan(4096) rfft of the
-//                            real parts of IN appended to OUT, and a 3-segment Welch PSD of them appended after that
+//                            real parts of IN appended to OUT, a 3-segment Welch PSD of them appended after that,
+//                            then the re and im planes of a lowered tensor.fft of IN's split planes
 #include <crdfft.hpp>
 
 #include <cuda_runtime.h>
@@ -76,6 +77,31 @@ int host_checks()
             return 1;
         }
     }
+    // the CEIR tensor.fft lowering: a rank-2 [6, 4096] op along its innermost axis is a batch of six 4096-point
+    // transforms; a dynamic extent is refused with the reference's reason
+    crdfft_ceir_fft_op op{};
+    op.num_operands = 2;
+    op.num_results = 2;
+    op.operand_is_tensor = 1;
+    op.element_is_f32 = 1;
+    op.rank = 2;
+    op.axis = -1;
+    op.shape[0] = 6;
+    op.shape[1] = 4096;
+    op.direction = "inverse";
+    const crdfft::TensorFftLowering l = crdfft::lower_tensor_fft(op);
+    if (!l.ok || l.desc.dims[0] != 4096 || l.desc.batch != 6 || l.direction != CRDFFT_INVERSE ||
+        l.desc.norm != CRDFFT_NORM_NONE)
+    {
+        std::puts("FAIL: tensor.fft lowering");
+        return 1;
+    }
+    op.shape[0] = -1;
+    if (crdfft::lower_tensor_fft(op).ok || crdfft::lower_tensor_fft(op).reject != CRDFFT_CEIR_SHAPE_NOT_STATIC)
+    {
+        std::puts("FAIL: dynamic extent accepted");
+        return 1;
+    }
     std::printf("host ok: %s\n", crdfft_status_string(CRDFFT_OK));
     return 0;
 }
@@ -93,10 +119,20 @@ int device_run(const char* in_path, const char* out_path)
     std::vector<float> xr(n);
     for (int64_t i = 0; i < n; ++i)
         xr[static_cast<size_t>(i)] = x[static_cast<size_t>(i)].real();
+    std::vector<float> xi(n);
+    for (int64_t i = 0; i < n; ++i)
+        xi[static_cast<size_t>(i)] = x[static_cast<size_t>(i)].imag();
     crdfft::cfloat* dx = nullptr;
     crdfft::cfloat* ds = nullptr;
     float* dr = nullptr;
     float* dp = nullptr;
+    float* di = nullptr; // the imaginary plane (the real plane is dr)
+    float* dpr = nullptr;
+    float* dpi = nullptr;
+    cudaMalloc(&di, n * sizeof(float));
+    cudaMalloc(&dpr, n * sizeof(float));
+    cudaMalloc(&dpi, n * sizeof(float));
+    cudaMemcpy(di, xi.data(), n * sizeof(float), cudaMemcpyHostToDevice);
     cudaMalloc(&dx, n * sizeof(crdfft::cfloat));
     cudaMalloc(&ds, (n / 2 + 1) * sizeof(crdfft::cfloat));
     cudaMalloc(&dr, n * sizeof(float));
@@ -119,6 +155,21 @@ int device_run(const char* in_path, const char* out_path)
         s.fs = 1.0;
         crdfft::SpectralPlan welch(s);
         welch.execute(dr, dp);
+        // a forward tensor.fft op on [4096] split-complex planes, lowered and run on the planes
+        crdfft_ceir_fft_op op{};
+        op.num_operands = 2;
+        op.num_results = 2;
+        op.operand_is_tensor = 1;
+        op.element_is_f32 = 1;
+        op.rank = 1;
+        op.axis = -1;
+        op.shape[0] = n;
+        op.direction = "forward";
+        const crdfft::TensorFftLowering l = crdfft::lower_tensor_fft(op);
+        if (!l.ok)
+            return 4;
+        crdfft::Plan tp(l.desc);
+        tp.execute_planar(dr, di, dpr, dpi, static_cast<crdfft::Direction>(l.direction));
     }
     catch (const crdfft::Error& e)
     {
@@ -128,7 +179,9 @@ int device_run(const char* in_path, const char* out_path)
     if (cudaDeviceSynchronize() != cudaSuccess)
         return 3;
     std::vector<crdfft::cfloat> y(n), sp(n / 2 + 1);
-    std::vector<float> psd(33);
+    std::vector<float> psd(33), pre(n), pim(n);
+    cudaMemcpy(pre.data(), dpr, n * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaMemcpy(pim.data(), dpi, n * sizeof(float), cudaMemcpyDeviceToHost);
     cudaMemcpy(y.data(), dx, n * sizeof(crdfft::cfloat), cudaMemcpyDeviceToHost);
     cudaMemcpy(sp.data(), ds, (n / 2 + 1) * sizeof(crdfft::cfloat), cudaMemcpyDeviceToHost);
     cudaMemcpy(psd.data(), dp, 33 * sizeof(float), cudaMemcpyDeviceToHost);
@@ -136,6 +189,11 @@ int device_run(const char* in_path, const char* out_path)
     o.write(reinterpret_cast<const char*>(y.data()), static_cast<std::streamsize>(y.size() * sizeof(crdfft::cfloat)));
     o.write(reinterpret_cast<const char*>(sp.data()), static_cast<std::streamsize>(sp.size() * sizeof(crdfft::cfloat)));
     o.write(reinterpret_cast<const char*>(psd.data()), static_cast<std::streamsize>(psd.size() * sizeof(float)));
+    o.write(reinterpret_cast<const char*>(pre.data()), static_cast<std::streamsize>(pre.size() * sizeof(float)));
+    o.write(reinterpret_cast<const char*>(pim.data()), static_cast<std::streamsize>(pim.size() * sizeof(float)));
+    cudaFree(di);
+    cudaFree(dpr);
+    cudaFree(dpi);
     cudaFree(dx);
     cudaFree(ds);
     cudaFree(dr);

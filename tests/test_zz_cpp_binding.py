@@ -1,5 +1,6 @@
 """The C++20 binding (include/crdfft.hpp) compiled with g++ against libcrdfft.so: the device-free paths on the CPU,
-and (GPU) a transform, a real transform and a Welch PSD from C++ host code checked against the FP64 oracle."""
+and (GPU) a transform, a real transform, a Welch PSD and a lowered CEIR tensor.fft on split-complex planes from C++
+host code checked against the FP64 oracle."""
 
 from __future__ import annotations
 
@@ -50,7 +51,11 @@ def test_cpp_binding_device(tmp_path):
     raw = np.fromfile(out, dtype=np.uint8)
     y = raw[: 8 * n].view(np.complex64)
     sp = raw[8 * n: 8 * n + 8 * (n // 2 + 1)].view(np.complex64)
-    psd = raw[8 * n + 8 * (n // 2 + 1):].view(np.float32)
+    off = 8 * n + 8 * (n // 2 + 1)
+    psd = raw[off: off + 4 * 33].view(np.float32)
+    planes = raw[off + 4 * 33:].view(np.float32)
+    got = planes[:n].astype(np.float64) + 1j * planes[n:].astype(np.float64)
+    assert oracle.rel_l2(got, oracle.fft64(x[None, :])[0]) <= 1e-6  # the lowered tensor.fft on split planes
     assert oracle.rel_l2(y, oracle.fft64(x[None, :])[0]) <= 1e-6
     assert oracle.rel_l2(sp, oracle.rfft64(x.real.astype(np.float64))) <= 1e-6
     want = S.welch(x.real[:128].astype(np.float64), 1.0, 64, 32)
