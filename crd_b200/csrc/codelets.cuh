@@ -1,4 +1,4 @@
-// Register-resident DFT codelets for radix 2, 3, 4, 5, 7, 8 and 16, and the complex helpers the pass kernels use.
+// Register-resident DFT codelets for radix 2, 3, 4, 5, 7, 8, 9 and 16, and the complex helpers the pass kernels use.
 //
 // These replace the reference's machine-generated straight-line SIMD codelets (engine/numerics/hesap-fft/kernels/
 // fft_*_codelets_*.cpp, emitted by scripts/gen_fft_batched.py and scripts/gen_fft_codelets.py) and add the odd radices
@@ -282,6 +282,45 @@ template <> struct Dft<5> : OddDft<5>
 };
 template <> struct Dft<7> : OddDft<7>
 {
+};
+
+// Multiply by the compile-time root W_9^J (forward sign) for J in {1, 2, 4}: cos/sin of 2πJ/9.
+template <int J> __device__ __forceinline__ float2 w9mul(float2 a)
+{
+    constexpr float c = J == 1 ? 0.76604444311897804f : J == 2 ? 0.17364817766693041f : -0.93969262078590832f;
+    constexpr float s = J == 1 ? 0.64278760968653933f : J == 2 ? 0.98480775301220802f : 0.34202014332566888f;
+    return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+// 9 = 3 x 3: DFT3 over n1 for each n2 (x[3 n1 + n2]), twiddle W_9^{n2 k1}, DFT3 over n2 -> y[k1 + 3 k2]. One stage of
+// radix 9 replaces two stages of radix 3 (one exchange through shared memory fewer) for lengths with 3^2 as a factor.
+template <> struct Dft<9>
+{
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        float2 a[3][3];
+#pragma unroll
+        for (int n2 = 0; n2 < 3; ++n2)
+        {
+#pragma unroll
+            for (int n1 = 0; n1 < 3; ++n1)
+                a[n2][n1] = v[3 * n1 + n2];
+            Dft<3>::run(a[n2]);
+        }
+        a[1][1] = w9mul<1>(a[1][1]);
+        a[1][2] = w9mul<2>(a[1][2]);
+        a[2][1] = w9mul<2>(a[2][1]);
+        a[2][2] = w9mul<4>(a[2][2]);
+#pragma unroll
+        for (int k1 = 0; k1 < 3; ++k1)
+        {
+            float2 b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+            Dft<3>::run(b);
+#pragma unroll
+            for (int k2 = 0; k2 < 3; ++k2)
+                v[k1 + 3 * k2] = b[k2];
+        }
+    }
 };
 
 } // namespace crdfft

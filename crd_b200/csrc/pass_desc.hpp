@@ -28,7 +28,7 @@ struct PassDesc
 {
     int n;                       // line length
     int nstages;                 // number of radix stages (product of radix[] == n)
-    int radix[kMaxStages];       // stage radices in execution order (each of 2,3,4,5,7,8,16)
+    int radix[kMaxStages];       // stage radices in execution order (each of 2,3,4,5,7,8,9,16, or 32)
     long long lines;             // total lines this launch transforms
     long long lines_per_group;   // lines per address group (a transform, for multi-line-per-transform passes)
     LineMap in;

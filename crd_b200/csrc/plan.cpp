@@ -167,6 +167,17 @@ bool radices_for(long long n, std::vector<int>& out, bool use32 = false)
         }
     if (m != 1)
         return false;
+    // pairs of 3s as radix-9 stages (one exchange through shared memory fewer each), placed before a last 3
+    int threes = 0;
+    while (!odd.empty() && odd.back() == 3)
+    {
+        odd.pop_back();
+        ++threes;
+    }
+    for (int i = 0; i < threes / 2; ++i)
+        odd.push_back(9);
+    if (threes % 2)
+        odd.push_back(3);
     const int a = twos / 4, b = twos % 4;
     if (b == 1 && a >= 1)
     {

@@ -1,7 +1,7 @@
 // crdfft_self_check: the device known-answer check. It has the role of the reference's fft_self_check
 // (engine/numerics/hesap-fft/src/fft_self_check.cpp:153-211), which runs a table's routines on small integer inputs
 // before first use. Here the answers come from a host FP64 DFT computed on the spot (the reference's outputs were
-// checked once against an mpmath DFT, :1-6), and the cases cover every codelet radix, a four-step, a real transform
+// checked once against an mpmath DFT, :1-6), and the cases cover every codelet radix (9 included), a four-step, a real transform
 // and a Bluestein size. Tolerance: max|gpu - dft| <= 1e-5 * (1 + max|dft|), the FP32 error of these sizes with room.
 
 #include "../../include/crdfft.h"
@@ -183,7 +183,8 @@ extern "C" crdfft_status crdfft_self_check(void)
         long long n;
         int dir;
     };
-    static const Case kCases[] = {{2, 0},    {4, 0},    {8, 1},   {16, 0},   {3, 0},   {5, 1},    {7, 0},
+    static const Case kCases[] = {{2, 0},    {4, 0},    {8, 1},   {16, 0},   {3, 0},   {5, 1},    {7, 0},   {9, 0},
+                                  {81, 1},   {2187, 0},
                                   {105, 0},  {105, 1},  {240, 0}, {1024, 0}, {1024, 1}, {4096, 0}, {17, 0},
                                   {32768, 0}, {32768, 1}};
     bool ok = true;

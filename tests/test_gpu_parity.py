@@ -53,6 +53,21 @@ def test_c2c_single_pass(n, inverse):
     _check(got, oracle.fft64(x, inverse), n)
 
 
+@pytest.mark.parametrize("n", [27, 81, 243, 729, 2187, 6561, 5103, 3 * 3 * 5 * 5 * 7 * 16])
+@pytest.mark.parametrize("inverse", [False, True])
+def test_c2c_radix9_lengths(n, inverse):
+    """Lengths with 3^2 as a factor run radix-9 stages (two radix-3 stages in one): single passes and a four-step."""
+    x, got, plan = _c2c(n, 3, inverse)
+    _check(got, oracle.fft64(x, inverse), n)
+
+
+def test_c2c_radix9_four_step():
+    n = 3 ** 10  # 243 x 243, each half 9 x 9 x 3
+    x, got, plan = _c2c(n, 2, False)
+    assert plan.info()["algorithm"] == "four-step"
+    _check(got, oracle.fft64(x), n)
+
+
 @pytest.mark.parametrize("n", [32768, 65536, 107520, 3 * 5 * 7 * 2 ** 9, 2 ** 20])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_c2c_four_step(n, inverse):
