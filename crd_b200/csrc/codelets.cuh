@@ -1,4 +1,4 @@
-// Register-resident DFT codelets for radix 2, 3, 4, 5, 7, 8, 9 and 16, and the complex helpers the pass kernels use.
+// Register-resident DFT codelets for radix 2, 3, 4, 5, 7, 8, 9, 16 and 25, and the complex helpers the pass kernels use.
 //
 // These replace the reference's machine-generated straight-line SIMD codelets (engine/numerics/hesap-fft/kernels/
 // fft_*_codelets_*.cpp, emitted by scripts/gen_fft_batched.py and scripts/gen_fft_codelets.py) and add the odd radices
@@ -284,6 +284,44 @@ template <> struct Dft<7> : OddDft<7>
 {
 };
 
+// Multiply by the compile-time root W_25^J (forward sign), J = n2 k1 for n2, k1 in 1..4: cos/sin of 2πJ/25.
+template <int J> __device__ __forceinline__ float2 w25mul(float2 a)
+{
+    static_assert(J == 1 || J == 2 || J == 3 || J == 4 || J == 6 || J == 8 || J == 9 || J == 12 || J == 16,
+                  "the products n2 k1 of the 5 x 5 split");
+    constexpr float c = J == 1 ? 0.9685831611286311f
+                          : J == 2 ? 0.8763066800438636f
+                          : J == 3 ? 0.7289686274214116f
+                          : J == 4 ? 0.5358267949789965f
+                          : J == 6 ? 0.06279051952931353f
+                          : J == 8 ? -0.4257792915650727f
+                          : J == 9 ? -0.6374239897486897f
+                          : J == 12 ? -0.9921147013144778f
+                                   : -0.6374239897486895f; // J == 16
+    constexpr float s = J == 1 ? 0.2486898871648548f
+                          : J == 2 ? 0.4817536741017153f
+                          : J == 3 ? 0.6845471059286886f
+                          : J == 4 ? 0.8443279255020151f
+                          : J == 6 ? 0.9980267284282716f
+                          : J == 8 ? 0.9048270524660195f
+                          : J == 9 ? 0.7705132427757893f
+                          : J == 12 ? 0.12533323356430454f
+                                   : -0.7705132427757894f; // J == 16
+    return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+// 25 = 5 x 5: DFT5 over n1 for each n2 (x[5 n1 + n2]), twiddle W_25^{n2 k1}, DFT5 over n2 -> y[k1 + 5 k2].
+template <int N2> __device__ __forceinline__ void w25row(float2* a)
+{
+    if constexpr (N2 > 0)
+    {
+        a[1] = w25mul<N2 * 1>(a[1]);
+        a[2] = w25mul<N2 * 2>(a[2]);
+        a[3] = w25mul<N2 * 3>(a[3]);
+        a[4] = w25mul<N2 * 4>(a[4]);
+    }
+}
+
 // Multiply by the compile-time root W_9^J (forward sign) for J in {1, 2, 4}: cos/sin of 2πJ/9.
 template <int J> __device__ __forceinline__ float2 w9mul(float2 a)
 {
@@ -291,6 +329,35 @@ template <int J> __device__ __forceinline__ float2 w9mul(float2 a)
     constexpr float s = J == 1 ? 0.64278760968653933f : J == 2 ? 0.98480775301220802f : 0.34202014332566888f;
     return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
 }
+
+template <> struct Dft<25>
+{
+    __device__ __forceinline__ static void run(float2* v)
+    {
+        float2 a[5][5];
+#pragma unroll
+        for (int n2 = 0; n2 < 5; ++n2)
+        {
+#pragma unroll
+            for (int n1 = 0; n1 < 5; ++n1)
+                a[n2][n1] = v[5 * n1 + n2];
+            Dft<5>::run(a[n2]);
+        }
+        w25row<1>(a[1]);
+        w25row<2>(a[2]);
+        w25row<3>(a[3]);
+        w25row<4>(a[4]);
+#pragma unroll
+        for (int k1 = 0; k1 < 5; ++k1)
+        {
+            float2 b[5] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1], a[4][k1]};
+            Dft<5>::run(b);
+#pragma unroll
+            for (int k2 = 0; k2 < 5; ++k2)
+                v[k1 + 5 * k2] = b[k2];
+        }
+    }
+};
 
 // 9 = 3 x 3: DFT3 over n1 for each n2 (x[3 n1 + n2]), twiddle W_9^{n2 k1}, DFT3 over n2 -> y[k1 + 3 k2]. One stage of
 // radix 9 replaces two stages of radix 3 (one exchange through shared memory fewer) for lengths with 3^2 as a factor.

@@ -81,6 +81,7 @@ __device__ __forceinline__ void dyn_stages(const int* radix, int nstages, const 
             case 5: dstage<5>(sl, tw, n, L, magic, jt, T, ok); break;
             case 7: dstage<7>(sl, tw, n, L, magic, jt, T, ok); break;
             case 9: dstage<9>(sl, tw, n, L, magic, jt, T, ok); break;
+            case 25: dstage<25>(sl, tw, n, L, magic, jt, T, ok); break;
             case 8: dstage<8>(sl, tw, n, L, magic, jt, T, ok); break;
             case 32: dstage<32>(sl, tw, n, L, magic, jt, T, ok); break;
             default: dstage<16>(sl, tw, n, L, magic, jt, T, ok); break;
@@ -233,6 +234,7 @@ __device__ __forceinline__ float2* dyn_stages_pp(const int* radix, int nstages, 
             case 5: pstage_at<5, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 7: pstage_at<7, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 9: pstage_at<9, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 25: pstage_at<25, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 8: pstage_at<8, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 32: pstage_at<32, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             default: pstage_at<16, INL>(a, b, tw, n, L, magic, jt, T, ok); break;

@@ -63,6 +63,7 @@ void pass_features(const PassDesc& d, const PassShape& sh, float* f)
             case 2: f[5] += 1; break;
             case 3: f[6] += 1; break;
             case 9: f[6] += 2; break;
+            case 25: f[7] += 2; break;
             case 5: f[7] += 1; break;
             case 7: f[8] += 1; break;
             default: break;
@@ -308,6 +309,7 @@ void decomp_features(long long n, int kind, long long n1, long long batch, bool 
                 case 2: f[at + 3] += 1; break;
                 case 3: f[at + 4] += 1; break;
                 case 9: f[at + 4] += 2; break;
+                case 25: f[at + 5] += 2; break;
                 case 5: f[at + 5] += 1; break;
                 case 7: f[at + 6] += 1; break;
                 default: break;

@@ -284,6 +284,7 @@ __device__ __forceinline__ void run_dynamic(const PassDesc& d, const Ctx& c, con
             case 5: stage_dyn<5, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
             case 7: stage_dyn<7, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
             case 9: stage_dyn<9, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
+            case 25: stage_dyn<25, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
             case 8: stage_dyn<8, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
             case 32: stage_dyn<32, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;
             default: stage_dyn<16, P, DL, DS, K>(d, c, lay, n, L, off, first, last); break;

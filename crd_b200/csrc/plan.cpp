@@ -167,7 +167,28 @@ bool radices_for(long long n, std::vector<int>& out, bool use32 = false)
         }
     if (m != 1)
         return false;
-    // pairs of 3s as radix-9 stages (one exchange through shared memory fewer each), placed before a last 3
+    // pairs of 5s as radix-25 stages and pairs of 3s as radix-9 stages (one exchange through shared memory fewer
+    // each), each before the odd one left over
+    if (std::getenv("CRDFFT_NO_RADIX25") == nullptr)
+    {
+        std::vector<int> grouped;
+        size_t i = 0;
+        while (i < odd.size() && odd[i] == 7)
+            grouped.push_back(odd[i++]);
+        int fives = 0;
+        while (i < odd.size() && odd[i] == 5)
+        {
+            ++fives;
+            ++i;
+        }
+        for (int k = 0; k < fives / 2; ++k)
+            grouped.push_back(25);
+        if (fives % 2)
+            grouped.push_back(5);
+        while (i < odd.size())
+            grouped.push_back(odd[i++]);
+        odd.swap(grouped);
+    }
     int threes = 0;
     while (!odd.empty() && odd.back() == 3)
     {

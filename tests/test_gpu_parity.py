@@ -53,10 +53,12 @@ def test_c2c_single_pass(n, inverse):
     _check(got, oracle.fft64(x, inverse), n)
 
 
-@pytest.mark.parametrize("n", [27, 81, 243, 729, 2187, 6561, 5103, 3 * 3 * 5 * 5 * 7 * 16])
+@pytest.mark.parametrize("n", [27, 81, 243, 729, 2187, 6561, 5103, 3 * 3 * 5 * 5 * 7 * 16, 25, 125, 625, 3125, 1000,
+                               3000, 5625, 7875])
 @pytest.mark.parametrize("inverse", [False, True])
 def test_c2c_radix9_lengths(n, inverse):
-    """Lengths with 3^2 as a factor run radix-9 stages (two radix-3 stages in one): single passes and a four-step."""
+    """Lengths with 3^2 or 5^2 as a factor run radix-9 and radix-25 stages (two radix-3 or radix-5 stages in one):
+    single passes and a four-step."""
     x, got, plan = _c2c(n, 3, inverse)
     _check(got, oracle.fft64(x, inverse), n)
 
