@@ -217,7 +217,8 @@ __device__ __forceinline__ void pstage_at(const float2* src, float2* dst, const 
 
 // All stages of a schedule, alternating between the line buffers a and b (a holds the input); returns the buffer
 // with the result. Every thread of the CTA calls it (one barrier a stage).
-template <bool INL = false>
+// R25: the schedule may hold radix-25 stages (a caller whose schedules never do leaves their code out).
+template <bool INL = false, bool R25 = true>
 __device__ __forceinline__ float2* dyn_stages_pp(const int* radix, int nstages, const float2* tw, int n, float2* a,
                                                  float2* b, int jt, int T, bool ok)
 {
@@ -234,7 +235,10 @@ __device__ __forceinline__ float2* dyn_stages_pp(const int* radix, int nstages, 
             case 5: pstage_at<5, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 7: pstage_at<7, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 9: pstage_at<9, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
-            case 25: pstage_at<25, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
+            case 25:
+                if constexpr (R25)
+                    pstage_at<25, INL>(a, b, tw, n, L, magic, jt, T, ok);
+                break;
             case 8: pstage_at<8, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             case 32: pstage_at<32, INL>(a, b, tw, n, L, magic, jt, T, ok); break;
             default: pstage_at<16, INL>(a, b, tw, n, L, magic, jt, T, ok); break;

@@ -137,7 +137,9 @@ struct Step
 // With use32, the lengths where a radix-32 schedule measured faster as a unit-stride single pass take it (one
 // exchange through shared memory fewer): 1024 = 32 32 (66 -> 94 % of HBM), 8192 = 32 16 16. (512, 16384 and 32 were
 // slower with radix-32 stages, and so were the strided passes of the four-step.)
-bool radices_for(long long n, std::vector<int>& out, bool use32 = false)
+// group25: pairs of 5s as radix-25 stages (off for the uneven kernel, whose inlined stages run out of registers with
+// a 25-point butterfly: 3.57 -> 3.72 ms for its 20,000-transform batch, where the line kernels gain 7-18 %).
+bool radices_for(long long n, std::vector<int>& out, bool use32 = false, bool group25 = true)
 {
     out.clear();
     if (n < 1)
@@ -169,7 +171,7 @@ bool radices_for(long long n, std::vector<int>& out, bool use32 = false)
         return false;
     // pairs of 5s as radix-25 stages and pairs of 3s as radix-9 stages (one exchange through shared memory fewer
     // each), each before the odd one left over
-    if (std::getenv("CRDFFT_NO_RADIX25") == nullptr)
+    if (group25 && std::getenv("CRDFFT_NO_RADIX25") == nullptr)
     {
         std::vector<int> grouped;
         size_t i = 0;
@@ -444,9 +446,10 @@ void root(long long k, long long n, double* re, double* im)
 // The stage-ordered twiddle table of a line length n with the planner's radix schedule: for each stage after the
 // first (radix R, after radices multiplying to L), W_{LR}^{r k} = W_n^{r k n/(L R)} at (r-1) L + k. Each entry is
 // computed in FP64 and narrowed once (fft.hpp:251-260).
-crdfft_status twiddle_table(Plan& p, long long n, const void** out, bool r32 = false)
+crdfft_status twiddle_table(Plan& p, long long n, const void** out, bool r32 = false, bool group25 = true)
 {
-    const long long key = r32 ? n | (1LL << 48) : n; // one table per (length, schedule family)
+    // one table per (length, schedule family)
+    const long long key = n | (r32 ? (1LL << 48) : 0) | (group25 ? 0 : (1LL << 49));
     auto it = p.tw_by_n.find(key);
     if (it != p.tw_by_n.end())
     {
@@ -454,7 +457,7 @@ crdfft_status twiddle_table(Plan& p, long long n, const void** out, bool r32 = f
         return CRDFFT_OK;
     }
     std::vector<int> rad;
-    if (!radices_for(n, rad, r32))
+    if (!radices_for(n, rad, r32, group25))
         return CRDFFT_UNSUPPORTED_SIZE;
     std::vector<float> h;
     long long L = 1;
@@ -2150,7 +2153,7 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
             return CRDFFT_OK;
         }
         std::vector<int> rad;
-        if (!radices_for(n, rad) || n > kUnevenSingle || static_cast<int>(rad.size()) > kMaxStages)
+        if (!radices_for(n, rad, false, false) || n > kUnevenSingle || static_cast<int>(rad.size()) > kMaxStages)
             return CRDFFT_UNSUPPORTED_SIZE;
         UnevenSched sc{};
         sc.n = static_cast<int>(n);
@@ -2158,7 +2161,7 @@ crdfft_status build_uneven(Plan& p, const int64_t* sizes, int64_t count, const i
         sc.nstages = static_cast<int>(rad.size());
         for (size_t i = 0; i < rad.size(); ++i)
             sc.radix[i] = rad[i];
-        const crdfft_status st = twiddle_table(p, n, &sc.tw);
+        const crdfft_status st = twiddle_table(p, n, &sc.tw, false, false);
         if (st != CRDFFT_OK)
             return st;
         *idx = static_cast<int>(scheds.size());

@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kUnevenThreads, 2)
             }
             else
             {
-                const float2* res = dyn_stages_pp<true>(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
+                const float2* res = dyn_stages_pp<true, false>(s.radix, s.nstages, static_cast<const float2*>(s.tw), s.n,
                                                   buf + lrow * pitch, tmp + lrow * pitch, tid - ll * T, T, ok);
                 tile = res - lrow * pitch;
             }
