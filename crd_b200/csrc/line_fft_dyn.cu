@@ -10,6 +10,8 @@
 #include "dyn_stage.cuh"
 #include "line_fft.cuh"
 
+#include <cstdlib>
+
 namespace crdfft
 {
 namespace lfft
@@ -17,7 +19,7 @@ namespace lfft
 namespace
 {
 
-template <PassMap MAP, bool EPI>
+template <PassMap MAP, bool EPI, bool INL>
 __global__ void __launch_bounds__(kMaxThreads) dyn_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
                                                               float2* __restrict__ gout)
 {
@@ -69,7 +71,7 @@ __global__ void __launch_bounds__(kMaxThreads) dyn_fft_kernel(const PassDesc d, 
     __syncthreads();
 
     // out of place between the two halves of shared memory (lpc lines each)
-    const float2* res = dyn_stages_pp(s_radix, d.nstages, static_cast<const float2*>(d.tw), n, sm + ll * pitch,
+    const float2* res = dyn_stages_pp<INL>(s_radix, d.nstages, static_cast<const float2*>(d.tw), n, sm + ll * pitch,
                                       sm + (lpc + ll) * pitch, jt, T, ll < lines_here);
     float2* tile = const_cast<float2*>(res) - ll * pitch; // the half that holds the result
 
@@ -88,9 +90,17 @@ KernelFn select_dynamic(const PassDesc& d, const PassShape& sh)
     if (sh.points_per_thread != 16)
         return nullptr;
     const bool epi = pass_epi(d);
+    // CRDFFT_DYN_INLINE=1: the stages inlined into the kernel instead of out-of-line calls
+    static const bool inl = std::getenv("CRDFFT_DYN_INLINE") != nullptr && std::atoi(std::getenv("CRDFFT_DYN_INLINE"));
+    if (inl)
+    {
+        if (sh.map == PassMap::Row)
+            return epi ? dyn_fft_kernel<PassMap::Row, true, true> : dyn_fft_kernel<PassMap::Row, false, true>;
+        return epi ? dyn_fft_kernel<PassMap::Col, true, true> : dyn_fft_kernel<PassMap::Col, false, true>;
+    }
     if (sh.map == PassMap::Row)
-        return epi ? dyn_fft_kernel<PassMap::Row, true> : dyn_fft_kernel<PassMap::Row, false>;
-    return epi ? dyn_fft_kernel<PassMap::Col, true> : dyn_fft_kernel<PassMap::Col, false>;
+        return epi ? dyn_fft_kernel<PassMap::Row, true, false> : dyn_fft_kernel<PassMap::Row, false, false>;
+    return epi ? dyn_fft_kernel<PassMap::Col, true, false> : dyn_fft_kernel<PassMap::Col, false, false>;
 }
 
 } // namespace lfft
