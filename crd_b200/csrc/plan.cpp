@@ -572,15 +572,21 @@ bool heuristic_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape
             return true;
         }
     }
-    for (int P : {16, 32}) // the radix-32 schedules exist at 32 points a thread only
-    {
-        const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, P);
-        if (sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit() && pass_has_kernel(d, sh))
+    // A compile-time schedule first, at either thread width (the radix-32 schedules exist at 32 points a thread
+    // only: without this order 1024 and 8192 took the run-time kernel at 16 points a thread, 4x slower for 1024),
+    // then the run-time schedule.
+    for (int pass = 0; pass < 2; ++pass)
+        for (int P : {16, 32})
         {
-            *out = sh;
-            return true;
+            const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, P);
+            if (sh.threads_per_line * sh.lines_per_cta > pass_threads_limit())
+                continue;
+            if (pass == 0 ? pass_has_static(d, P) : pass_has_kernel(d, sh))
+            {
+                *out = sh;
+                return true;
+            }
         }
-    }
     return false;
 }
 
