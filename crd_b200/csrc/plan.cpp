@@ -787,9 +787,8 @@ std::vector<Decomp> decomp_candidates(const Plan& p, long long n, long long istr
         out.push_back(Decomp{1, 0});
     if (cluster_ok(p, n, istride, idist, ostride, odist))
         out.push_back(Decomp{2, 0});
-    // Four-step splits: those whose two line lengths both have compile-time schedules (the run-time schedule is
-    // slower), and when there are fewer than two of those, also the four splits closest to square; the rule's own
-    // split is always among them.
+    // Four-step splits: those whose two line lengths both have compile-time schedules, and the four splits closest
+    // to square among the others (run on the run-time schedule); the rule's own split is always among them.
     if (n >= 2048 && n < (1LL << 31))
     {
         std::vector<std::pair<double, long long>> other;
@@ -803,10 +802,8 @@ std::vector<Decomp> decomp_candidates(const Plan& p, long long n, long long istr
                 other.emplace_back(std::fabs(std::log(static_cast<double>(a) * a / static_cast<double>(n))), a);
         }
         std::sort(other.begin(), other.end());
-        const size_t nstat = out.size() - (single_pass_ok(n) ? 1 : 0);
-        if (nstat < 2)
-            for (size_t i = 0; i < other.size() && i < 4; ++i)
-                out.push_back(Decomp{3, other[i].second});
+        for (size_t i = 0; i < other.size() && i < 4; ++i)
+            out.push_back(Decomp{3, other[i].second});
         long long r1 = 0, r2 = 0;
         if (four_step_split(n, &r1, &r2) && !decomp_valid(out, Decomp{3, r1}))
             out.push_back(Decomp{3, r1});
