@@ -447,34 +447,11 @@ __global__ void __launch_bounds__(kMaxThreads, (P <= 16 && S::n >= 256) ? 2 : 0)
     {
         const long long lines_here = d.lines - line0;
         const long long es = d.out.estride;
-        // Strided output of adjacent lines (the four-step's transposed store): lines 2i and 2i+1 of the CTA sit next to
-        // each other in memory, so a thread writes both as one 16-byte store (twice the run a warp writes, half the
-        // store instructions). Needs an even line count a CTA inside one group and 16-byte aligned pairs.
-        const bool pair = es != 1 && (lpc & 1) == 0 && d.out.ldist == 1 && d.lines_per_group % lpc == 0 &&
-                          (es & 1) == 0 && (d.out.gdist & 1) == 0 &&
-                          (reinterpret_cast<uintptr_t>(gout) & 15) == 0;
-        if (pair)
-        {
-            for_tile(n, lpc / 2, false, [&](int a2, int e) {
-                const int a = 2 * a2;
-                if (a + 1 < lines_here)
-                {
-                    const float2 v0 = epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e));
-                    const float2 v1 = epilogue<EPI>(d, c, s_q[a + 1], e, LayRow<1>{sm + (a + 1) * pitch}.at(e));
-                    __stcs(reinterpret_cast<float4*>(gout + s_out_off[a] + static_cast<long long>(e) * es),
-                           make_float4(v0.x, v0.y, v1.x, v1.y));
-                }
-                else if (a < lines_here)
-                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * es,
-                           epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
-            });
-        }
-        else
-            for_tile(n, lpc, es == 1, [&](int a, int e) {
-                if (a < lines_here)
-                    __stcs(gout + s_out_off[a] + static_cast<long long>(e) * es,
-                           epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
-            });
+        for_tile(n, lpc, es == 1, [&](int a, int e) {
+            if (a < lines_here)
+                __stcs(gout + s_out_off[a] + static_cast<long long>(e) * es,
+                       epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
+        });
     }
 }
 
