@@ -14,6 +14,33 @@
 namespace crdfft
 {
 
+// ---- complex values -------------------------------------------------------------------------------------------
+//
+// The codelets run on two value types. float2 is one complex value (x real, y imaginary). cpair is the same element
+// of two lines, real parts in one float2 and imaginary parts in another, so that one Blackwell paired FP32
+// instruction (FADD2, FMUL2, FFMA2: two lanes of an aligned register pair) does the work of both lines; every
+// operation below is the same arithmetic on each lane.
+struct cpair
+{
+    float2 re; // (line a, line b)
+    float2 im;
+};
+
+__device__ __forceinline__ float2 f2dup(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 f2sub(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\tsub.rn.f32x2 d, a, b;\n\t"
+        "mov.b64 {%0, %1}, d;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+__device__ __forceinline__ float2 f2neg(float2 a) { return f2mul(a, f2dup(-1.0f)); }
+
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
@@ -22,40 +49,97 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cneg(float2 a) { return make_float2(-a.x, -a.y); }
 // -i * a
 __device__ __forceinline__ float2 cmul_mi(float2 a) { return make_float2(a.y, -a.x); }
 // +i * a
 __device__ __forceinline__ float2 cmul_pi(float2 a) { return make_float2(-a.y, a.x); }
+// a + (-i) b and a - (-i) b
+__device__ __forceinline__ float2 add_mi(float2 a, float2 b) { return make_float2(a.x + b.y, a.y - b.x); }
+__device__ __forceinline__ float2 sub_mi(float2 a, float2 b) { return make_float2(a.x - b.y, a.y + b.x); }
+// a (c - i s): multiplication by the forward root of angle θ with c = cos θ, s = sin θ
+__device__ __forceinline__ float2 crot(float2 a, float c, float s) { return make_float2(a.x * c + a.y * s, a.y * c - a.x * s); }
+// H (1 - i) a, H (-1 - i) a, H (-1 + i) a, H (1 + i) a
+__device__ __forceinline__ float2 crot_h1(float2 a, float h) { return make_float2(h * (a.x + a.y), h * (a.y - a.x)); }
+__device__ __forceinline__ float2 crot_h3(float2 a, float h) { return make_float2(h * (a.y - a.x), -h * (a.x + a.y)); }
+__device__ __forceinline__ float2 crot_h5(float2 a, float h) { return make_float2(-h * (a.x + a.y), h * (a.x - a.y)); }
+__device__ __forceinline__ float2 crot_h7(float2 a, float h) { return make_float2(h * (a.x - a.y), h * (a.x + a.y)); }
+// acc + c a (real c)
+__device__ __forceinline__ float2 cmadd(float2 acc, float2 a, float c)
+{
+    return make_float2(fmaf(c, a.x, acc.x), fmaf(c, a.y, acc.y));
+}
+template <class C> __device__ __forceinline__ C czero();
+template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
+
+__device__ __forceinline__ cpair cadd(cpair a, cpair b) { return {f2add(a.re, b.re), f2add(a.im, b.im)}; }
+__device__ __forceinline__ cpair csub(cpair a, cpair b) { return {f2sub(a.re, b.re), f2sub(a.im, b.im)}; }
+__device__ __forceinline__ cpair cscale(cpair a, float s) { return {f2mul(a.re, f2dup(s)), f2mul(a.im, f2dup(s))}; }
+__device__ __forceinline__ cpair cneg(cpair a) { return {f2neg(a.re), f2neg(a.im)}; }
+__device__ __forceinline__ cpair cmul_mi(cpair a) { return {a.im, f2neg(a.re)}; }
+__device__ __forceinline__ cpair cmul_pi(cpair a) { return {f2neg(a.im), a.re}; }
+__device__ __forceinline__ cpair add_mi(cpair a, cpair b) { return {f2add(a.re, b.im), f2sub(a.im, b.re)}; }
+__device__ __forceinline__ cpair sub_mi(cpair a, cpair b) { return {f2sub(a.re, b.im), f2add(a.im, b.re)}; }
+__device__ __forceinline__ cpair crot(cpair a, float c, float s)
+{
+    return {f2fma(a.re, f2dup(c), f2mul(a.im, f2dup(s))), f2fma(a.im, f2dup(c), f2mul(a.re, f2dup(-s)))};
+}
+__device__ __forceinline__ cpair crot_h1(cpair a, float h)
+{
+    return {f2mul(f2add(a.re, a.im), f2dup(h)), f2mul(f2sub(a.im, a.re), f2dup(h))};
+}
+__device__ __forceinline__ cpair crot_h3(cpair a, float h)
+{
+    return {f2mul(f2sub(a.im, a.re), f2dup(h)), f2mul(f2add(a.re, a.im), f2dup(-h))};
+}
+__device__ __forceinline__ cpair crot_h5(cpair a, float h)
+{
+    return {f2mul(f2add(a.re, a.im), f2dup(-h)), f2mul(f2sub(a.re, a.im), f2dup(h))};
+}
+__device__ __forceinline__ cpair crot_h7(cpair a, float h)
+{
+    return {f2mul(f2sub(a.re, a.im), f2dup(h)), f2mul(f2add(a.re, a.im), f2dup(h))};
+}
+__device__ __forceinline__ cpair cmadd(cpair acc, cpair a, float c)
+{
+    return {f2fma(a.re, f2dup(c), acc.re), f2fma(a.im, f2dup(c), acc.im)};
+}
+template <> __device__ __forceinline__ cpair czero<cpair>() { return {make_float2(0.f, 0.f), make_float2(0.f, 0.f)}; }
+// a w for a twiddle w = (c, s) shared by both lines, given as the lane pairs (c, c) and (s, s)
+__device__ __forceinline__ cpair cmul_pair(cpair a, float2 cc, float2 ss)
+{
+    return {f2sub(f2mul(a.re, cc), f2mul(a.im, ss)), f2fma(a.re, ss, f2mul(a.im, cc))};
+}
 
 // Multiply by the compile-time root W_16^J (forward sign), specialised so the trivial roots cost no multiplies.
-template <int J> __device__ __forceinline__ float2 w16mul(float2 a)
+template <int J, class C> __device__ __forceinline__ C w16mul(C a)
 {
-    constexpr float C = 0.92387953251128675613f; // cos(π/8)
-    constexpr float S = 0.38268343236508977173f; // sin(π/8)
-    constexpr float H = 0.70710678118654752440f; // cos(π/4)
+    constexpr float CS = 0.92387953251128675613f; // cos(π/8)
+    constexpr float SN = 0.38268343236508977173f; // sin(π/8)
+    constexpr float H = 0.70710678118654752440f;  // cos(π/4)
     constexpr int j = J & 15;
     if constexpr (j == 0)
         return a;
     else if constexpr (j == 4)
         return cmul_mi(a);
     else if constexpr (j == 8)
-        return make_float2(-a.x, -a.y);
+        return cneg(a);
     else if constexpr (j == 12)
         return cmul_pi(a);
-    else if constexpr (j == 2) // H(1 - i)
-        return make_float2(H * (a.x + a.y), H * (a.y - a.x));
-    else if constexpr (j == 6) // H(-1 - i)
-        return make_float2(H * (a.y - a.x), -H * (a.x + a.y));
-    else if constexpr (j == 10) // H(-1 + i)
-        return make_float2(-H * (a.x + a.y), H * (a.x - a.y));
-    else if constexpr (j == 14) // H(1 + i)
-        return make_float2(H * (a.x - a.y), H * (a.x + a.y));
+    else if constexpr (j == 2)
+        return crot_h1(a, H);
+    else if constexpr (j == 6)
+        return crot_h3(a, H);
+    else if constexpr (j == 10)
+        return crot_h5(a, H);
+    else if constexpr (j == 14)
+        return crot_h7(a, H);
     else
     {
         // W_16^j = cos(2πj/16) - i sin(2πj/16); the remaining j are odd.
-        constexpr float c = (j == 1 || j == 15) ? C : (j == 3 || j == 13) ? S : (j == 5 || j == 11) ? -S : -C;
-        constexpr float s = (j == 1 || j == 7) ? S : (j == 3 || j == 5) ? C : (j == 9 || j == 15) ? -S : -C;
-        return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+        constexpr float c = (j == 1 || j == 15) ? CS : (j == 3 || j == 13) ? SN : (j == 5 || j == 11) ? -SN : -CS;
+        constexpr float s = (j == 1 || j == 7) ? SN : (j == 3 || j == 5) ? CS : (j == 9 || j == 15) ? -SN : -CS;
+        return crot(a, c, s);
     }
 }
 
@@ -63,9 +147,9 @@ template <int R> struct Dft;
 
 template <> struct Dft<2>
 {
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        const float2 a = v[0], b = v[1];
+        const C a = v[0], b = v[1];
         v[0] = cadd(a, b);
         v[1] = csub(a, b);
     }
@@ -73,23 +157,23 @@ template <> struct Dft<2>
 
 template <> struct Dft<4>
 {
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        const float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
-        const float2 s13 = cadd(v[1], v[3]), d13 = cmul_mi(csub(v[1], v[3]));
+        const C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+        const C s13 = cadd(v[1], v[3]), t13 = csub(v[1], v[3]);
         v[0] = cadd(s02, s13);
         v[2] = csub(s02, s13);
-        v[1] = cadd(d02, d13);
-        v[3] = csub(d02, d13);
+        v[1] = add_mi(d02, t13);
+        v[3] = sub_mi(d02, t13);
     }
 };
 
 template <> struct Dft<8>
 {
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        float2 e[4] = {v[0], v[2], v[4], v[6]};
-        float2 o[4] = {v[1], v[3], v[5], v[7]};
+        C e[4] = {v[0], v[2], v[4], v[6]};
+        C o[4] = {v[1], v[3], v[5], v[7]};
         Dft<4>::run(e);
         Dft<4>::run(o);
         o[1] = w16mul<2>(o[1]);
@@ -107,9 +191,9 @@ template <> struct Dft<8>
 template <> struct Dft<16>
 {
     // 16 = 4 x 4: DFT4 over n1 for each n2 (x[4 n1 + n2]), twiddle W_16^{n2 k1}, DFT4 over n2 -> y[k1 + 4 k2].
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        float2 a[4][4];
+        C a[4][4];
 #pragma unroll
         for (int n2 = 0; n2 < 4; ++n2)
         {
@@ -130,7 +214,7 @@ template <> struct Dft<16>
 #pragma unroll
         for (int k1 = 0; k1 < 4; ++k1)
         {
-            float2 b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
+            C b[4] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1]};
             Dft<4>::run(b);
 #pragma unroll
             for (int k2 = 0; k2 < 4; ++k2)
@@ -141,7 +225,7 @@ template <> struct Dft<16>
 
 // Multiply by the compile-time root W_32^J = cos(πJ/16) - i sin(πJ/16): the even J through W_16, the odd J from the
 // two first-octant pairs (cos, sin)(π/16) and (cos, sin)(3π/16) by the symmetries of the circle.
-template <int J> __device__ __forceinline__ float2 w32mul(float2 a)
+template <int J, class C> __device__ __forceinline__ C w32mul(C a)
 {
     constexpr int j = J & 31;
     if constexpr ((j & 1) == 0)
@@ -159,7 +243,7 @@ template <int J> __device__ __forceinline__ float2 w32mul(float2 a)
         constexpr float s = j == 1 ? S1 : j == 3 ? S3 : j == 5 ? C3 : j == 7 ? C1 : j == 9 ? C1 : j == 11 ? C3
                           : j == 13 ? S3 : j == 15 ? S1 : j == 17 ? -S1 : j == 19 ? -S3 : j == 21 ? -C3
                           : j == 23 ? -C1 : j == 25 ? -C1 : j == 27 ? -C3 : j == 29 ? -S3 : -S1;
-        return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+        return crot(a, c, s);
     }
 }
 
@@ -167,19 +251,19 @@ template <> struct Dft<32>
 {
     // 32 = 2 x 16: E = DFT16 of the even points, O = DFT16 of the odd points, y[k] = E[k] + W_32^k O[k] and
     // y[k + 16] = E[k] - W_32^k O[k] (k < 16).
-    template <int K> __device__ __forceinline__ static void combine(float2* v, const float2* e, const float2* o)
+    template <int K, class C> __device__ __forceinline__ static void combine(C* v, const C* e, const C* o)
     {
         if constexpr (K < 16)
         {
-            const float2 t = w32mul<K>(o[K]);
+            const C t = w32mul<K>(o[K]);
             v[K] = cadd(e[K], t);
             v[K + 16] = csub(e[K], t);
             combine<K + 1>(v, e, o);
         }
     }
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        float2 e[16], o[16];
+        C e[16], o[16];
 #pragma unroll
         for (int m = 0; m < 16; ++m)
         {
@@ -236,11 +320,11 @@ template <> struct OddRoots<7>
 
 template <int P> struct OddDft
 {
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
         constexpr int h = (P - 1) / 2;
-        float2 a[h + 1], b[h + 1];
-        float2 y0 = v[0];
+        C a[h + 1], b[h + 1];
+        C y0 = v[0];
 #pragma unroll
         for (int k = 1; k <= h; ++k)
         {
@@ -248,25 +332,21 @@ template <int P> struct OddDft
             b[k] = csub(v[k], v[P - k]);
             y0 = cadd(y0, a[k]);
         }
-        float2 out[P];
+        C out[P];
         out[0] = y0;
 #pragma unroll
         for (int m = 1; m <= h; ++m)
         {
-            float2 re = v[0];
-            float2 im = make_float2(0.f, 0.f);
+            C re = v[0];
+            C im = czero<C>();
 #pragma unroll
             for (int k = 1; k <= h; ++k)
             {
-                const float c = OddRoots<P>::c((k * m) % P);
-                const float s = OddRoots<P>::s((k * m) % P);
-                re.x = fmaf(c, a[k].x, re.x);
-                re.y = fmaf(c, a[k].y, re.y);
-                im.x = fmaf(s, b[k].x, im.x);
-                im.y = fmaf(s, b[k].y, im.y);
+                re = cmadd(re, a[k], OddRoots<P>::c((k * m) % P));
+                im = cmadd(im, b[k], OddRoots<P>::s((k * m) % P));
             }
-            out[m] = make_float2(re.x + im.y, re.y - im.x);
-            out[P - m] = make_float2(re.x - im.y, re.y + im.x);
+            out[m] = add_mi(re, im);
+            out[P - m] = sub_mi(re, im);
         }
 #pragma unroll
         for (int k = 0; k < P; ++k)
@@ -285,7 +365,7 @@ template <> struct Dft<7> : OddDft<7>
 };
 
 // Multiply by the compile-time root W_25^J (forward sign), J = n2 k1 for n2, k1 in 1..4: cos/sin of 2πJ/25.
-template <int J> __device__ __forceinline__ float2 w25mul(float2 a)
+template <int J, class C> __device__ __forceinline__ C w25mul(C a)
 {
     static_assert(J == 1 || J == 2 || J == 3 || J == 4 || J == 6 || J == 8 || J == 9 || J == 12 || J == 16,
                   "the products n2 k1 of the 5 x 5 split");
@@ -307,11 +387,11 @@ template <int J> __device__ __forceinline__ float2 w25mul(float2 a)
                           : J == 9 ? 0.7705132427757893f
                           : J == 12 ? 0.12533323356430454f
                                    : -0.7705132427757894f; // J == 16
-    return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+    return crot(a, c, s);
 }
 
 // 25 = 5 x 5: DFT5 over n1 for each n2 (x[5 n1 + n2]), twiddle W_25^{n2 k1}, DFT5 over n2 -> y[k1 + 5 k2].
-template <int N2> __device__ __forceinline__ void w25row(float2* a)
+template <int N2, class C> __device__ __forceinline__ void w25row(C* a)
 {
     if constexpr (N2 > 0)
     {
@@ -323,18 +403,18 @@ template <int N2> __device__ __forceinline__ void w25row(float2* a)
 }
 
 // Multiply by the compile-time root W_9^J (forward sign) for J in {1, 2, 4}: cos/sin of 2πJ/9.
-template <int J> __device__ __forceinline__ float2 w9mul(float2 a)
+template <int J, class C> __device__ __forceinline__ C w9mul(C a)
 {
     constexpr float c = J == 1 ? 0.76604444311897804f : J == 2 ? 0.17364817766693041f : -0.93969262078590832f;
     constexpr float s = J == 1 ? 0.64278760968653933f : J == 2 ? 0.98480775301220802f : 0.34202014332566888f;
-    return make_float2(a.x * c + a.y * s, a.y * c - a.x * s);
+    return crot(a, c, s);
 }
 
 template <> struct Dft<25>
 {
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        float2 a[5][5];
+        C a[5][5];
 #pragma unroll
         for (int n2 = 0; n2 < 5; ++n2)
         {
@@ -350,7 +430,7 @@ template <> struct Dft<25>
 #pragma unroll
         for (int k1 = 0; k1 < 5; ++k1)
         {
-            float2 b[5] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1], a[4][k1]};
+            C b[5] = {a[0][k1], a[1][k1], a[2][k1], a[3][k1], a[4][k1]};
             Dft<5>::run(b);
 #pragma unroll
             for (int k2 = 0; k2 < 5; ++k2)
@@ -363,9 +443,9 @@ template <> struct Dft<25>
 // radix 9 replaces two stages of radix 3 (one exchange through shared memory fewer) for lengths with 3^2 as a factor.
 template <> struct Dft<9>
 {
-    __device__ __forceinline__ static void run(float2* v)
+    template <class C> __device__ __forceinline__ static void run(C* v)
     {
-        float2 a[3][3];
+        C a[3][3];
 #pragma unroll
         for (int n2 = 0; n2 < 3; ++n2)
         {
@@ -381,7 +461,7 @@ template <> struct Dft<9>
 #pragma unroll
         for (int k1 = 0; k1 < 3; ++k1)
         {
-            float2 b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+            C b[3] = {a[0][k1], a[1][k1], a[2][k1]};
             Dft<3>::run(b);
 #pragma unroll
             for (int k2 = 0; k2 < 3; ++k2)

@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kMaxThreads)
     const long long line = line0 + ll;
     Ctx c;
     c.ok = line < d.lines;
-    c.q = (line % d.lines_per_group) / d.ftw_div;
+    c.q = line_row(d, line);
     c.in = gin + line_offset(d.in, line, d.lines_per_group);
     c.out = gout + line_offset(d.out, line, d.lines_per_group);
     c.jt = jt;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(kMaxThreads)
     init_scales(d, c);
     c.in_im = 1.0f;
     const LayRow<1> lay{sm + ll * line_pitch(n)};
-    const long long sig = line / nscales, s = line - sig * nscales;
+    const long long sig = idiv(line, nscales), s = line - sig * nscales;
     if (c.ok)
     {
         const float2* x = X + sig * n;

@@ -2,6 +2,7 @@
 // copy of the signals, the product of each signal's spectrum with every scale's kernel spectrum, and the epilogue
 // that turns each filtered sequence into coefficients (crd-hesap-wavelet cwt.hpp:509-516, 583-596). All three are
 // HBM-bound: one read and one write per element, 64-bit indices, grid-stride loops.
+#include "index.cuh"
 #include "kernels.hpp"
 
 #include <algorithm>
@@ -26,7 +27,7 @@ __global__ void __launch_bounds__(kThreads) cwt_pad_kernel(const float* __restri
     for (long long e = blockIdx.x * static_cast<long long>(kThreads) + threadIdx.x; e < total;
          e += static_cast<long long>(gridDim.x) * kThreads)
     {
-        const long long c = e / lfft, i = e - c * lfft;
+        const long long c = idiv(e, lfft), i = e - c * lfft;
         X[e] = i < n ? make_float2(__ldg(x + c * n + i), 0.0f) : make_float2(0.0f, 0.0f);
     }
 }
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__(kThreads) cwt_product_kernel(const float2* __r
                                                                long long lfft, long long nscales)
 {
     const long long line = blockIdx.y;
-    const long long c = line / nscales, s = line - c * nscales;
+    const long long c = idiv(line, nscales), s = line - c * nscales;
     const float2* x = X + c * lfft;
     const float2* k = K + s * lfft;
     float2* w = W + line * lfft;
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(kThreads) cwt_diff_kernel(const float2* __rest
                                                             float inv_lfft)
 {
     const long long line = blockIdx.y;
-    const CwtScale p = sc[line % nscales];
+    const CwtScale p = sc[imod(line, nscales)];
     const float2* w = W + line * lfft + p.off;
     float2* o = out + line * n;
     for (long long i = blockIdx.x * static_cast<long long>(kThreads) + threadIdx.x; i < n;

@@ -35,6 +35,17 @@ PipeFn s_512_pipe(const PassDesc&, const PassShape&);
 PipeFn s_4096_pipe(const PassDesc&, const PassShape&);
 PipeFn s_105_pipe(const PassDesc&, const PassShape&);
 
+KernelFn spill_free(KernelFn narrow, KernelFn wide)
+{
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(narrow)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return narrow;
+    }
+    return a.localSizeBytes > 0 ? wide : narrow;
+}
+
 KernelFn select_static(const PassDesc& d, const PassShape& sh)
 {
     for (auto f : {s_1024_classic, s_1024w_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic,
@@ -62,7 +73,10 @@ bool pass_has_static(const PassDesc& d, int points_per_thread)
 }
 
 int pass_lines_per_cta_limit() { return lfft::kMaxLinesPerCta; }
-int pass_threads_limit() { return lfft::kMaxThreads; }
+int pass_threads_limit(int points_per_thread, long long n)
+{
+    return lfft::max_threads(points_per_thread, static_cast<int>(n));
+}
 int pass_pipe_threads() { return lfft::kPipeThreads; }
 int pass_line_pitch(int n) { return lfft::line_pitch(n); }
 
@@ -161,7 +175,7 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
         if (cs.smem_bytes > 227 * 1024)
             return cudaErrorInvalidConfiguration;
     }
-    if (fn == nullptr || threads > lfft::kMaxThreads)
+    if (fn == nullptr || threads > lfft::max_threads(sh.points_per_thread, d.n))
         return cudaErrorInvalidConfiguration;
     if (groups > 0x7fffffffLL)
         return cudaErrorInvalidConfiguration;

@@ -23,6 +23,7 @@
 //    transforms the current group, so HBM reads stay in flight through the compute. Every barrier wait is bounded.
 
 #include "codelets.cuh"
+#include "index.cuh"
 #include "kernels.hpp"
 #include "pass_desc.hpp"
 
@@ -39,6 +40,18 @@ namespace lfft
 
 constexpr int kMaxLinesPerCta = 256;
 constexpr int kMaxThreads = 512;
+// The classic kernel's CTA size limit at P points a thread on lines of n points: 32 points a thread need more than
+// the 128 registers a 512-thread CTA allows, so they run at up to 256 threads a CTA, except on lines longer than
+// 8192 points, which need 512 threads a line.
+__host__ __device__ constexpr int max_threads(int P, int n) { return P <= 16 || n > 8192 ? kMaxThreads : 256; }
+// Register budgets of the classic kernel. Each instance compiles twice: 16 points a thread within 64 registers (four
+// 256-thread CTAs an SM) and within 80 (three); 32 points a thread within 128 and within 168 (lines of more than 8192
+// points, 512 threads a CTA, within 128 only). The launch takes the narrow build unless it spills, since a spill is
+// a local-memory round trip inside the stages (measured: an 8-byte spill made the 4096-point kernel 35 % slower than
+// the same code in 80 registers without one), while the extra registers cost resident warps (the 1024-point
+// four-step row pass ran 3 % slower in 80, the 105-point column pass 10 % slower).
+template <class S, int P> constexpr int line_regs_narrow() { return P <= 16 ? 64 : 128; }
+template <class S, int P> constexpr int line_regs_wide() { return P <= 16 ? 80 : (S::n > 8192 ? 128 : 168); }
 constexpr int kStaticThreads = 256; // the real-line and spectral kernels with a compile-time schedule
 constexpr int kPipeThreads = 256;
 
@@ -329,9 +342,17 @@ template <class S> __device__ __forceinline__ int sched_n(const PassDesc& d)
 // Global offset of line `line` under a line map.
 __device__ __forceinline__ long long line_offset(const LineMap& m, long long line, long long lpg)
 {
-    const long long g = line / lpg;
+    if (lpg == 1)
+        return line * m.gdist;
+    const long long g = idiv(line, lpg);
     const long long q = line - g * lpg;
     return g * m.gdist + q * m.ldist;
+}
+
+// The four-step twiddle row of a line: its index within its group divided by the pass's row divisor.
+__device__ __forceinline__ long long line_row(const PassDesc& d, long long line)
+{
+    return idiv(imod(line, d.lines_per_group), d.ftw_div);
 }
 
 // Visits every (line a < lpc, element e < n) of the CTA's tile once across its threads, consecutive threads along
@@ -376,11 +397,10 @@ __device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
 
 // ---- classic kernel ---------------------------------------------------------------------------------------------
 
-// 16 points a thread on lines of 256 points or more: registers for two 512-thread CTAs (or four of 256) an SM
-// (shorter lines keep the compiler's own choice, which used fewer registers).
-template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
-__global__ void __launch_bounds__(kMaxThreads, (P <= 16 && S::n >= 256) ? 2 : 0)
-    line_fft_kernel(const PassDesc d, const float2* __restrict__ gin, float2* __restrict__ gout)
+// REGS: the register budget (line_regs_narrow / line_regs_wide).
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI, int REGS>
+__global__ void __maxnreg__(REGS) line_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
+                                                  float2* __restrict__ gout)
 {
     extern __shared__ float2 sm[];
     __shared__ long long s_in_off[kMaxLinesPerCta];
@@ -413,7 +433,7 @@ __global__ void __launch_bounds__(kMaxThreads, (P <= 16 && S::n >= 256) ? 2 : 0)
             const long long line = line0 + i;
             s_in_off[i] = line_offset(d.in, line, d.lines_per_group);
             s_out_off[i] = line_offset(d.out, line, d.lines_per_group);
-            s_q[i] = static_cast<int>(line % d.lines_per_group) / d.ftw_div;
+            s_q[i] = static_cast<int>(line_row(d, line));
         }
         __syncthreads();
     }
@@ -421,7 +441,7 @@ __global__ void __launch_bounds__(kMaxThreads, (P <= 16 && S::n >= 256) ? 2 : 0)
     const long long line = line0 + ll;
     Ctx c;
     c.ok = line < d.lines;
-    c.q = (line % d.lines_per_group) / d.ftw_div;
+    c.q = line_row(d, line);
     c.in = gin + line_offset(d.in, line, d.lines_per_group);
     c.out = gout + line_offset(d.out, line, d.lines_per_group);
     c.jt = jt;
@@ -640,12 +660,12 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
             {
                 const long long ln = grp * lpc + i;
                 s_out_off[i] = line_offset(d.out, ln, d.lines_per_group);
-                s_q[i] = static_cast<int>(ln % d.lines_per_group) / d.ftw_div;
+                s_q[i] = static_cast<int>(line_row(d, ln));
             }
         }
         const long long line = grp * lpc + ll;
         c.ok = line < d.lines;
-        c.q = (line % d.lines_per_group) / d.ftw_div;
+        c.q = line_row(d, line);
         c.in = gin;
         c.out = gout + line_offset(d.out, line, d.lines_per_group);
         if constexpr (MAP == PassMap::Row)
@@ -683,19 +703,37 @@ __global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDes
 using KernelFn = void (*)(const PassDesc, const float2*, float2*);
 using PipeFn = void (*)(const PassDesc, const float2*, float2*, int, long long);
 
+// The build of one classic instance that launches: the narrow register budget unless its build spills (local
+// memory per thread above zero), decided once per instance.
+KernelFn spill_free(KernelFn narrow, KernelFn wide);
+
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI> KernelFn pick_regs()
+{
+    constexpr int a = line_regs_narrow<S, P>();
+    constexpr int b = line_regs_wide<S, P>();
+    if constexpr (a == b)
+        return line_fft_kernel<S, P, MAP, DL, DS, EPI, a>;
+    else
+    {
+        static const KernelFn k = spill_free(line_fft_kernel<S, P, MAP, DL, DS, EPI, a>,
+                                             line_fft_kernel<S, P, MAP, DL, DS, EPI, b>);
+        return k;
+    }
+}
+
 template <class S, int P, bool EPI> KernelFn pick_e(PassMap map, bool dl, bool ds)
 {
     if (map == PassMap::Row)
     {
-        if (dl && ds) return line_fft_kernel<S, P, PassMap::Row, true, true, EPI>;
-        if (dl) return line_fft_kernel<S, P, PassMap::Row, true, false, EPI>;
-        if (ds) return line_fft_kernel<S, P, PassMap::Row, false, true, EPI>;
-        return line_fft_kernel<S, P, PassMap::Row, false, false, EPI>;
+        if (dl && ds) return pick_regs<S, P, PassMap::Row, true, true, EPI>();
+        if (dl) return pick_regs<S, P, PassMap::Row, true, false, EPI>();
+        if (ds) return pick_regs<S, P, PassMap::Row, false, true, EPI>();
+        return pick_regs<S, P, PassMap::Row, false, false, EPI>();
     }
-    if (dl && ds) return line_fft_kernel<S, P, PassMap::Col, true, true, EPI>;
-    if (dl) return line_fft_kernel<S, P, PassMap::Col, true, false, EPI>;
-    if (ds) return line_fft_kernel<S, P, PassMap::Col, false, true, EPI>;
-    return line_fft_kernel<S, P, PassMap::Col, false, false, EPI>;
+    if (dl && ds) return pick_regs<S, P, PassMap::Col, true, true, EPI>();
+    if (dl) return pick_regs<S, P, PassMap::Col, true, false, EPI>();
+    if (ds) return pick_regs<S, P, PassMap::Col, false, true, EPI>();
+    return pick_regs<S, P, PassMap::Col, false, false, EPI>();
 }
 
 template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds, bool epi)

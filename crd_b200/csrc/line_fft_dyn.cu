@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(kMaxThreads) dyn_fft_kernel(const PassDesc d, 
         const long long line = line0 + i;
         s_in_off[i] = line_offset(d.in, line, d.lines_per_group);
         s_out_off[i] = line_offset(d.out, line, d.lines_per_group);
-        s_q[i] = static_cast<int>(line % d.lines_per_group) / d.ftw_div;
+        s_q[i] = static_cast<int>(line_row(d, line));
     }
     if (tid < kMaxStages)
         s_radix[tid] = d.radix[tid];

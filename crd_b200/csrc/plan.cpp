@@ -499,7 +499,7 @@ PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, in
     if (lpc <= 0)
         lpc = map == PassMap::Row ? std::max(1, 256 / T) : std::max(1, 512 / T);
     lpc = std::min(lpc, pass_lines_per_cta_limit());
-    while (lpc > 1 && lpc * T > pass_threads_limit())
+    while (lpc > 1 && lpc * T > pass_threads_limit(P, n))
         --lpc;
     const bool needs_smem = !(dl && ds && nstages == 1);
     while (needs_smem && lpc > 1 && lpc * pitch_bytes > kMaxSmemBytes)
@@ -566,7 +566,7 @@ bool heuristic_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape
     if (want32)
     {
         const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, 32);
-        if (sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit() && pass_has_kernel(d, sh))
+        if (sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit(sh.points_per_thread, d.n) && pass_has_kernel(d, sh))
         {
             *out = sh;
             return true;
@@ -579,7 +579,7 @@ bool heuristic_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape
         for (int P : {16, 32})
         {
             const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, P);
-            if (sh.threads_per_line * sh.lines_per_cta > pass_threads_limit())
+            if (sh.threads_per_line * sh.lines_per_cta > pass_threads_limit(P, d.n))
                 continue;
             if (pass == 0 ? pass_has_static(d, P) : pass_has_kernel(d, sh))
             {
@@ -596,7 +596,8 @@ std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl,
 {
     std::vector<PassShape> out;
     auto add = [&](const PassShape& sh) {
-        if (sh.threads_per_line * sh.lines_per_cta > (sh.pipelined ? pass_pipe_threads() : pass_threads_limit()))
+        if (sh.threads_per_line * sh.lines_per_cta >
+            (sh.pipelined ? pass_pipe_threads() : pass_threads_limit(sh.points_per_thread, d.n)))
             return;
         if (!pass_has_kernel(d, sh))
             return;
@@ -639,7 +640,8 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
         PassShape sh;
         if (w.pipelined ? pipe_shape(d, map, &sh, w.lines_per_cta)
                         : (sh = shape_with(d.n, d.nstages, map, dl, ds, w.points_per_thread, w.lines_per_cta),
-                           sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit() && pass_has_kernel(d, sh)))
+                           sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit(sh.points_per_thread, d.n) &&
+                               pass_has_kernel(d, sh)))
         {
             *out = sh;
             return true;

@@ -2,6 +2,7 @@
 // three chirp passes of Bluestein. All are streaming, HBM-bound grid-stride kernels.
 
 #include "codelets.cuh"
+#include "index.cuh"
 #include "kernels.hpp"
 
 #include <cuda_runtime.h>
@@ -118,7 +119,7 @@ __global__ void chirp_pre_kernel(const ChirpDesc p, const float2* x, float2* w)
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x)
     {
-        const long long t = i / p.m;
+        const long long t = idiv(i, p.m);
         const long long k = i - t * p.m;
         float2 r = make_float2(0.f, 0.f);
         if (k < p.n)
@@ -141,7 +142,7 @@ __global__ void spectrum_mul_kernel(const ChirpDesc p, float2* w)
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x)
     {
-        const long long t = i / p.m;
+        const long long t = idiv(i, p.m);
         const long long k = i - t * p.m;
         float2* wt = w + t * p.wdist;
         wt[k] = cmul(wt[k], bf[k]);
@@ -156,7 +157,7 @@ __global__ void chirp_post_kernel(const ChirpDesc p, const float2* w, float2* x)
     for (long long i = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; i < total;
          i += static_cast<long long>(gridDim.x) * blockDim.x)
     {
-        const long long t = i / p.n;
+        const long long t = idiv(i, p.n);
         const long long k = i - t * p.n;
         const float2 v = w[t * p.wdist + k];
         const float2 c = ch[k];

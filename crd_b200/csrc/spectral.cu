@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(DYN ? kMaxThreads : kStaticThreads, DYN ? 1 : 
     const int jt = tid - ll * T;
     const int pitch = line_pitch(M);
     const int nfreq = M + 1;
-    const long long g = blockIdx.x / sd.ntiles;
+    const long long g = idiv(blockIdx.x, sd.ntiles);
     const int tile = static_cast<int>(blockIdx.x - g * sd.ntiles);
     const long long seg0 = static_cast<long long>(tile) * lpc;
     const int nl = static_cast<int>(sd.nseg - seg0 < lpc ? sd.nseg - seg0 : lpc);

@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kTcThreads, 2)
     // Remaining stages on the FP32 pipes, the last one storing to global memory.
     Ctx c;
     c.ok = ok;
-    c.q = (line % d.lines_per_group) / d.ftw_div;
+    c.q = line_row(d, line);
     c.in = nullptr;
     c.out = gout + line_offset(d.out, ok ? line : line0, d.lines_per_group);
     c.jt = tid - ll * T;

@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n, GEOM), t
     const uint32_t tile_bytes = static_cast<uint32_t>(N) * kTmaCols * 8u;
 
     auto issue = [&](long long k, int b) {
-        const long long grp = k / tiles_per_group;
+        const long long grp = idiv(k, tiles_per_group);
         const int q0 = static_cast<int>(k - grp * tiles_per_group) * kTmaCols;
         uint64_t* bar = bars + b;
         mbar_expect_tx(bar, tile_bytes);
@@ -144,12 +144,12 @@ __global__ void __launch_bounds__(((S::n + P - 1) / P) * tma_cols(S::n, GEOM), t
             __syncthreads();
             return;
         }
-        const long long grp = k / tiles_per_group;
+        const long long grp = idiv(k, tiles_per_group);
         const long long q0 = (k - grp * tiles_per_group) * kTmaCols;
         const long long line = grp * n2 + q0 + ll;
         Ctx c;
         c.ok = true;
-        c.q = (q0 + ll) / d.ftw_div;
+        c.q = idiv(q0 + ll, d.ftw_div);
         c.in = nullptr;
         c.out = gout + line_offset(d.out, line, n2);
         c.jt = jt;
