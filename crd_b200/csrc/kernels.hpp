@@ -86,6 +86,7 @@ bool tma_col_supported(const PassDesc& d);
 cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStream_t stream);
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
+int pass_cta_line_pitch(int n, int lpc); // the compile-time-schedule kernel's line pitch (complex elements)
 int pass_threads_limit(int points_per_thread, long long n); // classic kernel CTA size limit
 int pass_pipe_threads();
 int pass_pipe_smem(int n, PassMap map, int lpc);

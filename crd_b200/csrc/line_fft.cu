@@ -46,6 +46,17 @@ KernelFn spill_free(KernelFn narrow, KernelFn wide)
     return a.localSizeBytes > 0 ? wide : narrow;
 }
 
+PipeFn spill_free_pipe(PipeFn narrow, PipeFn wide)
+{
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, reinterpret_cast<const void*>(narrow)) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return narrow;
+    }
+    return a.localSizeBytes > 0 ? wide : narrow;
+}
+
 KernelFn select_static(const PassDesc& d, const PassShape& sh)
 {
     for (auto f : {s_1024_classic, s_1024w_classic, s_256_classic, s_512_classic, s_4096_classic, s_4096c_classic,
@@ -79,6 +90,7 @@ int pass_threads_limit(int points_per_thread, long long n)
 }
 int pass_pipe_threads() { return lfft::kPipeThreads; }
 int pass_line_pitch(int n) { return lfft::line_pitch(n); }
+int pass_cta_line_pitch(int n, int lpc) { return lfft::cta_line_pitch(n, lpc); }
 
 int pass_pipe_smem(int n, PassMap map, int lpc)
 {
@@ -163,7 +175,7 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
         // an input pointer off a 16-byte boundary: the classic kernel with the same thread map
         cs.pipelined = false;
         cs.direct_load = sh.map == PassMap::Row ? d.in.estride == 1 : d.in.ldist == 1;
-        cs.smem_bytes = sh.lines_per_cta * lfft::line_pitch(d.n) * 8;
+        cs.smem_bytes = sh.lines_per_cta * lfft::cta_line_pitch(d.n, sh.lines_per_cta) * 8;
     }
     lfft::KernelFn fn = lfft::select_static(d, cs);
     if (fn == nullptr)

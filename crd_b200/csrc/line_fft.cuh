@@ -57,6 +57,18 @@ constexpr int kPipeThreads = 256;
 
 // Classic layout: one pad slot every 16 complex (128 bytes) keeps the strided stage accesses spread over the banks.
 __host__ __device__ constexpr int line_pitch(int n) { return (n + (n >> 4)) | 1; }
+// The compile-time-schedule kernel's lines: with 2, 4 or 8 lines a CTA, line l starts 16 / lpc bank slots (8-byte
+// slots, 16 to a 128-byte wavefront) after line l - 1 modulo 16, so that a warp reading the same elements of all its
+// lines (the last stage of a transposed store, the coalesced loads across lines) touches 16 distinct slots in each
+// half-warp: no bank conflict. Other line counts keep the odd pitch.
+__host__ __device__ constexpr int cta_line_pitch(int n, int lpc)
+{
+    if (lpc != 2 && lpc != 4 && lpc != 8)
+        return line_pitch(n);
+    const int base = n + (n >> 4);
+    const int want = 16 / lpc;
+    return base + (((want - base) % 16) + 16) % 16;
+}
 // Pipelined row layout: two pad slots (16 bytes) every 16 complex, so each 128-byte chunk of a line lands on a
 // 16-byte boundary for the bulk copy; the line pitch is 2 mod 4 slots to spread cross-line accesses.
 __host__ __device__ constexpr int pipe_row_pitch(int n)
@@ -411,7 +423,7 @@ __global__ void __maxnreg__(REGS) line_fft_kernel(const PassDesc d, const float2
     const int T = (n + P - 1) / P;
     const int lpc = blockDim.x / T;
     const int tid = threadIdx.x;
-    const int pitch = line_pitch(n);
+    const int pitch = cta_line_pitch(n, lpc);
     const long long line0 = static_cast<long long>(blockIdx.x) * lpc;
 
     int ll, jt;
@@ -465,6 +477,8 @@ __global__ void __maxnreg__(REGS) line_fft_kernel(const PassDesc d, const float2
 
     if constexpr (!DS)
     {
+        // (Storing the last stage straight from registers with the threads across the lines, which saves this
+        // shared-memory round trip and its bank conflicts, measured 20 % slower on the four-step row pass.)
         const long long lines_here = d.lines - line0;
         const long long es = d.out.estride;
         for_tile(n, lpc, es == 1, [&](int a, int e) {
@@ -577,10 +591,10 @@ __device__ __forceinline__ void pipe_issue(const PassDesc& d, const float2* gin,
     }
 }
 
-template <class S, int P, PassMap MAP, bool DS, bool EPI>
-__global__ void __launch_bounds__(kPipeThreads, 2) pipe_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
-                                                                   float2* __restrict__ gout, int lpc,
-                                                                   long long ngroups)
+// REGS: 80 (three 256-thread CTAs an SM) or 128 (two); the launch takes the 80-register build unless it spills.
+template <class S, int P, PassMap MAP, bool DS, bool EPI, int REGS>
+__global__ void __maxnreg__(REGS) pipe_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
+                                                  float2* __restrict__ gout, int lpc, long long ngroups)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ long long s_out_off[kMaxLinesPerCta];
@@ -741,11 +755,20 @@ template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds, bool epi)
     return epi ? pick_e<S, P, true>(map, dl, ds) : pick_e<S, P, false>(map, dl, ds);
 }
 
+PipeFn spill_free_pipe(PipeFn narrow, PipeFn wide);
+
+template <class S, int P, PassMap MAP, bool DS, bool EPI> PipeFn pick_pipe_regs()
+{
+    static const PipeFn k = spill_free_pipe(pipe_fft_kernel<S, P, MAP, DS, EPI, 80>,
+                                            pipe_fft_kernel<S, P, MAP, DS, EPI, 128>);
+    return k;
+}
+
 template <class S, int P, bool EPI> PipeFn pick_pipe_e(PassMap map, bool ds)
 {
     if (map == PassMap::Row)
-        return ds ? pipe_fft_kernel<S, P, PassMap::Row, true, EPI> : pipe_fft_kernel<S, P, PassMap::Row, false, EPI>;
-    return ds ? pipe_fft_kernel<S, P, PassMap::Col, true, EPI> : pipe_fft_kernel<S, P, PassMap::Col, false, EPI>;
+        return ds ? pick_pipe_regs<S, P, PassMap::Row, true, EPI>() : pick_pipe_regs<S, P, PassMap::Row, false, EPI>();
+    return ds ? pick_pipe_regs<S, P, PassMap::Col, true, EPI>() : pick_pipe_regs<S, P, PassMap::Col, false, EPI>();
 }
 
 template <class S, int P> PipeFn pick_pipe(PassMap map, bool ds, bool epi)

@@ -495,17 +495,18 @@ PassShape shape_with(long long n, int nstages, PassMap map, bool dl, bool ds, in
     sh.points_per_thread = P;
     const int T = static_cast<int>((n + P - 1) / P);
     sh.threads_per_line = T;
-    const int pitch_bytes = pass_line_pitch(static_cast<int>(n)) * 8;
+    // the compile-time-schedule kernel's pitch (at least the run-time kernel's, which sizes its own two buffers)
+    auto tile_bytes = [&](int l) { return l * pass_cta_line_pitch(static_cast<int>(n), l) * 8; };
     if (lpc <= 0)
         lpc = map == PassMap::Row ? std::max(1, 256 / T) : std::max(1, 512 / T);
     lpc = std::min(lpc, pass_lines_per_cta_limit());
     while (lpc > 1 && lpc * T > pass_threads_limit(P, n))
         --lpc;
     const bool needs_smem = !(dl && ds && nstages == 1);
-    while (needs_smem && lpc > 1 && lpc * pitch_bytes > kMaxSmemBytes)
+    while (needs_smem && lpc > 1 && tile_bytes(lpc) > kMaxSmemBytes)
         --lpc;
     sh.lines_per_cta = lpc;
-    sh.smem_bytes = needs_smem ? lpc * pitch_bytes : 0;
+    sh.smem_bytes = needs_smem ? tile_bytes(lpc) : 0;
     return sh;
 }
 
