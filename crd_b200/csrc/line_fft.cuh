@@ -40,18 +40,13 @@ namespace lfft
 
 constexpr int kMaxLinesPerCta = 256;
 constexpr int kMaxThreads = 512;
-// The classic kernel's CTA size limit at P points a thread on lines of n points: 32 points a thread need more than
-// the 128 registers a 512-thread CTA allows, so they run at up to 256 threads a CTA, except on lines longer than
-// 8192 points, which need 512 threads a line.
-__host__ __device__ constexpr int max_threads(int P, int n) { return P <= 16 || n > 8192 ? kMaxThreads : 256; }
-// Register budgets of the classic kernel. Each instance compiles twice: 16 points a thread within 64 registers (four
-// 256-thread CTAs an SM) and within 80 (three); 32 points a thread within 128 and within 168 (lines of more than 8192
-// points, 512 threads a CTA, within 128 only). The launch takes the narrow build unless it spills, since a spill is
-// a local-memory round trip inside the stages (measured: an 8-byte spill made the 4096-point kernel 35 % slower than
-// the same code in 80 registers without one), while the extra registers cost resident warps (the 1024-point
-// four-step row pass ran 3 % slower in 80, the 105-point column pass 10 % slower).
-template <class S, int P> constexpr int line_regs_narrow() { return P <= 16 ? 64 : 128; }
-template <class S, int P> constexpr int line_regs_wide() { return P <= 16 ? 80 : (S::n > 8192 ? 128 : 168); }
+// The classic kernel's CTA size limit (both register budgets fit a 512-thread CTA).
+__host__ __device__ constexpr int max_threads(int, int) { return kMaxThreads; }
+// Register budgets of the classic kernel: each instance compiles twice (line_fft_kernel, line_fft_kernel_wide) and
+// the launch takes the narrow build unless it spills, since a spill is a local-memory round trip inside the stages
+// (measured: an 8-byte spill made the 4096-point kernel 35 % slower than the same code in 80 registers without one),
+// while the extra registers cost resident warps (the 1024-point four-step row pass ran 3 % slower in 80, the 105-point
+// lines 20 % slower under a plain 128-register cap than under the launch-bounds hint).
 constexpr int kStaticThreads = 256; // the real-line and spectral kernels with a compile-time schedule
 constexpr int kPipeThreads = 256;
 
@@ -409,10 +404,9 @@ __device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
 
 // ---- classic kernel ---------------------------------------------------------------------------------------------
 
-// REGS: the register budget (line_regs_narrow / line_regs_wide).
-template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI, int REGS>
-__global__ void __maxnreg__(REGS) line_fft_kernel(const PassDesc d, const float2* __restrict__ gin,
-                                                  float2* __restrict__ gout)
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
+__device__ __forceinline__ void line_fft_body(const PassDesc& d, const float2* __restrict__ gin,
+                                              float2* __restrict__ gout)
 {
     extern __shared__ float2 sm[];
     __shared__ long long s_in_off[kMaxLinesPerCta];
@@ -487,6 +481,24 @@ __global__ void __maxnreg__(REGS) line_fft_kernel(const PassDesc d, const float2
                        epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
         });
     }
+}
+
+// The two register budgets of the classic kernel. The narrow build keeps the launch-bounds hint (two 512-thread CTAs
+// an SM at 16 points a thread on lines of 256 points or more, 64 registers; the compiler's own choice within 128
+// otherwise); the wide build caps the registers directly at 80 (16 points a thread; 32 points a thread keep 128,
+// what a 512-thread CTA allows) and is what launches when the narrow build spills.
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
+__global__ void __launch_bounds__(kMaxThreads, (P <= 16 && S::n >= 256) ? 2 : 0)
+    line_fft_kernel(const PassDesc d, const float2* __restrict__ gin, float2* __restrict__ gout)
+{
+    line_fft_body<S, P, MAP, DL, DS, EPI>(d, gin, gout);
+}
+
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
+__global__ void __maxnreg__(P <= 16 ? 80 : 128)
+    line_fft_kernel_wide(const PassDesc d, const float2* __restrict__ gin, float2* __restrict__ gout)
+{
+    line_fft_body<S, P, MAP, DL, DS, EPI>(d, gin, gout);
 }
 
 // ---- pipelined kernel -------------------------------------------------------------------------------------------
@@ -721,38 +733,39 @@ using PipeFn = void (*)(const PassDesc, const float2*, float2*, int, long long);
 // memory per thread above zero), decided once per instance.
 KernelFn spill_free(KernelFn narrow, KernelFn wide);
 
-template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI> KernelFn pick_regs()
+// wide: the shape asks for the 80-register build; otherwise the narrow build, unless it spills.
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI> KernelFn pick_regs(bool wide)
 {
-    constexpr int a = line_regs_narrow<S, P>();
-    constexpr int b = line_regs_wide<S, P>();
-    if constexpr (a == b)
-        return line_fft_kernel<S, P, MAP, DL, DS, EPI, a>;
+    if constexpr (P > 16) // 32 points a thread: 128 registers in both builds
+        return line_fft_kernel<S, P, MAP, DL, DS, EPI>;
     else
     {
-        static const KernelFn k = spill_free(line_fft_kernel<S, P, MAP, DL, DS, EPI, a>,
-                                             line_fft_kernel<S, P, MAP, DL, DS, EPI, b>);
+        if (wide)
+            return line_fft_kernel_wide<S, P, MAP, DL, DS, EPI>;
+        static const KernelFn k =
+            spill_free(line_fft_kernel<S, P, MAP, DL, DS, EPI>, line_fft_kernel_wide<S, P, MAP, DL, DS, EPI>);
         return k;
     }
 }
 
-template <class S, int P, bool EPI> KernelFn pick_e(PassMap map, bool dl, bool ds)
+template <class S, int P, bool EPI> KernelFn pick_e(PassMap map, bool dl, bool ds, bool wide)
 {
     if (map == PassMap::Row)
     {
-        if (dl && ds) return pick_regs<S, P, PassMap::Row, true, true, EPI>();
-        if (dl) return pick_regs<S, P, PassMap::Row, true, false, EPI>();
-        if (ds) return pick_regs<S, P, PassMap::Row, false, true, EPI>();
-        return pick_regs<S, P, PassMap::Row, false, false, EPI>();
+        if (dl && ds) return pick_regs<S, P, PassMap::Row, true, true, EPI>(wide);
+        if (dl) return pick_regs<S, P, PassMap::Row, true, false, EPI>(wide);
+        if (ds) return pick_regs<S, P, PassMap::Row, false, true, EPI>(wide);
+        return pick_regs<S, P, PassMap::Row, false, false, EPI>(wide);
     }
-    if (dl && ds) return pick_regs<S, P, PassMap::Col, true, true, EPI>();
-    if (dl) return pick_regs<S, P, PassMap::Col, true, false, EPI>();
-    if (ds) return pick_regs<S, P, PassMap::Col, false, true, EPI>();
-    return pick_regs<S, P, PassMap::Col, false, false, EPI>();
+    if (dl && ds) return pick_regs<S, P, PassMap::Col, true, true, EPI>(wide);
+    if (dl) return pick_regs<S, P, PassMap::Col, true, false, EPI>(wide);
+    if (ds) return pick_regs<S, P, PassMap::Col, false, true, EPI>(wide);
+    return pick_regs<S, P, PassMap::Col, false, false, EPI>(wide);
 }
 
-template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds, bool epi)
+template <class S, int P> KernelFn pick(PassMap map, bool dl, bool ds, bool epi, bool wide)
 {
-    return epi ? pick_e<S, P, true>(map, dl, ds) : pick_e<S, P, false>(map, dl, ds);
+    return epi ? pick_e<S, P, true>(map, dl, ds, wide) : pick_e<S, P, false>(map, dl, ds, wide);
 }
 
 PipeFn spill_free_pipe(PipeFn narrow, PipeFn wide);
@@ -798,7 +811,7 @@ inline bool same_radices(const PassDesc& d, std::initializer_list<int> rs)
     KernelFn NAME##_classic(const PassDesc& d, const PassShape& sh)                                                   \
     {                                                                                                                  \
         if (sh.points_per_thread == P_ && same_radices(d, {__VA_ARGS__}))                                              \
-            return pick<Sched<__VA_ARGS__>, P_>(sh.map, sh.direct_load, sh.direct_store, pass_epi(d));                 \
+            return pick<Sched<__VA_ARGS__>, P_>(sh.map, sh.direct_load, sh.direct_store, pass_epi(d), sh.wide_regs);    \
         return nullptr;                                                                                                \
     }
 #define CRDFFT_DEFINE_PIPE(NAME, P_, ...)                                                                             \

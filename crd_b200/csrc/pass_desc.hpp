@@ -74,6 +74,8 @@ struct PassShape
     bool direct_load;       // first stage reads global memory itself (coalesced for this map)
     bool direct_store;      // last stage writes global memory itself
     int smem_bytes;
+    bool wide_regs;         // compile-time schedules at 16 points a thread: the 80-register build (fewer resident
+                            // warps, no spill) instead of the 64-register one
 };
 
 } // namespace crdfft

@@ -604,9 +604,15 @@ std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl,
             return;
         for (const PassShape& o : out)
             if (o.pipelined == sh.pipelined && o.points_per_thread == sh.points_per_thread &&
-                o.lines_per_cta == sh.lines_per_cta)
+                o.lines_per_cta == sh.lines_per_cta && o.wide_regs == sh.wide_regs)
                 return;
         out.push_back(sh);
+        if (!sh.pipelined && sh.points_per_thread == 16 && pass_has_static(d, 16))
+        {
+            PassShape w = sh;
+            w.wide_regs = true; // the same shape on the 80-register build
+            out.push_back(w);
+        }
     };
     for (int P : {16, 32})
     {
@@ -641,6 +647,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
         PassShape sh;
         if (w.pipelined ? pipe_shape(d, map, &sh, w.lines_per_cta)
                         : (sh = shape_with(d.n, d.nstages, map, dl, ds, w.points_per_thread, w.lines_per_cta),
+                           sh.wide_regs = w.wide_regs,
                            sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit(sh.points_per_thread, d.n) &&
                                pass_has_kernel(d, sh)))
         {
@@ -677,6 +684,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
                 e.pipelined = top[best].pipelined;
                 e.points_per_thread = top[best].points_per_thread;
                 e.lines_per_cta = top[best].lines_per_cta;
+                e.wide_regs = top[best].wide_regs;
                 e.ms = ms[best];
                 wisdom_store(key, e);
                 *out = top[best];
@@ -707,6 +715,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
             e.pipelined = cands[best].pipelined;
             e.points_per_thread = cands[best].points_per_thread;
             e.lines_per_cta = cands[best].lines_per_cta;
+            e.wide_regs = cands[best].wide_regs;
             e.ms = ms[best];
             wisdom_store(key, e);
             *out = cands[best];

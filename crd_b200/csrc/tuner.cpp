@@ -157,8 +157,13 @@ std::string wisdom_export()
     std::ostringstream o;
     o << "crdfft-wisdom 1\n";
     for (const auto& kv : g_wisdom)
+    {
         o << kv.first << ' ' << (kv.second.pipelined ? 1 : 0) << ' ' << kv.second.points_per_thread << ' '
-          << kv.second.lines_per_cta << ' ' << kv.second.ms << '\n';
+          << kv.second.lines_per_cta << ' ' << kv.second.ms;
+        if (kv.second.wide_regs)
+            o << " w"; // the 80-register build
+        o << '\n';
+    }
     for (const auto& kv : g_decomp)
         o << kv.first << ' ' << kv.second.kind << ' ' << kv.second.n1 << ' ' << kv.second.ms << '\n';
     return o.str();
@@ -190,6 +195,13 @@ int wisdom_import(const std::string& text)
         WisdomEntry e;
         if (!(ls >> key >> pipe >> e.points_per_thread >> e.lines_per_cta >> e.ms))
             return -1;
+        std::string flag;
+        if (ls >> flag)
+        {
+            if (flag != "w")
+                return -1;
+            e.wide_regs = true;
+        }
         if ((e.points_per_thread != 16 && e.points_per_thread != 32) || e.lines_per_cta < 1 ||
             e.lines_per_cta > 256)
             return -1;
@@ -358,9 +370,9 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
         for (size_t i = 0; i < cands.size(); ++i)
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d lines=%lld ms=%.6f", key.c_str(),
-                          cands[i].pipelined ? 1 : 0, cands[i].points_per_thread, cands[i].lines_per_cta, d0.lines,
-                          static_cast<double>((*ms)[i]));
+            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d wide=%d lines=%lld ms=%.6f", key.c_str(),
+                          cands[i].pipelined ? 1 : 0, cands[i].points_per_thread, cands[i].lines_per_cta,
+                          cands[i].wide_regs ? 1 : 0, d0.lines, static_cast<double>((*ms)[i]));
             g_log += buf;
             float f[kPassFeatures];
             pass_features(d0, cands[i], f);

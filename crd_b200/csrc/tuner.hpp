@@ -32,6 +32,7 @@ struct WisdomEntry
     int points_per_thread = 16;
     int lines_per_cta = 1;
     float ms = 0.0f;
+    bool wide_regs = false;
 };
 
 // The geometry class of a pass: line length and radices, thread map, direct load/store, epilogue, line counts

@@ -123,3 +123,19 @@ def test_wisdom_text_round_trip_without_device():
         assert entries(H.wisdom_export()) == entries(text)
     finally:
         H.wisdom_forget()
+
+def test_wisdom_register_budget_flag_round_trips():
+    """A shape measured on the wide register build is remembered with a trailing `w`; any other trailing token is
+    refused."""
+    import crd_b200.hesap as H
+
+    H.wisdom_forget()
+    try:
+        text = "crdfft-wisdom 1\nDEV|n4096:r16.16.16:x 0 16 1 0.5 w\nDEV|n1024:r16.16.4:x 0 16 4 0.25\n"
+        H.wisdom_import(text)
+        lines = sorted(H.wisdom_export().splitlines()[1:])
+        assert lines == ["DEV|n1024:r16.16.4:x 0 16 4 0.25", "DEV|n4096:r16.16.16:x 0 16 1 0.5 w"]
+        with pytest.raises(_lib.CrdFftError):
+            H.wisdom_import("crdfft-wisdom 1\nDEV|n4096:r16.16.16:x 0 16 1 0.5 wide\n")
+    finally:
+        H.wisdom_forget()
