@@ -23,6 +23,14 @@
 
 namespace cg = cooperative_groups;
 
+// Cluster barrier, every thread of every CTA: arrive with release semantics (this CTA's shared-memory writes become
+// visible to the cluster), wait with acquire semantics. The .aligned forms (all threads of the warp execute them
+// together, which holds here) skip the per-thread convergence handling of the generic barrier.
+__device__ __forceinline__ void cluster_barrier()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 namespace crdfft
 {
 namespace lfft
@@ -69,7 +77,7 @@ __global__ void __launch_bounds__((S1::n * S2::n) / (P * C), MINB)
         const LayCol lay{buf + ll, PA};
         SchedRun<S1>::template go<P, true, false, false, Kind<PassMap::Col, EPI>>(dA, c, lay, N1);
     }
-    cluster.sync(); // every CTA's columns are in its shared memory
+    cluster_barrier(); // every CTA's columns are in its shared memory
 
     // ---- exchange: rows k1 of this CTA, all n2, times W_N^{n2 k1}. A thread keeps one column n2 (THREADS is a
     // multiple of N2), so it reads one remote CTA's shared memory, and the twiddles W_N^{n2 k1} come from the
@@ -89,7 +97,7 @@ __global__ void __launch_bounds__((S1::n * S2::n) / (P * C), MINB)
         const int k1 = rank * LB + kl0 + i * KSTEP;
         v[i] = cmul(remote[k1 * PA], __ldg(tw + k1 * N2));
     }
-    cluster.sync(); // every CTA has read what it needs; shared memory may be reused
+    cluster_barrier(); // every CTA's remote reads are performed (release); shared memory may be reused
 #pragma unroll
     for (int i = 0; i < PER; ++i)
         buf[n2 * PB + kl0 + i * KSTEP] = v[i];

@@ -322,8 +322,10 @@ void crdfft_set_planner_mode(int32_t mode);
 crdfft_status crdfft_set_decomposition(int64_t n, int32_t kind, int64_t n1);
 
 /* Wisdom as text ("crdfft-wisdom 1" then one line per pass class: key, pipelined, points a thread, lines a CTA,
- * measured ms), keyed by device name. Export writes a NUL-terminated string into buf when cap suffices and reports
- * the size needed; import merges entries and rejects a malformed text (CRDFFT_INVALID_ARG) without changes. */
+ * measured ms, and a trailing "w" when the pass runs the 80-register build of its kernel; decompositions on lines
+ * starting "D|": key, kind, n1, ms), keyed by device name. Export writes a NUL-terminated string into buf when cap
+ * suffices and reports the size needed; import merges entries and rejects a malformed text (CRDFFT_INVALID_ARG)
+ * without changes. */
 crdfft_status crdfft_wisdom_export(char* buf, size_t cap, size_t* needed);
 crdfft_status crdfft_wisdom_import(const char* text);
 void crdfft_wisdom_forget(void);
