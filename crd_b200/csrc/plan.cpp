@@ -949,7 +949,13 @@ Decomp choose_decomp(const Plan& p, long long n, long long batch, long long istr
         if (k == 1)
             return order[0].second;
     }
-    const long long sample = std::max(1LL, std::min(batch, (64LL << 20) / (8 * n)));
+    // a sample of kPlannerSampleBytes of input (two buffers of it must fit beside the device's current use)
+    size_t free_b = 0, total_b = 0;
+    const bool roomy = cudaMemGetInfo(&free_b, &total_b) == cudaSuccess &&
+                       free_b > static_cast<size_t>(4 * kPlannerSampleBytes);
+    cudaGetLastError();
+    const long long sample_bytes = roomy ? kPlannerSampleBytes : kPlannerSmallSampleBytes;
+    const long long sample = std::max(1LL, std::min(batch, sample_bytes / (8 * n)));
     int best = -1;
     std::vector<float> ms(k, -1.0f);
     for (size_t i = 0; i < k; ++i)

@@ -302,24 +302,32 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
     if (cands.empty())
         return -1;
     PassDesc d = d0;
-    // Whole groups, up to 64 MiB of line data (at least one group; column tiles stay whole).
-    const long long per_line = static_cast<long long>(d.n) * 8;
-    long long lines = std::max<long long>(1, (64LL << 20) / per_line);
-    if (d.lines_per_group > 1)
-        lines = std::max(d.lines_per_group, lines / d.lines_per_group * d.lines_per_group);
-    lines = std::min(lines, d.lines);
-    d.lines = lines;
-    const long long in_ext = extent(d.in, lines, d.lines_per_group, d.n);
-    const long long out_ext = extent(d.out, lines, d.lines_per_group, d.n);
     void* in = nullptr;
     void* out = nullptr;
-    if (cudaMalloc(&in, static_cast<size_t>(in_ext) * 8) != cudaSuccess)
-        return -1;
-    if (cudaMalloc(&out, static_cast<size_t>(out_ext) * 8) != cudaSuccess)
+    long long lines = 0, in_ext = 0, out_ext = 0;
+    // Whole groups, up to the sample size of line data (at least one group; column tiles stay whole); the small
+    // sample when the large one cannot be allocated.
+    for (long long bytes : {kPlannerSampleBytes, kPlannerSmallSampleBytes})
     {
-        cudaFree(in);
-        return -1;
+        const long long per_line = static_cast<long long>(d.n) * 8;
+        lines = std::max<long long>(1, bytes / per_line);
+        if (d.lines_per_group > 1)
+            lines = std::max(d.lines_per_group, lines / d.lines_per_group * d.lines_per_group);
+        lines = std::min(lines, d0.lines);
+        in_ext = extent(d.in, lines, d.lines_per_group, d.n);
+        out_ext = extent(d.out, lines, d.lines_per_group, d.n);
+        if (cudaMalloc(&in, static_cast<size_t>(in_ext) * 8) == cudaSuccess)
+        {
+            if (cudaMalloc(&out, static_cast<size_t>(out_ext) * 8) == cudaSuccess)
+                break;
+            cudaFree(in);
+            in = nullptr;
+        }
+        cudaGetLastError(); // the failed allocation's error is not the caller's
     }
+    if (in == nullptr || out == nullptr)
+        return -1;
+    d.lines = lines;
     cudaStream_t st = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);

@@ -45,8 +45,16 @@ std::string wisdom_export();
 int wisdom_import(const std::string& text); // entries read, or -1 on a malformed line
 void wisdom_forget();
 
+// Bytes of input the measuring planner times a candidate on (a pass's lines, or a decomposition's transforms): large
+// enough that a launch runs in the steady state of a large batch. On 64 MiB samples the ramp and tail of a 30 us
+// launch decided the ranking (the 4096-point pass ranked 32 points a thread first; on 2 GiB it is 2-3 % slower).
+// Falls back to 64 MiB when the device cannot hold two sample buffers.
+inline constexpr long long kPlannerSampleBytes = 512LL << 20;
+inline constexpr long long kPlannerSmallSampleBytes = 64LL << 20;
+
 // Times each candidate (1 warm-up, min of 3 launches, CUDA events, each after an L2-sized read so that the input
-// comes from HBM as in a large batch) on scratch buffers sized for up to 64 MiB of the pass's lines; returns the index of the fastest, or -1 if none could run. ms receives each candidate's time
+// comes from HBM as in a large batch) on scratch buffers sized for up to kPlannerSampleBytes of the pass's lines;
+// returns the index of the fastest, or -1 if none could run. ms receives each candidate's time
 // (or a negative value when it failed). Appends every timing to the planner log.
 // `heuristic` is the index of the heuristic's own choice among the candidates (or -1), marked in the log.
 int measure_shapes(const PassDesc& d, const std::string& key, const std::vector<PassShape>& cands,
