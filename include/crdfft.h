@@ -297,8 +297,8 @@ int64_t crdfft_uneven_offsets(const int64_t* sizes, int64_t count, int64_t* offs
 /* How plan creation picks each pass's launch shape (kernel variant, points a thread, lines a CTA):
  *   CRDFFT_PLANNER_ESTIMATE  remembered wisdom for the pass's geometry class, else a fixed heuristic (default)
  *   CRDFFT_PLANNER_MEASURE   remembered wisdom, else time every candidate on the device (scratch buffers of up to
- *                            64 MiB per pass, each timed launch after an L2-sized read so that its input comes
- *                            from HBM) and remember the fastest
+ *                            512 MiB per pass, 64 MiB when the device is short of memory, each timed launch after
+ *                            an L2-sized read so that its input comes from HBM) and remember the fastest
  * Two levels are planned this way: the decomposition of each 1-D transform length (one pass, the cluster four-step,
  * or the two-pass four-step n1 x n2 for every split whose halves fit one CTA; timed as whole executes of a sample of
  * the batch, up to 256 MiB) and the launch shape of each pass. The reference plans from the size alone from a board
