@@ -313,15 +313,21 @@ struct Plan
     std::map<std::tuple<const void*, void*, int>, cudaGraphExec_t> graphs;
     std::mutex graphs_mu;
     // Host-buffer execute (crdfft_execute_host): chunk plans, staging buffers and streams, made by the first call.
+    // Host-memory execute: a three-stage pipeline over chunks of the batch, each stage on its own stream (copy in,
+    // transform, copy out) and kHostSlots buffer slots, so that both copy engines stay busy while the transforms run.
+    static constexpr int kHostSlots = 3;
     struct HostPipe
     {
         long long chunk = 0;             // transforms a chunk
         Plan* full = nullptr;            // plan of `chunk` transforms
         Plan* tail = nullptr;            // plan of the last, shorter chunk (or null)
-        void* din[2] = {nullptr, nullptr};
-        void* dout[2] = {nullptr, nullptr};
-        cudaStream_t st[2] = {nullptr, nullptr};
-        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        void* din[kHostSlots] = {};
+        void* dout[kHostSlots] = {};
+        cudaStream_t st[3] = {nullptr, nullptr, nullptr}; // copy in, transform, copy out
+        cudaEvent_t loaded[kHostSlots] = {};   // a slot's input is on the device
+        cudaEvent_t computed[kHostSlots] = {}; // a slot's transform is done (its input is free, its output ready)
+        cudaEvent_t drained[kHostSlots] = {};  // a slot's output is back on the host (its output buffer is free)
+        cudaEvent_t start = nullptr;           // the caller's stream at the call
     };
     HostPipe* host = nullptr;
     std::mutex host_mu;
@@ -342,18 +348,22 @@ struct Plan
     {
         if (host != nullptr)
         {
-            for (int i = 0; i < 2; ++i)
+            for (cudaStream_t st : host->st)
+                if (st != nullptr)
+                {
+                    cudaStreamSynchronize(st);
+                    cudaStreamDestroy(st);
+                }
+            for (int i = 0; i < kHostSlots; ++i)
             {
-                if (host->st[i] != nullptr)
-                    cudaStreamSynchronize(host->st[i]);
                 cudaFree(host->din[i]);
                 cudaFree(host->dout[i]);
-                if (host->st[i] != nullptr)
-                    cudaStreamDestroy(host->st[i]);
+                for (cudaEvent_t e : {host->loaded[i], host->computed[i], host->drained[i]})
+                    if (e != nullptr)
+                        cudaEventDestroy(e);
             }
-            for (cudaEvent_t e : host->ev)
-                if (e != nullptr)
-                    cudaEventDestroy(e);
+            if (host->start != nullptr)
+                cudaEventDestroy(host->start);
             delete host->full;
             delete host->tail;
             delete host;
@@ -3018,11 +3028,14 @@ crdfft_status host_pipe_setup(Plan& p, const HostLayout& L)
     const size_t in_bytes = static_cast<size_t>((h->chunk - 1) * L.idist + L.in_ext) * L.in_elem;
     const size_t out_bytes = static_cast<size_t>((h->chunk - 1) * L.odist + L.out_ext) * L.out_elem;
     bool ok = true;
-    for (int i = 0; i < 2 && ok; ++i)
+    for (int i = 0; i < Plan::kHostSlots && ok; ++i)
         ok = dev_alloc(&h->din[i], in_bytes) == cudaSuccess && dev_alloc(&h->dout[i], out_bytes) == cudaSuccess &&
-             cudaStreamCreateWithFlags(&h->st[i], cudaStreamNonBlocking) == cudaSuccess;
+             cudaEventCreateWithFlags(&h->loaded[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&h->computed[i], cudaEventDisableTiming) == cudaSuccess &&
+             cudaEventCreateWithFlags(&h->drained[i], cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; i < 3 && ok; ++i)
-        ok = cudaEventCreateWithFlags(&h->ev[i], cudaEventDisableTiming) == cudaSuccess;
+        ok = cudaStreamCreateWithFlags(&h->st[i], cudaStreamNonBlocking) == cudaSuccess;
+    ok = ok && cudaEventCreateWithFlags(&h->start, cudaEventDisableTiming) == cudaSuccess;
     p.host = h.release();
     return ok ? CRDFFT_OK : CRDFFT_OOM;
 }
@@ -3053,36 +3066,53 @@ crdfft_status crdfft_execute_host(crdfft_plan* plan, const void* in, void* out, 
             return st;
     }
     Plan::HostPipe& h = *p.host;
-    if (h.st[1] == nullptr || h.ev[2] == nullptr)
+    if (h.st[2] == nullptr || h.start == nullptr)
         return CRDFFT_OOM;
     const cudaStream_t user = static_cast<cudaStream_t>(stream);
-    // the internal streams start after the work already on the caller's stream
-    if (cudaEventRecord(h.ev[2], user) != cudaSuccess || cudaStreamWaitEvent(h.st[0], h.ev[2], 0) != cudaSuccess ||
-        cudaStreamWaitEvent(h.st[1], h.ev[2], 0) != cudaSuccess)
+    const cudaStream_t s_in = h.st[0], s_run = h.st[1], s_out = h.st[2];
+    // the three stages start after the work already on the caller's stream
+    if (cudaEventRecord(h.start, user) != cudaSuccess)
         return CRDFFT_LAUNCH;
+    for (cudaStream_t st : h.st)
+        if (cudaStreamWaitEvent(st, h.start, 0) != cudaSuccess)
+            return CRDFFT_LAUNCH;
     const char* hin = static_cast<const char*>(in);
     char* hout = static_cast<char*>(out);
-    int k = 0;
-    for (long long t0 = 0; t0 < p.desc.batch; t0 += h.chunk, k ^= 1)
+    long long k = 0;
+    for (long long t0 = 0; t0 < p.desc.batch; t0 += h.chunk, ++k)
     {
+        const int s = static_cast<int>(k % Plan::kHostSlots);
+        const bool reused = k >= Plan::kHostSlots; // the slot served chunk k - kHostSlots
         const long long c = std::min(h.chunk, p.desc.batch - t0);
         Plan* cp = c == h.chunk ? h.full : h.tail;
         const size_t ib = static_cast<size_t>((c - 1) * L.idist + L.in_ext) * L.in_elem;
         const size_t ob = static_cast<size_t>((c - 1) * L.odist + L.out_ext) * L.out_elem;
-        if (cudaMemcpyAsync(h.din[k], hin + static_cast<size_t>(t0 * L.idist) * L.in_elem, ib, cudaMemcpyHostToDevice,
-                            h.st[k]) != cudaSuccess)
+        // copy in once the slot's previous transform has read its input
+        if ((reused && cudaStreamWaitEvent(s_in, h.computed[s], 0) != cudaSuccess) ||
+            cudaMemcpyAsync(h.din[s], hin + static_cast<size_t>(t0 * L.idist) * L.in_elem, ib,
+                            cudaMemcpyHostToDevice, s_in) != cudaSuccess ||
+            cudaEventRecord(h.loaded[s], s_in) != cudaSuccess)
             return CRDFFT_LAUNCH;
-        const crdfft_status st = run(*cp, h.din[k], h.dout[k], direction, h.st[k]);
+        // transform once the input is in and the slot's previous output has been copied out
+        if (cudaStreamWaitEvent(s_run, h.loaded[s], 0) != cudaSuccess ||
+            (reused && cudaStreamWaitEvent(s_run, h.drained[s], 0) != cudaSuccess))
+            return CRDFFT_LAUNCH;
+        const crdfft_status st = run(*cp, h.din[s], h.dout[s], direction, s_run);
         if (st != CRDFFT_OK)
             return st;
-        if (cudaMemcpyAsync(hout + static_cast<size_t>(t0 * L.odist) * L.out_elem, h.dout[k], ob,
-                            cudaMemcpyDeviceToHost, h.st[k]) != cudaSuccess)
+        if (cudaEventRecord(h.computed[s], s_run) != cudaSuccess)
+            return CRDFFT_LAUNCH;
+        // copy out once the transform is done
+        if (cudaStreamWaitEvent(s_out, h.computed[s], 0) != cudaSuccess ||
+            cudaMemcpyAsync(hout + static_cast<size_t>(t0 * L.odist) * L.out_elem, h.dout[s], ob,
+                            cudaMemcpyDeviceToHost, s_out) != cudaSuccess ||
+            cudaEventRecord(h.drained[s], s_out) != cudaSuccess)
             return CRDFFT_LAUNCH;
     }
-    // the caller's stream waits for both internal streams
-    for (int i = 0; i < 2; ++i)
-        if (cudaEventRecord(h.ev[i], h.st[i]) != cudaSuccess || cudaStreamWaitEvent(user, h.ev[i], 0) != cudaSuccess)
-            return CRDFFT_LAUNCH;
+    // the caller's stream waits for the last copy out (which follows every transform and every copy in)
+    const int last = static_cast<int>((k - 1) % Plan::kHostSlots);
+    if (cudaStreamWaitEvent(user, h.drained[last], 0) != cudaSuccess)
+        return CRDFFT_LAUNCH;
     return CRDFFT_OK;
 }
 

@@ -120,12 +120,12 @@ crdfft_status crdfft_execute(crdfft_plan* plan, const void* in, void* out, int32
 
 /* Run the plan on HOST buffers, the way the reference's plans are called (FftPlan::execute transforms a span of CPU
  * memory in place, fft.hpp:409-413): `in` and `out` are host memory laid out as the plan's descriptor says (element
- * stride 1; in == out allowed). The batch is cut into chunks (an eighth of the batch, 4 to 64 MiB of input); each
- * chunk's copy to the device, its transform and its copy back go on one of two internal streams in turn, so the
- * copies in both directions and the transforms of different chunks overlap. Convolution plans are not supported. Use page-locked host memory (cudaHostAlloc / pinned tensors): with
+ * stride 1; in == out allowed). The batch is cut into chunks (an eighth of the batch, 4 to 64 MiB of input) that run
+ * through a three-stage pipeline, each stage on its own internal stream (copy to the device, transform, copy back)
+ * with three staging slots, so the copies in both directions and the transforms of different chunks overlap. Convolution plans are not supported. Use page-locked host memory (cudaHostAlloc / pinned tensors): with
  * pageable memory the result is the same but the copies do not overlap. The work is ordered after everything
  * already queued on `stream`, and `stream` waits for all of it: synchronise `stream` before reading `out`. The first
- * call on a plan allocates its device staging buffers (two chunks each way) and the chunk plans; calls on one plan
+ * call on a plan allocates its device staging buffers (three chunks each way) and the chunk plans; calls on one plan
  * must not overlap. Uneven-batch plans are not supported (CRDFFT_INVALID_ARG). */
 crdfft_status crdfft_execute_host(crdfft_plan* plan, const void* in, void* out, int32_t direction, void* stream);
 
