@@ -16,30 +16,8 @@ namespace crdfft
 
 // ---- complex values -------------------------------------------------------------------------------------------
 //
-// The codelets run on two value types. float2 is one complex value (x real, y imaginary). cpair is the same element
-// of two lines, real parts in one float2 and imaginary parts in another, so that one Blackwell paired FP32
-// instruction (FADD2, FMUL2, FFMA2: two lanes of an aligned register pair) does the work of both lines; every
-// operation below is the same arithmetic on each lane.
-struct cpair
-{
-    float2 re; // (line a, line b)
-    float2 im;
-};
-
-__device__ __forceinline__ float2 f2dup(float c) { return make_float2(c, c); }
-__device__ __forceinline__ float2 f2add(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 f2mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 f2fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 f2sub(float2 a, float2 b)
-{
-    float2 r;
-    asm("{\n\t.reg .b64 a, b, d;\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\tsub.rn.f32x2 d, a, b;\n\t"
-        "mov.b64 {%0, %1}, d;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 f2neg(float2 a) { return f2mul(a, f2dup(-1.0f)); }
+// The codelets are templates over the value type they transform (float2: x real, y imaginary), written against the
+// small set of operations below, so a kernel could instantiate them for another representation of complex values.
 
 __device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
@@ -71,45 +49,6 @@ __device__ __forceinline__ float2 cmadd(float2 acc, float2 a, float c)
 }
 template <class C> __device__ __forceinline__ C czero();
 template <> __device__ __forceinline__ float2 czero<float2>() { return make_float2(0.f, 0.f); }
-
-__device__ __forceinline__ cpair cadd(cpair a, cpair b) { return {f2add(a.re, b.re), f2add(a.im, b.im)}; }
-__device__ __forceinline__ cpair csub(cpair a, cpair b) { return {f2sub(a.re, b.re), f2sub(a.im, b.im)}; }
-__device__ __forceinline__ cpair cscale(cpair a, float s) { return {f2mul(a.re, f2dup(s)), f2mul(a.im, f2dup(s))}; }
-__device__ __forceinline__ cpair cneg(cpair a) { return {f2neg(a.re), f2neg(a.im)}; }
-__device__ __forceinline__ cpair cmul_mi(cpair a) { return {a.im, f2neg(a.re)}; }
-__device__ __forceinline__ cpair cmul_pi(cpair a) { return {f2neg(a.im), a.re}; }
-__device__ __forceinline__ cpair add_mi(cpair a, cpair b) { return {f2add(a.re, b.im), f2sub(a.im, b.re)}; }
-__device__ __forceinline__ cpair sub_mi(cpair a, cpair b) { return {f2sub(a.re, b.im), f2add(a.im, b.re)}; }
-__device__ __forceinline__ cpair crot(cpair a, float c, float s)
-{
-    return {f2fma(a.re, f2dup(c), f2mul(a.im, f2dup(s))), f2fma(a.im, f2dup(c), f2mul(a.re, f2dup(-s)))};
-}
-__device__ __forceinline__ cpair crot_h1(cpair a, float h)
-{
-    return {f2mul(f2add(a.re, a.im), f2dup(h)), f2mul(f2sub(a.im, a.re), f2dup(h))};
-}
-__device__ __forceinline__ cpair crot_h3(cpair a, float h)
-{
-    return {f2mul(f2sub(a.im, a.re), f2dup(h)), f2mul(f2add(a.re, a.im), f2dup(-h))};
-}
-__device__ __forceinline__ cpair crot_h5(cpair a, float h)
-{
-    return {f2mul(f2add(a.re, a.im), f2dup(-h)), f2mul(f2sub(a.re, a.im), f2dup(h))};
-}
-__device__ __forceinline__ cpair crot_h7(cpair a, float h)
-{
-    return {f2mul(f2sub(a.re, a.im), f2dup(h)), f2mul(f2add(a.re, a.im), f2dup(h))};
-}
-__device__ __forceinline__ cpair cmadd(cpair acc, cpair a, float c)
-{
-    return {f2fma(a.re, f2dup(c), acc.re), f2fma(a.im, f2dup(c), acc.im)};
-}
-template <> __device__ __forceinline__ cpair czero<cpair>() { return {make_float2(0.f, 0.f), make_float2(0.f, 0.f)}; }
-// a w for a twiddle w = (c, s) shared by both lines, given as the lane pairs (c, c) and (s, s)
-__device__ __forceinline__ cpair cmul_pair(cpair a, float2 cc, float2 ss)
-{
-    return {f2sub(f2mul(a.re, cc), f2mul(a.im, ss)), f2fma(a.re, ss, f2mul(a.im, cc))};
-}
 
 // Multiply by the compile-time root W_16^J (forward sign), specialised so the trivial roots cost no multiplies.
 template <int J, class C> __device__ __forceinline__ C w16mul(C a)
