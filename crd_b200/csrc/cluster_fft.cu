@@ -5,7 +5,7 @@
 //            read straight from HBM (coalesced across the CTA's adjacent columns), result kept in shared memory
 //   exchange cluster barrier; CTA c gathers rows k1 in [c N1/C, (c+1) N1/C) of all columns from the other CTAs'
 //            shared memory (distributed shared memory reads), multiplying by the four-step twiddle W_N^{n2 k1}
-//            (a full N-entry table tw[k1 N2 + n2], L2-resident and shared by every transform);
+//            (factored into two 32 KiB tables that stay in L1, shared by every transform);
 //            a second cluster barrier, then it stores them into its own (reused) shared memory
 //   phase B  CTA c transforms its rows: length-N2 DFTs over n2, written straight to X[k1 + N1 k2] (coalesced across
 //            its adjacent rows)
@@ -80,8 +80,9 @@ __global__ void __launch_bounds__((S1::n * S2::n) / (P * C), MINB)
     cluster_barrier(); // every CTA's columns are in its shared memory
 
     // ---- exchange: rows k1 of this CTA, all n2, times W_N^{n2 k1}. A thread keeps one column n2 (THREADS is a
-    // multiple of N2), so it reads one remote CTA's shared memory, and the twiddles W_N^{n2 k1} come from the
-    // table tw[k1 N2 + n2], consecutive across the threads of a warp.
+    // multiple of N2), so it reads one remote CTA's shared memory, and the twiddle W_N^{n2 k1} is
+    // hi[(n2>>4) N1 + k1] * lo[16 k1 + (n2&15)]: for one k1, a warp's 32 columns read two hi entries and 16
+    // consecutive lo entries (L1-resident tables).
     static_assert(THREADS % N2 == 0, "a thread keeps one column through the exchange");
     constexpr int PER = (LB * N2) / THREADS;
     constexpr int KSTEP = THREADS / N2;
@@ -90,12 +91,13 @@ __global__ void __launch_bounds__((S1::n * S2::n) / (P * C), MINB)
     const int kl0 = tid / N2;
     const int src = n2 / LA;
     const float2* remote = cluster.map_shared_rank(buf, src) + (n2 - src * LA);
-    const float2* tw = static_cast<const float2*>(dA.ftw_hi) + n2;
+    const float2* twh = static_cast<const float2*>(dA.ftw_hi) + (n2 >> 4) * N1;
+    const float2* twl = static_cast<const float2*>(dA.ftw_lo) + (n2 & 15);
 #pragma unroll
     for (int i = 0; i < PER; ++i)
     {
         const int k1 = rank * LB + kl0 + i * KSTEP;
-        v[i] = cmul(remote[k1 * PA], __ldg(tw + k1 * N2));
+        v[i] = cmul(remote[k1 * PA], cmul(__ldg(twh + k1), __ldg(twl + k1 * 16)));
     }
     cluster_barrier(); // every CTA's remote reads are performed (release); shared memory may be reused
 #pragma unroll

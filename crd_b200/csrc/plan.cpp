@@ -1252,26 +1252,20 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     if (dc.kind == 2 && cluster_split(n, &n1, &n2))
     {
         // One cluster per transform: columns of n1, DSMEM transpose with the four-step twiddle, rows of n2. The
-        // twiddle is one full table tw[k1 n2 + j] = W_n^{j k1} (FP64 roots, narrowed).
+        // twiddle W_n^{j k1} (column j, row k1) is factored like the two-pass four-step's, hi[(j>>4) n1 + k1] times
+        // lo[16 k1 + (j&15)]: two tables of 32 KiB that stay in L1, where one full 512 KiB table was read from L2
+        // between the cluster barriers.
         Step s;
         s.kind = StepKind::Cluster;
-        std::vector<float> full(static_cast<size_t>(2 * n));
-        for (long long k1 = 0; k1 < n1; ++k1)
-            for (long long j = 0; j < n2; ++j)
-            {
-                double re, im;
-                root(j * k1, n, &re, &im);
-                full[static_cast<size_t>(2 * (k1 * n2 + j))] = static_cast<float>(re);
-                full[static_cast<size_t>(2 * (k1 * n2 + j) + 1)] = static_cast<float>(im);
-            }
-        void* dfull = nullptr;
-        crdfft_status st = upload_table(p, full, &dfull);
+        const void* hi = nullptr;
+        const void* lo = nullptr;
+        crdfft_status st = four_step_tables(p, n, n1, n2, &hi, &lo);
         if (st != CRDFFT_OK)
             return st;
         FourStepTw ftw;
         ftw.M = n;
-        ftw.hi = dfull;
-        ftw.lo = nullptr;
+        ftw.hi = hi;
+        ftw.lo = lo;
         st = make_pass_desc(p, n1, batch * n2, n2, LineMap{n, 1, n2}, LineMap{n, 1, n2}, conj_in, false, 1.0f, ftw,
                             &s.pass);
         if (st != CRDFFT_OK)
