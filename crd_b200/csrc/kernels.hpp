@@ -84,6 +84,9 @@ cudaError_t launch_welch_finish(const SpectralDesc& sd, const void* part, void* 
 // The four-step column pass as a persistent kernel fed by 2-D tensor copies (tma_col.cu).
 bool tma_col_supported(const PassDesc& d);
 cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStream_t stream);
+// The four-step row pass with its transposed tile stored by the Tensor Memory Accelerator (tma_col.cu).
+bool row_tstore_supported(const PassDesc& d, const PassShape& sh);
+cudaError_t launch_row_tstore(const PassDesc& d, const PassShape& sh, const void* in, void* out, cudaStream_t stream);
 int pass_lines_per_cta_limit();
 int pass_line_pitch(int n);
 int pass_cta_line_pitch(int n, int lpc); // the compile-time-schedule kernel's line pitch (complex elements)

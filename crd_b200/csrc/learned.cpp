@@ -86,7 +86,7 @@ void pass_features(const PassDesc& d, const PassShape& sh, float* f)
         return (m.ldist != 1 && m.ldist % 16 != 0) || (m.gdist % 16 != 0 && m.gdist != 0);
     };
     f[22] = (padded(d.in) || padded(d.out)) ? 1.0f : 0.0f;
-    f[23] = sh.pipelined ? 1.0f : 0.0f;
+    f[23] = sh.pipelined ? 1.0f : (sh.tma_store ? 0.5f : 0.0f); // bulk-copy-fed, tensor-store row pass, classic
     f[24] = sh.points_per_thread == 32 ? 1.0f : (sh.wide_regs ? 0.5f : 0.0f); // 16 narrow, 16 wide, 32
     f[25] = lg2(sh.lines_per_cta);
     f[26] = lg2(static_cast<double>(sh.threads_per_line) * sh.lines_per_cta);

@@ -100,6 +100,8 @@ int pass_pipe_smem(int n, PassMap map, int lpc)
 
 bool pass_has_kernel(const PassDesc& d, const PassShape& sh)
 {
+    if (sh.tma_store)
+        return row_tstore_supported(d, sh);
     if (sh.pipelined)
         return lfft::select_pipe(d, sh) != nullptr;
     return lfft::select_static(d, sh) != nullptr || lfft::select_dynamic(d, sh) != nullptr;
@@ -151,6 +153,16 @@ cudaError_t launch_line_pass(const PassDesc& d, const PassShape& sh, const void*
     const long long groups = (d.lines + sh.lines_per_cta - 1) / sh.lines_per_cta;
     if (groups <= 0)
         return cudaSuccess;
+    if (sh.tma_store && (reinterpret_cast<uintptr_t>(out) & 15u) == 0)
+        return launch_row_tstore(d, sh, in, out, stream);
+    if (sh.tma_store)
+    {
+        // an output off a 16-byte boundary (the tensor map needs one): the thread-stored kernel, same lines a CTA
+        PassShape cs = sh;
+        cs.tma_store = false;
+        cs.smem_bytes = sh.lines_per_cta * lfft::cta_line_pitch(d.n, sh.lines_per_cta) * 8;
+        return launch_line_pass(d, cs, in, out, stream);
+    }
     if (sh.pipelined && (reinterpret_cast<uintptr_t>(in) & 15u) == 0)
     {
         lfft::PipeFn fn = lfft::select_pipe(d, sh);

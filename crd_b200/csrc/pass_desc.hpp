@@ -76,6 +76,7 @@ struct PassShape
     int smem_bytes;
     bool wide_regs;         // compile-time schedules at 16 points a thread: the 80-register build (fewer resident
                             // warps, no spill) instead of the 64-register one
+    bool tma_store;         // the row pass of a four-step: the transposed tile leaves by tensor stores (tma_col.cu)
 };
 
 } // namespace crdfft

@@ -585,15 +585,23 @@ bool heuristic_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape
     }
     // A compile-time schedule first, at either thread width (the radix-32 schedules exist at 32 points a thread
     // only: without this order 1024 and 8192 took the run-time kernel at 16 points a thread, 4x slower for 1024),
-    // then the run-time schedule.
+    // then the run-time schedule. A four-step row pass the tensor-store kernel takes goes to it (its transposed
+    // store is 40 % of the thread-stored pass's time).
     for (int pass = 0; pass < 2; ++pass)
         for (int P : {16, 32})
         {
-            const PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, P);
+            PassShape sh = shape_with(d.n, d.nstages, map, dl, ds, P);
             if (sh.threads_per_line * sh.lines_per_cta > pass_threads_limit(P, d.n))
                 continue;
             if (pass == 0 ? pass_has_static(d, P) : pass_has_kernel(d, sh))
             {
+                PassShape t = sh;
+                t.tma_store = true;
+                if (pass == 0 && row_tstore_supported(d, t))
+                {
+                    t.smem_bytes = 1024 + t.lines_per_cta * pass_cta_line_pitch(d.n, t.lines_per_cta) * 8;
+                    sh = t;
+                }
                 *out = sh;
                 return true;
             }
@@ -614,7 +622,7 @@ std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl,
             return;
         for (const PassShape& o : out)
             if (o.pipelined == sh.pipelined && o.points_per_thread == sh.points_per_thread &&
-                o.lines_per_cta == sh.lines_per_cta && o.wide_regs == sh.wide_regs)
+                o.lines_per_cta == sh.lines_per_cta && o.wide_regs == sh.wide_regs && o.tma_store == sh.tma_store)
                 return;
         out.push_back(sh);
         if (!sh.pipelined && sh.points_per_thread == 16 && pass_has_static(d, 16))
@@ -622,6 +630,13 @@ std::vector<PassShape> candidate_shapes(const PassDesc& d, PassMap map, bool dl,
             PassShape w = sh;
             w.wide_regs = true; // the same shape on the 80-register build
             out.push_back(w);
+        }
+        PassShape t = sh;
+        t.tma_store = true; // a four-step row pass whose transposed tile leaves by tensor stores
+        if (!sh.pipelined && row_tstore_supported(d, t))
+        {
+            t.smem_bytes = 1024 + t.lines_per_cta * pass_cta_line_pitch(d.n, t.lines_per_cta) * 8;
+            out.push_back(t);
         }
     };
     for (int P : {16, 32})
@@ -657,7 +672,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
         PassShape sh;
         if (w.pipelined ? pipe_shape(d, map, &sh, w.lines_per_cta)
                         : (sh = shape_with(d.n, d.nstages, map, dl, ds, w.points_per_thread, w.lines_per_cta),
-                           sh.wide_regs = w.wide_regs,
+                           sh.wide_regs = w.wide_regs, sh.tma_store = w.tma_store,
                            sh.threads_per_line * sh.lines_per_cta <= pass_threads_limit(sh.points_per_thread, d.n) &&
                                pass_has_kernel(d, sh)))
         {
@@ -695,6 +710,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
                 e.points_per_thread = top[best].points_per_thread;
                 e.lines_per_cta = top[best].lines_per_cta;
                 e.wide_regs = top[best].wide_regs;
+                e.tma_store = top[best].tma_store;
                 e.ms = ms[best];
                 wisdom_store(key, e);
                 *out = top[best];
@@ -726,6 +742,7 @@ bool choose_shape(const PassDesc& d, PassMap map, bool dl, bool ds, PassShape* o
             e.points_per_thread = cands[best].points_per_thread;
             e.lines_per_cta = cands[best].lines_per_cta;
             e.wide_regs = cands[best].wide_regs;
+            e.tma_store = cands[best].tma_store;
             e.ms = ms[best];
             wisdom_store(key, e);
             *out = cands[best];

@@ -11,6 +11,9 @@
 //
 // Every wait is bounded (the pass's spin limit): a wait that runs out sets the plan's status word, waits (bounded)
 // for the copies the CTA still has in flight and returns.
+//
+// The file also holds the four-step's row pass whose transposed tile leaves by 2-D tensor stores
+// (row_tstore_kernel, below): the other half of the four-step, with the Tensor Memory Accelerator on its strided side.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -198,6 +201,107 @@ TmaFn tma_select(const PassDesc& d, int* P)
     return nullptr;
 }
 
+// ---- row pass with a tensor store --------------------------------------------------------------------------------
+//
+// The four-step's row pass writes its lines transposed: element e of line q of a group goes to (t n + e) lpg + q, so
+// a CTA of lpc lines writes runs of lpc elements, 32 bytes for four lines. Issued by the threads, those stores take
+// a quarter of the L1 data pipe's wavefronts and, with the transposed tile read back from shared memory, 40 % of
+// the pass's time (measured by leaving the global store out of a copy of the kernel: 0.527 -> 0.319 ms per GiB).
+// Here the threads only put the tile into shared memory in the output's order, a dense [n][lpc] block, and one
+// thread hands it to the Tensor Memory Accelerator as 2-D stores of at most 256 rows: the copy engine does the
+// scattered writes, not the load/store unit.
+//
+// The stages are the line kernel's (row map, first stage reading HBM directly); every tile is whole (the launch
+// checks lines % lpc == 0 and lines_per_group % lpc == 0), so a tile's lines are consecutive lines of one group.
+
+// policy: an L2 eviction policy (evict-first for a pass's output, as the thread-stored kernel's streaming stores):
+// the output is not read again soon, and left at normal priority its dirty lines stay in L2 until the next
+// operation's traffic pushes them out.
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, const void* src, uint64_t policy)
+{
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group.L2::cache_hint [%0, {%1, %2}], [%3], %4;" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(smem_addr(src)), "l"(policy)
+                 : "memory");
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+template <class S, int P, bool EPI>
+__global__ void __launch_bounds__(kMaxThreads, 2)
+    row_tstore_kernel(const __grid_constant__ CUtensorMap map, const PassDesc d, const float2* __restrict__ gin)
+{
+    constexpr int N = S::n;
+    constexpr int T = N / P;
+    constexpr int BOX = N < 256 ? N : 256; // rows of one store box
+    static_assert(N % P == 0 && N % BOX == 0, "whole threads and whole boxes");
+    extern __shared__ unsigned char smraw[];
+    // the tile from the first 1 KiB boundary of the dynamic shared memory (tensor-copy sources 128-byte aligned)
+    float2* sm = reinterpret_cast<float2*>(smraw + ((1024u - (smem_addr(smraw) & 1023u)) & 1023u));
+    const int lpc = blockDim.x / T;
+    const int tid = threadIdx.x;
+    const int pitch = cta_line_pitch(N, lpc);
+    const long long line0 = static_cast<long long>(blockIdx.x) * lpc;
+
+    const int ll = tid / T;
+    Ctx c;
+    c.ok = true;
+    c.q = 0;
+    c.in = gin + line_offset(d.in, line0 + ll, d.lines_per_group);
+    c.out = nullptr;
+    c.jt = tid - ll * T;
+    c.T = T;
+    init_scales(d, c);
+    SchedRun<S>::template go<P, true, false, false, Kind<PassMap::Row, EPI>>(d, c, LayRow<1>{sm + ll * pitch}, N);
+
+    // The tile in output order, in place: every thread first reads its P elements (lines fastest across the
+    // threads, so a warp reads the same elements of every line: no bank conflict with the staggered line starts),
+    // then writes them at e * lpc + a (a warp writes 32 consecutive slots).
+    const int a = tid % lpc;
+    const int e0 = tid / lpc; // T threads a line: e = e0 + k T covers the line once
+    float2 v[P];
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+    {
+        const int e = e0 + k * T;
+        v[k] = epilogue<EPI>(d, c, 0, e, LayRow<1>{sm + a * pitch}.at(e));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < P; ++k)
+        sm[(e0 + k * T) * lpc + a] = v[k];
+    fence_proxy_async(); // these generic writes before the copy engine's reads
+    __syncthreads();
+    if (tid == 0)
+    {
+        const long long g = idiv(line0, d.lines_per_group);
+        const int x = static_cast<int>(line0 - g * d.lines_per_group);
+        const uint64_t policy = l2_evict_first_policy();
+#pragma unroll 1
+        for (int b = 0; b < N / BOX; ++b)
+            tma_store_2d(&map, x, static_cast<int>(g * N + b * BOX), sm + b * BOX * lpc, policy);
+        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        // the shared memory must outlive the copy engine's reads of it
+        asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    }
+}
+
+using RowTstoreFn = void (*)(const CUtensorMap, const PassDesc, const float2*);
+
+RowTstoreFn row_tstore_select(const PassDesc& d, bool epi)
+{
+    if (d.n == 1024 && same_radices(d, {16, 16, 4}))
+        return epi ? row_tstore_kernel<Sched<16, 16, 4>, 16, true> : row_tstore_kernel<Sched<16, 16, 4>, 16, false>;
+    if (d.n == 512 && same_radices(d, {16, 8, 4}))
+        return epi ? row_tstore_kernel<Sched<16, 8, 4>, 16, true> : row_tstore_kernel<Sched<16, 8, 4>, 16, false>;
+    return nullptr;
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encoder()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
@@ -279,6 +383,58 @@ cudaError_t launch_tma_col(const PassDesc& d, const void* in, void* out, cudaStr
     const int threads = ((d.n + P - 1) / P) * cols;
     fn<<<static_cast<unsigned>(grid), threads, smem, stream>>>(map, d, static_cast<float2*>(out), nbuf, box_rows,
                                                                tiles);
+    return cudaGetLastError();
+}
+
+// The row pass with a tensor store: rows read unit-stride (the first stage loads them directly), each group of
+// lines_per_group lines written transposed as a [groups * n] x lines_per_group matrix (element e of line q of group
+// t at (t n + e) lines_per_group + q), whole tiles of an even number of lines, no four-step twiddle, a schedule the
+// kernel has (512 or 1024 points, 16 points a thread).
+bool row_tstore_supported(const PassDesc& d, const PassShape& sh)
+{
+    const int lpc = sh.lines_per_cta;
+    const long long lpg = d.lines_per_group;
+    if (sh.pipelined || sh.map != PassMap::Row || !sh.direct_load || sh.direct_store || sh.points_per_thread != 16)
+        return false;
+    if (lpc < 2 || lpc % 2 != 0 || lpc * (d.n / 16) > lfft::kMaxThreads)
+        return false;
+    if (d.in.estride != 1 || d.out.ldist != 1 || d.out.estride != lpg || d.out.gdist != d.n * lpg || d.ftw_M != 0)
+        return false;
+    if (lpg % lpc != 0 || d.lines % lpg != 0 || (lpg * 8) % 16 != 0 || d.lines / lpg * d.n > 0x7fffffffLL)
+        return false;
+    return lfft::row_tstore_select(d, false) != nullptr && lfft::encoder() != nullptr;
+}
+
+cudaError_t launch_row_tstore(const PassDesc& d, const PassShape& sh, const void* in, void* out, cudaStream_t stream)
+{
+    if (!row_tstore_supported(d, sh) || (reinterpret_cast<uintptr_t>(out) & 15) != 0)
+        return cudaErrorInvalidConfiguration;
+    const bool epi = d.conj_in != 0 || d.conj_out != 0 || d.scale != 1.0f;
+    lfft::RowTstoreFn fn = lfft::row_tstore_select(d, epi);
+    const int lpc = sh.lines_per_cta;
+    const long long lpg = d.lines_per_group;
+    const long long groups = d.lines / lpg;
+    const int box_rows = d.n < 256 ? d.n : 256;
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(lpg), static_cast<cuuint64_t>(groups * d.n)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(lpg) * 8};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(lpc), static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    if (lfft::encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, out, dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue; // the tensor map was refused
+    const int smem = 1024 + lpc * lfft::cta_line_pitch(d.n, lpc) * 8;
+    if (smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        if (e != cudaSuccess)
+            return e;
+    }
+    const long long grid = d.lines / lpc;
+    if (grid > 0x7fffffffLL)
+        return cudaErrorInvalidConfiguration;
+    fn<<<static_cast<unsigned>(grid), (d.n / 16) * lpc, smem, stream>>>(map, d, static_cast<const float2*>(in));
     return cudaGetLastError();
 }
 

@@ -162,6 +162,8 @@ std::string wisdom_export()
           << kv.second.lines_per_cta << ' ' << kv.second.ms;
         if (kv.second.wide_regs)
             o << " w"; // the 80-register build
+        if (kv.second.tma_store)
+            o << " t"; // the tensor-store row pass
         o << '\n';
     }
     for (const auto& kv : g_decomp)
@@ -196,11 +198,14 @@ int wisdom_import(const std::string& text)
         if (!(ls >> key >> pipe >> e.points_per_thread >> e.lines_per_cta >> e.ms))
             return -1;
         std::string flag;
-        if (ls >> flag)
+        while (ls >> flag)
         {
-            if (flag != "w")
+            if (flag == "w")
+                e.wide_regs = true;
+            else if (flag == "t")
+                e.tma_store = true;
+            else
                 return -1;
-            e.wide_regs = true;
         }
         if ((e.points_per_thread != 16 && e.points_per_thread != 32) || e.lines_per_cta < 1 ||
             e.lines_per_cta > 256)
@@ -378,9 +383,10 @@ int measure_shapes(const PassDesc& d0, const std::string& key, const std::vector
         for (size_t i = 0; i < cands.size(); ++i)
         {
             char buf[256];
-            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d wide=%d lines=%lld ms=%.6f", key.c_str(),
-                          cands[i].pipelined ? 1 : 0, cands[i].points_per_thread, cands[i].lines_per_cta,
-                          cands[i].wide_regs ? 1 : 0, d0.lines, static_cast<double>((*ms)[i]));
+            std::snprintf(buf, sizeof(buf), "%s pipelined=%d P=%d lpc=%d wide=%d tstore=%d lines=%lld ms=%.6f",
+                          key.c_str(), cands[i].pipelined ? 1 : 0, cands[i].points_per_thread, cands[i].lines_per_cta,
+                          cands[i].wide_regs ? 1 : 0, cands[i].tma_store ? 1 : 0, d0.lines,
+                          static_cast<double>((*ms)[i]));
             g_log += buf;
             float f[kPassFeatures];
             pass_features(d0, cands[i], f);

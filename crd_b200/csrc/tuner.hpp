@@ -33,6 +33,7 @@ struct WisdomEntry
     int lines_per_cta = 1;
     float ms = 0.0f;
     bool wide_regs = false;
+    bool tma_store = false;
 };
 
 // The geometry class of a pass: line length and radices, thread map, direct load/store, epilogue, line counts
