@@ -139,3 +139,22 @@ def test_wisdom_register_budget_flag_round_trips():
             H.wisdom_import("crdfft-wisdom 1\nDEV|n4096:r16.16.16:x 0 16 1 0.5 wide\n")
     finally:
         H.wisdom_forget()
+
+
+def test_wisdom_tensor_store_flag_round_trips():
+    """A row pass measured with its tile stored by the Tensor Memory Accelerator is remembered with a trailing `t`,
+    alone or after `w`; another spelling of the flag is refused."""
+    import crd_b200.hesap as H
+
+    H.wisdom_forget()
+    try:
+        text = ("crdfft-wisdom 1\nDEV|n1024:r16.16.4:x 0 16 4 0.25 t\nDEV|n512:r16.8.4:x 0 16 4 0.125 w t\n"
+                "DEV|n4096:r16.16.16:x 0 16 1 0.5\n")
+        H.wisdom_import(text)
+        lines = sorted(H.wisdom_export().splitlines()[1:])
+        assert lines == ["DEV|n1024:r16.16.4:x 0 16 4 0.25 t", "DEV|n4096:r16.16.16:x 0 16 1 0.5",
+                         "DEV|n512:r16.8.4:x 0 16 4 0.125 w t"]
+        with pytest.raises(_lib.CrdFftError):
+            H.wisdom_import("crdfft-wisdom 1\nDEV|n1024:r16.16.4:x 0 16 4 0.25 tstore\n")
+    finally:
+        H.wisdom_forget()
