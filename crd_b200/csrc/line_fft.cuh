@@ -481,6 +481,25 @@ __device__ __forceinline__ void line_fft_body(const PassDesc& d, const float2* _
                        epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
         });
     }
+
+    if constexpr (MAP == PassMap::Row && DL && !DS)
+    {
+        // A dead input (a four-step intermediate in L2, read by the first stage, which ends with a barrier: every
+        // thread's loads of the CTA's lines are done): drop its 128-byte L2 lines, so that L2 does not write them
+        // back to HBM. Unit-stride lines of whole 128-byte lines only; last, where the kernel holds the fewest values.
+        if (d.discard_in && d.in.estride == 1 && (n & 15) == 0)
+        {
+            const int per = n / 16;
+            const long long lines_here = d.lines - line0;
+            for (int i = tid; i < lpc * per; i += blockDim.x)
+            {
+                const int a = i / per;
+                const float2* p = gin + s_in_off[a] + (i - a * per) * 16;
+                if (a < lines_here && (reinterpret_cast<uintptr_t>(p) & 127) == 0)
+                    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+            }
+        }
+    }
 }
 
 // The two register budgets of the classic kernel. The narrow build keeps the launch-bounds hint (two 512-thread CTAs

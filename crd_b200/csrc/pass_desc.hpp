@@ -44,7 +44,8 @@ struct PassDesc
     const void* ftw_lo;
     long long ftw_M;
     int ftw_div;
-    int ftw_unused;
+    int discard_in;              // the input is dead once this pass has read it (a four-step intermediate read from
+                                 // L2): the classic row kernel drops its 128-byte L2 lines without a write-back
     int conj_in;                 // conjugate every input element (inverse via conj(DFT(conj x)))
     int conj_out;                // conjugate every output element
     float scale;                 // multiply every output element (1 = off)

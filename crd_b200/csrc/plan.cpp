@@ -1052,7 +1052,7 @@ crdfft_status make_pass_desc(Plan& p, long long n, long long lines, long long lp
         return st;
     d.ftw_M = ftw.M;
     d.ftw_div = ftw.div > 0 ? ftw.div : 1;
-    d.ftw_unused = 0;
+    d.discard_in = 0;
     d.ftw_hi = ftw.hi;
     d.ftw_lo = ftw.lo;
     d.err = p.err;
@@ -1190,6 +1190,14 @@ long long wave_bytes()
 bool tma_col_enabled()
 {
     const char* e = std::getenv("CRDFFT_TMA_COL");
+    return e == nullptr || std::atoi(e) != 0;
+}
+
+// The L2 wave's row pass drops the intermediate's L2 lines once it has read them (CRDFFT_L2_DISCARD=0: kept, and
+// written back to HBM when L2 evicts them). Read at plan creation.
+bool l2_discard()
+{
+    const char* e = std::getenv("CRDFFT_L2_DISCARD");
     return e == nullptr || std::atoi(e) != 0;
 }
 
@@ -1357,6 +1365,10 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
         }
         else if (r2c_fused != nullptr && *r2c_fused)
             return CRDFFT_UNSUPPORTED_SIZE; // every wave takes the same form
+        // an L2 wave's intermediate is read once, from L2, by this row pass: its lines are dropped there instead of
+        // being written back to HBM (1 GB of the 3.1 GB 107520 moved a GiB)
+        if (l2w && l2_discard())
+            s2.pass.discard_in = 1;
         s2.lane = lane;
         steps.push_back(s2);
     }
