@@ -49,6 +49,7 @@ std::atomic<int> g_fail_alloc_after{0};
 thread_local Arena* t_arena = nullptr; // plan memory comes from this arena instead of cudaMalloc when set
 std::atomic<int> g_debug_stall{0};
 constexpr int kSpinLimit = 1 << 22; // bounded waits: about a second of try_wait polling
+constexpr int kMaxLanes = 4;       // internal streams a plan may run L2-sized four-step waves on
 
 cudaError_t dev_alloc(void** p, size_t bytes)
 {
@@ -125,7 +126,7 @@ struct Step
     SpectralDesc sdesc{}; // Spectral, WelchFinish
     RowR2CDesc rr{};      // RowR2C
     int sthreads = 0, ssmem = 0;
-    int lane = 0;     // 0: the caller's stream; 1, 2: the plan's two internal streams (L2-sized four-step waves)
+    int lane = 0;     // 0: the caller's stream; 1 .. kMaxLanes: the plan's internal streams (L2-sized four-step waves)
     RealRecombine real{};
     ChirpDesc chirp{};
     BufRef src, dst;
@@ -339,10 +340,10 @@ struct Plan
     // Radix-32 schedules for the lengths that have them (FP32 unit-stride passes); off for the tensor-core precision
     // forms and the uneven batch, whose kernels take the radix-16 schedules.
     bool use32 = true;
-    // Two internal streams for steps with lane 1 / 2, forked from and joined back to the caller's stream.
-    cudaStream_t lanes[2] = {nullptr, nullptr};
+    // Internal streams for steps with lane 1 .. kMaxLanes, forked from and joined back to the caller's stream.
+    cudaStream_t lanes[kMaxLanes] = {};
     cudaEvent_t fork = nullptr;
-    cudaEvent_t join[2] = {nullptr, nullptr};
+    cudaEvent_t join[kMaxLanes] = {};
 
     ~Plan()
     {
@@ -370,7 +371,7 @@ struct Plan
         }
         for (auto& kv : graphs)
             cudaGraphExecDestroy(kv.second);
-        for (int i = 0; i < 2; ++i)
+        for (int i = 0; i < kMaxLanes; ++i)
         {
             if (lanes[i] != nullptr)
                 cudaStreamDestroy(lanes[i]);
@@ -1193,6 +1194,16 @@ bool tma_col_enabled()
     return e == nullptr || std::atoi(e) != 0;
 }
 
+// L2 waves run round-robin over this many internal streams and workspace slots (CRDFFT_L2_LANES, 2 .. kMaxLanes).
+// Two measured best for 107520 (2.170 ms per 2 GiB; three lanes 2.286 with 24 MiB waves, 2.172 with 16 MiB, four
+// 2.422): more than about 48 MiB of waves in flight pushes the intermediates out of L2.
+int l2_lanes()
+{
+    const char* e = std::getenv("CRDFFT_L2_LANES");
+    const int v = e != nullptr ? std::atoi(e) : 2;
+    return v < 2 ? 2 : (v > kMaxLanes ? kMaxLanes : v);
+}
+
 // The L2 wave's row pass drops the intermediate's L2 lines once it has read them (CRDFFT_L2_DISCARD=0: kept, and
 // written back to HBM when L2 evicts them). Read at plan creation.
 bool l2_discard()
@@ -1317,21 +1328,22 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     crdfft_status st = four_step_tables(p, n, n1, n2, &hi, &lo);
     if (st != CRDFFT_OK)
         return st;
-    // L2 waves: a wave small enough that pass 1's output is still in L2 when pass 2 reads it, two workspace slots,
-    // consecutive waves on the plan's two internal streams so that one wave's pass 2 overlaps the next one's pass 1
-    // (and fills its tail). Otherwise one large wave at a time on the caller's stream.
+    // L2 waves: a wave small enough that pass 1's output is still in L2 when pass 2 reads it, one workspace slot a
+    // lane, consecutive waves round-robin on the plan's internal streams so that one wave's pass 2 overlaps the next
+    // one's pass 1 (and fills its tail). Otherwise one large wave at a time on the caller's stream.
     // (Transforms above 2 MiB are left to large waves: a 24 MiB wave of them is too few tiles to fill the GPU.)
     const bool l2w = l2_waves() && t_arena == nullptr && n * 8 <= l2_wave_max_transform() &&
                      batch * n * 8 > 2 * l2_wave_bytes();
     long long wave = std::max(1LL, (l2w ? l2_wave_bytes() : wave_bytes()) / (n * 8));
     wave = std::min(wave, batch);
-    *ws_need = (l2w ? 2 : 1) * wave * n;
+    const int nl = l2_lanes();
+    *ws_need = (l2w ? nl : 1) * wave * n;
     int wi = 0;
     for (long long t0 = 0; t0 < batch; t0 += wave, ++wi)
     {
         const long long w = std::min(wave, batch - t0);
-        const long long slot_off = l2w ? (wi & 1) * wave * n : 0;
-        const int lane = l2w ? 1 + (wi & 1) : 0;
+        const long long slot_off = l2w ? (wi % nl) * wave * n : 0;
+        const int lane = l2w ? 1 + wi % nl : 0;
         // pass 1: columns n2' in [0, n2), elements n1' along stride n2 -> scratch Y[t][k1][n2']
         Step s1;
         FourStepTw ftw;
@@ -2714,37 +2726,48 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
         return CRDFFT_INVALID_ARG;
     if (p.uneven)
         return run_uneven(p, in, out, dir, stream);
-    // Steps on the plan's internal streams (lanes 1, 2) fork from the caller's stream and join back before the next
-    // step on the caller's stream, and at the end.
+    // Steps on the plan's internal streams (lanes 1 .. kMaxLanes) fork from the caller's stream and join back before
+    // the next step on the caller's stream, and at the end.
     const cudaStream_t user = stream;
-    bool forked = false;
+    bool forked = false;          // the current segment's fork event is recorded
+    bool on[kMaxLanes] = {};      // lanes forked in the current segment
     auto join = [&]() {
-        for (int i = 0; i < 2; ++i)
-            if (cudaEventRecord(p.join[i], p.lanes[i]) != cudaSuccess ||
-                cudaStreamWaitEvent(user, p.join[i], 0) != cudaSuccess)
-                return false;
+        for (int i = 0; i < kMaxLanes; ++i)
+            if (on[i])
+            {
+                if (cudaEventRecord(p.join[i], p.lanes[i]) != cudaSuccess ||
+                    cudaStreamWaitEvent(user, p.join[i], 0) != cudaSuccess)
+                    return false;
+                on[i] = false;
+            }
         forked = false;
         return true;
     };
     for (const Step& s : p.steps[dir])
     {
-        if (s.lane != 0 && !forked)
+        if (s.lane != 0)
         {
-            if (p.lanes[0] == nullptr)
-            {
-                for (int i = 0; i < 2; ++i)
-                    if (cudaStreamCreateWithFlags(&p.lanes[i], cudaStreamNonBlocking) != cudaSuccess ||
-                        cudaEventCreateWithFlags(&p.join[i], cudaEventDisableTiming) != cudaSuccess)
-                        return CRDFFT_LAUNCH;
-                if (cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming) != cudaSuccess)
-                    return CRDFFT_LAUNCH;
-            }
-            if (cudaEventRecord(p.fork, user) != cudaSuccess || cudaStreamWaitEvent(p.lanes[0], p.fork, 0) != cudaSuccess ||
-                cudaStreamWaitEvent(p.lanes[1], p.fork, 0) != cudaSuccess)
+            const int li = s.lane - 1;
+            if (p.lanes[li] == nullptr &&
+                (cudaStreamCreateWithFlags(&p.lanes[li], cudaStreamNonBlocking) != cudaSuccess ||
+                 cudaEventCreateWithFlags(&p.join[li], cudaEventDisableTiming) != cudaSuccess))
                 return CRDFFT_LAUNCH;
-            forked = true;
+            if (p.fork == nullptr && cudaEventCreateWithFlags(&p.fork, cudaEventDisableTiming) != cudaSuccess)
+                return CRDFFT_LAUNCH;
+            if (!forked)
+            {
+                if (cudaEventRecord(p.fork, user) != cudaSuccess)
+                    return CRDFFT_LAUNCH;
+                forked = true;
+            }
+            if (!on[li])
+            {
+                if (cudaStreamWaitEvent(p.lanes[li], p.fork, 0) != cudaSuccess)
+                    return CRDFFT_LAUNCH;
+                on[li] = true;
+            }
         }
-        else if (s.lane == 0 && forked && !join())
+        else if (forked && !join())
             return CRDFFT_LAUNCH;
         stream = s.lane == 0 ? user : p.lanes[s.lane - 1];
         void* src = resolve(s.src, in, out, p.ws);
