@@ -180,6 +180,34 @@ bool cwt_lines_supported(const PassDesc& d);
 cudaError_t launch_cwt_lines(const PassDesc& d, const void* X, const void* K, const CwtScale* scales, long long nscales,
                              long long n, void* out, cudaStream_t stream);
 
+// The two-pass four-step as one persistent launch over L2-sized waves (chain_fft.cu). col: the column pass of wave 0
+// (lines wave_t * n2, maps relative to the wave's first transform, the four-step twiddle on); row: its row pass
+// (lines wave_t * n1, input in the wave's slot). ctr: 1 + 2 waves ints, zero before the launch (the tile ticket, then
+// each wave's finished column tiles, then its finished row tiles).
+constexpr int kChainThreads = 256;
+struct ChainDesc
+{
+    PassDesc col;
+    PassDesc row;
+    long long waves;      // W = ceil(batch / wave_t)
+    long long wave_t;     // transforms a wave
+    long long batch;
+    long long idist;      // complex elements between transforms, input and output
+    long long odist;
+    long long slot_elems; // wave_t * n: one wave's intermediate
+    int slots;            // intermediate slots (waves in flight)
+    int lag;              // a wave's row tiles follow the column tiles of the wave `lag` later; 1 <= lag < slots
+    int col_lpc;          // lines a column tile (chain_lines_per_tile(n1))
+    int row_lpc;          // lines a row tile
+    long long col_items;  // column tiles a wave: ceil(wave_t * n2 / col_lpc)
+    long long row_items;  // row tiles a wave: ceil(wave_t * n1 / row_lpc)
+    int* ctr;
+    int spin_limit;       // polls a dependency wait may take before it gives up (status word |= 1)
+};
+bool chain_supported(const PassDesc& col, const PassDesc& row);
+int chain_lines_per_tile(int n);
+cudaError_t launch_chain(const ChainDesc& cd, const void* in, void* out, void* ws, cudaStream_t stream);
+
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).
 cudaError_t launch_scale(void* data, long long count, float s, cudaStream_t stream);
 cudaError_t launch_planar_gather(const void* re, const void* im, void* out, long long count, cudaStream_t stream);

@@ -404,6 +404,107 @@ __device__ __forceinline__ void init_scales(const PassDesc& d, Ctx& c)
 
 // ---- classic kernel ---------------------------------------------------------------------------------------------
 
+// One tile of a pass inside a kernel that picks its tiles itself (chain_fft.cu): lines [blk * lpc, blk * lpc + lpc)
+// of the `nlines` lines the maps address from gin / gout; `tid` is threadIdx.x. The CTA may be wider than the tile:
+// threads from lpc * T on take part in the barriers only. The same steps as the classic kernel's body below, which
+// keeps its own copy (its launch shape fixes the tile, and its register allocation stays as measured).
+template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
+__device__ __forceinline__ void line_fft_tile(const PassDesc& d, const float2* __restrict__ gin,
+                                              float2* __restrict__ gout, long long blk, int lpc, long long nlines,
+                                              int tid)
+{
+    extern __shared__ float2 sm[];
+    __shared__ long long s_in_off[kMaxLinesPerCta];
+    __shared__ long long s_out_off[kMaxLinesPerCta];
+    __shared__ int s_q[kMaxLinesPerCta];
+
+    const int n = sched_n<S>(d);
+    const int T = (n + P - 1) / P;
+    const int pitch = cta_line_pitch(n, lpc);
+    const long long line0 = blk * lpc;
+
+    int ll, jt;
+    if constexpr (MAP == PassMap::Row)
+    {
+        ll = tid / T;
+        jt = tid - ll * T;
+    }
+    else
+    {
+        jt = tid / lpc;
+        ll = tid - jt * lpc;
+    }
+
+    if (!DL || !DS)
+    {
+        for (int i = tid; i < lpc; i += blockDim.x)
+        {
+            const long long line = line0 + i;
+            s_in_off[i] = line_offset(d.in, line, d.lines_per_group);
+            s_out_off[i] = line_offset(d.out, line, d.lines_per_group);
+            s_q[i] = static_cast<int>(line_row(d, line));
+        }
+        __syncthreads();
+    }
+
+    const long long line = line0 + ll;
+    Ctx c;
+    c.ok = line < nlines && tid < lpc * T;
+    c.q = line_row(d, line);
+    c.in = gin + line_offset(d.in, line, d.lines_per_group);
+    c.out = gout + line_offset(d.out, line, d.lines_per_group);
+    c.jt = jt;
+    c.T = T;
+    init_scales(d, c);
+    const LayRow<1> lay{sm + ll * pitch};
+
+    if constexpr (!DL)
+    {
+        // Cooperative coalesced load of the CTA's lines: threads run along whichever axis is unit-stride in memory.
+        const long long lines_here = nlines - line0;
+        const long long es = d.in.estride;
+        for_tile(n, lpc, es == 1, [&](int a, int e) {
+            if (a < lines_here)
+                LayRow<1>{sm + a * pitch}.at(e) = load_in<EPI>(c, gin + s_in_off[a] + static_cast<long long>(e) * es);
+        });
+        __syncthreads();
+    }
+
+    SchedRun<S>::template go<P, DL, DS, false, Kind<MAP, EPI>>(d, c, lay, n);
+
+    if constexpr (!DS)
+    {
+        // (Storing the last stage straight from registers with the threads across the lines, which saves this
+        // shared-memory round trip and its bank conflicts, measured 20 % slower on the four-step row pass.)
+        const long long lines_here = nlines - line0;
+        const long long es = d.out.estride;
+        for_tile(n, lpc, es == 1, [&](int a, int e) {
+            if (a < lines_here)
+                __stcs(gout + s_out_off[a] + static_cast<long long>(e) * es,
+                       epilogue<EPI>(d, c, s_q[a], e, LayRow<1>{sm + a * pitch}.at(e)));
+        });
+    }
+
+    if constexpr (MAP == PassMap::Row && DL && !DS)
+    {
+        // A dead input (a four-step intermediate in L2, read by the first stage, which ends with a barrier: every
+        // thread's loads of the CTA's lines are done): drop its 128-byte L2 lines, so that L2 does not write them
+        // back to HBM. Unit-stride lines of whole 128-byte lines only; last, where the kernel holds the fewest values.
+        if (d.discard_in && d.in.estride == 1 && (n & 15) == 0)
+        {
+            const int per = n / 16;
+            const long long lines_here = nlines - line0;
+            for (int i = tid; i < lpc * per; i += blockDim.x)
+            {
+                const int a = i / per;
+                const float2* p = gin + s_in_off[a] + (i - a * per) * 16;
+                if (a < lines_here && (reinterpret_cast<uintptr_t>(p) & 127) == 0)
+                    asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+            }
+        }
+    }
+}
+
 template <class S, int P, PassMap MAP, bool DL, bool DS, bool EPI>
 __device__ __forceinline__ void line_fft_body(const PassDesc& d, const float2* __restrict__ gin,
                                               float2* __restrict__ gout)

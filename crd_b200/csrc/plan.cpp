@@ -109,7 +109,8 @@ enum class StepKind : int
     ChirpPre,
     SpecMul,
     ChirpPost,
-    Scale
+    Scale,
+    Chain
 };
 
 struct Step
@@ -129,6 +130,8 @@ struct Step
     int lane = 0;     // 0: the caller's stream; 1 .. kMaxLanes: the plan's internal streams (L2-sized four-step waves)
     RealRecombine real{};
     ChirpDesc chirp{};
+    ChainDesc chain{};  // Chain: the persistent four-step; aux is its first workspace slot, counters after the slots
+    BufRef aux{};
     BufRef src, dst;
     long long count = 0;
     float scale = 1.0f;
@@ -1246,6 +1249,22 @@ long long l2_wave_max_transform()
     return v;
 }
 
+// The four-step as one persistent launch over L2-sized waves (chain_fft.cu) where an instance exists for its two
+// line lengths (CRDFFT_CHAIN=1 on, 0 off); its wave size (CRDFFT_CHAIN_WAVE_BYTES) and number of intermediate slots
+// in flight (CRDFFT_CHAIN_SLOTS, 3 .. 8; a wave's row tiles trail its column tiles by slots / 2 waves).
+bool chain_enabled()
+{
+    const char* e = std::getenv("CRDFFT_CHAIN");
+    return e != nullptr && std::atoi(e) != 0;
+}
+long long chain_wave_bytes() { return env_bytes("CRDFFT_CHAIN_WAVE_BYTES", 16LL << 20); }
+int chain_slots()
+{
+    const char* e = std::getenv("CRDFFT_CHAIN_SLOTS");
+    const int v = e != nullptr ? std::atoi(e) : 4;
+    return v < 3 ? 3 : (v > 8 ? 8 : v);
+}
+
 // A batch of 1-D complex transforms of length n: element j of transform t at base + t*dist + j*stride on each side.
 // Appends the steps of one direction; `ws_off` is where in the workspace this transform's scratch may start; the
 // scratch it needs is returned in *ws_need (complex elements).
@@ -1328,6 +1347,63 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
     crdfft_status st = four_step_tables(p, n, n1, n2, &hi, &lo);
     if (st != CRDFFT_OK)
         return st;
+    // The chained form: every wave's two passes as tiles of one persistent launch (forward and inverse alike).
+    if (chain_enabled() && r2c_wn == nullptr && t_arena == nullptr && istride == 1 &&
+        n * 8 <= chain_wave_bytes() && batch * n * 8 > 2 * chain_wave_bytes())
+    {
+        ChainDesc cd{};
+        cd.wave_t = std::min(batch, std::max(1LL, chain_wave_bytes() / (n * 8)));
+        const int l1 = chain_lines_per_tile(static_cast<int>(n1));
+        const int l2 = chain_lines_per_tile(static_cast<int>(n2));
+        FourStepTw ftw;
+        ftw.M = n;
+        ftw.hi = hi;
+        ftw.lo = lo;
+        st = make_pass_desc(p, n1, cd.wave_t * n2, n2, LineMap{idist, 1, n2}, LineMap{n, 1, n2}, conj_in, false,
+                            1.0f, ftw, &cd.col);
+        if (st != CRDFFT_OK)
+            return st;
+        st = make_pass_desc(p, n2, cd.wave_t * n1, n1, LineMap{n, n2, 1}, LineMap{odist, ostride, n1 * ostride}, false,
+                            conj_out, scale, FourStepTw{}, &cd.row);
+        if (st != CRDFFT_OK)
+            return st;
+        cd.row.discard_in = l2_discard() ? 1 : 0;
+        if (l1 >= 1 && l2 >= 1 && l1 <= pass_lines_per_cta_limit() && l2 <= pass_lines_per_cta_limit() &&
+            chain_supported(cd.col, cd.row))
+        {
+            cd.batch = batch;
+            cd.waves = (batch + cd.wave_t - 1) / cd.wave_t;
+            cd.idist = idist;
+            cd.odist = odist;
+            cd.slot_elems = cd.wave_t * n;
+            cd.slots = chain_slots();
+            // a wave's row tiles trail its column tiles by half the slots, and the slot they free is refilled by
+            // the column tiles as many waves later: both waits then point at least two list segments back (with
+            // slots - 1, the column tiles waited on row tiles claimed just before them, a stall every wave)
+            cd.lag = cd.slots / 2;
+            cd.col_lpc = l1;
+            cd.row_lpc = l2;
+            cd.col_items = (cd.wave_t * n2 + l1 - 1) / l1;
+            cd.row_items = (cd.wave_t * n1 + l2 - 1) / l2;
+            cd.spin_limit = g_debug_stall.load() ? (1 << 10) : (1 << 20);
+            const long long ctr_bytes = (1 + 2 * cd.waves) * 4;
+            const long long ctr_off = ws_off + cd.slots * cd.slot_elems;
+            *ws_need = cd.slots * cd.slot_elems + (ctr_bytes + 7) / 8;
+            Step z;
+            z.kind = StepKind::Zero;
+            z.count = ctr_bytes;
+            z.src = z.dst = BufRef{Buf::Ws, ctr_off};
+            steps.push_back(z);
+            Step c;
+            c.kind = StepKind::Chain;
+            c.chain = cd;
+            c.src = src;
+            c.dst = dst;
+            c.aux = BufRef{Buf::Ws, ws_off};
+            steps.push_back(c);
+            return CRDFFT_OK;
+        }
+    }
     // L2 waves: a wave small enough that pass 1's output is still in L2 when pass 2 reads it, one workspace slot a
     // lane, consecutive waves round-robin on the plan's internal streams so that one wave's pass 2 overlaps the next
     // one's pass 1 (and fills its tail). Otherwise one large wave at a time on the caller's stream.
@@ -2801,6 +2877,14 @@ crdfft_status run(Plan& p, const void* in, void* out, int dir, cudaStream_t stre
             case StepKind::SpecMul: e = launch_spectrum_mul(s.chirp, dst, stream); break;
             case StepKind::ChirpPost: e = launch_chirp_post(s.chirp, src, dst, stream); break;
             case StepKind::Scale: e = launch_scale(dst, s.count, s.scale, stream); break;
+            case StepKind::Chain:
+            {
+                ChainDesc cd = s.chain;
+                void* wsb = resolve(s.aux, in, out, p.ws);
+                cd.ctr = reinterpret_cast<int*>(static_cast<char*>(wsb) + cd.slots * cd.slot_elems * 8);
+                e = launch_chain(cd, src, dst, wsb, stream);
+                break;
+            }
         }
         if (e != cudaSuccess)
         {
