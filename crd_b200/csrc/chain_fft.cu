@@ -2,7 +2,8 @@
 // are tiles of one work list, one CTA a tile, each CTA claiming its tile in list order from a device counter when it
 // starts (whatever order the hardware starts CTAs in).
 //
-// The work list, for waves w = 0 .. W-1 of wave_t transforms each (C column tiles and R row tiles a wave):
+// The work list (chain_list.hpp), for waves w = 0 .. W-1 of wave_t transforms each (C column tiles and R row tiles
+// a wave):
 //     col(0) .. col(lag-1) | col(lag) row(0) | col(lag+1) row(1) | ... | [no-op col tiles] row(W-1)
 // A row tile of wave w waits until the C column tiles of wave w have signalled; a column tile of wave w >= slots
 // waits until the R row tiles of wave w - slots have signalled (the wave's intermediate slot is free again). Both
@@ -19,6 +20,7 @@
 // column / twiddle / row steps over its own cache-sized blocks (engine/numerics/hesap-fft/kernels/fft_kernels.cpp:
 // 2363-2658).
 
+#include "chain_list.hpp"
 #include "kernels.hpp"
 #include "line_fft.cuh"
 
@@ -63,24 +65,10 @@ __global__ void __maxnreg__(80) chain_fft_kernel(const ChainDesc cd, const float
     const int C = static_cast<int>(cd.col_items);
     const int R = static_cast<int>(cd.row_items);
     const int W = static_cast<int>(cd.waves);
-    const int head = cd.lag * C;
-    bool is_col;
-    int w, idx;
-    if (t < head)
-    {
-        is_col = true;
-        w = t / C;
-        idx = t - w * C;
-    }
-    else
-    {
-        const int u = t - head;
-        const int sg = u / (C + R);
-        const int r = u - sg * (C + R);
-        is_col = r < C;
-        w = is_col ? sg + cd.lag : sg;
-        idx = is_col ? r : r - C;
-    }
+    const ChainTile tile = chain_tile_at(t, C, R, cd.lag);
+    const bool is_col = tile.col;
+    const int w = tile.wave;
+    const int idx = tile.idx;
     if (w >= W)
         return; // a no-op column tile past the last wave (the list's tail holds row tiles only)
     int* const col_done = cd.ctr + 1;
@@ -162,8 +150,6 @@ bool chain_supported(const PassDesc& col, const PassDesc& row)
     return col.in.ldist == 1 && col.out.ldist == 1 && row.in.estride == 1 && row.ftw_M == 0 && col.ftw_M != 0;
 }
 
-int chain_lines_per_tile(int n) { return kChainThreads / ((n + 15) / 16); }
-
 int chain_smem_bytes(int n1, int n2)
 {
     const int l1 = chain_lines_per_tile(n1);
@@ -186,7 +172,7 @@ cudaError_t launch_chain(const ChainDesc& cd, const void* in, void* out, void* w
         if (e != cudaSuccess)
             return e;
     }
-    const long long total = cd.lag * cd.col_items + cd.waves * (cd.col_items + cd.row_items);
+    const long long total = chain_list_length(cd.waves, cd.col_items, cd.row_items, cd.lag);
     if (total >= 0x7fffffffLL)
         return cudaErrorInvalidConfiguration;
     const long long grid = total;

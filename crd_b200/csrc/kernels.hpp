@@ -2,6 +2,7 @@
 
 #pragma once
 
+#include "chain_list.hpp"
 #include "pass_desc.hpp"
 #include "../../include/crdfft.h"
 
@@ -184,7 +185,6 @@ cudaError_t launch_cwt_lines(const PassDesc& d, const void* X, const void* K, co
 // (lines wave_t * n2, maps relative to the wave's first transform, the four-step twiddle on); row: its row pass
 // (lines wave_t * n1, input in the wave's slot). ctr: 1 + 2 waves ints, zero before the launch (the tile ticket, then
 // each wave's finished column tiles, then its finished row tiles).
-constexpr int kChainThreads = 256;
 struct ChainDesc
 {
     PassDesc col;
@@ -205,7 +205,6 @@ struct ChainDesc
     int spin_limit;       // polls a dependency wait may take before it gives up (status word |= 1)
 };
 bool chain_supported(const PassDesc& col, const PassDesc& row);
-int chain_lines_per_tile(int n);
 cudaError_t launch_chain(const ChainDesc& cd, const void* in, void* out, void* ws, cudaStream_t stream);
 
 // Elementwise scale of `count` complex values (used by normalisations that no pass can absorb).

@@ -1377,10 +1377,7 @@ crdfft_status plan_c2c_1d(Plan& p, long long n, long long batch, long long istri
             cd.odist = odist;
             cd.slot_elems = cd.wave_t * n;
             cd.slots = chain_slots();
-            // a wave's row tiles trail its column tiles by half the slots, and the slot they free is refilled by
-            // the column tiles as many waves later: both waits then point at least two list segments back (with
-            // slots - 1, the column tiles waited on row tiles claimed just before them, a stall every wave)
-            cd.lag = cd.slots / 2;
+            cd.lag = chain_lag(cd.slots);
             cd.col_lpc = l1;
             cd.row_lpc = l2;
             cd.col_items = (cd.wave_t * n2 + l1 - 1) / l1;
